@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""H-matvec benchmark on one node (one process per GPU).
+
+Workload: 3DR0-H planar square crack, 256 x 256 rectangles on [-1,1]^2 in
+z = 0 (196,608 DoF), E = 1, nu = 0.25, leaf 32, eta 3, ACA eps 1e-5; the
+reference's own host code builds the H-matrix (mesh, kernel, cluster tree,
+ACA: libbigwham_host.so), the blocks are uploaded once in FP64, FP32 and BF16
+(per-block FP32 scale), and one step is one H x over the whole matrix with
+x ~ U(-1,1) (seed 1) resident in HBM.  The headline value is the BF16-storage
+(FP32 accumulation) rate; the FP64 and FP32 rates ride along.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (weak scaling, no collective on the data
+path): rank 0 builds the H-matrix once and shares the flat blocks through
+shared memory; every rank uploads and applies its own copy.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "H-matvec/s, 3DR0-H 196,608 DoF (BF16 blocks + FP32 accumulate; FP64 and FP32 alongside)"
+UNIT = "matvec/s"
+PROPS = [1.0, 0.25]
+LEAF, ETA, EPS = 32, 3.0, 1e-5
+L2_NOTE = "inputs larger than L2: every step streams all block data (GB-scale) from HBM"
+
+
+def workload(n):
+    return {"workload": f"3DR0-H square crack {n}x{n} rectangles ({3 * n * n:,} DoF), E=1 nu=0.25, "
+                        f"leaf {LEAF}, eta {ETA:g}, ACA eps {EPS:g}, one H x per step, x~U(-1,1) seed 1",
+            "mesh": f"{n}x{n}", "dof": 3 * n * n, "l2": L2_NOTE}
+
+
+def read_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic(kernel_key):
+    """Per-launch DRAM traffic of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(kernel_key)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=None)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from bigwham_dev_b200.meshes import square_crack_3d
+
+    base = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True,
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup}
+    try:
+        from oracle import RefHmat, ref_available
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({**base, "unavailable": f"oracle import failed: {e}"}))
+        return 0
+    if not ref_available():
+        print(json.dumps({**base, "unavailable": "reference library oracle/_ref/libbigwham_ref.so not built"}))
+        return 0
+    threads = os.cpu_count() or 1
+    coor, conn = square_crack_3d(a.mesh)
+    t0 = time.time()
+    R = RefHmat("3DR0-H", coor, conn, PROPS, LEAF, ETA, EPS, n_threads=threads)
+    build_s = time.time() - t0
+    x = np.random.default_rng(1).uniform(-1.0, 1.0, R.shape[1])
+    t0 = time.perf_counter()
+    R.matvec(x)
+    est = time.perf_counter() - t0
+    for _ in range(max(0, min(a.warmup, int(5.0 / max(est, 1e-6))) - 1)):
+        R.matvec(x)
+    k = max(1, min(a.steps, int(a.ref_budget_s / max(est, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        R.matvec(x)
+    dt = time.perf_counter() - t0
+    v = k / dt
+    sample = (f"{k} of {a.steps} steps timed (each a full BigWhamIO::MatVec of the {3 * a.mesh * a.mesh:,}-DoF "
+              f"H-matrix, OpenMP over {threads} threads, 1 BLAS thread); H-matrix build {build_s:.1f} s untimed")
+    print(json.dumps({**base, "value": v, "ms_per_step": 1e3 * dt / k, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f64", "data": "synthetic mesh (no dataset)", "config": workload(a.mesh),
+                      "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                                       "sample": sample},
+                      "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+# ----------------------------------------------------------------------------- our arm
+def build_hmatrix(a, world, rank, local):
+    """Returns (io or None, HmatGpu, setup info).  N = 1: the product host path
+    (BigWhamIO built by the reference's code, HmatGpu installed via setHmat).
+    N > 1: rank 0 builds once and shares the flat blocks in /dev/shm."""
+    from bigwham_dev_b200 import HmatGpu
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+    from bigwham_dev_b200.meshes import square_crack_3d
+
+    precs = ("fp64", "fp32", "bf16")
+    info = {}
+    coor, conn = square_crack_3d(a.mesh)
+    if world == 1:
+        t0 = time.time()
+        io = BigWhamIOGpu(coor, conn, "3DR0-H", PROPS, os.cpu_count() or 1, useCuda=False, device=local)
+        io.build_hierarchical_matrix(LEAF, ETA, EPS)
+        info["host_build_s"] = round(time.time() - t0, 2)
+        t0 = time.time()
+        io.use_cuda = True
+        h = io.attach_gpu(precs, transpose=False)
+        info["upload_s"] = round(time.time() - t0, 2)
+        info["compression"] = io.get_compression_ratio()
+        return io, h, info
+    # replicas: one build, shared through /dev/shm
+    tag = os.environ.get("TORCHELASTIC_RUN_ID", "bench") + f"_{a.mesh}"
+    d = os.path.join("/dev/shm", f"bw_blocks_{tag}")
+    keys = ("fr", "lr", "fr_data", "lr_data", "perm0", "perm1")
+    if rank == 0:
+        t0 = time.time()
+        io = BigWhamIOGpu(coor, conn, "3DR0-H", PROPS, os.cpu_count() or 1, useCuda=False, device=local)
+        io.build_hierarchical_matrix(LEAF, ETA, EPS)
+        os.makedirs(d, exist_ok=True)
+        alloc_paths = {}
+
+        def alloc(shape, dtype, _n=[0]):
+            name = keys[_n[0]]
+            _n[0] += 1
+            path = os.path.join(d, name + ".bin")
+            alloc_paths[name] = (path, shape, np.dtype(dtype).str)
+            return np.lib.format.open_memmap(path, mode="w+", dtype=dtype, shape=shape)
+
+        ex = io.export_blocks(alloc)
+        for k in keys:
+            ex[k].flush()
+        with open(os.path.join(d, "meta.json"), "w") as f:
+            json.dump({"dof": ex["dof"], "n_rows": ex["n_rows"], "n_cols": ex["n_cols"]}, f)
+        info["host_build_s"] = round(time.time() - t0, 2)
+        io.close()
+    barrier(world)
+    with open(os.path.join(d, "meta.json")) as f:
+        meta = json.load(f)
+    arr = {k: np.load(os.path.join(d, k + ".bin"), mmap_mode="r") for k in keys}
+    t0 = time.time()
+    h = HmatGpu.from_flat(meta["dof"], meta["n_rows"], meta["n_cols"], arr["fr"], arr["lr"], arr["fr_data"],
+                          arr["lr_data"], arr["perm0"], arr["perm1"], device=local, precisions=precs)
+    info["upload_s"] = round(time.time() - t0, 2)
+    barrier(world)
+    if rank == 0:
+        for k in keys:
+            os.unlink(os.path.join(d, k + ".bin"))
+        os.unlink(os.path.join(d, "meta.json"))
+        os.rmdir(d)
+    return None, h, info
+
+
+def cpu_baseline(a, x_host, y_fp64):
+    """The reference's own OpenMP CPU matvec (oracle/_ref) on the same
+    H-matrix definition and x, on this host's cores; bounded sample."""
+    try:
+        from oracle import RefHmat, ref_available
+    except Exception as e:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}, None
+    if not ref_available():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}, None
+    from bigwham_dev_b200.meshes import square_crack_3d
+
+    threads = os.cpu_count() or 1
+    coor, conn = square_crack_3d(a.mesh)
+    t0 = time.time()
+    R = RefHmat("3DR0-H", coor, conn, PROPS, LEAF, ETA, EPS, n_threads=threads)
+    build_s = time.time() - t0
+    y_ref = R.matvec(x_host)
+    t0 = time.perf_counter()
+    R.matvec(x_host)
+    est = time.perf_counter() - t0
+    k = max(2, min(50, int(a.cpu_budget_s / max(est, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        R.matvec(x_host)
+    dt = time.perf_counter() - t0
+    parity = float(np.linalg.norm(y_fp64 - y_ref) / np.linalg.norm(y_ref))
+    del R
+    return ({"value": k / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+             "sample": f"{k} full BigWhamIO::MatVec calls on the same {3 * a.mesh * a.mesh:,}-DoF H-matrix "
+                       f"(reference build {build_s:.1f} s, untimed), {threads} OpenMP threads, 1 BLAS thread"},
+            parity)
+
+
+def run_ours(a):
+    import torch
+
+    world, rank, local = dist_setup(a.gpus)
+    torch.cuda.set_device(local)
+    io, h, setup = build_hmatrix(a, world, rank, local)
+    dev = torch.device("cuda", local)
+    n_in, n_out = h.n_cols, h.n_rows
+    x_host = np.random.default_rng(1).uniform(-1.0, 1.0, n_in)
+    x = torch.from_numpy(x_host).to(dev)
+    ys = {p: torch.empty(n_out, dtype=torch.float64, device=dev) for p in ("fp64", "fp32", "bf16")}
+    stream = torch.cuda.current_stream(dev)
+    peak, peak_kind = read_peak()
+    clocks = ClockSampler(local)
+    res = {}
+    clocks.start()
+    for p in ("fp64", "fp32", "bf16"):
+        y = ys[p]
+        for _ in range(a.warmup):
+            h.matvec(x, p, out=y)
+        h.sync(stream)
+        barrier(world)
+        torch.cuda.synchronize()
+        h.set_timing(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            h.matvec(x, p, out=y)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_total = e0.elapsed_time(e1)
+        launch_ms, nrec = h.timing_read()
+        h.set_timing(False)
+        h.sync(stream)
+        ms_total = max_over_ranks(ms_total, world)
+        b1, b2 = h.phase_bytes(p)
+        t_stream = (launch_ms[1] + launch_ms[2]) / max(1, nrec)  # ms per step in the streaming kernel
+        res[p] = {"ms_per_step": ms_total / a.steps, "value": world * a.steps / (ms_total / 1e3),
+                  "algorithmic_bytes": h.algorithmic_bytes(p), "phase_bytes": [b1, b2],
+                  "launch_ms_per_step": [v / max(1, nrec) for v in launch_ms],
+                  "stream_kernel_gbs": (b1 + b2) / (t_stream * 1e-3) / 1e9,
+                  "matvec_gbs": h.algorithmic_bytes(p) / (ms_total / a.steps * 1e-3) / 1e9}
+    # end-to-end through the reference-facing call with host buffers, headline precision
+    e2e_steps = max(1, min(a.steps, 200))
+    if io is not None:
+        io.set_precision("bf16")
+        for _ in range(min(3, a.warmup)):
+            io.matvec(x_host)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            y_e2e = io.matvec(x_host)  # BigWhamIO::MatVec -> HmatGpu -> bw_matvec_host
+        dt = time.perf_counter() - t0
+        e2e_path = "BigWhamIO::MatVec(host arrays) -> HmatGpu::matvecOriginal -> bw_matvec_host"
+    else:
+        for _ in range(min(3, a.warmup)):
+            h.matvec(x_host, "bf16")
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            y_e2e = h.matvec(x_host, "bf16")  # bw_matvec_host
+        dt = time.perf_counter() - t0
+        e2e_path = "bw_matvec_host (host arrays)"
+    dt = max_over_ranks(dt, world)
+    clk = clocks.stop()
+    y64 = ys["fp64"].cpu().numpy()
+    errs = {p: float(np.linalg.norm(ys[p].cpu().numpy() - y64) / np.linalg.norm(y64)) for p in ("fp32", "bf16")}
+    errs["e2e_bf16_vs_device_bf16"] = float(np.linalg.norm(y_e2e - ys["bf16"].cpu().numpy()) / np.linalg.norm(y64))
+    if rank != 0:
+        return 0
+    cpu, parity = (None, None)
+    if world == 1 and not a.no_cpu_baseline:
+        if io is not None:
+            io.close()
+        cpu, parity = cpu_baseline(a, x_host, y64)
+    head = res["bf16"]
+    b1, b2 = head["phase_bytes"]
+    t_stream = head["launch_ms_per_step"][1] + head["launch_ms_per_step"][2]
+    achieved = (b1 + b2) / (t_stream * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16", "data": "synthetic mesh (generated; no dataset), x ~ U(-1,1) seed 1",
+        "config": {**workload(a.mesh), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   **setup},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6650 GB/s",
+                     "kernel": "stream_panels_kernel<Bf16> (phase 1 + phase 2 launches of one step)",
+                     "bytes_per_step": b1 + b2, "traffic": read_traffic("stream_panels_bf16")},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * e2e_steps / dt, "unit": UNIT, "h2d_bytes_per_step": 8 * n_in,
+                "d2h_bytes_per_step": 8 * n_out, "path": e2e_path, "timer": "host wall clock, synchronous calls"},
+        "gpu_launches": 3 * a.steps,
+        "clocks": clk,
+        "precisions": {p: {k: v for k, v in res[p].items()} for p in res},
+        "speedup_vs_fp64": res["bf16"]["value"] / res["fp64"]["value"],
+        "speedup_fp32_vs_fp64": res["fp32"]["value"] / res["fp64"]["value"],
+        "rel_err_vs_fp64_gpu": errs,
+        "fp64_gpu_vs_reference_rel_err": parity,
+    }
+    print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--mesh", type=int, default=256, help="rectangles per side (256 -> 196,608 DoF)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=10.0)
+    ap.add_argument("--ref-budget-s", type=float, default=60.0)
+    a = ap.parse_args(argv)
+    if a.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,290 @@
+"""BigWham's Python interface with the B200 backend behind it.
+
+Mirrors the reference's ``bigwham4py`` (interfaces/python/bigwham4py/bigwham4py.py)
+for the matvec path:
+
+* ``BigWhamIOGpu`` stands for the pybind11 ``BigWhamIOSelf``
+  (interfaces/python/py_bigwham.cc:141-260): same constructor arguments, same
+  method names (build_hierarchical_matrix, matvec, matvec_permute,
+  matvec_raw_ptr, get_diagonal, get_permutation, ...).  The H-matrix is
+  built by the reference's own host code (compiled into libbigwham_host.so) and
+  then uploaded once; every matvec afterwards runs on the GPU.
+* ``BEMatrix`` is the scipy ``LinearOperator`` of the reference
+  (bigwham4py.py:49-485) with ``useCuda=True`` meaning this backend.
+
+Driven through the C ABI of include/bigwham_host.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _capi as A
+from .hmat import HmatGpu, _prec_flag
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+HOST_LIB_PATH = os.path.join(_HERE, "_lib", "libbigwham_host.so")
+
+kernels_id = ["2DS0-H", "2DS1-H", "S3DS0-H", "Axi3DS0-H", "3DT0-H", "3DT6-H", "3DR0-H", "3DR0-H-mode1"]
+
+_P, _I64 = C.c_void_p, C.c_int64
+_HSIGS = {
+    "bwh_create": (C.c_int, [_P, _I64, _P, _I64, C.c_char_p, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_P)]),
+    "bwh_build": (C.c_int, [_P, C.c_int, C.c_double, C.c_double]),
+    "bwh_attach_gpu": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
+    "bwh_set_precision": (C.c_int, [_P, C.c_int]),
+    "bwh_matvec": (C.c_int, [_P, _P, _P]),
+    "bwh_matvec_perm": (C.c_int, [_P, _P, _P]),
+    "bwh_matvec_raw_ptr": (C.c_int, [_P, _P, _P]),
+    "bwh_diagonal": (C.c_int, [_P, _P]),
+    "bwh_size": (_I64, [_P, C.c_int]),
+    "bwh_dof": (C.c_int, [_P]),
+    "bwh_compression": (C.c_double, [_P]),
+    "bwh_hmat_time": (C.c_double, [_P]),
+    "bwh_permutation": (C.c_int, [_P, _P]),
+    "bwh_collocation_points": (_I64, [_P, _P]),
+    "bwh_hpattern": (_I64, [_P, _P]),
+    "bwh_n_blocks": (_I64, [_P, C.c_int]),
+    "bwh_entries": (_I64, [_P, C.c_int]),
+    "bwh_export": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "bwh_gpu_handle": (_P, [_P]),
+    "bwh_destroy": (C.c_int, [_P]),
+    "bwh_last_error": (C.c_char_p, []),
+}
+_hlib = None
+
+
+def host_lib():
+    global _hlib
+    if _hlib is None:
+        if not os.path.exists(HOST_LIB_PATH):
+            raise RuntimeError(f"host adapter not built: {HOST_LIB_PATH} is missing "
+                               f"(python -m bigwham_dev_b200.build --host, needs the BigWham sources)")
+        A.lib()  # the CUDA backend first (libbigwham_host.so links against it)
+        L = C.CDLL(HOST_LIB_PATH)
+        for name, (res, args) in _HSIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _hlib = L
+    return _hlib
+
+
+def _check(st):
+    if st != 0:
+        raise RuntimeError("bigwham_host: " + (host_lib().bwh_last_error() or b"").decode(errors="replace"))
+
+
+class BigWhamIOGpu:
+    """BigWhamIO (square self-interaction) with the GPU matvec installed."""
+
+    def __init__(self, coor, conn, kernel: str, properties, n_openMP_threads: int = 8, n_GPUs: int = 1,
+                 verbose: bool = False, homogeneous_size_pattern: bool = False, useCuda: bool = True,
+                 fixed_rank: int = -1, device: int = 0):
+        if kernel not in kernels_id:
+            raise ValueError(f"invalid kernel {kernel}; available: {', '.join(kernels_id)}")
+        L = host_lib()
+        coor = np.ascontiguousarray(coor, dtype=np.float64).ravel()
+        conn = np.ascontiguousarray(conn, dtype=np.int32).ravel()
+        props = np.ascontiguousarray(properties, dtype=np.float64).ravel()
+        h = C.c_void_p()
+        _check(L.bwh_create(coor.ctypes.data, coor.size, conn.ctypes.data, conn.size, kernel.encode(),
+                            props.ctypes.data, props.size, int(n_openMP_threads), int(verbose), int(fixed_rank),
+                            C.byref(h)))
+        self._h = h
+        self._L = L
+        self.kernel = kernel
+        self.use_cuda = bool(useCuda)
+        self.device = int(device)
+        self.gpu: HmatGpu | None = None
+        self._precisions = ("fp64",)
+        self._transpose = False
+
+    # ---------------------------------------------------------------- build
+    def set_gpu_storage(self, precisions=("fp64",), transpose: bool = False) -> None:
+        """Precisions (and H^T) to lay out on the device at the next build."""
+        self._precisions = tuple(precisions)
+        self._transpose = bool(transpose)
+
+    def build_hierarchical_matrix(self, max_leaf_size: int, eta: float, eps_aca: float) -> None:
+        _check(self._L.bwh_build(self._h, int(max_leaf_size), float(eta), float(eps_aca)))
+        if self.use_cuda:
+            self.attach_gpu(self._precisions, self._transpose)
+
+    def attach_gpu(self, precisions=("fp64",), transpose: bool = False, release_host: bool = True) -> HmatGpu:
+        flags = 0
+        for p in precisions:
+            flags |= _prec_flag(p)
+        if transpose:
+            flags |= A.BW_STORE_TRANSPOSE
+        _check(self._L.bwh_attach_gpu(self._h, self.device, flags, int(release_host)))
+        h = self._L.bwh_gpu_handle(self._h)
+        self.gpu = HmatGpu._borrow(h, self.get_dof(), self.matrix_size(0), self.matrix_size(1), precisions,
+                                   transpose, owner=self)
+        self.set_precision(precisions[0] if "fp64" not in precisions else "fp64")
+        return self.gpu
+
+    def set_precision(self, precision) -> None:
+        """Precision of the reference-facing calls (matvec, matvec_raw_ptr)."""
+        _check(self._L.bwh_set_precision(self._h, _prec_flag(precision)))
+
+    # ---------------------------------------------------------------- products (reference names)
+    def matvec(self, x):
+        """BigWhamIO::MatVec: host arrays, original ordering."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.matrix_size(0))
+        _check(self._L.bwh_matvec(self._h, x.ctypes.data, y.ctypes.data))
+        return y
+
+    def matvec_permute(self, x):
+        """BigWhamIO::MatVecPerm: host arrays, permuted ordering."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.matrix_size(0))
+        _check(self._L.bwh_matvec_perm(self._h, x.ctypes.data, y.ctypes.data))
+        return y
+
+    def matvec_raw_ptr(self, x: int, y: int) -> None:
+        """BigWhamIO::MatVec(double*, double*): device pointers (CuPy / torch / JAX)."""
+        _check(self._L.bwh_matvec_raw_ptr(self._h, C.c_void_p(int(x)), C.c_void_p(int(y))))
+
+    # ---------------------------------------------------------------- queries (reference names)
+    def matrix_size(self, k: int) -> int:
+        return int(self._L.bwh_size(self._h, int(k)))
+
+    def get_dof(self) -> int:
+        return int(self._L.bwh_dof(self._h))
+
+    def get_compression_ratio(self) -> float:
+        return float(self._L.bwh_compression(self._h))
+
+    def get_hmat_time(self) -> float:
+        return float(self._L.bwh_hmat_time(self._h))
+
+    def get_diagonal(self):
+        d = np.empty(max(self.matrix_size(0), self.matrix_size(1)))
+        _check(self._L.bwh_diagonal(self._h, d.ctypes.data))
+        return d
+
+    def get_permutation(self):
+        p = np.empty(self.matrix_size(1) // self.get_dof(), np.int64)
+        _check(self._L.bwh_permutation(self._h, p.ctypes.data))
+        return p
+
+    def get_collocation_points(self):
+        n = self._L.bwh_collocation_points(self._h, None)
+        out = np.empty(n)
+        self._L.bwh_collocation_points(self._h, out.ctypes.data)
+        return out
+
+    def get_hpattern(self):
+        n = self._L.bwh_hpattern(self._h, None)
+        out = np.empty(n)
+        self._L.bwh_hpattern(self._h, out.ctypes.data)
+        return out.reshape(-1, 6)
+
+    def n_blocks(self):
+        return int(self._L.bwh_n_blocks(self._h, 0)), int(self._L.bwh_n_blocks(self._h, 1))
+
+    def export_blocks(self, alloc=np.empty) -> dict:
+        """Flat copy of the built H-matrix (before attach_gpu): pattern,
+        permutations and block data, as HmatGpu.add_flat takes them.  `alloc`
+        (shape, dtype) -> array lets the caller place the arrays (e.g. in
+        shared memory)."""
+        nfr, nlr = self.n_blocks()
+        dof = self.get_dof()
+        out = {"dof": dof, "n_rows": self.matrix_size(0), "n_cols": self.matrix_size(1),
+               "fr": alloc((nfr, 4), np.int64), "lr": alloc((nlr, 5), np.int64),
+               "fr_data": alloc((int(self._L.bwh_entries(self._h, 0)),), np.float64),
+               "lr_data": alloc((int(self._L.bwh_entries(self._h, 1)),), np.float64),
+               "perm0": alloc((self.matrix_size(0) // dof,), np.int64),
+               "perm1": alloc((self.matrix_size(1) // dof,), np.int64)}
+        _check(self._L.bwh_export(self._h, *(out[k].ctypes.data for k in
+                                             ("fr", "lr", "fr_data", "lr_data", "perm0", "perm1"))))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            if self.gpu is not None:
+                self.gpu.close()
+                self.gpu = None
+            self._L.bwh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+try:
+    from scipy.sparse.linalg import LinearOperator as _LinOp
+except Exception:  # pragma: no cover - scipy is part of the image
+    _LinOp = object
+
+
+class BEMatrix(_LinOp):
+    """scipy LinearOperator over the GPU H-matrix (reference: bigwham4py.BEMatrix)."""
+
+    def __init__(self, kernel: str, coor, conn, properties, max_leaf_size: int = 32, eta: float = 3.0,
+                 eps_aca: float = 1.0e-3, n_openMP_threads: int = 8, n_GPUs: int = 1, directly_build: bool = True,
+                 verbose: bool = False, homogeneous_size_pattern: bool = False, fixed_rank=-1, useCuda=True,
+                 precisions=("fp64",), transpose: bool = False, device: int = 0):
+        self.kernel_ = kernel
+        self.max_leaf_size_, self.eta_, self.eps_aca_ = int(max_leaf_size), float(eta), float(eps_aca)
+        self.H_ = BigWhamIOGpu(coor, conn, kernel, properties, n_openMP_threads, n_GPUs, verbose,
+                               homogeneous_size_pattern, useCuda, fixed_rank, device)
+        self.H_.set_gpu_storage(precisions, transpose)
+        self.built_ = False
+        shape = (0, 0)
+        if directly_build:
+            self._build()
+            shape = (self.H_.matrix_size(0), self.H_.matrix_size(1))
+        self.dtype_ = np.dtype(float)
+        super().__init__(self.dtype_, shape)
+
+    def _build(self):
+        if not self.built_:
+            self.H_.build_hierarchical_matrix(self.max_leaf_size_, self.eta_, self.eps_aca_)
+            self.built_ = True
+            super().__init__(np.dtype(float), (self.H_.matrix_size(0), self.H_.matrix_size(1)))
+
+    def _matvec(self, v):
+        return self.H_.matvec(np.asarray(v, dtype=np.float64).ravel())
+
+    def _rmatvec(self, v):
+        if self.H_.gpu is None or not self.H_.gpu.has_transpose:
+            raise RuntimeError("H^T not stored: build with transpose=True")
+        return self.H_.gpu.rmatvec(np.asarray(v, dtype=np.float64).ravel())
+
+    def _matvec_torch(self, x, y):
+        """y = H x on CUDA float64 torch tensors (device pointers, as _matvec_cupy)."""
+        assert x.is_cuda and y.is_cuda and x.dtype == y.dtype and str(x.dtype) == "torch.float64"
+        self.H_.matvec_raw_ptr(x.data_ptr(), y.data_ptr())
+
+    def _matvec_cupy(self, x, y):
+        self.H_.matvec_raw_ptr(x.data.ptr, y.data.ptr)
+
+    def getCompression(self) -> float:
+        return self.H_.get_compression_ratio()
+
+    def getPermutation(self):
+        return self.H_.get_permutation()
+
+    def getCollocationPoints(self):
+        return self.H_.get_collocation_points()
+
+    def getSpatialDimension(self):
+        return 2 if self.kernel_.startswith("2D") else 3
+
+    def H_diag(self):
+        return self.H_.get_diagonal()
+
+    def H_jacobi_prec(self):
+        """Jacobi preconditioner (bigwham4py.py:373-380)."""
+        from scipy.sparse.linalg import LinearOperator
+
+        inv = 1.0 / self.H_diag()
+        return LinearOperator(self.shape, lambda v: inv * np.asarray(v).ravel(), dtype=float)

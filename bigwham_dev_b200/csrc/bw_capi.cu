@@ -1,0 +1,716 @@
+// C ABI of the B200 H-matrix backend (declarations: include/bigwham_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "bigwham_b200.h"
+#include "bw_kernels.cuh"
+#include "bw_layout.h"
+
+namespace {
+
+using bw::Chunk;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct OomError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct UnsupportedError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define BW_CUDA(call)                                                                             \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+  } while (0)
+
+std::mutex g_err_mu;
+std::string g_last_create_error;
+
+int prec_index(int flags) {
+  const int p = flags & (BW_FP64 | BW_FP32 | BW_BF16);
+  if (p == BW_FP64) return 0;
+  if (p == BW_FP32) return 1;
+  if (p == BW_BF16) return 2;
+  return -1;
+}
+
+struct DevPhase {
+  void *data = nullptr;
+  Chunk *chunks = nullptr;
+  int32_t *cta = nullptr;
+  int64_t n_chunks = 0;
+  int64_t n_elems = 0;
+};
+
+}  // namespace
+
+struct bw_hmat {
+  int device = -1;
+  int dof = 1;
+  int64_t n_rows = 0, n_cols = 0;
+  std::vector<int64_t> perm0, perm1;
+  bw::Problem prob;
+  bool finalized = false;
+  bool plan_only = false;
+  int stored = 0;          // precision mask
+  bool has_t = false;      // transposed operator stored
+  int grid = 148;
+  bw::OperatorPlan op[2];  // forward, transposed
+  DevPhase dev[2][3][2];   // [operator][precision][phase]
+  std::vector<unsigned char> host_data[2][3][2];  // BW_PLAN_ONLY
+  int32_t *d_perm0 = nullptr, *d_perm1 = nullptr;
+  void *d_xp = nullptr, *d_t = nullptr;
+  double *d_xh = nullptr, *d_yh = nullptr;
+  int *d_err = nullptr;
+  int *h_err = nullptr;    // pinned
+  cudaStream_t stream = nullptr;
+  int64_t dev_bytes = 0, dev_limit = 0;
+  int64_t entries = 0, sum_rank = 0;
+  int64_t n_fr = 0, n_lr = 0;
+  std::vector<double> diag_perm;
+  std::string err;
+  long long spin_limit = 2000000000LL;  // 2 s bound on every in-kernel wait
+  // optional per-launch timing (bw_set_timing / bw_timing_read)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;     // 4 events per recorded matvec
+  size_t ev_used = 0;                   // matvecs recorded since the last read
+
+  cudaEvent_t *timing_slot() {
+    if (!timing) return nullptr;
+    const size_t kMax = 200000;
+    if (ev_used >= kMax) return nullptr;
+    if (4 * (ev_used + 1) > ev_pool.size()) {
+      const size_t grow = std::max<size_t>(64, ev_pool.size() / 4);
+      for (size_t i = 0; i < 4 * grow; i++) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) throw CudaError("cudaEventCreate failed");
+        ev_pool.push_back(e);
+      }
+    }
+    return &ev_pool[4 * ev_used++];
+  }
+
+  void *dmalloc(size_t bytes) {
+    if (dev_limit > 0 && dev_bytes + (int64_t)bytes > dev_limit)
+      throw OomError("device allocation of " + std::to_string(bytes) + " bytes exceeds the configured limit");
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw OomError("cudaMalloc(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    }
+    dev_bytes += (int64_t)bytes;
+    return p;
+  }
+  void release() {
+    if (device >= 0) cudaSetDevice(device);
+    for (auto &o : dev)
+      for (auto &p : o)
+        for (auto &ph : p) {
+          cudaFree(ph.data);
+          cudaFree(ph.chunks);
+          cudaFree(ph.cta);
+          ph = DevPhase{};
+        }
+    cudaFree(d_perm0);
+    cudaFree(d_perm1);
+    cudaFree(d_xp);
+    cudaFree(d_t);
+    cudaFree(d_xh);
+    cudaFree(d_yh);
+    cudaFree(d_err);
+    if (h_err) cudaFreeHost(h_err);
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    ev_pool.clear();
+    ev_used = 0;
+    if (stream) cudaStreamDestroy(stream);
+    d_perm0 = d_perm1 = nullptr;
+    d_xp = d_t = nullptr;
+    d_xh = d_yh = nullptr;
+    d_err = nullptr;
+    h_err = nullptr;
+    stream = nullptr;
+    dev_bytes = 0;
+  }
+};
+
+namespace {
+
+template <typename F> int guarded(bw_hmat *h, F &&f) {
+  try {
+    return f();
+  } catch (const OomError &e) {
+    if (h) h->err = e.what();
+    return BW_ERR_OOM;
+  } catch (const CudaError &e) {
+    if (h) h->err = e.what();
+    return BW_ERR_CUDA;
+  } catch (const StateError &e) {
+    if (h) h->err = e.what();
+    return BW_ERR_STATE;
+  } catch (const UnsupportedError &e) {
+    if (h) h->err = e.what();
+    return BW_ERR_UNSUPPORTED;
+  } catch (const std::bad_alloc &) {
+    if (h) h->err = "host allocation failed";
+    return BW_ERR_OOM;
+  } catch (const std::exception &e) {
+    if (h) h->err = e.what();
+    return BW_ERR_ARG;
+  }
+}
+
+template <typename S> void set_smem_attr() {
+  static bool done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && done[dev]) return;
+  BW_CUDA(cudaFuncSetAttribute(bw::stream_panels_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               bw::SmemLayout<S>::kTotal));
+  if (dev < 64) done[dev] = true;
+}
+
+// Upload the data of one phase in pieces through two pinned staging buffers.
+void upload_phase(bw_hmat *h, int o, int prec, int phase) {
+  const bw::OperatorPlan &op = h->op[o];
+  const bw::PhasePlan &ph = op.ph[phase];
+  const int es = bw::esize_of(prec);
+  DevPhase &dp = h->dev[o][prec][phase];
+  dp.n_elems = ph.n_elems;
+  const bw::ChunkPlan &cp = ph.cp[prec];
+  dp.n_chunks = (int64_t)cp.chunks.size();
+  if (h->plan_only) {
+    auto &buf = h->host_data[o][prec][phase];
+    buf.assign((size_t)ph.n_elems * es, 0);
+    bw::fill_items(h->prob, o == 1, op, phase, prec, 0, (int64_t)ph.items.size(), 0, buf.data());
+    return;
+  }
+  dp.data = h->dmalloc((size_t)ph.n_elems * es);
+  dp.chunks = static_cast<Chunk *>(h->dmalloc(std::max<size_t>(1, cp.chunks.size()) * sizeof(Chunk)));
+  dp.cta = static_cast<int32_t *>(h->dmalloc(cp.cta_ptr.size() * sizeof(int32_t)));
+  if (!cp.chunks.empty())
+    BW_CUDA(cudaMemcpy(dp.chunks, cp.chunks.data(), cp.chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+  BW_CUDA(cudaMemcpy(dp.cta, cp.cta_ptr.data(), cp.cta_ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+
+  const size_t kPiece = size_t(256) << 20;
+  unsigned char *stage[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  BW_CUDA(cudaMallocHost(&stage[0], kPiece));
+  BW_CUDA(cudaMallocHost(&stage[1], kPiece));
+  BW_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  BW_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  bool used[2] = {false, false};
+  try {
+    const int64_t nit = (int64_t)ph.items.size();
+    auto item_start = [&](int64_t q) { return q < nit ? ph.items[q].data_off : ph.n_elems; };
+    int64_t q = 0;
+    int which = 0;
+    while (q < nit) {
+      // grow the piece while it fits (at least one item)
+      int64_t qe = q + 1;
+      while (qe < nit && (item_start(qe + 1) - item_start(q)) * es <= (int64_t)kPiece) qe++;
+      const int64_t e0 = item_start(q), e1 = item_start(qe);
+      const size_t bytes = (size_t)(e1 - e0) * es;
+      if (bytes > kPiece) throw std::runtime_error("item larger than the staging piece");
+      if (used[which]) BW_CUDA(cudaEventSynchronize(ev[which]));
+      std::memset(stage[which], 0, bytes);
+      bw::fill_items(h->prob, o == 1, op, phase, prec, q, qe, e0, stage[which]);
+      BW_CUDA(cudaMemcpyAsync(static_cast<unsigned char *>(dp.data) + (size_t)e0 * es, stage[which], bytes,
+                              cudaMemcpyHostToDevice, h->stream));
+      BW_CUDA(cudaEventRecord(ev[which], h->stream));
+      used[which] = true;
+      which ^= 1;
+      q = qe;
+    }
+    // tail slack
+    const int64_t tail0 = item_start(nit);
+    BW_CUDA(cudaMemsetAsync(static_cast<unsigned char *>(dp.data) + (size_t)tail0 * es, 0,
+                            (size_t)(ph.n_elems - tail0) * es, h->stream));
+    BW_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (...) {
+    cudaStreamSynchronize(h->stream);
+    cudaFreeHost(stage[0]);
+    cudaFreeHost(stage[1]);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    throw;
+  }
+  cudaFreeHost(stage[0]);
+  cudaFreeHost(stage[1]);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+}
+
+void compute_diagonal(bw_hmat *h) {
+  // Hmat::diagonal (src/hmat/hmatrix/hmat.cc:256-285): entries of the FR blocks
+  // with (i + i0) == (j + j0) in scalar units.  The reference skips FR blocks
+  // that lie strictly below/above the diagonal; the index test covers that.
+  const int64_t n = std::max(h->n_rows, h->n_cols);
+  h->diag_perm.assign((size_t)n, 0.0);
+  for (const bw::FullBlock &b : h->prob.fr) {
+    const int64_t lo = std::max(b.i0, b.j0), hi = std::min(b.i0 + b.m, b.j0 + b.n);
+    for (int64_t d = lo; d < hi; d++) h->diag_perm[(size_t)d] = b.a.at(d - b.i0, d - b.j0);
+  }
+}
+
+template <typename S>
+void launch_matvec(bw_hmat *h, int o, int prec, const double *x, double *y, bool permuted, cudaStream_t st) {
+  using G = typename bw::Store<S>::G;
+  const bw::OperatorPlan &op = h->op[o];
+  const int32_t *perm_in = permuted ? nullptr : (o == 0 ? h->d_perm1 : h->d_perm0);
+  const int32_t *perm_out = permuted ? nullptr : (o == 0 ? h->d_perm0 : h->d_perm1);
+  const int n_in = (int)op.n_in;
+  G *xp = static_cast<G *>(h->d_xp);
+  G *t = static_cast<G *>(h->d_t);
+  cudaEvent_t *ev = h->timing_slot();
+  if (ev) BW_CUDA(cudaEventRecord(ev[0], st));
+  if (n_in > 0) {
+    bw::gather_x_kernel<G><<<(n_in + 255) / 256, 256, 0, st>>>(x, xp, perm_in, h->dof, n_in);
+    BW_CUDA(cudaGetLastError());
+  }
+  if (ev) BW_CUDA(cudaEventRecord(ev[1], st));
+  set_smem_attr<S>();
+  for (int phase = 0; phase < 2; phase++) {
+    const DevPhase &dp = h->dev[o][prec][phase];
+    if (dp.n_chunks == 0) {
+      if (ev) BW_CUDA(cudaEventRecord(ev[2 + phase], st));
+      continue;
+    }
+    bw::StreamArgs a{};
+    a.data = dp.data;
+    a.chunks = dp.chunks;
+    a.cta_ptr = dp.cta;
+    a.xsrc = xp;
+    a.tsrc = t;
+    a.t_out = t;
+    a.y_out = y;
+    a.perm_out = perm_out;
+    a.dof = h->dof;
+    a.phase = phase + 1;
+    a.err = h->d_err;
+    a.spin_limit = h->spin_limit;
+    bw::stream_panels_kernel<S><<<h->grid, bw::kThreads, bw::SmemLayout<S>::kTotal, st>>>(a);
+    BW_CUDA(cudaGetLastError());
+    if (ev) BW_CUDA(cudaEventRecord(ev[2 + phase], st));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *bw_version(void) { return "bigwham_b200 0.1 (sm_100a)"; }
+
+int bw_create(int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0, const int64_t *perm1, int device,
+              bw_hmat **out) {
+  if (!out) return BW_ERR_ARG;
+  *out = nullptr;
+  auto fail = [](const std::string &m, int code) {
+    std::lock_guard<std::mutex> g(g_err_mu);
+    g_last_create_error = m;
+    return code;
+  };
+  if (dof < 1 || n_rows < 0 || n_cols < 0 || n_rows % dof || n_cols % dof)
+    return fail("bad sizes: n_rows and n_cols must be non-negative multiples of dof >= 1", BW_ERR_ARG);
+  if (n_rows > INT32_MAX || n_cols > INT32_MAX) return fail("sizes above 2^31-1 are not supported", BW_ERR_ARG);
+  if ((n_rows && !perm0) || (n_cols && !perm1)) return fail("null permutation", BW_ERR_ARG);
+  std::unique_ptr<bw_hmat> h(new bw_hmat);
+  h->dof = dof;
+  h->n_rows = n_rows;
+  h->n_cols = n_cols;
+  h->perm0.assign(perm0, perm0 + n_rows / dof);
+  h->perm1.assign(perm1, perm1 + n_cols / dof);
+  for (auto *pv : {&h->perm0, &h->perm1}) {
+    const int64_t np = (int64_t)pv->size();
+    std::vector<char> seen((size_t)np, 0);
+    for (int64_t v : *pv) {
+      if (v < 0 || v >= np || seen[(size_t)v]) return fail("permutation is not a permutation of 0..n-1", BW_ERR_ARG);
+      seen[(size_t)v] = 1;
+    }
+  }
+  h->prob.dof = dof;
+  h->prob.n_rows = n_rows;
+  h->prob.n_cols = n_cols;
+  h->device = device;
+  if (device >= 0) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device >= ndev) {
+      cudaGetLastError();
+      return fail("CUDA device " + std::to_string(device) + " not available", BW_ERR_CUDA);
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return fail("cudaSetDevice failed", BW_ERR_CUDA);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    h->grid = sms > 0 ? sms : 148;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail("cudaStreamCreate failed", BW_ERR_CUDA);
+  }
+  *out = h.release();
+  return BW_OK;
+}
+
+int bw_add_full(bw_hmat *h, int64_t i0, int64_t j0, int64_t m, int64_t n, const double *a, int64_t lda) {
+  if (!h) return BW_ERR_ARG;
+  if (h->finalized) {
+    h->err = "bw_add_full after bw_finalize";
+    return BW_ERR_STATE;
+  }
+  return guarded(h, [&] {
+    h->prob.fr.push_back({i0, j0, m, n, bw::View{a, lda, false}});
+    return BW_OK;
+  });
+}
+
+int bw_add_lowrank(bw_hmat *h, int64_t i0, int64_t j0, int64_t m, int64_t n, int64_t r, const double *A,
+                   int64_t lda, const double *B, int64_t ldb) {
+  if (!h) return BW_ERR_ARG;
+  if (h->finalized) {
+    h->err = "bw_add_lowrank after bw_finalize";
+    return BW_ERR_STATE;
+  }
+  return guarded(h, [&] {
+    h->prob.lr.push_back({i0, j0, m, n, r, bw::View{A, lda, false}, bw::View{B, ldb, false}});
+    return BW_OK;
+  });
+}
+
+int bw_set_device_limit(bw_hmat *h, int64_t bytes) {
+  if (!h || bytes < 0) return BW_ERR_ARG;
+  h->dev_limit = bytes;
+  return BW_OK;
+}
+
+int bw_finalize(bw_hmat *h, int flags) {
+  if (!h) return BW_ERR_ARG;
+  if (h->finalized) {
+    h->err = "bw_finalize called twice";
+    return BW_ERR_STATE;
+  }
+  int rc = guarded(h, [&] {
+    int mask = flags & (BW_FP64 | BW_FP32 | BW_BF16);
+    if (!mask) mask = BW_FP64;
+    h->plan_only = (flags & BW_PLAN_ONLY) != 0;
+    if (!h->plan_only && h->device < 0) throw StateError("handle has no device; use BW_PLAN_ONLY");
+    if (h->device >= 0) BW_CUDA(cudaSetDevice(h->device));
+    const bool want_t = (flags & BW_STORE_TRANSPOSE) != 0;
+    const bool check = (flags & BW_NO_FINITE_CHECK) == 0;
+    // statistics
+    h->entries = 0;
+    h->sum_rank = 0;
+    h->n_fr = (int64_t)h->prob.fr.size();
+    h->n_lr = (int64_t)h->prob.lr.size();
+    for (auto &b : h->prob.fr) h->entries += b.m * b.n;
+    for (auto &b : h->prob.lr) {
+      h->entries += b.r * (b.m + b.n);
+      h->sum_rank += b.r;
+    }
+    for (int o = 0; o < (want_t ? 2 : 1); o++) {
+      bw::build_operator(h->prob, o == 1, h->op[o]);
+      bw::compute_scales(h->prob, o == 1, check && o == 0, h->op[o]);
+      for (int p = 0; p < 3; p++)
+        if (mask & (1 << p)) bw::build_chunks(h->prob, o == 1, p, h->grid, h->op[o]);
+    }
+    compute_diagonal(h);
+    if (!h->plan_only) {
+      // size check before any allocation
+      int64_t need = 0;
+      for (int o = 0; o < (want_t ? 2 : 1); o++)
+        for (int p = 0; p < 3; p++)
+          if (mask & (1 << p))
+            for (int ph = 0; ph < 2; ph++)
+              need += h->op[o].ph[ph].n_elems * bw::esize_of(p) +
+                      (int64_t)h->op[o].ph[ph].cp[p].chunks.size() * (int64_t)sizeof(Chunk);
+      if (h->dev_limit > 0 && need > h->dev_limit)
+        throw OomError("layout needs " + std::to_string(need) + " device bytes, above the configured limit of " +
+                       std::to_string(h->dev_limit));
+      const int64_t nmax = std::max(h->n_rows, h->n_cols);
+      std::vector<int32_t> p32;
+      p32.assign(h->perm0.begin(), h->perm0.end());
+      h->d_perm0 = static_cast<int32_t *>(h->dmalloc(std::max<size_t>(1, p32.size()) * 4));
+      if (!p32.empty()) BW_CUDA(cudaMemcpy(h->d_perm0, p32.data(), p32.size() * 4, cudaMemcpyHostToDevice));
+      p32.assign(h->perm1.begin(), h->perm1.end());
+      h->d_perm1 = static_cast<int32_t *>(h->dmalloc(std::max<size_t>(1, p32.size()) * 4));
+      if (!p32.empty()) BW_CUDA(cudaMemcpy(h->d_perm1, p32.data(), p32.size() * 4, cudaMemcpyHostToDevice));
+      h->d_xp = h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8);
+      h->d_t = h->dmalloc((size_t)std::max<int64_t>(1, h->sum_rank) * 8);
+      h->d_xh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
+      h->d_yh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
+      h->d_err = static_cast<int *>(h->dmalloc(sizeof(int)));
+      BW_CUDA(cudaMemset(h->d_err, 0, sizeof(int)));
+      BW_CUDA(cudaMallocHost(&h->h_err, sizeof(int)));
+      *h->h_err = 0;
+    }
+    for (int o = 0; o < (want_t ? 2 : 1); o++)
+      for (int p = 0; p < 3; p++)
+        if (mask & (1 << p))
+          for (int ph = 0; ph < 2; ph++) upload_phase(h, o, p, ph);
+    h->stored = mask;
+    h->has_t = want_t;
+    h->finalized = true;
+    return BW_OK;
+  });
+  // the borrowed block pointers are not used after this point (the host plan
+  // keeps only indices; a plan-only handle keeps its converted copy)
+  if (rc != BW_OK && !h->plan_only) h->release();
+  if (rc == BW_OK) {
+    h->prob.fr.clear();
+    h->prob.lr.clear();
+    h->prob.fr.shrink_to_fit();
+    h->prob.lr.shrink_to_fit();
+  }
+  return rc;
+}
+
+int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream) {
+  if (!h) return BW_ERR_ARG;
+  return guarded(h, [&] {
+    if (!h->finalized) throw StateError("bw_matvec before bw_finalize");
+    if (h->plan_only) throw StateError("handle was finalized with BW_PLAN_ONLY (no device data)");
+    const int p = prec_index(flags);
+    if (p < 0) throw std::invalid_argument("flags must name exactly one of BW_FP64, BW_FP32, BW_BF16");
+    if (!(h->stored & (1 << p))) throw UnsupportedError("precision not stored by bw_finalize");
+    const bool tr = (flags & BW_TRANSPOSE) != 0;
+    if (tr && !h->has_t) throw UnsupportedError("transposed layout not stored (finalize with BW_STORE_TRANSPOSE)");
+    const int64_t nin = tr ? h->n_rows : h->n_cols, nout = tr ? h->n_cols : h->n_rows;
+    if ((nin && !x) || (nout && !y)) throw std::invalid_argument("null vector");
+    if (x && y) {
+      const char *xb = reinterpret_cast<const char *>(x), *yb = reinterpret_cast<const char *>(y);
+      if (xb < yb + nout * 8 && yb < xb + nin * 8) throw std::invalid_argument("x and y overlap");
+    }
+    BW_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool perm = (flags & BW_PERMUTED) != 0;
+    const int o = tr ? 1 : 0;
+    if (p == 0)
+      launch_matvec<double>(h, o, 0, x, y, perm, st);
+    else if (p == 1)
+      launch_matvec<float>(h, o, 1, x, y, perm, st);
+    else
+      launch_matvec<bw::Bf16>(h, o, 2, x, y, perm, st);
+    return BW_OK;
+  });
+}
+
+int bw_sync(bw_hmat *h, void *stream) {
+  if (!h) return BW_ERR_ARG;
+  return guarded(h, [&] {
+    if (!h->finalized || h->plan_only) throw StateError("no device state");
+    BW_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BW_CUDA(cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BW_CUDA(cudaStreamSynchronize(st));
+    if (*h->h_err != 0) {
+      const int code = *h->h_err;
+      BW_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
+      BW_CUDA(cudaStreamSynchronize(st));
+      char buf[64];
+      snprintf(buf, sizeof buf, "kernel error word 0x%x", code);
+      h->err = buf;
+      return BW_ERR_DEVICE;
+    }
+    return BW_OK;
+  });
+}
+
+int bw_matvec_host(bw_hmat *h, const double *x, double *y, int flags) {
+  if (!h) return BW_ERR_ARG;
+  int rc = guarded(h, [&] {
+    if (!h->finalized || h->plan_only) throw StateError("no device state");
+    const bool tr = (flags & BW_TRANSPOSE) != 0;
+    const int64_t nin = tr ? h->n_rows : h->n_cols, nout = tr ? h->n_cols : h->n_rows;
+    if ((nin && !x) || (nout && !y)) throw std::invalid_argument("null vector");
+    BW_CUDA(cudaSetDevice(h->device));
+    BW_CUDA(cudaMemcpyAsync(h->d_xh, x, (size_t)nin * 8, cudaMemcpyHostToDevice, h->stream));
+    return BW_OK;
+  });
+  if (rc != BW_OK) return rc;
+  rc = bw_matvec(h, h->d_xh, h->d_yh, flags, h->stream);
+  if (rc != BW_OK) return rc;
+  rc = guarded(h, [&] {
+    const bool tr = (flags & BW_TRANSPOSE) != 0;
+    const int64_t nout = tr ? h->n_cols : h->n_rows;
+    BW_CUDA(cudaMemcpyAsync(y, h->d_yh, (size_t)nout * 8, cudaMemcpyDeviceToHost, h->stream));
+    return BW_OK;
+  });
+  if (rc != BW_OK) return rc;
+  return bw_sync(h, h->stream);
+}
+
+int bw_matmat(bw_hmat *h, const double *X, int64_t ldx, double *Y, int64_t ldy, int nrhs, int flags,
+              void *stream) {
+  if (!h) return BW_ERR_ARG;
+  if (nrhs < 0) return BW_ERR_ARG;
+  const bool tr = (flags & BW_TRANSPOSE) != 0;
+  const int64_t nin = tr ? h->n_rows : h->n_cols, nout = tr ? h->n_cols : h->n_rows;
+  if (ldx < nin || ldy < nout) {
+    h->err = "leading dimension too small";
+    return BW_ERR_ARG;
+  }
+  for (int k = 0; k < nrhs; k++) {
+    int rc = bw_matvec(h, X + k * ldx, Y + k * ldy, flags, stream);
+    if (rc != BW_OK) return rc;
+  }
+  return BW_OK;
+}
+
+int bw_diagonal(bw_hmat *h, double *d, int flags) {
+  if (!h || !d) return BW_ERR_ARG;
+  return guarded(h, [&] {
+    if (!h->finalized) throw StateError("bw_diagonal before bw_finalize");
+    const int64_t n = (int64_t)h->diag_perm.size();
+    if (flags & BW_PERMUTED) {
+      std::memcpy(d, h->diag_perm.data(), (size_t)n * 8);
+      return BW_OK;
+    }
+    // Hmat::diagonalOriginal (hmat.cc:240-254): permuted back with permutation_1_
+    std::memset(d, 0, (size_t)n * 8);
+    const int dof = h->dof;
+    for (size_t i = 0; i < h->perm1.size(); i++)
+      for (int j = 0; j < dof; j++) d[dof * h->perm1[i] + j] = h->diag_perm[dof * i + j];
+    return BW_OK;
+  });
+}
+
+int bw_info(const bw_hmat *h, int64_t *out, int n) {
+  if (!h || !out) return BW_ERR_ARG;
+  const int64_t v[] = {h->n_rows,
+                       h->n_cols,
+                       h->dof,
+                       h->n_fr,
+                       h->n_lr,
+                       h->entries,
+                       h->sum_rank,
+                       h->op[0].n_panels,
+                       h->dev_bytes,
+                       h->grid,
+                       (int64_t)h->op[0].ph[0].cp[0].chunks.size(),
+                       (int64_t)h->op[0].ph[1].cp[0].chunks.size(),
+                       h->stored};
+  const int nv = (int)(sizeof(v) / sizeof(v[0]));
+  for (int i = 0; i < n && i < nv; i++) out[i] = v[i];
+  return BW_OK;
+}
+
+int bw_algorithmic_bytes(const bw_hmat *h, int precision, int64_t *bytes) {
+  if (!h || !bytes) return BW_ERR_ARG;
+  const int p = prec_index(precision);
+  if (p < 0) return BW_ERR_ARG;
+  int64_t b = h->entries * bw::esize_of(p) + 8 * (h->n_rows + h->n_cols);
+  if (p == 2) b += 4 * ((int64_t)h->op[0].scale_fr.size() + 2 * (int64_t)h->op[0].scale_a.size());
+  *bytes = b;
+  return BW_OK;
+}
+
+int bw_last_error(const bw_hmat *h, char *buf, size_t len) {
+  if (!buf || len == 0) return BW_ERR_ARG;
+  std::string m;
+  if (h) {
+    m = h->err;
+  } else {
+    std::lock_guard<std::mutex> g(g_err_mu);
+    m = g_last_create_error;
+  }
+  const size_t k = std::min(len - 1, m.size());
+  std::memcpy(buf, m.data(), k);
+  buf[k] = 0;
+  return BW_OK;
+}
+
+int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_chunks, int32_t *chunks,
+                   int64_t *n_elems, double *data, int64_t *n_cta, int32_t *cta_ptr) {
+  if (!h || phase < 1 || phase > 2) return BW_ERR_ARG;
+  const int p = prec_index(precision);
+  if (p < 0 || !h->finalized || !(h->stored & (1 << p))) return BW_ERR_STATE;
+  const int o = transposed ? 1 : 0;
+  if (o == 1 && !h->has_t) return BW_ERR_UNSUPPORTED;
+  const bw::PhasePlan &ph = h->op[o].ph[phase - 1];
+  const bw::ChunkPlan &cp = ph.cp[p];
+  if (n_chunks) *n_chunks = (int64_t)cp.chunks.size();
+  if (n_elems) *n_elems = ph.n_elems;
+  if (n_cta) *n_cta = (int64_t)cp.cta_ptr.size();
+  if (chunks) std::memcpy(chunks, cp.chunks.data(), cp.chunks.size() * sizeof(Chunk));
+  if (cta_ptr) std::memcpy(cta_ptr, cp.cta_ptr.data(), cp.cta_ptr.size() * sizeof(int32_t));
+  if (data) {
+    if (!h->plan_only) return BW_ERR_STATE;
+    const auto &buf = h->host_data[o][p][phase - 1];
+    for (int64_t i = 0; i < ph.n_elems; i++) {
+      if (p == 0)
+        data[i] = reinterpret_cast<const double *>(buf.data())[i];
+      else if (p == 1)
+        data[i] = reinterpret_cast<const float *>(buf.data())[i];
+      else
+        data[i] = bw::from_bf16(reinterpret_cast<const uint16_t *>(buf.data())[i]);
+    }
+  }
+  return BW_OK;
+}
+
+int bw_set_timing(bw_hmat *h, int enable) {
+  if (!h) return BW_ERR_ARG;
+  h->timing = enable != 0;
+  h->ev_used = 0;
+  return BW_OK;
+}
+
+int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs) {
+  if (!h || !ms) return BW_ERR_ARG;
+  return guarded(h, [&] {
+    ms[0] = ms[1] = ms[2] = 0.0;
+    if (h->ev_used > 0) {
+      BW_CUDA(cudaSetDevice(h->device));
+      BW_CUDA(cudaEventSynchronize(h->ev_pool[4 * h->ev_used - 1]));
+      for (size_t i = 0; i < h->ev_used; i++)
+        for (int k = 0; k < 3; k++) {
+          float v = 0.0f;
+          BW_CUDA(cudaEventElapsedTime(&v, h->ev_pool[4 * i + k], h->ev_pool[4 * i + k + 1]));
+          ms[k] += v;
+        }
+    }
+    if (n_matvecs) *n_matvecs = (int64_t)h->ev_used;
+    h->ev_used = 0;
+    return BW_OK;
+  });
+}
+
+int bw_phase_bytes(const bw_hmat *h, int precision, int transposed, int64_t *phase1, int64_t *phase2) {
+  if (!h || !phase1 || !phase2) return BW_ERR_ARG;
+  const int p = prec_index(precision);
+  if (p < 0) return BW_ERR_ARG;
+  const int o = transposed ? 1 : 0;
+  if (o == 1 && !h->has_t) return BW_ERR_UNSUPPORTED;
+  // Algorithmic bytes per launch (the split of bw_algorithmic_bytes): stored
+  // entries the launch streams, x (8 bytes per input) counted in phase 1, y
+  // (8 bytes per output) and the BF16 block scales in phase 2.
+  const int es = bw::esize_of(p);
+  int64_t e[2] = {0, 0};
+  for (int ph = 0; ph < 2; ph++)
+    for (const bw::Item &it : h->op[o].ph[ph].items) e[ph] += int64_t(it.h) * it.ncols;
+  *phase1 = e[0] * es + 8 * h->op[o].n_in;
+  *phase2 = e[1] * es + 8 * h->op[o].n_out;
+  if (p == 2) *phase2 += 4 * ((int64_t)h->op[o].scale_fr.size() + 2 * (int64_t)h->op[o].scale_a.size());
+  return BW_OK;
+}
+
+int bw_destroy(bw_hmat *h) {
+  if (!h) return BW_OK;
+  h->release();
+  delete h;
+  return BW_OK;
+}
+
+}  // extern "C"

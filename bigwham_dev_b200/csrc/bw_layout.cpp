@@ -1,0 +1,401 @@
+// Host-side layout builder (see bw_layout.h for the scheme).
+#include "bw_layout.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <numeric>
+#include <queue>
+#include <stdexcept>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace bw {
+
+int esize_of(int prec) { return prec == 0 ? 8 : (prec == 1 ? 4 : 2); }
+
+// Round-to-nearest-even FP32 -> BF16 on the bit pattern (NaN kept quiet).
+uint16_t to_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return static_cast<uint16_t>((u >> 16) | 0x40u);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return static_cast<uint16_t>(u >> 16);
+}
+
+float from_bf16(uint16_t b) {
+  uint32_t u = static_cast<uint32_t>(b) << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+namespace {
+
+// The blocks of the operator being laid out: H itself, or H^T built from the
+// same storage (FR: A^T; LR: (A B)^T = B^T A^T, i.e. A' = B^T and B' = A^T).
+struct EffFull {
+  int64_t i0, j0, m, n;
+  View a;
+};
+struct EffLow {
+  int64_t i0, j0, m, n, r;
+  View A, B;
+};
+
+View flip(View v) {
+  v.trans = !v.trans;
+  return v;
+}
+
+EffFull eff_full(const Problem &p, bool tr, size_t k) {
+  const FullBlock &b = p.fr[k];
+  if (!tr) return {b.i0, b.j0, b.m, b.n, b.a};
+  return {b.j0, b.i0, b.n, b.m, flip(b.a)};
+}
+
+EffLow eff_low(const Problem &p, bool tr, size_t k) {
+  const LowRankBlock &b = p.lr[k];
+  if (!tr) return {b.i0, b.j0, b.m, b.n, b.r, b.A, b.B};
+  return {b.j0, b.i0, b.n, b.m, b.r, flip(b.B), flip(b.A)};
+}
+
+[[noreturn]] void fail(const std::string &msg) { throw std::runtime_error(msg); }
+
+int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
+  const int64_t n_out = tr ? p.n_cols : p.n_rows;
+  const int64_t n_in = tr ? p.n_rows : p.n_cols;
+  op = OperatorPlan{};
+  op.n_out = n_out;
+  op.n_in = n_in;
+  const size_t nfr = p.fr.size(), nlr = p.lr.size();
+
+  // ---- range checks
+  for (size_t k = 0; k < nfr; k++) {
+    const FullBlock &b = p.fr[k];
+    if (b.m <= 0 || b.n <= 0 || b.i0 < 0 || b.j0 < 0 || b.i0 + b.m > p.n_rows || b.j0 + b.n > p.n_cols)
+      fail("full block " + std::to_string(k) + " out of range");
+    if (!b.a.p || b.a.ld < b.m) fail("full block " + std::to_string(k) + ": null data or lda < m");
+  }
+  for (size_t k = 0; k < nlr; k++) {
+    const LowRankBlock &b = p.lr[k];
+    if (b.m <= 0 || b.n <= 0 || b.r < 0 || b.i0 < 0 || b.j0 < 0 || b.i0 + b.m > p.n_rows ||
+        b.j0 + b.n > p.n_cols)
+      fail("low-rank block " + std::to_string(k) + " out of range");
+    if (b.r > 0 && (!b.A.p || !b.B.p || b.A.ld < b.m || b.B.ld < b.r))
+      fail("low-rank block " + std::to_string(k) + ": null data or leading dimension too small");
+    if (b.r > 65535) fail("low-rank block " + std::to_string(k) + ": rank above 65535");
+  }
+
+  // ---- t offsets (phase-1 outputs, one slot per rank column)
+  op.t_off.resize(nlr);
+  int64_t t = 0;
+  for (size_t k = 0; k < nlr; k++) {
+    op.t_off[k] = t;
+    t += p.lr[k].r;
+  }
+  op.t_len = t;
+  if (t > INT32_MAX || n_out > INT32_MAX || n_in > INT32_MAX) fail("problem too large for 32-bit offsets");
+
+  // ---- row panels: finest partition of [0, n_out) by block row boundaries
+  std::vector<int64_t> bounds{0, n_out};
+  for (size_t k = 0; k < nfr; k++) {
+    EffFull b = eff_full(p, tr, k);
+    bounds.push_back(b.i0);
+    bounds.push_back(b.i0 + b.m);
+  }
+  for (size_t k = 0; k < nlr; k++) {
+    EffLow b = eff_low(p, tr, k);
+    bounds.push_back(b.i0);
+    bounds.push_back(b.i0 + b.m);
+  }
+  std::sort(bounds.begin(), bounds.end());
+  bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
+  std::vector<int64_t> pb;  // panel starts, with tall panels split at kHMax rows
+  for (size_t i = 0; i + 1 < bounds.size(); i++) {
+    for (int64_t s = bounds[i]; s < bounds[i + 1]; s += kHMax) pb.push_back(s);
+  }
+  pb.push_back(n_out);
+  const size_t npan = pb.size() - 1;
+  op.n_panels = static_cast<int64_t>(npan);
+
+  // blocks covering each panel (panels sorted; a block covers a contiguous panel range)
+  auto first_panel = [&](int64_t row) {
+    return static_cast<size_t>(std::upper_bound(pb.begin(), pb.end(), row) - pb.begin()) - 1;
+  };
+  struct Cover {
+    int kind;  // 0 FR, 1 LR
+    int64_t k;
+    int64_t j0, n;
+  };
+  std::vector<std::vector<Cover>> cov(npan);
+  for (size_t k = 0; k < nfr; k++) {
+    EffFull b = eff_full(p, tr, k);
+    for (size_t q = first_panel(b.i0); q < npan && pb[q] < b.i0 + b.m; q++) cov[q].push_back({0, (int64_t)k, b.j0, b.n});
+  }
+  for (size_t k = 0; k < nlr; k++) {
+    EffLow b = eff_low(p, tr, k);
+    for (size_t q = first_panel(b.i0); q < npan && pb[q] < b.i0 + b.m; q++) cov[q].push_back({1, (int64_t)k, b.j0, b.n});
+  }
+  // coverage: the column intervals of each panel must tile [0, n_in) exactly
+  for (size_t q = 0; q < npan; q++) {
+    auto &c = cov[q];
+    std::sort(c.begin(), c.end(), [](const Cover &a, const Cover &b) { return a.j0 < b.j0; });
+    int64_t at = 0;
+    for (const Cover &e : c) {
+      if (e.j0 < at) fail("blocks overlap in rows [" + std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
+      if (e.j0 > at) fail("columns [" + std::to_string(at) + ", " + std::to_string(e.j0) + ") not covered in rows [" +
+                          std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
+      at = e.j0 + e.n;
+    }
+    if (at != n_in) fail("columns [" + std::to_string(at) + ", " + std::to_string(n_in) + ") not covered in rows [" +
+                         std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
+  }
+
+  // ---- phase 1 items: B of every low-rank block, rows split at kHMax
+  PhasePlan &p1 = op.ph[0];
+  int64_t off = 0;
+  for (size_t k = 0; k < nlr; k++) {
+    EffLow b = eff_low(p, tr, k);
+    for (int64_t r0 = 0; r0 < b.r; r0 += kHMax) {
+      Item it;
+      it.h = static_cast<int32_t>(std::min<int64_t>(kHMax, b.r - r0));
+      it.hpad = it.h + (it.h & 1);
+      it.ncols = b.n;
+      it.out_off = static_cast<int32_t>(op.t_off[k] + r0);
+      it.data_off = off;
+      it.segs.push_back({2, (int64_t)k, r0, b.n, 0, b.j0});
+      off = align_up(off + it.hpad * it.ncols, kItemAlign);
+      p1.items.push_back(std::move(it));
+    }
+  }
+  p1.n_elems = off + kItemAlign;  // slack so 16-byte rounded copies stay inside
+
+  // ---- phase 2 items: row panels; FR slices first (they do not depend on t)
+  PhasePlan &p2 = op.ph[1];
+  off = 0;
+  for (size_t q = 0; q < npan; q++) {
+    Item it;
+    it.h = static_cast<int32_t>(pb[q + 1] - pb[q]);
+    it.hpad = it.h + (it.h & 1);
+    it.out_off = static_cast<int32_t>(pb[q]);
+    it.data_off = off;
+    it.ncols = 0;
+    for (int pass = 0; pass < 2; pass++) {
+      for (const Cover &e : cov[q]) {
+        if (e.kind != pass) continue;
+        if (e.kind == 0) {
+          EffFull b = eff_full(p, tr, e.k);
+          it.segs.push_back({0, e.k, pb[q] - b.i0, b.n, 0, b.j0});
+          it.ncols += b.n;
+        } else {
+          EffLow b = eff_low(p, tr, e.k);
+          if (b.r == 0) continue;
+          it.segs.push_back({1, e.k, pb[q] - b.i0, b.r, 1, op.t_off[e.k]});
+          it.ncols += b.r;
+        }
+      }
+    }
+    off = align_up(off + it.hpad * it.ncols, kItemAlign);
+    p2.items.push_back(std::move(it));
+  }
+  p2.n_elems = off + kItemAlign;
+}
+
+void compute_scales(const Problem &p, bool tr, bool check_finite, OperatorPlan &op) {
+  const int64_t nfr = (int64_t)p.fr.size(), nlr = (int64_t)p.lr.size();
+  op.scale_fr.assign(nfr, 1.0f);
+  op.scale_a.assign(nlr, 1.0f);
+  op.scale_b.assign(nlr, 1.0f);
+  int64_t bad_fr = -1, bad_lr = -1;
+  auto maxabs = [](const View &v, int64_t m, int64_t n, bool &finite) {
+    double s = 0.0;
+    for (int64_t j = 0; j < n; j++)
+      for (int64_t i = 0; i < m; i++) {
+        double a = std::fabs(v.at(i, j));
+        if (!(a <= 1.0e300)) finite = false;
+        s = std::max(s, a);
+      }
+    return s;
+  };
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t k = 0; k < nfr; k++) {
+    EffFull b = eff_full(p, tr, k);
+    bool fin = true;
+    double s = maxabs(b.a, b.m, b.n, fin);
+    op.scale_fr[k] = (s > 0 && std::isfinite(s)) ? static_cast<float>(s) : 1.0f;
+    if (!fin) {
+#pragma omp critical
+      bad_fr = std::max(bad_fr, k);
+    }
+  }
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t k = 0; k < nlr; k++) {
+    EffLow b = eff_low(p, tr, k);
+    if (b.r == 0) continue;
+    bool fin = true;
+    double sa = maxabs(b.A, b.m, b.r, fin);
+    double sb = maxabs(b.B, b.r, b.n, fin);
+    op.scale_a[k] = (sa > 0 && std::isfinite(sa)) ? static_cast<float>(sa) : 1.0f;
+    op.scale_b[k] = (sb > 0 && std::isfinite(sb)) ? static_cast<float>(sb) : 1.0f;
+    if (!fin) {
+#pragma omp critical
+      bad_lr = std::max(bad_lr, k);
+    }
+  }
+  if (check_finite && bad_fr >= 0) fail("non-finite entry in full block " + std::to_string(bad_fr));
+  if (check_finite && bad_lr >= 0) fail("non-finite entry in low-rank block " + std::to_string(bad_lr));
+}
+
+namespace {
+
+float seg_scale(const OperatorPlan &op, const Segment &s, int prec) {
+  if (prec != 2) return 1.0f;
+  if (s.kind == 0) return op.scale_fr[s.block];
+  if (s.kind == 2) return op.scale_a[s.block] * op.scale_b[s.block];
+  return 1.0f;  // LR A slices: the scale of A is folded into t
+}
+
+void chunk_items(const OperatorPlan &op, const PhasePlan &ph, int prec, std::vector<std::vector<Chunk>> &per_item) {
+  const int es = esize_of(prec);
+  per_item.assign(ph.items.size(), {});
+  for (size_t q = 0; q < ph.items.size(); q++) {
+    const Item &it = ph.items[q];
+    const int64_t cap = std::max<int64_t>(1, std::min<int64_t>(kMaxCols, kStageBytes / (int64_t(it.hpad) * es)));
+    std::vector<Chunk> &out = per_item[q];
+    Chunk cur{};
+    int64_t col = 0;  // item column of the next column to place
+    auto open = [&](float sc) {
+      std::memset(&cur, 0, sizeof(cur));
+      cur.data_off = it.data_off + col * it.hpad;
+      cur.hpad = it.hpad;
+      cur.rows = it.h;
+      cur.out_off = it.out_off;
+      cur.scale = sc;
+    };
+    auto close = [&]() {
+      if (out.empty()) cur.flags |= kFirst;
+      out.push_back(cur);
+    };
+    bool have = false;
+    for (const Segment &s : it.segs) {
+      const float sc = seg_scale(op, s, prec);
+      int64_t done = 0;
+      while (done < s.ncols) {
+        const int nseg = (cur.flags >> 8) & 0xf;
+        if (have && (cur.ncols >= cap || nseg >= kMaxSeg || cur.scale != sc)) {
+          close();
+          have = false;
+        }
+        if (!have) {
+          open(sc);
+          have = true;
+        }
+        const int ns = (cur.flags >> 8) & 0xf;
+        const int64_t take = std::min<int64_t>(s.ncols - done, cap - cur.ncols);
+        cur.seg_off[ns] = static_cast<int32_t>(s.src_off + done);
+        cur.seg_cols[ns] = static_cast<uint16_t>(take);
+        cur.flags = (cur.flags & ~(0xfu << 8)) | (uint32_t(ns + 1) << 8);
+        if (s.src) cur.flags |= (1u << (16 + ns));
+        cur.ncols += static_cast<int32_t>(take);
+        done += take;
+        col += take;
+      }
+    }
+    if (!have) {  // an item without columns still writes its (zero) output
+      open(1.0f);
+      have = true;
+    }
+    close();
+    out.back().flags |= kLast;
+  }
+}
+
+}  // namespace
+
+void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &op) {
+  (void)p;
+  (void)tr;
+  const int es = esize_of(prec);
+  for (int phase = 0; phase < 2; phase++) {
+    PhasePlan &ph = op.ph[phase];
+    std::vector<std::vector<Chunk>> per_item;
+    chunk_items(op, ph, prec, per_item);
+    // LPT: items by decreasing cost onto the least-loaded CTA.  Cost is the
+    // bytes streamed plus a fixed per-chunk overhead (descriptor, gather,
+    // barrier round trip) expressed in bytes.
+    const int64_t n = (int64_t)ph.items.size();
+    std::vector<int64_t> cost(n);
+    for (int64_t q = 0; q < n; q++)
+      cost[q] = int64_t(ph.items[q].hpad) * ph.items[q].ncols * es + 2048 * (int64_t)per_item[q].size();
+    std::vector<int64_t> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+    using Slot = std::pair<int64_t, int>;  // load, cta
+    std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+    for (int c = 0; c < grid; c++) heap.push({0, c});
+    std::vector<std::vector<int64_t>> bins(grid);
+    for (int64_t q : order) {
+      Slot s = heap.top();
+      heap.pop();
+      bins[s.second].push_back(q);
+      s.first += cost[q];
+      heap.push(s);
+    }
+    ChunkPlan &cp = ph.cp[prec];
+    cp.chunks.clear();
+    cp.cta_ptr.assign(grid + 1, 0);
+    for (int c = 0; c < grid; c++) {
+      cp.cta_ptr[c] = static_cast<int32_t>(cp.chunks.size());
+      for (int64_t q : bins[c]) cp.chunks.insert(cp.chunks.end(), per_item[q].begin(), per_item[q].end());
+    }
+    cp.cta_ptr[grid] = static_cast<int32_t>(cp.chunks.size());
+    if (cp.chunks.size() > (size_t)INT32_MAX) fail("too many chunks");
+  }
+}
+
+void fill_items(const Problem &p, bool tr, const OperatorPlan &op, int phase, int prec, int64_t i_begin,
+                int64_t i_end, int64_t base, void *dst) {
+  const PhasePlan &ph = op.ph[phase];
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t q = i_begin; q < i_end; q++) {
+    const Item &it = ph.items[q];
+    int64_t col = 0;
+    for (const Segment &s : it.segs) {
+      View v;
+      double inv = 1.0;
+      if (s.kind == 0) {
+        v = eff_full(p, tr, s.block).a;
+        if (prec == 2) inv = 1.0 / op.scale_fr[s.block];
+      } else if (s.kind == 1) {
+        v = eff_low(p, tr, s.block).A;
+        if (prec == 2) inv = 1.0 / op.scale_a[s.block];
+      } else {
+        v = eff_low(p, tr, s.block).B;
+        if (prec == 2) inv = 1.0 / op.scale_b[s.block];
+      }
+      for (int64_t c = 0; c < s.ncols; c++) {
+        const int64_t e0 = it.data_off + (col + c) * it.hpad - base;
+        for (int64_t i = 0; i < it.hpad; i++) {
+          const double val = (i < it.h) ? v.at(s.row0 + i, c) : 0.0;
+          if (prec == 0)
+            static_cast<double *>(dst)[e0 + i] = val;
+          else if (prec == 1)
+            static_cast<float *>(dst)[e0 + i] = static_cast<float>(val);
+          else
+            static_cast<uint16_t *>(dst)[e0 + i] = to_bf16(static_cast<float>(val * inv));
+        }
+      }
+      col += s.ncols;
+    }
+  }
+}
+
+}  // namespace bw

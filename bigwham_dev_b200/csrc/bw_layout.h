@@ -1,0 +1,142 @@
+// Host-side layout builder for the streamed H-matrix matvec.
+//
+// The reference applies y = sum_FR A x + sum_LR A (B x) block by block
+// (src/hmat/hmatrix/hmat.cc:472-537).  On the device the same product runs as
+// two streaming passes over re-laid-out block data:
+//
+//  phase 1 ("B stage"):   t_b = B_b x[cols_b] for every low-rank block b.
+//      One item per block (rows split above kHMax): the r x n matrix B_b,
+//      column-major with its row count padded to an even number.
+//  phase 2 ("row panels"): y[p] = sum over the blocks that cover row panel p of
+//      (slice of A_b or of the full block) times (t_b or x[cols]).
+//      Row panels are the finest partition of the rows by block boundaries, so
+//      every block covers whole panels.  One item per panel: the slices of all
+//      covering blocks side by side, column-major (ld = padded panel height).
+//
+// Every item is a dense column-major panel times a gathered vector; an item is
+// owned by one CTA, so outputs are written once, without atomics.  An item is
+// cut into chunks of at most kStageBytes; a chunk is the unit one TMA bulk copy
+// stages into shared memory, and carries up to kMaxSeg "gather segments" that
+// say where the vector values of its columns come from (x or t).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace bw {
+
+constexpr int kStageBytes = 32768;   // bytes of block data per pipeline stage
+constexpr int kMaxCols = 512;        // columns per chunk (size of a stage's gather buffer)
+constexpr int kMaxSeg = 4;           // gather segments per chunk
+constexpr int kHMax = 512;           // max padded rows of one item
+constexpr int kItemAlign = 64;       // item start alignment, in elements
+
+// Chunk flags
+constexpr uint32_t kFirst = 1u;      // first chunk of an item: reset accumulators
+constexpr uint32_t kLast = 2u;       // last chunk of an item: reduce and write the output
+// bits 8..11: number of segments; bits 16..19: source of segment k (0 = x, 1 = t)
+
+// One chunk descriptor, 64 bytes, read by the producer warp and copied into
+// shared memory for the consumer warps.
+struct alignas(16) Chunk {
+  int64_t data_off;      // element offset of the chunk's first column in the data array
+  int32_t ncols;         // columns in this chunk
+  int32_t hpad;          // padded row count of the item (even)
+  int32_t rows;          // rows of the item to write (<= hpad)
+  int32_t out_off;       // first output index: t offset (phase 1) or row (phase 2)
+  float scale;           // multiplies this chunk's partial sums (BF16 block scale)
+  uint32_t flags;        // kFirst | kLast | nseg << 8 | src bits << 16
+  int32_t seg_off[kMaxSeg];   // element offset of each segment in its source vector
+  uint16_t seg_cols[kMaxSeg]; // columns of each segment
+  int32_t reserved[2];
+};
+static_assert(sizeof(Chunk) == 64, "chunk descriptor must be 64 bytes");
+
+// A read-only view of a column-major block (or of its transpose).
+struct View {
+  const double *p = nullptr;
+  int64_t ld = 0;
+  bool trans = false;
+  double at(int64_t i, int64_t j) const { return trans ? p[i * ld + j] : p[i + j * ld]; }
+};
+
+struct FullBlock {
+  int64_t i0, j0, m, n;
+  View a;
+};
+struct LowRankBlock {
+  int64_t i0, j0, m, n, r;
+  View A, B;  // A: m x r, B: r x n
+};
+
+// Where the columns of one segment come from and where its data lives.
+struct Segment {
+  int kind;        // 0: FR slice, 1: LR A slice, 2: LR B rows
+  int64_t block;   // block index
+  int64_t row0;    // first row of the block (or of B) in this item
+  int64_t ncols;   // columns
+  int src;         // 0: x, 1: t
+  int64_t src_off; // offset in x or t
+};
+
+struct Item {
+  int64_t data_off;   // element offset in the phase's data array
+  int32_t h, hpad;    // rows, padded rows
+  int64_t ncols;      // total columns
+  int32_t out_off;
+  std::vector<Segment> segs;
+};
+
+// Per precision: chunk list ordered by CTA, and the CTA ranges.
+struct ChunkPlan {
+  std::vector<Chunk> chunks;
+  std::vector<int32_t> cta_ptr;  // grid + 1
+};
+
+struct PhasePlan {
+  std::vector<Item> items;
+  int64_t n_elems = 0;  // size of the data array in elements
+  ChunkPlan cp[3];      // FP64, FP32, BF16
+};
+
+struct OperatorPlan {
+  int64_t n_out = 0, n_in = 0;  // rows of the operator, columns
+  int64_t t_len = 0;            // sum of ranks
+  std::vector<int64_t> t_off;   // per LR block
+  std::vector<float> scale_fr;  // BF16 scales per FR block
+  std::vector<float> scale_a, scale_b;  // BF16 scales per LR block
+  PhasePlan ph[2];
+  int64_t n_panels = 0;
+};
+
+struct Problem {
+  int dof = 1;
+  int64_t n_rows = 0, n_cols = 0;
+  std::vector<FullBlock> fr;
+  std::vector<LowRankBlock> lr;
+};
+
+// Validates the pattern and builds the structural plan (items) of the operator
+// (transposed = true builds H^T from the same blocks).  Throws std::runtime_error
+// with a message on a malformed pattern.
+void build_operator(const Problem &p, bool transposed, OperatorPlan &op);
+
+// Computes BF16 per-block scales (max |entry|, 1 if the block is zero), and
+// checks that every entry is finite when check_finite is set.
+void compute_scales(const Problem &p, bool transposed, bool check_finite, OperatorPlan &op);
+
+// Splits every item into chunks for one precision (0 FP64, 1 FP32, 2 BF16) and
+// assigns items to `grid` CTAs (longest-processing-time first, cost = bytes).
+void build_chunks(const Problem &p, bool transposed, int prec, int grid, OperatorPlan &op);
+
+// Writes the data of items [i_begin, i_end) of one phase, converted to the
+// precision, into dst (dst[0] is element `base` of the phase's array).
+void fill_items(const Problem &p, bool transposed, const OperatorPlan &op, int phase, int prec, int64_t i_begin,
+                int64_t i_end, int64_t base, void *dst);
+
+int esize_of(int prec);
+uint16_t to_bf16(float f);
+float from_bf16(uint16_t b);
+
+}  // namespace bw

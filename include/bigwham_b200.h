@@ -1,0 +1,175 @@
+/* bigwham_b200 -- B200 (sm_100a) H-matrix x vector backend, C ABI.
+ *
+ * Drop-in boundary for BigWham's H-matrix matvec.  The reference keeps
+ * building the H-matrix on the host (mesh, kernel, cluster tree,
+ * admissibility, ACA); its full-rank blocks and low-rank blocks are handed to
+ * this library once, which re-lays them out in device memory and applies the
+ * operator with hand-written CUDA kernels.
+ *
+ * Units: rows/columns are SCALAR indices (collocation point * dof + component),
+ * i.e. the reference's HPattern entries multiplied by the dof dimension
+ * (src/hmat/hmatrix/h_pattern.h:21-33).  Blocks are column-major with a
+ * leading dimension, as il::Array2D stores them (il/il/container/2d/Array2D.h:840).
+ *
+ * Every entry point returns an int status (BW_OK == 0) and never exits the
+ * process; bw_last_error() gives the message.  Calls on one handle must be
+ * ordered on one CUDA stream (they share the handle's scratch vectors).
+ */
+#ifndef BIGWHAM_B200_H
+#define BIGWHAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bw_hmat bw_hmat;
+
+/* status codes */
+enum {
+  BW_OK = 0,
+  BW_ERR_ARG = 1,         /* bad argument, malformed pattern, non-finite block entry */
+  BW_ERR_STATE = 2,       /* call not valid in the handle's state (e.g. matvec before finalize) */
+  BW_ERR_OOM = 3,         /* device or host allocation failed, or above the configured limit */
+  BW_ERR_CUDA = 4,        /* a CUDA runtime call failed */
+  BW_ERR_DEVICE = 5,      /* a kernel reported an error word (e.g. a bounded wait ran out) */
+  BW_ERR_UNSUPPORTED = 6  /* precision or operation not stored / not available */
+};
+
+/* storage / precision flags */
+enum {
+  BW_FP64 = 1,            /* FP64 blocks, FP64 accumulation */
+  BW_FP32 = 2,            /* FP32 blocks, FP32 accumulation */
+  BW_BF16 = 4,            /* BF16 blocks with a per-block FP32 scale, FP32 accumulation */
+  BW_STORE_TRANSPOSE = 16,/* bw_finalize: also lay out H^T for bw_matvec(..., BW_TRANSPOSE) */
+  BW_NO_FINITE_CHECK = 32,/* bw_finalize: skip the non-finite entry check */
+  BW_PLAN_ONLY = 64       /* bw_finalize: build the host plan only (no device); for inspection */
+};
+
+/* matvec flags (OR with exactly one of BW_FP64 / BW_FP32 / BW_BF16) */
+enum {
+  BW_PERMUTED = 256,      /* x and y are in the clustered (permuted) ordering:
+                             Hmat::matvec instead of Hmat::matvecOriginal */
+  BW_TRANSPOSE = 512      /* apply H^T instead of H */
+};
+
+/* Create an empty handle.
+ * dof: dofs per collocation point; n_rows, n_cols: scalar sizes (Hmat::size(0/1),
+ * src/hmat/hmatrix/hmat.h:80); perm0 (n_rows/dof) and perm1 (n_cols/dof): the
+ * row / column permutations (HRepresentation::permutation_0_/_1_,
+ * src/hmat/hierarchical_representation.h:28-29), copied.
+ * device: CUDA device ordinal, or -1 for a host-only plan (BW_PLAN_ONLY).
+ * Replaces: the HmatCuda constructor's upload set-up
+ * (src/hmat/hmatrix/hmat_cuda.cc:98-329). */
+int bw_create(int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0, const int64_t *perm1, int device,
+              bw_hmat **out);
+
+/* Register a full-rank block: rows [i0, i0+m), cols [j0, j0+n), column-major
+ * with leading dimension lda >= m.  The pointer is BORROWED until bw_finalize
+ * returns (no copy is made before then).
+ * Replaces: the FR half of HmatCuda::copyToDevice (hmat_cuda.cc:331-1183). */
+int bw_add_full(bw_hmat *h, int64_t i0, int64_t j0, int64_t m, int64_t n, const double *a, int64_t lda);
+
+/* Register a low-rank block y[i0:i0+m] += A (B x[j0:j0+n]) with A m x r
+ * (lda >= m) and B r x n (ldb >= r), both column-major, exactly as
+ * bigwham::LowRank stores them (src/hmat/hmatrix/LowRank.h:18-24,
+ * hmat.cc:524-526).  r may differ block to block.  Pointers are BORROWED until
+ * bw_finalize returns.  Replaces: the LR half of HmatCuda::copyToDevice. */
+int bw_add_lowrank(bw_hmat *h, int64_t i0, int64_t j0, int64_t m, int64_t n, int64_t r, const double *A,
+                   int64_t lda, const double *B, int64_t ldb);
+
+/* Validate the pattern (in range, no overlaps, every row/column covered),
+ * build the device layout for the precisions in `flags` (BW_FP64 | BW_FP32 |
+ * BW_BF16, optionally BW_STORE_TRANSPOSE, BW_NO_FINITE_CHECK, BW_PLAN_ONLY)
+ * and upload it.  Synchronous.  After it returns the borrowed block pointers
+ * are no longer used. */
+int bw_finalize(bw_hmat *h, int flags);
+
+/* y = H x (or H^T x with BW_TRANSPOSE) on DEVICE pointers, stream-ordered on
+ * `stream` (a cudaStream_t; 0 is the legacy default stream).  Original dof
+ * ordering unless BW_PERMUTED.  x and y must not overlap.  Does not
+ * synchronize.
+ * Replaces: Hmat<double>::matvecOriginal(double*, double*) / matvec(double*,
+ * double*) (src/hmat/hmatrix/hmat.h:91,95; HmatCuda overrides at
+ * hmat_cuda.cc:2397-2460), reached from BigWhamIO::MatVec(double*, double*)
+ * (src/io/bigwham_io.cc:935-941) and py_bigwham matvec_raw_ptr
+ * (interfaces/python/py_bigwham.cc:213-222). */
+int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream);
+
+/* Same product on HOST arrays: copies x to the device, runs bw_matvec on the
+ * handle's stream, copies y back and synchronizes.
+ * Replaces: Hmat<double>::matvecOriginal(il::ArrayView<double>) / matvec(...)
+ * (hmat.cc:572-635 / :472-537), reached from BigWhamIO::MatVec(il::ArrayView)
+ * (bigwham_io.cc:927-933) and MatVecPerm (bigwham_io.cc:965-980). */
+int bw_matvec_host(bw_hmat *h, const double *x, double *y, int flags);
+
+/* Y = H X for nrhs right-hand sides on DEVICE pointers; X is n_cols x nrhs
+ * (column stride ldx), Y is n_rows x nrhs (column stride ldy), FP64.
+ * No reference counterpart. */
+int bw_matmat(bw_hmat *h, const double *X, int64_t ldx, double *Y, int64_t ldy, int nrhs, int flags,
+              void *stream);
+
+/* Diagonal of H into a HOST array of length max(n_rows, n_cols), original
+ * ordering unless BW_PERMUTED.  Replaces: Hmat::diagonalOriginal / diagonal
+ * (hmat.cc:240-285) and HmatCuda::setDiagonal (hmat_cuda.cc:2462-2493). */
+int bw_diagonal(bw_hmat *h, double *d, int flags);
+
+/* Wait for the handle's pending work on `stream` and read the device error
+ * word; BW_ERR_DEVICE if a kernel reported one (the word is then cleared). */
+int bw_sync(bw_hmat *h, void *stream);
+
+/* Sizes and statistics.  Fills up to n values of:
+ * [0] n_rows [1] n_cols [2] dof [3] n_full [4] n_lowrank [5] stored entries
+ * (Hmat::nbOfEntries, hmat.cc:299-313) [6] sum of ranks [7] n row panels
+ * [8] device bytes in use [9] grid CTAs [10] phase-1 chunks (FP64)
+ * [11] phase-2 chunks (FP64) [12] stored precisions mask.  Returns BW_OK. */
+int bw_info(const bw_hmat *h, int64_t *out, int n);
+
+/* Algorithmic bytes of one matvec in the given precision: stored entries x
+ * element size (+ the BF16 per-block scales) + 8 bytes per input and per output
+ * scalar.  Fills *bytes. */
+int bw_algorithmic_bytes(const bw_hmat *h, int precision, int64_t *bytes);
+
+/* Last error message of the handle (or of the last failed bw_create when h is
+ * NULL), NUL-terminated into buf. */
+int bw_last_error(const bw_hmat *h, char *buf, size_t len);
+
+/* Cap on the device bytes bw_finalize may allocate (0 = no cap).  Exceeding it
+ * makes bw_finalize return BW_ERR_OOM before allocating. */
+int bw_set_device_limit(bw_hmat *h, int64_t bytes);
+
+/* Host view of the built plan for one precision and phase (1: low-rank B
+ * stage, 2: row panels), for inspection and testing.  Any output pointer may be
+ * NULL; counts are always written.  chunks: n_chunks x 16 int32 words in the
+ * layout documented in bw_layout.h; data: n_elems values converted to double
+ * (BF16 values times nothing: the per-chunk scale is in the chunk words);
+ * cta_ptr: grid+1 offsets.  Only valid on a handle finalized with BW_PLAN_ONLY. */
+int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_chunks,
+                   int32_t *chunks, int64_t *n_elems, double *data, int64_t *n_cta, int32_t *cta_ptr);
+
+/* Per-launch timing for benchmarks.  With timing enabled every bw_matvec
+ * records CUDA events on its stream around its three launches (x gather,
+ * phase 1, phase 2).  bw_timing_read waits for the last recorded event, writes
+ * the summed durations in milliseconds of the three launch kinds into ms[0..2]
+ * and the number of recorded matvecs, and clears the record. */
+int bw_set_timing(bw_hmat *h, int enable);
+int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs);
+
+/* Algorithmic bytes of each streaming launch of one matvec: phase 1 reads the
+ * low-rank B factors (+ x, + t written), phase 2 reads the full blocks and the
+ * A factors (+ y written).  Stored entries only: padding is not counted. */
+int bw_phase_bytes(const bw_hmat *h, int precision, int transposed, int64_t *phase1, int64_t *phase2);
+
+/* Release everything. */
+int bw_destroy(bw_hmat *h);
+
+/* Library version string. */
+const char *bw_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BIGWHAM_B200_H */

@@ -1,0 +1,87 @@
+/* bigwham_host -- C ABI of BigWhamIO with the B200 backend installed.
+ *
+ * libbigwham_host.so contains the reference's own, unmodified host code
+ * (mesh, elastic kernels, cluster tree, admissibility, ACA; compiled from its
+ * sources) plus the HmatGpu adapter (bigwham_dev_b200/host/hmat_gpu.h).  These
+ * entry points mirror the methods the reference's pybind11 module exposes on
+ * BigWhamIOSelf (interfaces/python/py_bigwham.cc:141-260) for the matvec path,
+ * so a ctypes / cgo / JNI caller can drive the whole flow without C++.
+ *
+ * All functions return 0 on success; on failure a non-zero status and the
+ * message from bwh_last_error().
+ */
+#ifndef BIGWHAM_HOST_H
+#define BIGWHAM_HOST_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bwh_io bwh_io;
+struct bw_hmat;
+
+/* BigWhamIO(coor, conn, kernel, properties, n_openMP_threads, n_GPUs, verbose,
+ * homogeneous_size_pattern, useCuda = false, fixed_rank)
+ * (src/io/bigwham_io.h:73-82; py_bigwham.cc:144). */
+int bwh_create(const double *coor, int64_t n_coor, const int *conn, int64_t n_conn, const char *kernel,
+               const double *properties, int n_properties, int n_openmp_threads, int verbose, int fixed_rank,
+               bwh_io **out);
+
+/* BigWhamIO::BuildHierarchicalMatrix (bigwham_io.cc:635-704), host build. */
+int bwh_build(bwh_io *io, int max_leaf_size, double eta, double eps_aca);
+
+/* Upload the built H-matrix to `device` in the precisions of `storage`
+ * (BW_FP64 | BW_FP32 | BW_BF16 [| BW_STORE_TRANSPOSE]) and install it with
+ * BigWhamIO::setHmat (bigwham_io.h:206).  After this call every matvec below
+ * runs on the GPU.  release_host: drop the reference's host copy of the
+ * low-rank factors (the GPU keeps its own). */
+int bwh_attach_gpu(bwh_io *io, int device, int storage, int release_host);
+
+/* Precision of the reference-facing matvec calls (one of BW_FP64, BW_FP32, BW_BF16). */
+int bwh_set_precision(bwh_io *io, int precision);
+
+/* BigWhamIO::MatVec(il::ArrayView) -- host arrays, original ordering. */
+int bwh_matvec(bwh_io *io, const double *x, double *y);
+/* BigWhamIO::MatVecPerm -- host arrays, permuted ordering. */
+int bwh_matvec_perm(bwh_io *io, const double *x, double *y);
+/* BigWhamIO::MatVec(double*, double*) -- device pointers (matvec_raw_ptr). */
+int bwh_matvec_raw_ptr(bwh_io *io, double *x, double *y);
+/* BigWhamIO::GetDiagonal (original ordering). */
+int bwh_diagonal(bwh_io *io, double *d);
+
+int64_t bwh_size(const bwh_io *io, int k);
+int bwh_dof(const bwh_io *io);
+double bwh_compression(const bwh_io *io);
+double bwh_hmat_time(const bwh_io *io);
+/* GetPermutation (bigwham_io.cc): n_points int64 values. */
+int bwh_permutation(const bwh_io *io, int64_t *perm);
+/* GetCollocationPoints: returns the count; fills `out` when non-null. */
+int64_t bwh_collocation_points(const bwh_io *io, double *out);
+/* GetHPattern: 6 doubles per block; returns the count; fills `out` when non-null. */
+int64_t bwh_hpattern(const bwh_io *io, double *out);
+/* Block counts of the pattern: kind 0 full rank, 1 low rank. */
+int64_t bwh_n_blocks(const bwh_io *io, int kind);
+
+/* Stored entries of the FR blocks (kind 0) or of the LR factors A and B (kind 1). */
+int64_t bwh_entries(const bwh_io *io, int kind);
+/* Copy the built H-matrix out, before bwh_attach_gpu: fr (n_FR x 4: i0, j0,
+ * iend, jend in points), lr (n_LR x 5: ..., r), the FR blocks back to back and
+ * per LR block A then B (column-major), and both permutations.  This is the
+ * flat form bw_add_* accept and the form of the benchmark's block cache. */
+int bwh_export(const bwh_io *io, int64_t *fr, int64_t *lr, double *fr_data, double *lr_data, int64_t *perm0,
+               int64_t *perm1);
+
+/* The device H-matrix after bwh_attach_gpu (owned by io), for the
+ * extensions of include/bigwham_b200.h (precision choice, H^T, matmat). */
+struct bw_hmat *bwh_gpu_handle(bwh_io *io);
+
+int bwh_destroy(bwh_io *io);
+const char *bwh_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BIGWHAM_HOST_H */

@@ -1,0 +1,157 @@
+// Oracle-side C entry points over the UNMODIFIED reference library.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is linked, together with the reference
+// sources compiled by oracle/Makefile, into oracle/_ref/libbigwham_ref.so.  Only
+// the test suite, the smoke check and the CPU-baseline leg of the benchmark may
+// load that library.  It exposes the reference's own construction
+// (BigWhamIO ctor + BuildHierarchicalMatrix, src/io/bigwham_io.cc:41-290 and
+// :635-704) and the reference's own OpenMP CPU matvec
+// (BigWhamIO::MatVec -> Hmat<double>::matvecOriginal, src/io/bigwham_io.cc:927-933,
+// src/hmat/hmatrix/hmat.cc:572-635) to Python through ctypes, plus read access
+// to the built blocks so golden vectors can be dumped.
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "cblas.h"
+#include "io/bigwham_io.h"
+
+#ifdef BIGWHAM_OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+struct RefHandle {
+  std::unique_ptr<BigWhamIO> io;
+};
+RefHandle *H(void *h) { return static_cast<RefHandle *>(h); }
+}  // namespace
+
+extern "C" {
+
+// Sets the OpenMP thread count used by the reference and pins the BLAS to one
+// thread, as the reference expects (the parallelism is over blocks).
+int ref_set_threads(int n) {
+  openblas_set_num_threads(1);
+#ifdef BIGWHAM_OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+// Square self-interaction BigWhamIO (src/io/bigwham_io.h:73-82); CUDA off.
+void *ref_create(const double *coor, int64_t n_coor, const int *conn, int64_t n_conn, const char *kernel,
+                 const double *props, int n_props, int n_threads, int verbose) {
+  try {
+    std::vector<double> c(coor, coor + n_coor);
+    std::vector<int> e(conn, conn + n_conn);
+    std::vector<double> p(props, props + n_props);
+    auto *h = new RefHandle;
+    h->io.reset(new BigWhamIO(c, e, std::string(kernel), p, n_threads, 0, verbose != 0, false, false, -1));
+    return h;
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+int ref_build(void *h, int leaf, double eta, double eps) {
+  try {
+    H(h)->io->BuildHierarchicalMatrix(leaf, eta, eps);
+    return H(h)->io->is_built() ? 0 : 2;
+  } catch (...) {
+    return 1;
+  }
+}
+
+int64_t ref_size(void *h, int k) { return H(h)->io->getHmat()->size(k); }
+int ref_dof(void *h) { return H(h)->io->dof_dimension(); }
+double ref_compression(void *h) { return H(h)->io->GetCompressionRatio(); }
+
+int64_t ref_n_blocks(void *h, int kind) {
+  auto p = H(h)->io->getHmat()->pattern();
+  return kind == 0 ? p.n_FRB : p.n_LRB;
+}
+
+// FR: 4 int64 per block (i0, j0, iend, jend) in collocation-point units.
+// LR: 5 int64 per block (i0, j0, iend, jend, rank in scalar columns), h_pattern.h:21-33, hmat.cc:390.
+int ref_pattern(void *h, int64_t *fr, int64_t *lr) {
+  auto p = H(h)->io->getHmat()->pattern();
+  for (il::int_t k = 0; k < p.n_FRB; k++)
+    for (int r = 0; r < 4; r++) fr[4 * k + r] = p.FRB_pattern(r + 1, k);
+  for (il::int_t k = 0; k < p.n_LRB; k++)
+    for (int r = 0; r < 5; r++) lr[5 * k + r] = p.LRB_pattern(r + 1, k);
+  return 0;
+}
+
+int ref_permutation(void *h, int64_t *p0, int64_t *p1) {
+  auto hr = H(h)->io->getHmat()->get_hr();
+  for (il::int_t i = 0; i < hr->permutation_0_.size(); i++) p0[i] = hr->permutation_0_[i];
+  for (il::int_t i = 0; i < hr->permutation_1_.size(); i++) p1[i] = hr->permutation_1_[i];
+  return 0;
+}
+
+static void copy_colmajor(const il::Array2D<double> &a, double *out) {
+  auto v = a.view();
+  const il::int_t m = v.size(0), n = v.size(1);
+  for (il::int_t j = 0; j < n; j++)
+    for (il::int_t i = 0; i < m; i++) out[i + j * m] = v(i, j);
+}
+
+// Full-rank block k, column-major m x n (scalar units).
+int ref_fr_block(void *h, int64_t k, double *out) {
+  const auto &fr = H(h)->io->getHmat()->get_full_rank_blocks();
+  if (k < 0 || k >= (int64_t)fr.size()) return 1;
+  copy_colmajor(*fr[k], out);
+  return 0;
+}
+
+// Low-rank block k: A (m x r) and B (r x n), both column-major (LowRank.h:18-24).
+int ref_lr_block(void *h, int64_t k, double *A, double *B) {
+  const auto &lr = H(h)->io->getHmat()->get_low_rank_blocks();
+  if (k < 0 || k >= (int64_t)lr.size()) return 1;
+  copy_colmajor(lr[k]->A, A);
+  copy_colmajor(lr[k]->B, B);
+  return 0;
+}
+
+// BigWhamIO::MatVec in the original dof ordering (bigwham_io.cc:927-933).
+int ref_matvec(void *h, const double *x, double *y) {
+  const int64_t n = H(h)->io->getHmat()->size(1);
+  il::ArrayView<double> xv{x, n};
+  il::Array<double> out = H(h)->io->MatVec(xv);
+  std::memcpy(y, out.data(), sizeof(double) * out.size());
+  return 0;
+}
+
+// BigWhamIO::MatVecPerm in the permuted ordering (bigwham_io.cc:965-980).
+int ref_matvec_perm(void *h, const double *x, double *y) {
+  const int64_t n = H(h)->io->getHmat()->size(1);
+  il::ArrayView<double> xv{x, n};
+  il::Array<double> out = H(h)->io->MatVecPerm(xv);
+  std::memcpy(y, out.data(), sizeof(double) * out.size());
+  return 0;
+}
+
+// BigWhamIO::GetDiagonal, original ordering (bigwham_io.cc:909-916).
+int ref_diagonal(void *h, double *d) {
+  std::vector<double> v;
+  H(h)->io->GetDiagonal(v);
+  std::memcpy(d, v.data(), sizeof(double) * v.size());
+  return 0;
+}
+
+// Collocation points, flattened row-major (n_points x spatial_dim).
+int64_t ref_collocation_points(void *h, double *out) {
+  std::vector<double> v = H(h)->io->GetCollocationPoints();
+  if (out) std::memcpy(out, v.data(), sizeof(double) * v.size());
+  return (int64_t)v.size();
+}
+
+void ref_destroy(void *h) { delete H(h); }
+
+}  // extern "C"

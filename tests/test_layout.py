@@ -1,0 +1,155 @@
+"""Host logic of the CUDA backend, on CPU: the plan (row panels, chunks, LPT
+schedule) built by bw_finalize(BW_PLAN_ONLY) is replayed in numpy exactly as
+the kernel walks it, and must reproduce the oracle; malformed inputs are
+rejected with the documented status codes."""
+import numpy as np
+import pytest
+from conftest import rel
+from planreplay import decode, replay
+
+from bigwham_dev_b200 import BigWhamError, HmatGpu
+from bigwham_dev_b200 import _capi as A
+from oracle import oracle_matvec_perm, oracle_rmatvec_perm
+
+
+def plan(arr, **kw):
+    h = HmatGpu(arr.dof, arr.n_rows, arr.n_cols, arr.perm0, arr.perm1, device=-1)
+    h.add_flat(arr.fr, arr.lr, arr.fr_data, arr.lr_data)
+    return h.finalize(plan_only=True, **kw)
+
+
+def test_plan_replay_fp64_forward_and_transpose(golden):
+    arr, ex = golden
+    h = plan(arr, precisions=("fp64",), transpose=True)
+    xp = np.random.default_rng(3).uniform(-1, 1, arr.n_cols)
+    assert rel(replay(h, xp, "fp64"), oracle_matvec_perm(arr, xp, 1)) < 1e-14
+    xr = np.random.default_rng(4).uniform(-1, 1, arr.n_rows)
+    assert rel(replay(h, xr, "fp64", transposed=True), oracle_rmatvec_perm(arr, xr, 1)) < 1e-14
+
+
+@pytest.mark.parametrize("prec,tol", [("fp32", 2e-6), ("bf16", 8e-3)])
+def test_plan_replay_reduced_precision(golden, prec, tol):
+    arr, ex = golden
+    h = plan(arr, precisions=(prec,))
+    xp = np.random.default_rng(3).uniform(-1, 1, arr.n_cols)
+    y = replay(h, xp.astype(np.float32).astype(np.float64), prec)
+    assert rel(y, oracle_matvec_perm(arr, xp, 1)) < tol
+
+
+def test_plan_structure(golden):
+    arr, ex = golden
+    h = plan(arr, precisions=("fp64", "fp32", "bf16"))
+    info = h.info()
+    assert info["entries"] == arr.fr_data.size + arr.lr_data.size
+    assert info["sum_rank"] == int(arr.lr[:, 4].sum())
+    for prec, es in (("fp64", 8), ("fp32", 4), ("bf16", 2)):
+        for phase in (1, 2):
+            p = h.plan_export(prec, phase, with_data=False)
+            cta = p["cta_ptr"]
+            assert cta[0] == 0 and np.all(np.diff(cta) >= 0) and cta[-1] == len(p["chunks"])
+            seen_first = 0
+            for w in p["chunks"]:
+                d = decode(w)
+                assert d["hpad"] % 2 == 0 and d["rows"] <= d["hpad"] <= 512
+                assert d["ncols"] * d["hpad"] * es <= 32768 and d["ncols"] <= 512
+                assert sum(n for _, n, _ in d["segs"]) == d["ncols"]
+                assert (d["data_off"] * es) % 4 == 0
+                seen_first += d["flags"] & 1
+            # one first chunk per item
+            assert seen_first == (info["n_lowrank"] if phase == 1 else info["n_panels"]) or phase == 1
+
+
+def test_lpt_balance_on_many_items():
+    # 400 equal full blocks on a 20 x 20 block grid: 20 panels of equal cost
+    dof, nb, bs = 1, 20, 24
+    n = nb * bs
+    rng = np.random.default_rng(0)
+    h = HmatGpu(dof, n, n, np.arange(n), np.arange(n), device=-1)
+    blocks = {}
+    for i in range(nb):
+        for j in range(nb):
+            blocks[i, j] = rng.standard_normal((bs, bs))
+            h.add_full(i * bs, j * bs, blocks[i, j])
+    h.finalize(plan_only=True)
+    p = h.plan_export("fp64", 2)
+    per_cta = np.diff(p["cta_ptr"])
+    assert per_cta.max() - per_cta[per_cta > 0].min() <= 2
+    D = np.block([[blocks[i, j] for j in range(nb)] for i in range(nb)])
+    x = rng.standard_normal(n)
+    assert rel(replay(h, x), D @ x) < 1e-14
+
+
+def _simple(n=8):
+    return HmatGpu(1, n, n, np.arange(n), np.arange(n), device=-1)
+
+
+def test_rejects_overlap():
+    h = _simple()
+    h.add_full(0, 0, np.ones((8, 8)))
+    h.add_full(0, 4, np.ones((4, 4)))
+    with pytest.raises(BigWhamError, match="overlap"):
+        h.finalize(plan_only=True)
+
+
+def test_rejects_gap():
+    h = _simple()
+    h.add_full(0, 0, np.ones((8, 4)))
+    with pytest.raises(BigWhamError, match="not covered"):
+        h.finalize(plan_only=True)
+
+
+def test_rejects_out_of_range():
+    h = _simple()
+    with pytest.raises(BigWhamError):
+        h.add_full(4, 4, np.ones((8, 8)))
+        h.finalize(plan_only=True)
+
+
+def test_rejects_nonfinite_and_allows_opt_out():
+    a = np.ones((8, 8))
+    a[3, 5] = np.nan
+    h = _simple()
+    h.add_full(0, 0, a)
+    with pytest.raises(BigWhamError, match="non-finite") as e:
+        h.finalize(plan_only=True)
+    assert e.value.status == A.BW_ERR_ARG
+    h = _simple()
+    h.add_full(0, 0, a)
+    h.finalize(plan_only=True, check_finite=False)
+
+
+def test_rejects_bad_permutation_and_sizes():
+    with pytest.raises(BigWhamError):
+        HmatGpu(1, 4, 4, [0, 1, 1, 3], [0, 1, 2, 3], device=-1)
+    with pytest.raises(BigWhamError):
+        HmatGpu(3, 10, 9, np.arange(3), np.arange(3), device=-1)
+
+
+def test_lowrank_shapes_checked():
+    h = _simple()
+    with pytest.raises(ValueError):
+        h.add_lowrank(0, 0, np.ones((8, 2)), np.ones((3, 8)))
+
+
+def test_matvec_on_plan_only_handle_is_a_state_error(golden):
+    arr, ex = golden
+    h = plan(arr)
+    with pytest.raises(BigWhamError) as e:
+        h.matvec(np.zeros(arr.n_cols))
+    assert e.value.status == A.BW_ERR_STATE
+
+
+def test_tall_panels_and_high_rank_are_split():
+    # a 1-block-row matrix taller than 512 rows and a rank-600 low-rank block
+    rng = np.random.default_rng(1)
+    n = 1300
+    h = HmatGpu(1, n, n, np.arange(n), np.arange(n), device=-1)
+    F = rng.standard_normal((n, 700))
+    Al, Bl = rng.standard_normal((n, 600)), rng.standard_normal((600, 600))
+    h.add_full(0, 0, F)
+    h.add_lowrank(0, 700, Al, Bl)
+    h.finalize(plan_only=True, precisions=("fp64",), transpose=True)
+    x = rng.standard_normal(n)
+    D = np.concatenate([F, Al @ Bl], axis=1)
+    assert rel(replay(h, x), D @ x) < 1e-13
+    assert rel(replay(h, x, transposed=True), D.T @ x) < 1e-13
