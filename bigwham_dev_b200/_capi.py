@@ -32,6 +32,7 @@ _SIGS = {
     "bw_finalize": (C.c_int, [_P, C.c_int]),
     "bw_matvec": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "bw_matvec_host": (C.c_int, [_P, _P, _P, C.c_int]),
+    "bw_matvec_static_scratch": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "bw_matmat": (C.c_int, [_P, _P, _I64, _P, _I64, C.c_int, C.c_int, _P]),
     "bw_diagonal": (C.c_int, [_P, _P, C.c_int]),
     "bw_sync": (C.c_int, [_P, _P]),

@@ -310,6 +310,76 @@ void launch_matvec(bw_hmat *h, int o, int prec, const double *x, double *y, bool
   }
 }
 
+// ----------------------------------------------------------------------------
+// Static scratch for bw_matvec_static_scratch.
+//
+// Some callers cannot let a library allocate device memory: a host process
+// whose device memory is owned by another allocator (a framework's caching
+// pool, or a solver that reserved the whole card up front), and code on a
+// latency-critical path where cudaMalloc / cudaFree are not allowed because
+// they can synchronize the whole device.  For them this entry point keeps its
+// scratch vectors (the gathered input and the low-rank intermediates t) in a
+// fixed array that is part of the library image: BW_STATIC_SCRATCH_BYTES of
+// device memory on every GPU that loads the library, held until the process
+// exits.  All calls on a device share the one array, so calls whose kernels
+// overlap on the GPU (several streams, several handles) race on it.
+static __device__ __align__(256) unsigned char bw_static_scratch[BW_STATIC_SCRATCH_BYTES];
+
+// Device address of bw_static_scratch, looked up once per device with that
+// device current (the host-side name is only a stand-in for the symbol).
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_mu;
+void *g_static_ptr[kMaxStaticDevices] = {};
+
+void *static_scratch_ptr(int device) {
+  if (device < 0 || device >= kMaxStaticDevices) throw UnsupportedError("device ordinal too large for the static scratch");
+  std::lock_guard<std::mutex> g(g_static_mu);
+  if (!g_static_ptr[device]) {
+    void *p = nullptr;
+    BW_CUDA(cudaGetSymbolAddress(&p, bw_static_scratch));
+    g_static_ptr[device] = p;
+  }
+  return g_static_ptr[device];
+}
+
+// The three launches of one matvec with caller-provided scratch pointers
+// (same kernels and arguments as launch_matvec).
+template <typename S>
+void launch_matvec_on(bw_hmat *h, int o, int prec, const double *x, double *y, bool permuted, cudaStream_t st,
+                      void *xp_buf, void *t_buf) {
+  using G = typename bw::Store<S>::G;
+  const bw::OperatorPlan &op = h->op[o];
+  const int32_t *perm_in = permuted ? nullptr : (o == 0 ? h->d_perm1 : h->d_perm0);
+  const int32_t *perm_out = permuted ? nullptr : (o == 0 ? h->d_perm0 : h->d_perm1);
+  const int n_in = (int)op.n_in;
+  G *xp = static_cast<G *>(xp_buf);
+  G *t = static_cast<G *>(t_buf);
+  if (n_in > 0) {
+    bw::gather_x_kernel<G><<<(n_in + 255) / 256, 256, 0, st>>>(x, xp, perm_in, h->dof, n_in);
+    BW_CUDA(cudaGetLastError());
+  }
+  set_smem_attr<S>();
+  for (int phase = 0; phase < 2; phase++) {
+    const DevPhase &dp = h->dev[o][prec][phase];
+    if (dp.n_chunks == 0) continue;
+    bw::StreamArgs a{};
+    a.data = dp.data;
+    a.chunks = dp.chunks;
+    a.cta_ptr = dp.cta;
+    a.xsrc = xp;
+    a.tsrc = t;
+    a.t_out = t;
+    a.y_out = y;
+    a.perm_out = perm_out;
+    a.dof = h->dof;
+    a.phase = phase + 1;
+    a.err = h->d_err;
+    a.spin_limit = h->spin_limit;
+    bw::stream_panels_kernel<S><<<h->grid, bw::kThreads, bw::SmemLayout<S>::kTotal, st>>>(a);
+    BW_CUDA(cudaGetLastError());
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -502,6 +572,46 @@ int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream) {
       launch_matvec<float>(h, o, 1, x, y, perm, st);
     else
       launch_matvec<bw::Bf16>(h, o, 2, x, y, perm, st);
+    return BW_OK;
+  });
+}
+
+int bw_matvec_static_scratch(bw_hmat *h, const double *x, double *y, int flags, void *stream) {
+  if (!h) return BW_ERR_ARG;
+  return guarded(h, [&] {
+    if (!h->finalized) throw StateError("bw_matvec_static_scratch before bw_finalize");
+    if (h->plan_only) throw StateError("handle was finalized with BW_PLAN_ONLY (no device data)");
+    const int p = prec_index(flags);
+    if (p < 0) throw std::invalid_argument("flags must name exactly one of BW_FP64, BW_FP32, BW_BF16");
+    if (!(h->stored & (1 << p))) throw UnsupportedError("precision not stored by bw_finalize");
+    const bool tr = (flags & BW_TRANSPOSE) != 0;
+    if (tr && !h->has_t) throw UnsupportedError("transposed layout not stored (finalize with BW_STORE_TRANSPOSE)");
+    const int64_t nin = tr ? h->n_rows : h->n_cols, nout = tr ? h->n_cols : h->n_rows;
+    if ((nin && !x) || (nout && !y)) throw std::invalid_argument("null vector");
+    if (x && y) {
+      const char *xb = reinterpret_cast<const char *>(x), *yb = reinterpret_cast<const char *>(y);
+      if (xb < yb + nout * 8 && yb < xb + nin * 8) throw std::invalid_argument("x and y overlap");
+    }
+    // scratch: gathered x, then t at the next 256-byte boundary
+    const int64_t gsize = p == 0 ? 8 : 4;
+    const int64_t t_at = (nin * gsize + 255) / 256 * 256;
+    const int64_t need = t_at + h->sum_rank * gsize;
+    if (need > (int64_t)BW_STATIC_SCRATCH_BYTES)
+      throw std::invalid_argument("this H-matrix needs " + std::to_string(need) +
+                                  " bytes of scratch, above the static maximum of " +
+                                  std::to_string((long long)BW_STATIC_SCRATCH_BYTES) +
+                                  " bytes; use bw_matvec instead");
+    BW_CUDA(cudaSetDevice(h->device));
+    unsigned char *base = static_cast<unsigned char *>(static_scratch_ptr(h->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const bool perm = (flags & BW_PERMUTED) != 0;
+    const int o = tr ? 1 : 0;
+    if (p == 0)
+      launch_matvec_on<double>(h, o, 0, x, y, perm, st, base, base + t_at);
+    else if (p == 1)
+      launch_matvec_on<float>(h, o, 1, x, y, perm, st, base, base + t_at);
+    else
+      launch_matvec_on<bw::Bf16>(h, o, 2, x, y, perm, st, base, base + t_at);
     return BW_OK;
   });
 }

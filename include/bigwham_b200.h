@@ -98,6 +98,27 @@ int bw_finalize(bw_hmat *h, int flags);
  * (interfaces/python/py_bigwham.cc:213-222). */
 int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream);
 
+/* Bytes of device memory reserved by bw_matvec_static_scratch (per device). */
+#define BW_STATIC_SCRATCH_BYTES (16u << 20)
+
+/* y = H x like bw_matvec, but without any device allocation, ever: for callers
+ * that cannot let a library call cudaMalloc -- a process whose device memory
+ * belongs to another allocator (a framework's caching pool, a solver that
+ * reserved the card up front), or a latency-critical path where cudaMalloc /
+ * cudaFree are not allowed because they can synchronize the device.  The
+ * caller passes x and y; the scratch vectors live in a fixed device array of
+ * BW_STATIC_SCRATCH_BYTES (16 MiB) compiled into the library, which every GPU
+ * that loads the library holds until the process exits.  H-matrices needing
+ * more scratch than that (8 or 4 bytes per input plus per low-rank rank
+ * column, e.g. ~15.3 MB for FP64 at 196,608 DoF) are rejected with BW_ERR_ARG.
+ * The first call on a device looks the array's address up (once per device);
+ * make that first call before any stream capture.  Every call overwrites the
+ * scratch before reading it, so nothing in it needs to start at zero, and the
+ * array keeps the last call's contents.  All calls on a device share the one
+ * array: calls whose kernels overlap on the GPU (several streams or several
+ * handles) race on it.  No counterpart in the reference. */
+int bw_matvec_static_scratch(bw_hmat *h, const double *x, double *y, int flags, void *stream);
+
 /* Same product on HOST arrays: copies x to the device, runs bw_matvec on the
  * handle's stream, copies y back and synchronizes.
  * Replaces: Hmat<double>::matvecOriginal(il::ArrayView<double>) / matvec(...)
