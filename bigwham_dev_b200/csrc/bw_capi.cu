@@ -74,6 +74,7 @@ struct bw_hmat {
   DevPhase dev[2][3][2];   // [operator][precision][phase]
   std::vector<unsigned char> host_data[2][3][2];  // BW_PLAN_ONLY
   int32_t *d_perm0 = nullptr, *d_perm1 = nullptr;
+  float *d_tscale[2] = {nullptr, nullptr};  // BF16 per-t-entry scales, per operator
   void *d_xp = nullptr, *d_t = nullptr;
   double *d_xh = nullptr, *d_yh = nullptr;
   int *d_err = nullptr;
@@ -129,6 +130,9 @@ struct bw_hmat {
         }
     cudaFree(d_perm0);
     cudaFree(d_perm1);
+    cudaFree(d_tscale[0]);
+    cudaFree(d_tscale[1]);
+    d_tscale[0] = d_tscale[1] = nullptr;
     cudaFree(d_xp);
     cudaFree(d_t);
     cudaFree(d_xh);
@@ -191,16 +195,16 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   const bw::PhasePlan &ph = op.ph[phase];
   const int es = bw::esize_of(prec);
   DevPhase &dp = h->dev[o][prec][phase];
-  dp.n_elems = ph.n_elems;
+  dp.n_elems = ph.n_elems[prec];
   const bw::ChunkPlan &cp = ph.cp[prec];
   dp.n_chunks = (int64_t)cp.chunks.size();
   if (h->plan_only) {
     auto &buf = h->host_data[o][prec][phase];
-    buf.assign((size_t)ph.n_elems * es, 0);
+    buf.assign((size_t)ph.n_elems[prec] * es, 0);
     bw::fill_items(h->prob, o == 1, op, phase, prec, 0, (int64_t)ph.items.size(), 0, buf.data());
     return;
   }
-  dp.data = h->dmalloc((size_t)ph.n_elems * es);
+  dp.data = h->dmalloc((size_t)ph.n_elems[prec] * es);
   dp.chunks = static_cast<Chunk *>(h->dmalloc(std::max<size_t>(1, cp.chunks.size()) * sizeof(Chunk)));
   dp.cta = static_cast<int32_t *>(h->dmalloc(cp.cta_ptr.size() * sizeof(int32_t)));
   if (!cp.chunks.empty())
@@ -217,7 +221,7 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   bool used[2] = {false, false};
   try {
     const int64_t nit = (int64_t)ph.items.size();
-    auto item_start = [&](int64_t q) { return q < nit ? ph.items[q].data_off : ph.n_elems; };
+    auto item_start = [&](int64_t q) { return q < nit ? ph.items[q].off[prec] : ph.n_elems[prec]; };
     int64_t q = 0;
     int which = 0;
     while (q < nit) {
@@ -240,7 +244,7 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
     // tail slack
     const int64_t tail0 = item_start(nit);
     BW_CUDA(cudaMemsetAsync(static_cast<unsigned char *>(dp.data) + (size_t)tail0 * es, 0,
-                            (size_t)(ph.n_elems - tail0) * es, h->stream));
+                            (size_t)(ph.n_elems[prec] - tail0) * es, h->stream));
     BW_CUDA(cudaStreamSynchronize(h->stream));
   } catch (...) {
     cudaStreamSynchronize(h->stream);
@@ -298,6 +302,7 @@ void launch_matvec(bw_hmat *h, int o, int prec, const double *x, double *y, bool
     a.xsrc = xp;
     a.tsrc = t;
     a.t_out = t;
+    a.t_scale = prec == 2 ? h->d_tscale[o] : nullptr;
     a.y_out = y;
     a.perm_out = perm_out;
     a.dof = h->dof;
@@ -369,6 +374,7 @@ void launch_matvec_on(bw_hmat *h, int o, int prec, const double *x, double *y, b
     a.xsrc = xp;
     a.tsrc = t;
     a.t_out = t;
+    a.t_scale = prec == 2 ? h->d_tscale[o] : nullptr;
     a.y_out = y;
     a.perm_out = perm_out;
     a.dof = h->dof;
@@ -503,7 +509,7 @@ int bw_finalize(bw_hmat *h, int flags) {
         for (int p = 0; p < 3; p++)
           if (mask & (1 << p))
             for (int ph = 0; ph < 2; ph++)
-              need += h->op[o].ph[ph].n_elems * bw::esize_of(p) +
+              need += h->op[o].ph[ph].n_elems[p] * bw::esize_of(p) +
                       (int64_t)h->op[o].ph[ph].cp[p].chunks.size() * (int64_t)sizeof(Chunk);
       if (h->dev_limit > 0 && need > h->dev_limit)
         throw OomError("layout needs " + std::to_string(need) + " device bytes, above the configured limit of " +
@@ -516,6 +522,12 @@ int bw_finalize(bw_hmat *h, int flags) {
       p32.assign(h->perm1.begin(), h->perm1.end());
       h->d_perm1 = static_cast<int32_t *>(h->dmalloc(std::max<size_t>(1, p32.size()) * 4));
       if (!p32.empty()) BW_CUDA(cudaMemcpy(h->d_perm1, p32.data(), p32.size() * 4, cudaMemcpyHostToDevice));
+      if (mask & BW_BF16)
+        for (int o = 0; o < (want_t ? 2 : 1); o++) {
+          const std::vector<float> &ts = h->op[o].t_scale;
+          h->d_tscale[o] = static_cast<float *>(h->dmalloc(std::max<size_t>(1, ts.size()) * 4));
+          BW_CUDA(cudaMemcpy(h->d_tscale[o], ts.data(), ts.size() * 4, cudaMemcpyHostToDevice));
+        }
       h->d_xp = h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8);
       h->d_t = h->dmalloc((size_t)std::max<int64_t>(1, h->sum_rank) * 8);
       h->d_xh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
@@ -751,14 +763,14 @@ int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, i
   const bw::PhasePlan &ph = h->op[o].ph[phase - 1];
   const bw::ChunkPlan &cp = ph.cp[p];
   if (n_chunks) *n_chunks = (int64_t)cp.chunks.size();
-  if (n_elems) *n_elems = ph.n_elems;
+  if (n_elems) *n_elems = ph.n_elems[p];
   if (n_cta) *n_cta = (int64_t)cp.cta_ptr.size();
-  if (chunks) std::memcpy(chunks, cp.chunks.data(), cp.chunks.size() * sizeof(Chunk));
+  if (chunks) std::memcpy(chunks, cp.chunks.data(), cp.chunks.size() * sizeof(Chunk));  // kChunkWords int32 each
   if (cta_ptr) std::memcpy(cta_ptr, cp.cta_ptr.data(), cp.cta_ptr.size() * sizeof(int32_t));
   if (data) {
     if (!h->plan_only) return BW_ERR_STATE;
     const auto &buf = h->host_data[o][p][phase - 1];
-    for (int64_t i = 0; i < ph.n_elems; i++) {
+    for (int64_t i = 0; i < ph.n_elems[p]; i++) {
       if (p == 0)
         data[i] = reinterpret_cast<const double *>(buf.data())[i];
       else if (p == 1)
@@ -813,6 +825,17 @@ int bw_phase_bytes(const bw_hmat *h, int precision, int transposed, int64_t *pha
   *phase1 = e[0] * es + 8 * h->op[o].n_in;
   *phase2 = e[1] * es + 8 * h->op[o].n_out;
   if (p == 2) *phase2 += 4 * ((int64_t)h->op[o].scale_fr.size() + 2 * (int64_t)h->op[o].scale_a.size());
+  return BW_OK;
+}
+
+int bw_plan_tscale(const bw_hmat *h, int transposed, int64_t *n, float *out) {
+  if (!h || !n) return BW_ERR_ARG;
+  if (!h->finalized) return BW_ERR_STATE;
+  const int o = transposed ? 1 : 0;
+  if (o == 1 && !h->has_t) return BW_ERR_UNSUPPORTED;
+  const std::vector<float> &ts = h->op[o].t_scale;
+  *n = (int64_t)ts.size();
+  if (out) std::memcpy(out, ts.data(), ts.size() * 4);
   return BW_OK;
 }
 

@@ -5,25 +5,36 @@
 // stages the block data with one TMA bulk copy (cp.async.bulk, 16-byte aligned
 // window around the chunk) and gathers the chunk's vector values with
 // cp.async, into a ring of kStages shared-memory stages guarded by mbarriers.
-// Warps 1..8 are consumers: each thread owns two adjacent rows of the item and
-// a contiguous range of the chunk's columns, accumulates in registers, and at
-// the item's last chunk the column partial sums are reduced in shared memory
-// and written once (t for phase 1, y for phase 2, with the row permutation
-// applied on the fly).  Every wait is a bounded mbarrier try_wait loop; on
-// timeout the kernel records an error word and returns.
+// Warps 1..8 are consumers and own the item's output rows:
+//  * FP64 / FP32: each thread owns 2 (FP64) or 4 (FP32) adjacent rows and a
+//    contiguous range of the chunk's columns and accumulates with FMAs;
+//  * BF16: tensor cores.  The chunk is stored in 8x8 tiles, so ldmatrix.trans
+//    loads 16x16 A fragments from 128-byte contiguous shared memory; the
+//    vector is the B operand (column 0: its BF16 rounding, column 1: the BF16
+//    rounding of the remainder, so the product keeps ~16 bits of the FP32
+//    vector), mma.m16n8k16 accumulates in FP32 registers across the item.
+// At the item's last chunk the partial sums are reduced in shared memory and
+// written once (t for phase 1, y for phase 2, with the row permutation applied
+// on the fly).  Every wait is a bounded mbarrier try_wait loop; on timeout the
+// kernel records an error word and returns.
 #pragma once
 
-#include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <cstdint>
 
 #include "bw_layout.h"
 
 namespace bw {
 
-constexpr int kStages = 5;
+constexpr int kStages = 6;
 constexpr int kConsumerWarps = 8;
 constexpr int kConsumers = 32 * kConsumerWarps;
 constexpr int kThreads = 32 + kConsumers;
+// Partial sums per reduction buffer: Q * hpad <= 2 * kConsumers (FP64, 2 rows
+// per thread), <= 4 * kConsumers (FP32, 4 rows), kparts * hpad <= 1024 (BF16).
+template <typename G> constexpr int red_per_buf() { return sizeof(G) == 8 ? 2 * kConsumers : 1024; }
 
 // error words
 constexpr int kErrTimeoutEmpty = 0x101;
@@ -38,12 +49,13 @@ struct StreamArgs {
   const void *xsrc;           // gathered x (compute type), permuted order
   const void *tsrc;           // t (compute type)
   void *t_out;                // phase-1 output (compute type)
+  const float *t_scale;       // phase 1: per-t-entry output scale (BF16), or null
   double *y_out;              // phase-2 output
   const int32_t *perm_out;    // phase 2: point permutation of the output, or null
   int dof;
   int phase;                  // 1 or 2
   int *err;
-  long long spin_limit;        // bound of every wait, in nanoseconds
+  long long spin_limit;       // bound of every wait, in nanoseconds
 };
 
 // ----------------------------------------------------------------------------- PTX helpers
@@ -94,15 +106,12 @@ __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-
-// Bounded wait: returns false when `limit_ns` nanoseconds passed without the
-// phase completing.
+// Bounded wait: false when `limit_ns` nanoseconds passed without the phase completing.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
@@ -112,42 +121,63 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long l
   }
   return true;
 }
-
 __device__ __forceinline__ void set_error(int *err, int code) { atomicCAS(err, 0, code); }
 
+// Four 8x8 b16 matrices from shared memory, transposed into mma A-fragment order.
+__device__ __forceinline__ void ldmatrix_x4_trans(uint32_t addr, uint32_t &a0, uint32_t &a1, uint32_t &a2,
+                                                  uint32_t &a3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
+               : "=r"(a0), "=r"(a1), "=r"(a2), "=r"(a3)
+               : "r"(addr));
+}
+// D(16x8, f32) += A(16x16, bf16, row) * B(16x8, bf16, col)
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+
 // ----------------------------------------------------------------------------- storage traits
-struct Bf16 {};  // storage tag: 16-bit brain float with per-chunk FP32 scale
+struct Bf16 {};  // storage tag: 16-bit brain float, 8x8-tiled items
 
 template <typename S> struct Store;
 template <> struct Store<double> {
   using G = double;   // compute / gather type
   static constexpr int kEsize = 8;
+  static constexpr int kRows = 2;  // rows per consumer thread
 };
 template <> struct Store<float> {
   using G = float;
   static constexpr int kEsize = 4;
+  static constexpr int kRows = 4;
 };
 template <> struct Store<Bf16> {
   using G = float;
   static constexpr int kEsize = 2;
+  static constexpr int kRows = 0;  // tensor-core path
 };
 
-// Partial sums of two adjacent rows over columns [c0, c1) of a staged chunk.
-// `base` points at the chunk's first element in shared memory; pair p of
-// column c is at element 2 * (c * hp + p).
-template <typename S>
-__device__ __forceinline__ void chunk_dot(const unsigned char *base, const typename Store<S>::G *g, int hp, int rp,
-                                          int c0, int c1, typename Store<S>::G &o0, typename Store<S>::G &o1);
+// Partial sums of R adjacent rows over columns [c0, c1) of a column-major chunk.
+template <typename S, int R>
+__device__ __forceinline__ void chunk_dot(const unsigned char *base, const typename Store<S>::G *g, int hv, int rv,
+                                          int c0, int c1, typename Store<S>::G (&o)[R]);
 
 template <>
-__device__ __forceinline__ void chunk_dot<double>(const unsigned char *base, const double *g, int hp, int rp, int c0,
-                                                  int c1, double &o0, double &o1) {
-  const double2 *d = reinterpret_cast<const double2 *>(base) + rp;
+__device__ __forceinline__ void chunk_dot<double, 2>(const unsigned char *base, const double *g, int hv, int rv,
+                                                     int c0, int c1, double (&o)[2]) {
+  const double2 *d = reinterpret_cast<const double2 *>(base) + rv;
   double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
   int c = c0;
 #pragma unroll 1
   for (; c + 4 <= c1; c += 4) {
-    const double2 w0 = d[(c + 0) * hp], w1 = d[(c + 1) * hp], w2 = d[(c + 2) * hp], w3 = d[(c + 3) * hp];
+    const double2 w0 = d[(c + 0) * hv], w1 = d[(c + 1) * hv], w2 = d[(c + 2) * hv], w3 = d[(c + 3) * hv];
     const double g0 = g[c], g1 = g[c + 1], g2 = g[c + 2], g3 = g[c + 3];
     a0 = fma(w0.x, g0, a0);
     a1 = fma(w0.y, g0, a1);
@@ -159,71 +189,52 @@ __device__ __forceinline__ void chunk_dot<double>(const unsigned char *base, con
     b1 = fma(w3.y, g3, b1);
   }
   for (; c < c1; c++) {
-    const double2 w = d[c * hp];
+    const double2 w = d[c * hv];
     a0 = fma(w.x, g[c], a0);
     a1 = fma(w.y, g[c], a1);
   }
-  o0 = a0 + b0;
-  o1 = a1 + b1;
+  o[0] = a0 + b0;
+  o[1] = a1 + b1;
 }
 
 template <>
-__device__ __forceinline__ void chunk_dot<float>(const unsigned char *base, const float *g, int hp, int rp, int c0,
-                                                 int c1, float &o0, float &o1) {
-  const float2 *d = reinterpret_cast<const float2 *>(base) + rp;
-  float a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+__device__ __forceinline__ void chunk_dot<float, 4>(const unsigned char *base, const float *g, int hv, int rv,
+                                                    int c0, int c1, float (&o)[4]) {
+  const float4 *d = reinterpret_cast<const float4 *>(base) + rv;
+  float a0 = 0, a1 = 0, a2 = 0, a3 = 0, b0 = 0, b1 = 0, b2 = 0, b3 = 0;
   int c = c0;
 #pragma unroll 1
   for (; c + 4 <= c1; c += 4) {
-    const float2 w0 = d[(c + 0) * hp], w1 = d[(c + 1) * hp], w2 = d[(c + 2) * hp], w3 = d[(c + 3) * hp];
+    const float4 w0 = d[(c + 0) * hv], w1 = d[(c + 1) * hv], w2 = d[(c + 2) * hv], w3 = d[(c + 3) * hv];
     const float g0 = g[c], g1 = g[c + 1], g2 = g[c + 2], g3 = g[c + 3];
     a0 = fmaf(w0.x, g0, a0);
     a1 = fmaf(w0.y, g0, a1);
+    a2 = fmaf(w0.z, g0, a2);
+    a3 = fmaf(w0.w, g0, a3);
     b0 = fmaf(w1.x, g1, b0);
     b1 = fmaf(w1.y, g1, b1);
+    b2 = fmaf(w1.z, g1, b2);
+    b3 = fmaf(w1.w, g1, b3);
     a0 = fmaf(w2.x, g2, a0);
     a1 = fmaf(w2.y, g2, a1);
+    a2 = fmaf(w2.z, g2, a2);
+    a3 = fmaf(w2.w, g2, a3);
     b0 = fmaf(w3.x, g3, b0);
     b1 = fmaf(w3.y, g3, b1);
+    b2 = fmaf(w3.z, g3, b2);
+    b3 = fmaf(w3.w, g3, b3);
   }
   for (; c < c1; c++) {
-    const float2 w = d[c * hp];
+    const float4 w = d[c * hv];
     a0 = fmaf(w.x, g[c], a0);
     a1 = fmaf(w.y, g[c], a1);
+    a2 = fmaf(w.z, g[c], a2);
+    a3 = fmaf(w.w, g[c], a3);
   }
-  o0 = a0 + b0;
-  o1 = a1 + b1;
-}
-
-__device__ __forceinline__ float bf_lo(uint32_t w) { return __uint_as_float(w << 16); }
-__device__ __forceinline__ float bf_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
-
-template <>
-__device__ __forceinline__ void chunk_dot<Bf16>(const unsigned char *base, const float *g, int hp, int rp, int c0,
-                                                int c1, float &o0, float &o1) {
-  const uint32_t *d = reinterpret_cast<const uint32_t *>(base) + rp;
-  float a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-  int c = c0;
-#pragma unroll 1
-  for (; c + 4 <= c1; c += 4) {
-    const uint32_t w0 = d[(c + 0) * hp], w1 = d[(c + 1) * hp], w2 = d[(c + 2) * hp], w3 = d[(c + 3) * hp];
-    const float g0 = g[c], g1 = g[c + 1], g2 = g[c + 2], g3 = g[c + 3];
-    a0 = fmaf(bf_lo(w0), g0, a0);
-    a1 = fmaf(bf_hi(w0), g0, a1);
-    b0 = fmaf(bf_lo(w1), g1, b0);
-    b1 = fmaf(bf_hi(w1), g1, b1);
-    a0 = fmaf(bf_lo(w2), g2, a0);
-    a1 = fmaf(bf_hi(w2), g2, a1);
-    b0 = fmaf(bf_lo(w3), g3, b0);
-    b1 = fmaf(bf_hi(w3), g3, b1);
-  }
-  for (; c < c1; c++) {
-    const uint32_t w = d[c * hp];
-    a0 = fmaf(bf_lo(w), g[c], a0);
-    a1 = fmaf(bf_hi(w), g[c], a1);
-  }
-  o0 = a0 + b0;
-  o1 = a1 + b1;
+  o[0] = a0 + b0;
+  o[1] = a1 + b1;
+  o[2] = a2 + b2;
+  o[3] = a3 + b3;
 }
 
 // ----------------------------------------------------------------------------- shared memory
@@ -232,22 +243,23 @@ template <typename S> struct SmemLayout {
   static constexpr int kDataBytes = kStageBytes + 32;
   static constexpr int kGBytes = kMaxCols * sizeof(G);
   static constexpr int kStageSize = kDataBytes + kGBytes + (int)sizeof(Chunk);
-  static constexpr int kRedBytes = 2 * 2 * kConsumers * (int)sizeof(G);  // double-buffered [Q][hpad]
+  static constexpr int kRedPer = red_per_buf<G>();
+  static constexpr int kRedBytes = 2 * kRedPer * (int)sizeof(G);
   static constexpr int kBarBytes = (2 * kStages + 1) * 8;
   static constexpr int kTotal = kStages * kStageSize + kRedBytes + kBarBytes;
   static_assert(kStageSize % 16 == 0, "stage must keep 16-byte alignment");
+  static_assert(kTotal <= 232448, "shared memory above the 227 KB per-CTA limit");
 };
 
-// Words 0..15 of a descriptor, broadcast from lane `src`.
 struct DescRegs {
-  uint32_t w[16];
+  uint32_t w[kChunkWords];
 };
 
-__device__ __forceinline__ void load_desc_batch(const Chunk *chunks, int idx, int end, DescRegs &r) {
+__device__ __forceinline__ void load_desc(const Chunk *chunks, int idx, int end, DescRegs &r) {
   if (idx < end) {
     const uint4 *p = reinterpret_cast<const uint4 *>(chunks + idx);
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < kChunkWords / 4; k++) {
       const uint4 v = __ldg(p + k);
       r.w[4 * k + 0] = v.x;
       r.w[4 * k + 1] = v.y;
@@ -256,8 +268,27 @@ __device__ __forceinline__ void load_desc_batch(const Chunk *chunks, int idx, in
     }
   } else {
 #pragma unroll
-    for (int k = 0; k < 16; k++) r.w[k] = 0;
+    for (int k = 0; k < kChunkWords; k++) r.w[k] = 0;
   }
+}
+
+// Segment of chunk column c: index, first column, and source offset
+// (words 8..15: seg_off, 16..19: seg_cols pairs).
+__device__ __forceinline__ int seg_of(const uint32_t (&w)[kChunkWords], int nseg, int c, int &start, int &off) {
+  int acc = 0, sg = 0;
+  start = 0;
+  off = static_cast<int>(w[8]);
+#pragma unroll
+  for (int k = 0; k < kMaxSeg; k++) {
+    const int ck = static_cast<int>((w[16 + (k >> 1)] >> ((k & 1) * 16)) & 0xffffu);
+    if (k < nseg && c >= acc) {
+      sg = k;
+      start = acc;
+      off = static_cast<int>(w[8 + k]);
+    }
+    acc += ck;
+  }
+  return sg;
 }
 
 template <typename S>
@@ -265,6 +296,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
   using G = typename Store<S>::G;
   using L = SmemLayout<S>;
   constexpr int es = Store<S>::kEsize;
+  constexpr bool kTensor = Store<S>::kRows == 0;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char *stage0 = smem;
   G *red = reinterpret_cast<G *>(smem + kStages * L::kStageSize);
@@ -292,12 +324,12 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
     const G *xs = static_cast<const G *>(a.xsrc);
     const G *ts = static_cast<const G *>(a.tsrc);
     DescRegs cur, nxt;
-    load_desc_batch(a.chunks, cb + lane, ce, nxt);
+    load_desc(a.chunks, cb + lane, ce, nxt);
     bool ok = true;
     int issued = 0;
     for (int bb = cb; bb < ce && ok; bb += 32) {
       cur = nxt;
-      load_desc_batch(a.chunks, bb + 32 + lane, ce, nxt);
+      load_desc(a.chunks, bb + 32 + lane, ce, nxt);
       const int nb = min(32, ce - bb);
       for (int k = 0; k < nb; k++) {
         const int i = bb + k - cb;
@@ -308,20 +340,23 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
           ok = false;
           break;
         }
-        uint32_t w[16];
+        uint32_t w[kChunkWords];
 #pragma unroll
-        for (int q = 0; q < 16; q++) w[q] = __shfl_sync(0xffffffffu, cur.w[q], k);
+        for (int q = 0; q < kChunkWords; q++) w[q] = __shfl_sync(0xffffffffu, cur.w[q], k);
         const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
         const int ncols = static_cast<int>(w[2]);
         const int hpad = static_cast<int>(w[3]);
-        const uint32_t flags = w[7];
+        const uint32_t flags = w[6];
         unsigned char *st = stage0 + s * L::kStageSize;
         G *gs = reinterpret_cast<G *>(st + L::kDataBytes);
         if (lane == 0) {
           uint4 *dd = reinterpret_cast<uint4 *>(st + L::kDataBytes + L::kGBytes);
 #pragma unroll
-          for (int q = 0; q < 4; q++) dd[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-          const unsigned long long bytes = static_cast<unsigned long long>(ncols) * hpad * es;
+          for (int q = 0; q < kChunkWords / 4; q++)
+            dd[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+          const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
+                                                  : static_cast<unsigned long long>(ncols);
+          const unsigned long long bytes = cols * hpad * es;
           if (ncols > 0 && bytes <= static_cast<unsigned long long>(kStageBytes)) {
             const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
                                            static_cast<unsigned long long>(data_off) * es;
@@ -336,22 +371,16 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         }
         // gather the chunk's vector values
         const int nseg = static_cast<int>((flags >> 8) & 0xfu);
-        const int e0 = static_cast<int>(w[12] & 0xffffu);
-        const int e1 = e0 + static_cast<int>(w[12] >> 16);
-        const int e2 = e1 + static_cast<int>(w[13] & 0xffffu);
         const int gcols = ncols <= kMaxCols ? ncols : 0;
         for (int c = lane; c < gcols; c += 32) {
-          const int sg = (c >= e0) + (c >= e1) + (c >= e2);
-          const int start = sg == 0 ? 0 : (sg == 1 ? e0 : (sg == 2 ? e1 : e2));
-          if (sg < nseg) {
-            const G *src = ((flags >> (16 + sg)) & 1u) ? ts : xs;
-            const uint32_t so = sg == 0 ? w[8] : (sg == 1 ? w[9] : (sg == 2 ? w[10] : w[11]));
-            const G *p = src + static_cast<int>(so) + (c - start);
-            if (sizeof(G) == 8)
-              cp_async_8(gs + c, p);
-            else
-              cp_async_4(gs + c, p);
-          }
+          int start, off;
+          const int sg = seg_of(w, nseg, c, start, off);
+          const G *src = ((flags >> (16 + sg)) & 1u) ? ts : xs;
+          const G *p = src + off + (c - start);
+          if (sizeof(G) == 8)
+            cp_async_8(gs + c, p);
+          else
+            cp_async_4(gs + c, p);
         }
         cp_async_arrive_noinc(&full[s]);
         issued++;
@@ -369,10 +398,24 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
 
   // -------------------------------------------------------------------- consumers
   const int ct = threadIdx.x - 32;
-  int hp = 1, Q = 1, rp = 0, cq = 0;
-  bool active = false;
-  G acc0 = 0, acc1 = 0;
+  const int cw = warp - 1;
   uint32_t items = 0;
+  // FMA path state
+  constexpr int R = kTensor ? 1 : Store<S>::kRows;
+  int hv = 1, Q = 1, rv = 0, cq = 0;
+  bool active = false;
+  G acc[R];
+#pragma unroll
+  for (int r = 0; r < R; r++) acc[r] = 0;
+  // tensor path state
+  int nMt = 1, kparts = 1, mg = 0, kp = 0;
+  bool wact = false;
+  float tacc[kTensor ? 8 : 1][4];
+#pragma unroll
+  for (int j = 0; j < (kTensor ? 8 : 1); j++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) tacc[j][q] = 0.f;
+
   for (int i = 0; i < ce - cb; i++) {
     const int s = i % kStages;
     const uint32_t use = static_cast<uint32_t>(i / kStages);
@@ -386,32 +429,133 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
     const uint32_t flags = d.flags;
     const int ncols = d.ncols;
     const int hpad = d.hpad;
-    if (flags & kFirst) {
-      hp = hpad >> 1;
-      Q = kConsumers / hp;
-      rp = ct % hp;
-      cq = ct / hp;
-      active = cq < Q;
-      acc0 = 0;
-      acc1 = 0;
-    }
-    if (active && ncols > 0 && ncols <= kMaxCols) {
-      const int c0 = (cq * ncols) / Q, c1 = ((cq + 1) * ncols) / Q;
-      const int soff = static_cast<int>((static_cast<unsigned long long>(d.data_off) * es) & 15ull);
-      G p0, p1;
-      chunk_dot<S>(st + soff, gs, hp, rp, c0, c1, p0, p1);
-      const G sc = static_cast<G>(d.scale);
-      acc0 += sc * p0;
-      acc1 += sc * p1;
-    }
     const int rows = d.rows, out_off = d.out_off;
+    if constexpr (!kTensor) {
+      if (flags & kFirst) {
+        hv = hpad / R;
+        Q = kConsumers / hv;
+        rv = ct % hv;
+        cq = ct / hv;
+        active = cq < Q;
+#pragma unroll
+        for (int r = 0; r < R; r++) acc[r] = 0;
+      }
+      if (active && ncols > 0 && ncols <= kMaxCols) {
+        const int c0 = (cq * ncols) / Q, c1 = ((cq + 1) * ncols) / Q;
+        const int soff = static_cast<int>((static_cast<unsigned long long>(d.data_off) * es) & 15ull);
+        G p[R];
+        chunk_dot<S, R>(st + soff, gs, hv, rv, c0, c1, p);
+#pragma unroll
+        for (int r = 0; r < R; r++) acc[r] += p[r];
+      }
+    } else {
+      if (flags & kFirst) {
+        nMt = (hpad + 15) >> 4;
+        const int mgroups = (nMt + 7) >> 3;
+        kparts = kConsumerWarps / mgroups;
+        mg = cw / kparts;
+        kp = cw % kparts;
+        wact = mg < mgroups;
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) tacc[j][q] = 0.f;
+      }
+      if (wact && ncols > 0 && ncols <= kMaxCols) {
+        const int nseg = static_cast<int>((flags >> 8) & 0xfu);
+        const int grp = lane >> 2, tq = lane & 3;
+        const uint32_t sbase = smem_u32(st);  // BF16 chunks start 16-byte aligned (offset 0)
+        const int nks = (ncols + 15) >> 4;
+        const int mat = lane >> 3, mr = lane & 7;
+        // per-column BF16 block scale: segment ends and scales of this chunk
+        int send[kMaxSeg];
+        float sscl[kMaxSeg];
+        {
+          int acc_c = 0;
+#pragma unroll
+          for (int k = 0; k < kMaxSeg; k++) {
+            acc_c += k < nseg ? static_cast<int>(d.seg_cols[k]) : 0;
+            send[k] = k < nseg ? acc_c : 0x7fffffff;
+            sscl[k] = d.seg_scale[k];
+          }
+        }
+        for (int ks = kp; ks < nks; ks += kparts) {
+          // B fragment: lanes 0-3 hold the BF16-rounded vector (column 0),
+          // lanes 4-7 the BF16-rounded remainder (column 1), others zero.
+          uint32_t b0 = 0, b1 = 0;
+          if (grp < 2) {
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              const int c = 16 * ks + 2 * tq + (e & 1) + (e >> 1) * 8;
+              float x = 0.f;
+              if (c < ncols) {
+                float sc = sscl[0];
+#pragma unroll
+                for (int k = 1; k < kMaxSeg; k++)
+                  if (c >= send[k - 1]) sc = sscl[k];
+                x = gs[c] * sc;
+              }
+              const float hi = __bfloat162float(__float2bfloat16_rn(x));
+              v[e] = grp == 0 ? hi : x - hi;
+            }
+            b0 = pack_bf16x2(v[0], v[1]);
+            b1 = pack_bf16x2(v[2], v[3]);
+          }
+          const bool k2 = 16 * ks + 8 < ncols;  // second 8-column group present
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const int mt = mg * 8 + j;
+            if (mt < nMt) {
+              const bool m2 = mt * 16 + 8 < hpad;  // second 8-row group present
+              int kg = 2 * ks + (mat >> 1), rg = 2 * mt + (mat & 1);
+              const bool valid = (!(mat & 2) || k2) && (!(mat & 1) || m2);
+              if (!valid) {
+                kg = 2 * ks;
+                rg = 2 * mt;
+              }
+              const uint32_t addr = sbase + 2u * static_cast<uint32_t>(kg * 8 * hpad + rg * 64 + mr * 8);
+              uint32_t a0, a1, a2, a3;
+              ldmatrix_x4_trans(addr, a0, a1, a2, a3);
+              if (!m2) {
+                a1 = 0;
+                a3 = 0;
+              }
+              if (!k2) {
+                a2 = 0;
+                a3 = 0;
+              }
+              mma_bf16_16816(tacc[j], a0, a1, a2, a3, b0, b1);
+            }
+          }
+        }
+      }
+    }
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     if (flags & kLast) {
-      G *rb = red + (items & 1u) * (2 * kConsumers);
-      if (active) {
-        rb[cq * hpad + 2 * rp] = acc0;
-        rb[cq * hpad + 2 * rp + 1] = acc1;
+      G *rb = red + (items & 1u) * L::kRedPer;
+      int nred;
+      if constexpr (!kTensor) {
+        if (active) {
+#pragma unroll
+          for (int r = 0; r < R; r++) rb[cq * hpad + R * rv + r] = acc[r];
+        }
+        nred = Q;
+      } else {
+        if (wact && (lane & 3) == 0) {
+          const int g8 = lane >> 2;
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const int mt = mg * 8 + j;
+            if (mt < nMt) {
+              const int row = mt * 16 + g8;
+              if (row < hpad) rb[kp * hpad + row] = tacc[j][0] + tacc[j][1];
+              if (row + 8 < hpad) rb[kp * hpad + row + 8] = tacc[j][2] + tacc[j][3];
+            }
+          }
+        }
+        nred = kparts;
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(redbar);
@@ -421,8 +565,9 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
       }
       for (int r = ct; r < rows; r += kConsumers) {
         G sum = 0;
-        for (int q = 0; q < Q; q++) sum += rb[q * hpad + r];
+        for (int q = 0; q < nred; q++) sum += rb[q * hpad + r];
         if (a.phase == 1) {
+          if (a.t_scale) sum *= a.t_scale[out_off + r];
           static_cast<G *>(a.t_out)[out_off + r] = sum;
         } else {
           const int row = out_off + r;

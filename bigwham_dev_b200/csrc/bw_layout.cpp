@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <numeric>
 #include <queue>
 #include <stdexcept>
@@ -93,16 +94,57 @@ void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
       fail("low-rank block " + std::to_string(k) + ": null data or leading dimension too small");
     if (b.r > 65535) fail("low-rank block " + std::to_string(k) + ": rank above 65535");
   }
+  if (n_out > INT32_MAX || n_in > INT32_MAX) fail("problem too large for 32-bit offsets");
 
-  // ---- t offsets (phase-1 outputs, one slot per rank column)
-  op.t_off.resize(nlr);
-  int64_t t = 0;
+  // ---- phase 1: B factors stacked per column cluster; t follows stack order
+  std::map<std::pair<int64_t, int64_t>, std::vector<int64_t>> stacks;  // (j0, n) -> blocks
   for (size_t k = 0; k < nlr; k++) {
-    op.t_off[k] = t;
-    t += p.lr[k].r;
+    EffLow b = eff_low(p, tr, k);
+    if (b.r > 0) stacks[{b.j0, b.n}].push_back((int64_t)k);
   }
+  op.t_off.assign(nlr, 0);
+  int64_t t = 0;
+  for (auto &kv : stacks)
+    for (int64_t k : kv.second) {
+      op.t_off[k] = t;
+      t += eff_low(p, tr, k).r;
+    }
   op.t_len = t;
-  if (t > INT32_MAX || n_out > INT32_MAX || n_in > INT32_MAX) fail("problem too large for 32-bit offsets");
+  if (t > INT32_MAX) fail("sum of ranks above 2^31-1");
+  op.n_stacks = (int64_t)stacks.size();
+  PhasePlan &p1 = op.ph[0];
+  for (auto &kv : stacks) {
+    const int64_t j0 = kv.first.first, n = kv.first.second;
+    int64_t R = 0;
+    for (int64_t k : kv.second) R += eff_low(p, tr, k).r;
+    // equal cuts of at most kHMax rows, multiples of kRowAlign except the last
+    const int64_t nit = (R + kHMax - 1) / kHMax;
+    const int64_t cut = align_up((R + nit - 1) / nit, kRowAlign);
+    size_t bi = 0;      // block of the stack
+    int64_t br = 0;     // next row inside that block
+    for (int64_t r0 = 0; r0 < R; r0 += cut) {
+      Item it;
+      it.h = static_cast<int32_t>(std::min<int64_t>(cut, R - r0));
+      it.hpad = static_cast<int32_t>(align_up(it.h, kRowAlign));
+      it.ncols = n;
+      it.out_off = static_cast<int32_t>(op.t_off[kv.second[bi]] + br);
+      int64_t need = it.h;
+      while (need > 0) {
+        const int64_t k = kv.second[bi];
+        const int64_t rk = eff_low(p, tr, k).r;
+        const int64_t take = std::min<int64_t>(need, rk - br);
+        it.pieces.push_back({k, br, take});
+        need -= take;
+        br += take;
+        if (br == rk) {
+          bi++;
+          br = 0;
+        }
+      }
+      it.segs.push_back({2, -1, 0, n, 0, j0});
+      p1.items.push_back(std::move(it));
+    }
+  }
 
   // ---- row panels: finest partition of [0, n_out) by block row boundaries
   std::vector<int64_t> bounds{0, n_out};
@@ -118,15 +160,18 @@ void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
   }
   std::sort(bounds.begin(), bounds.end());
   bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
-  std::vector<int64_t> pb;  // panel starts, with tall panels split at kHMax rows
+  std::vector<int64_t> pb;  // panel starts, with tall panels cut into equal parts of <= kHMax rows
   for (size_t i = 0; i + 1 < bounds.size(); i++) {
-    for (int64_t s = bounds[i]; s < bounds[i + 1]; s += kHMax) pb.push_back(s);
+    const int64_t H = bounds[i + 1] - bounds[i];
+    const int64_t nit = (H + kHMax - 1) / kHMax;
+    const int64_t cut = align_up((H + nit - 1) / nit, kRowAlign);
+    for (int64_t s = bounds[i]; s < bounds[i + 1]; s += cut) pb.push_back(s);
   }
   pb.push_back(n_out);
   const size_t npan = pb.size() - 1;
   op.n_panels = static_cast<int64_t>(npan);
 
-  // blocks covering each panel (panels sorted; a block covers a contiguous panel range)
+  // blocks covering each panel (a block covers a contiguous range of panels)
   auto first_panel = [&](int64_t row) {
     return static_cast<size_t>(std::upper_bound(pb.begin(), pb.end(), row) - pb.begin()) - 1;
   };
@@ -138,11 +183,13 @@ void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
   std::vector<std::vector<Cover>> cov(npan);
   for (size_t k = 0; k < nfr; k++) {
     EffFull b = eff_full(p, tr, k);
-    for (size_t q = first_panel(b.i0); q < npan && pb[q] < b.i0 + b.m; q++) cov[q].push_back({0, (int64_t)k, b.j0, b.n});
+    for (size_t q = first_panel(b.i0); q < npan && pb[q] < b.i0 + b.m; q++)
+      cov[q].push_back({0, (int64_t)k, b.j0, b.n});
   }
   for (size_t k = 0; k < nlr; k++) {
     EffLow b = eff_low(p, tr, k);
-    for (size_t q = first_panel(b.i0); q < npan && pb[q] < b.i0 + b.m; q++) cov[q].push_back({1, (int64_t)k, b.j0, b.n});
+    for (size_t q = first_panel(b.i0); q < npan && pb[q] < b.i0 + b.m; q++)
+      cov[q].push_back({1, (int64_t)k, b.j0, b.n});
   }
   // coverage: the column intervals of each panel must tile [0, n_in) exactly
   for (size_t q = 0; q < npan; q++) {
@@ -150,44 +197,25 @@ void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
     std::sort(c.begin(), c.end(), [](const Cover &a, const Cover &b) { return a.j0 < b.j0; });
     int64_t at = 0;
     for (const Cover &e : c) {
-      if (e.j0 < at) fail("blocks overlap in rows [" + std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
-      if (e.j0 > at) fail("columns [" + std::to_string(at) + ", " + std::to_string(e.j0) + ") not covered in rows [" +
-                          std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
+      if (e.j0 < at)
+        fail("blocks overlap in rows [" + std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
+      if (e.j0 > at)
+        fail("columns [" + std::to_string(at) + ", " + std::to_string(e.j0) + ") not covered in rows [" +
+             std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
       at = e.j0 + e.n;
     }
-    if (at != n_in) fail("columns [" + std::to_string(at) + ", " + std::to_string(n_in) + ") not covered in rows [" +
-                         std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
+    if (at != n_in)
+      fail("columns [" + std::to_string(at) + ", " + std::to_string(n_in) + ") not covered in rows [" +
+           std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
   }
 
-  // ---- phase 1 items: B of every low-rank block, rows split at kHMax
-  PhasePlan &p1 = op.ph[0];
-  int64_t off = 0;
-  for (size_t k = 0; k < nlr; k++) {
-    EffLow b = eff_low(p, tr, k);
-    for (int64_t r0 = 0; r0 < b.r; r0 += kHMax) {
-      Item it;
-      it.h = static_cast<int32_t>(std::min<int64_t>(kHMax, b.r - r0));
-      it.hpad = it.h + (it.h & 1);
-      it.ncols = b.n;
-      it.out_off = static_cast<int32_t>(op.t_off[k] + r0);
-      it.data_off = off;
-      it.segs.push_back({2, (int64_t)k, r0, b.n, 0, b.j0});
-      off = align_up(off + it.hpad * it.ncols, kItemAlign);
-      p1.items.push_back(std::move(it));
-    }
-  }
-  p1.n_elems = off + kItemAlign;  // slack so 16-byte rounded copies stay inside
-
-  // ---- phase 2 items: row panels; FR slices first (they do not depend on t)
+  // ---- phase 2 items: one per panel; FR slices first (they do not depend on t)
   PhasePlan &p2 = op.ph[1];
-  off = 0;
   for (size_t q = 0; q < npan; q++) {
     Item it;
     it.h = static_cast<int32_t>(pb[q + 1] - pb[q]);
-    it.hpad = it.h + (it.h & 1);
+    it.hpad = static_cast<int32_t>(align_up(it.h, kRowAlign));
     it.out_off = static_cast<int32_t>(pb[q]);
-    it.data_off = off;
-    it.ncols = 0;
     for (int pass = 0; pass < 2; pass++) {
       for (const Cover &e : cov[q]) {
         if (e.kind != pass) continue;
@@ -203,10 +231,8 @@ void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
         }
       }
     }
-    off = align_up(off + it.hpad * it.ncols, kItemAlign);
     p2.items.push_back(std::move(it));
   }
-  p2.n_elems = off + kItemAlign;
 }
 
 void compute_scales(const Problem &p, bool tr, bool check_finite, OperatorPlan &op) {
@@ -252,6 +278,11 @@ void compute_scales(const Problem &p, bool tr, bool check_finite, OperatorPlan &
   }
   if (check_finite && bad_fr >= 0) fail("non-finite entry in full block " + std::to_string(bad_fr));
   if (check_finite && bad_lr >= 0) fail("non-finite entry in low-rank block " + std::to_string(bad_lr));
+  op.t_scale.assign((size_t)std::max<int64_t>(1, op.t_len), 1.0f);
+  for (int64_t k = 0; k < nlr; k++) {
+    const int64_t r = p.lr[k].r;
+    for (int64_t i = 0; i < r; i++) op.t_scale[op.t_off[k] + i] = op.scale_a[k] * op.scale_b[k];
+  }
 }
 
 namespace {
@@ -259,63 +290,59 @@ namespace {
 float seg_scale(const OperatorPlan &op, const Segment &s, int prec) {
   if (prec != 2) return 1.0f;
   if (s.kind == 0) return op.scale_fr[s.block];
-  if (s.kind == 2) return op.scale_a[s.block] * op.scale_b[s.block];
-  return 1.0f;  // LR A slices: the scale of A is folded into t
+  return 1.0f;  // LR A slices and B stacks: the scales are folded into t (t_scale)
 }
 
-void chunk_items(const OperatorPlan &op, const PhasePlan &ph, int prec, std::vector<std::vector<Chunk>> &per_item) {
+// Chunks of one item for one precision.
+void chunk_item(const OperatorPlan &op, const Item &it, int prec, std::vector<Chunk> &out) {
   const int es = esize_of(prec);
-  per_item.assign(ph.items.size(), {});
-  for (size_t q = 0; q < ph.items.size(); q++) {
-    const Item &it = ph.items[q];
-    const int64_t cap = std::max<int64_t>(1, std::min<int64_t>(kMaxCols, kStageBytes / (int64_t(it.hpad) * es)));
-    std::vector<Chunk> &out = per_item[q];
-    Chunk cur{};
-    int64_t col = 0;  // item column of the next column to place
-    auto open = [&](float sc) {
-      std::memset(&cur, 0, sizeof(cur));
-      cur.data_off = it.data_off + col * it.hpad;
-      cur.hpad = it.hpad;
-      cur.rows = it.h;
-      cur.out_off = it.out_off;
-      cur.scale = sc;
-    };
-    auto close = [&]() {
-      if (out.empty()) cur.flags |= kFirst;
-      out.push_back(cur);
-    };
-    bool have = false;
-    for (const Segment &s : it.segs) {
-      const float sc = seg_scale(op, s, prec);
-      int64_t done = 0;
-      while (done < s.ncols) {
-        const int nseg = (cur.flags >> 8) & 0xf;
-        if (have && (cur.ncols >= cap || nseg >= kMaxSeg || cur.scale != sc)) {
-          close();
-          have = false;
-        }
-        if (!have) {
-          open(sc);
-          have = true;
-        }
-        const int ns = (cur.flags >> 8) & 0xf;
-        const int64_t take = std::min<int64_t>(s.ncols - done, cap - cur.ncols);
-        cur.seg_off[ns] = static_cast<int32_t>(s.src_off + done);
-        cur.seg_cols[ns] = static_cast<uint16_t>(take);
-        cur.flags = (cur.flags & ~(0xfu << 8)) | (uint32_t(ns + 1) << 8);
-        if (s.src) cur.flags |= (1u << (16 + ns));
-        cur.ncols += static_cast<int32_t>(take);
-        done += take;
-        col += take;
-      }
+  const bool tiled = prec == 2;
+  int64_t cap;
+  if (tiled)
+    cap = std::min<int64_t>(kMaxCols, (kStageBytes / (8 * int64_t(it.hpad) * es)) * 8);
+  else
+    cap = std::max<int64_t>(1, std::min<int64_t>(kMaxCols, kStageBytes / (int64_t(it.hpad) * es)));
+  // column -> segment map of the item
+  std::vector<int64_t> seg_start(it.segs.size() + 1, 0);
+  for (size_t s = 0; s < it.segs.size(); s++) seg_start[s + 1] = seg_start[s] + it.segs[s].ncols;
+  int64_t c0 = 0;
+  size_t s_at = 0;  // segment containing column c0
+  do {
+    int64_t take = std::min<int64_t>(cap, it.ncols - c0);
+    // at most kMaxSeg segment pieces
+    while (s_at < it.segs.size() && seg_start[s_at + 1] <= c0) s_at++;
+    if (s_at + kMaxSeg < it.segs.size()) {
+      const int64_t lim = seg_start[s_at + kMaxSeg] - c0;  // columns covered by kMaxSeg pieces
+      if (lim < take) take = lim;
     }
-    if (!have) {  // an item without columns still writes its (zero) output
-      open(1.0f);
-      have = true;
+    // tiled chunks start on 8-column groups: cut at a multiple of 8 unless it is the item's end
+    if (tiled && c0 + take < it.ncols) take = (take / 8) * 8;
+    if (it.ncols > 0 && take <= 0) throw std::runtime_error("internal: empty chunk");
+    Chunk ch;
+    std::memset(&ch, 0, sizeof ch);
+    ch.data_off = it.off[prec] + (tiled ? (c0 / 8) * 8 * int64_t(it.hpad) : c0 * int64_t(it.hpad));
+    ch.ncols = static_cast<int32_t>(take);
+    ch.hpad = it.hpad;
+    ch.rows = it.h;
+    ch.out_off = it.out_off;
+    int ns = 0;
+    for (size_t s = s_at; s < it.segs.size() && seg_start[s] < c0 + take; s++) {
+      const int64_t a = std::max<int64_t>(c0, seg_start[s]), b = std::min<int64_t>(c0 + take, seg_start[s + 1]);
+      if (b <= a) continue;
+      if (ns >= kMaxSeg) throw std::runtime_error("internal: too many segments in a chunk");
+      const Segment &sg = it.segs[s];
+      ch.seg_off[ns] = static_cast<int32_t>(sg.src_off + (a - seg_start[s]));
+      ch.seg_cols[ns] = static_cast<uint16_t>(b - a);
+      ch.seg_scale[ns] = seg_scale(op, sg, prec);
+      if (sg.src) ch.flags |= 1u << (16 + ns);
+      ns++;
     }
-    close();
-    out.back().flags |= kLast;
-  }
+    ch.flags |= uint32_t(ns) << 8;
+    if (out.empty() || (out.back().flags & kLast)) ch.flags |= kFirst;
+    c0 += take;
+    if (c0 >= it.ncols) ch.flags |= kLast;
+    out.push_back(ch);
+  } while (c0 < it.ncols);
 }
 
 }  // namespace
@@ -326,15 +353,22 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
   const int es = esize_of(prec);
   for (int phase = 0; phase < 2; phase++) {
     PhasePlan &ph = op.ph[phase];
-    std::vector<std::vector<Chunk>> per_item;
-    chunk_items(op, ph, prec, per_item);
+    // data layout of this precision
+    int64_t off = 0;
+    for (Item &it : ph.items) {
+      it.off[prec] = off;
+      off = align_up(off + item_elems(prec, it.hpad, it.ncols), kItemAlign);
+    }
+    ph.n_elems[prec] = off + kItemAlign;  // slack so 16-byte rounded copies stay inside
+    std::vector<std::vector<Chunk>> per_item(ph.items.size());
+    for (size_t q = 0; q < ph.items.size(); q++) chunk_item(op, ph.items[q], prec, per_item[q]);
     // LPT: items by decreasing cost onto the least-loaded CTA.  Cost is the
     // bytes streamed plus a fixed per-chunk overhead (descriptor, gather,
     // barrier round trip) expressed in bytes.
     const int64_t n = (int64_t)ph.items.size();
     std::vector<int64_t> cost(n);
     for (int64_t q = 0; q < n; q++)
-      cost[q] = int64_t(ph.items[q].hpad) * ph.items[q].ncols * es + 2048 * (int64_t)per_item[q].size();
+      cost[q] = item_elems(prec, ph.items[q].hpad, ph.items[q].ncols) * es + 2048 * (int64_t)per_item[q].size();
     std::vector<int64_t> order(n);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
@@ -364,9 +398,29 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
 void fill_items(const Problem &p, bool tr, const OperatorPlan &op, int phase, int prec, int64_t i_begin,
                 int64_t i_end, int64_t base, void *dst) {
   const PhasePlan &ph = op.ph[phase];
+  auto put = [&](int64_t e, double val, double inv) {
+    if (prec == 0)
+      static_cast<double *>(dst)[e] = val;
+    else if (prec == 1)
+      static_cast<float *>(dst)[e] = static_cast<float>(val);
+    else
+      static_cast<uint16_t *>(dst)[e] = to_bf16(static_cast<float>(val * inv));
+  };
 #pragma omp parallel for schedule(dynamic, 4)
   for (int64_t q = i_begin; q < i_end; q++) {
     const Item &it = ph.items[q];
+    const int64_t e0 = it.off[prec] - base;
+    if (phase == 0) {  // stacked B rows, one segment of columns
+      int64_t row = 0;
+      for (const RowPiece &pc : it.pieces) {
+        const View B = eff_low(p, tr, pc.block).B;
+        const double inv = prec == 2 ? 1.0 / op.scale_b[pc.block] : 1.0;
+        for (int64_t c = 0; c < it.ncols; c++)
+          for (int64_t i = 0; i < pc.n; i++) put(e0 + item_index(prec, it.hpad, row + i, c), B.at(pc.r0 + i, c), inv);
+        row += pc.n;
+      }
+      continue;
+    }
     int64_t col = 0;
     for (const Segment &s : it.segs) {
       View v;
@@ -374,25 +428,12 @@ void fill_items(const Problem &p, bool tr, const OperatorPlan &op, int phase, in
       if (s.kind == 0) {
         v = eff_full(p, tr, s.block).a;
         if (prec == 2) inv = 1.0 / op.scale_fr[s.block];
-      } else if (s.kind == 1) {
+      } else {
         v = eff_low(p, tr, s.block).A;
         if (prec == 2) inv = 1.0 / op.scale_a[s.block];
-      } else {
-        v = eff_low(p, tr, s.block).B;
-        if (prec == 2) inv = 1.0 / op.scale_b[s.block];
       }
-      for (int64_t c = 0; c < s.ncols; c++) {
-        const int64_t e0 = it.data_off + (col + c) * it.hpad - base;
-        for (int64_t i = 0; i < it.hpad; i++) {
-          const double val = (i < it.h) ? v.at(s.row0 + i, c) : 0.0;
-          if (prec == 0)
-            static_cast<double *>(dst)[e0 + i] = val;
-          else if (prec == 1)
-            static_cast<float *>(dst)[e0 + i] = static_cast<float>(val);
-          else
-            static_cast<uint16_t *>(dst)[e0 + i] = to_bf16(static_cast<float>(val * inv));
-        }
-      }
+      for (int64_t c = 0; c < s.ncols; c++)
+        for (int64_t i = 0; i < it.h; i++) put(e0 + item_index(prec, it.hpad, i, col + c), v.at(s.row0 + i, c), inv);
       col += s.ncols;
     }
   }

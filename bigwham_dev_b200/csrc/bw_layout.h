@@ -4,20 +4,25 @@
 // (src/hmat/hmatrix/hmat.cc:472-537).  On the device the same product runs as
 // two streaming passes over re-laid-out block data:
 //
-//  phase 1 ("B stage"):   t_b = B_b x[cols_b] for every low-rank block b.
-//      One item per block (rows split above kHMax): the r x n matrix B_b,
-//      column-major with its row count padded to an even number.
+//  phase 1 ("B stage"):   t = B_b x[cols_b] for every low-rank block b.
+//      The B factors of all low-rank blocks that share one column cluster are
+//      stacked into one tall matrix (they multiply the same slice of x); the
+//      stack is cut into items of at most kHMax rows.  t is ordered by stack.
 //  phase 2 ("row panels"): y[p] = sum over the blocks that cover row panel p of
 //      (slice of A_b or of the full block) times (t_b or x[cols]).
 //      Row panels are the finest partition of the rows by block boundaries, so
 //      every block covers whole panels.  One item per panel: the slices of all
-//      covering blocks side by side, column-major (ld = padded panel height).
+//      covering blocks side by side.
 //
-// Every item is a dense column-major panel times a gathered vector; an item is
-// owned by one CTA, so outputs are written once, without atomics.  An item is
-// cut into chunks of at most kStageBytes; a chunk is the unit one TMA bulk copy
-// stages into shared memory, and carries up to kMaxSeg "gather segments" that
-// say where the vector values of its columns come from (x or t).
+// Every item is a dense h x n matrix times a gathered vector, owned by one
+// CTA, so outputs are written once, without atomics.  Rows are padded to a
+// multiple of 8.  FP64 and FP32 items are column-major (ld = padded rows);
+// BF16 items are stored as 8x8 tiles (column group, then row group, then
+// 8 columns x 8 contiguous rows) so that tensor-core fragment loads from shared
+// memory are 128-byte contiguous.  An item is cut into chunks of at most
+// kStageBytes; a chunk is what one TMA bulk copy stages into shared memory,
+// and carries up to kMaxSeg "gather segments" that say where the vector values
+// of its columns come from (x or t) and which BF16 block scale applies.
 #pragma once
 
 #include <cstdint>
@@ -28,30 +33,32 @@ namespace bw {
 
 constexpr int kStageBytes = 32768;   // bytes of block data per pipeline stage
 constexpr int kMaxCols = 512;        // columns per chunk (size of a stage's gather buffer)
-constexpr int kMaxSeg = 4;           // gather segments per chunk
+constexpr int kMaxSeg = 8;           // gather segments per chunk (>= 8: any 8 columns fit one chunk)
 constexpr int kHMax = 512;           // max padded rows of one item
+constexpr int kRowAlign = 8;         // padded rows are a multiple of this
 constexpr int kItemAlign = 64;       // item start alignment, in elements
 
 // Chunk flags
 constexpr uint32_t kFirst = 1u;      // first chunk of an item: reset accumulators
 constexpr uint32_t kLast = 2u;       // last chunk of an item: reduce and write the output
-// bits 8..11: number of segments; bits 16..19: source of segment k (0 = x, 1 = t)
+// bits 8..11: number of segments; bits 16..23: source of segment k (0 = x, 1 = t)
 
-// One chunk descriptor, 64 bytes, read by the producer warp and copied into
-// shared memory for the consumer warps.
+// One chunk descriptor, 112 bytes (28 words), read by the producer warp and
+// copied into shared memory for the consumer warps.
 struct alignas(16) Chunk {
-  int64_t data_off;      // element offset of the chunk's first column in the data array
-  int32_t ncols;         // columns in this chunk
-  int32_t hpad;          // padded row count of the item (even)
-  int32_t rows;          // rows of the item to write (<= hpad)
-  int32_t out_off;       // first output index: t offset (phase 1) or row (phase 2)
-  float scale;           // multiplies this chunk's partial sums (BF16 block scale)
-  uint32_t flags;        // kFirst | kLast | nseg << 8 | src bits << 16
+  int64_t data_off;           // element offset of the chunk's first column in the data array
+  int32_t ncols;              // columns in this chunk
+  int32_t hpad;               // padded row count of the item (multiple of 8)
+  int32_t rows;               // rows of the item to write (<= hpad)
+  int32_t out_off;            // first output index: t offset (phase 1) or row (phase 2)
+  uint32_t flags;             // kFirst | kLast | nseg << 8 | src bits << 16
+  uint32_t reserved0;
   int32_t seg_off[kMaxSeg];   // element offset of each segment in its source vector
   uint16_t seg_cols[kMaxSeg]; // columns of each segment
-  int32_t reserved[2];
+  float seg_scale[kMaxSeg];   // multiplies the vector values of the segment (BF16 block scale)
 };
-static_assert(sizeof(Chunk) == 64, "chunk descriptor must be 64 bytes");
+static_assert(sizeof(Chunk) == 112, "chunk descriptor must be 112 bytes");
+constexpr int kChunkWords = sizeof(Chunk) / 4;
 
 // A read-only view of a column-major block (or of its transpose).
 struct View {
@@ -70,22 +77,29 @@ struct LowRankBlock {
   View A, B;  // A: m x r, B: r x n
 };
 
-// Where the columns of one segment come from and where its data lives.
+// Column segment of an item: where its vector values come from and, for
+// phase 2, which block slice fills its data.
 struct Segment {
-  int kind;        // 0: FR slice, 1: LR A slice, 2: LR B rows
-  int64_t block;   // block index
-  int64_t row0;    // first row of the block (or of B) in this item
+  int kind;        // 0: FR slice, 1: LR A slice, 2: LR B stack (rows from Item::pieces)
+  int64_t block;   // block index (kinds 0, 1)
+  int64_t row0;    // first row of the block in this item (kinds 0, 1)
   int64_t ncols;   // columns
   int src;         // 0: x, 1: t
   int64_t src_off; // offset in x or t
 };
 
+// Rows [r0, r0 + n) of the B factor of low-rank block `block` (phase 1).
+struct RowPiece {
+  int64_t block, r0, n;
+};
+
 struct Item {
-  int64_t data_off;   // element offset in the phase's data array
-  int32_t h, hpad;    // rows, padded rows
-  int64_t ncols;      // total columns
-  int32_t out_off;
+  int64_t off[3] = {0, 0, 0};  // element offset in the phase's data array, per precision
+  int32_t h = 0, hpad = 0;     // rows, padded rows
+  int64_t ncols = 0;           // total columns
+  int32_t out_off = 0;
   std::vector<Segment> segs;
+  std::vector<RowPiece> pieces;  // phase 1 only
 };
 
 // Per precision: chunk list ordered by CTA, and the CTA ranges.
@@ -96,8 +110,8 @@ struct ChunkPlan {
 
 struct PhasePlan {
   std::vector<Item> items;
-  int64_t n_elems = 0;  // size of the data array in elements
-  ChunkPlan cp[3];      // FP64, FP32, BF16
+  int64_t n_elems[3] = {0, 0, 0};  // size of the data array in elements, per precision
+  ChunkPlan cp[3];                 // FP64, FP32, BF16
 };
 
 struct OperatorPlan {
@@ -106,8 +120,10 @@ struct OperatorPlan {
   std::vector<int64_t> t_off;   // per LR block
   std::vector<float> scale_fr;  // BF16 scales per FR block
   std::vector<float> scale_a, scale_b;  // BF16 scales per LR block
+  std::vector<float> t_scale;   // BF16: per t entry, scale_a * scale_b of its block
   PhasePlan ph[2];
   int64_t n_panels = 0;
+  int64_t n_stacks = 0;
 };
 
 struct Problem {
@@ -122,18 +138,31 @@ struct Problem {
 // with a message on a malformed pattern.
 void build_operator(const Problem &p, bool transposed, OperatorPlan &op);
 
-// Computes BF16 per-block scales (max |entry|, 1 if the block is zero), and
-// checks that every entry is finite when check_finite is set.
+// Computes BF16 per-block scales (max |entry|, 1 if the block is zero) and the
+// per-t-entry scales, and checks that every entry is finite when check_finite.
 void compute_scales(const Problem &p, bool transposed, bool check_finite, OperatorPlan &op);
 
-// Splits every item into chunks for one precision (0 FP64, 1 FP32, 2 BF16) and
-// assigns items to `grid` CTAs (longest-processing-time first, cost = bytes).
+// Lays out every item for one precision (0 FP64, 1 FP32, 2 BF16), splits it
+// into chunks, and assigns items to `grid` CTAs (longest-processing-time
+// first, cost = bytes).
 void build_chunks(const Problem &p, bool transposed, int prec, int grid, OperatorPlan &op);
 
 // Writes the data of items [i_begin, i_end) of one phase, converted to the
-// precision, into dst (dst[0] is element `base` of the phase's array).
+// precision and in its layout, into dst (dst[0] is element `base` of the
+// phase's array).
 void fill_items(const Problem &p, bool transposed, const OperatorPlan &op, int phase, int prec, int64_t i_begin,
                 int64_t i_end, int64_t base, void *dst);
+
+// Element index of (row i, column c) of an item inside the item's data.
+inline int64_t item_index(int prec, int64_t hpad, int64_t i, int64_t c) {
+  if (prec == 2) return (c >> 3) * (8 * hpad) + (i >> 3) * 64 + (c & 7) * 8 + (i & 7);
+  return c * hpad + i;
+}
+// Elements an item occupies.
+inline int64_t item_elems(int prec, int64_t hpad, int64_t ncols) {
+  if (prec == 2) return ((ncols + 7) / 8) * 8 * hpad;
+  return ncols * hpad;
+}
 
 int esize_of(int prec);
 uint16_t to_bf16(float f);

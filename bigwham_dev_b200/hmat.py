@@ -221,7 +221,7 @@ class HmatGpu:
         f = _prec_flag(precision)
         A.check(self._lib.bw_plan_export(self._h, f, phase, int(transposed), C.byref(nc), None, C.byref(ne), None,
                                          C.byref(nt), None), self._h)
-        chunks = np.zeros((nc.value, 16), np.int32)
+        chunks = np.zeros((nc.value, 28), np.int32)
         cta = np.zeros(nt.value, np.int32)
         data = np.zeros(ne.value) if with_data else None
         A.check(self._lib.bw_plan_export(self._h, f, phase, int(transposed), C.byref(nc), chunks.ctypes.data,

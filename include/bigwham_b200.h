@@ -163,9 +163,10 @@ int bw_set_device_limit(bw_hmat *h, int64_t bytes);
 
 /* Host view of the built plan for one precision and phase (1: low-rank B
  * stage, 2: row panels), for inspection and testing.  Any output pointer may be
- * NULL; counts are always written.  chunks: n_chunks x 16 int32 words in the
- * layout documented in bw_layout.h; data: n_elems values converted to double
- * (BF16 values times nothing: the per-chunk scale is in the chunk words);
+ * NULL; counts are always written.  chunks: n_chunks x 28 int32 words in the
+ * layout of bw::Chunk (bigwham_dev_b200/csrc/bw_layout.h); data: n_elems values
+ * converted to double, in the precision's layout (column-major items for FP64 /
+ * FP32, 8x8 tiles for BF16; BF16 values divided by their block scale);
  * cta_ptr: grid+1 offsets.  Only valid on a handle finalized with BW_PLAN_ONLY. */
 int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_chunks,
                    int32_t *chunks, int64_t *n_elems, double *data, int64_t *n_cta, int32_t *cta_ptr);
@@ -182,6 +183,10 @@ int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs);
  * low-rank B factors (+ x, + t written), phase 2 reads the full blocks and the
  * A factors (+ y written).  Stored entries only: padding is not counted. */
 int bw_phase_bytes(const bw_hmat *h, int precision, int transposed, int64_t *phase1, int64_t *phase2);
+
+/* Per-t-entry output scales of phase 1 (BF16: scale(A) * scale(B) of the
+ * entry's low-rank block; 1 elsewhere), for inspection and testing. */
+int bw_plan_tscale(const bw_hmat *h, int transposed, int64_t *n, float *out);
 
 /* Release everything. */
 int bw_destroy(bw_hmat *h);

@@ -47,16 +47,22 @@ def test_plan_structure(golden):
             p = h.plan_export(prec, phase, with_data=False)
             cta = p["cta_ptr"]
             assert cta[0] == 0 and np.all(np.diff(cta) >= 0) and cta[-1] == len(p["chunks"])
-            seen_first = 0
+            open_item = False
             for w in p["chunks"]:
                 d = decode(w)
-                assert d["hpad"] % 2 == 0 and d["rows"] <= d["hpad"] <= 512
-                assert d["ncols"] * d["hpad"] * es <= 32768 and d["ncols"] <= 512
-                assert sum(n for _, n, _ in d["segs"]) == d["ncols"]
-                assert (d["data_off"] * es) % 4 == 0
-                seen_first += d["flags"] & 1
-            # one first chunk per item
-            assert seen_first == (info["n_lowrank"] if phase == 1 else info["n_panels"]) or phase == 1
+                assert d["hpad"] % 8 == 0 and d["rows"] <= d["hpad"] <= 512
+                cols = (d["ncols"] + 7) // 8 * 8 if prec == "bf16" else d["ncols"]
+                assert cols * d["hpad"] * es <= 32768 and d["ncols"] <= 512
+                assert sum(n for _, n, _, _ in d["segs"]) == d["ncols"]
+                assert (d["data_off"] * es) % 16 == 0  # every chunk starts 16-byte aligned
+                if prec == "bf16":
+                    assert d["data_off"] % (8 * d["hpad"]) % 64 == 0
+                else:
+                    assert all(sc == 1.0 for _, _, _, sc in d["segs"])
+                # chunks of one item are consecutive: FIRST opens, LAST closes
+                assert bool(d["flags"] & 1) != open_item
+                open_item = not (d["flags"] & 2)
+            assert not open_item
 
 
 def test_lpt_balance_on_many_items():
