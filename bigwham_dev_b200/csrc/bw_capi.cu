@@ -496,7 +496,7 @@ int bw_finalize(bw_hmat *h, int flags) {
       h->sum_rank += b.r;
     }
     for (int o = 0; o < (want_t ? 2 : 1); o++) {
-      bw::build_operator(h->prob, o == 1, h->op[o]);
+      bw::build_operator(h->prob, o == 1, h->grid, h->op[o]);
       bw::compute_scales(h->prob, o == 1, check && o == 0, h->op[o]);
       for (int p = 0; p < 3; p++)
         if (mask & (1 << p)) bw::build_chunks(h->prob, o == 1, p, h->grid, h->op[o]);
@@ -528,8 +528,9 @@ int bw_finalize(bw_hmat *h, int flags) {
           h->d_tscale[o] = static_cast<float *>(h->dmalloc(std::max<size_t>(1, ts.size()) * 4));
           BW_CUDA(cudaMemcpy(h->d_tscale[o], ts.data(), ts.size() * 4, cudaMemcpyHostToDevice));
         }
-      h->d_xp = h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8);
-      h->d_t = h->dmalloc((size_t)std::max<int64_t>(1, h->sum_rank) * 8);
+      // +16 bytes: the kernels stage vector segments in 16-byte aligned windows
+      h->d_xp = h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8 + 16);
+      h->d_t = h->dmalloc((size_t)std::max<int64_t>(1, h->sum_rank) * 8 + 16);
       h->d_xh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
       h->d_yh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
       h->d_err = static_cast<int *>(h->dmalloc(sizeof(int)));
@@ -606,8 +607,9 @@ int bw_matvec_static_scratch(bw_hmat *h, const double *x, double *y, int flags, 
     }
     // scratch: gathered x, then t at the next 256-byte boundary
     const int64_t gsize = p == 0 ? 8 : 4;
-    const int64_t t_at = (nin * gsize + 255) / 256 * 256;
-    const int64_t need = t_at + h->sum_rank * gsize;
+    // +16 bytes after each vector: segments are staged in 16-byte aligned windows
+    const int64_t t_at = (nin * gsize + 16 + 255) / 256 * 256;
+    const int64_t need = t_at + h->sum_rank * gsize + 16;
     if (need > (int64_t)BW_STATIC_SCRATCH_BYTES)
       throw std::invalid_argument("this H-matrix needs " + std::to_string(need) +
                                   " bytes of scratch, above the static maximum of " +

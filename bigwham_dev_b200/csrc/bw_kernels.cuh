@@ -2,9 +2,10 @@
 //
 // One persistent kernel per phase (see bw_layout.h).  Each CTA owns a fixed,
 // host-scheduled list of chunks.  Warp 0 is the producer: for every chunk it
-// stages the block data with one TMA bulk copy (cp.async.bulk, 16-byte aligned
-// window around the chunk) and gathers the chunk's vector values with
-// cp.async, into a ring of kStages shared-memory stages guarded by mbarriers.
+// stages the block data with one TMA bulk copy (cp.async.bulk of the 16-byte
+// aligned window around the chunk) and each of the chunk's <= 8 vector
+// segments (contiguous runs of x or t) with one more, into a ring of kStages
+// shared-memory stages; one mbarrier per stage counts the bytes.
 // Warps 1..8 are consumers and own the item's output rows:
 //  * FP64 / FP32: each thread owns 2 (FP64) or 4 (FP32) adjacent rows and a
 //    contiguous range of the chunk's columns and accumulates with FMAs;
@@ -91,17 +92,6 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ void cp_async_4(void *dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_8(void *dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-// Arrive on `bar` once this thread's earlier cp.async copies have landed
-// (counts against the barrier's expected arrivals).
-__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -164,7 +154,8 @@ template <> struct Store<Bf16> {
   static constexpr int kRows = 0;  // tensor-core path
 };
 
-// Partial sums of R adjacent rows over columns [c0, c1) of a column-major chunk.
+// Adds the partial sums of R adjacent rows over columns [c0, c1) of a
+// column-major chunk to o; the vector value of column c is g[c].
 template <typename S, int R>
 __device__ __forceinline__ void chunk_dot(const unsigned char *base, const typename Store<S>::G *g, int hv, int rv,
                                           int c0, int c1, typename Store<S>::G (&o)[R]);
@@ -193,8 +184,8 @@ __device__ __forceinline__ void chunk_dot<double, 2>(const unsigned char *base, 
     a0 = fma(w.x, g[c], a0);
     a1 = fma(w.y, g[c], a1);
   }
-  o[0] = a0 + b0;
-  o[1] = a1 + b1;
+  o[0] += a0 + b0;
+  o[1] += a1 + b1;
 }
 
 template <>
@@ -231,17 +222,18 @@ __device__ __forceinline__ void chunk_dot<float, 4>(const unsigned char *base, c
     a2 = fmaf(w.z, g[c], a2);
     a3 = fmaf(w.w, g[c], a3);
   }
-  o[0] = a0 + b0;
-  o[1] = a1 + b1;
-  o[2] = a2 + b2;
-  o[3] = a3 + b3;
+  o[0] += a0 + b0;
+  o[1] += a1 + b1;
+  o[2] += a2 + b2;
+  o[3] += a3 + b3;
 }
 
 // ----------------------------------------------------------------------------- shared memory
 template <typename S> struct SmemLayout {
   using G = typename Store<S>::G;
   static constexpr int kDataBytes = kStageBytes + 32;
-  static constexpr int kGBytes = kMaxCols * sizeof(G);
+  // gather area: each segment lands 16-byte aligned with up to 15 bytes of slack each side
+  static constexpr int kGBytes = kMaxCols * (int)sizeof(G) + kMaxSeg * 32;
   static constexpr int kStageSize = kDataBytes + kGBytes + (int)sizeof(Chunk);
   static constexpr int kRedPer = red_per_buf<G>();
   static constexpr int kRedBytes = 2 * kRedPer * (int)sizeof(G);
@@ -272,24 +264,58 @@ __device__ __forceinline__ void load_desc(const Chunk *chunks, int idx, int end,
   }
 }
 
-// Segment of chunk column c: index, first column, and source offset
-// (words 8..15: seg_off, 16..19: seg_cols pairs).
-__device__ __forceinline__ int seg_of(const uint32_t (&w)[kChunkWords], int nseg, int c, int &start, int &off) {
-  int acc = 0, sg = 0;
-  start = 0;
-  off = static_cast<int>(w[8]);
+// Gather layout of a chunk's segments.  Segment k is the contiguous run
+// src_k[0 .. cols_k) of x or t; it is staged by one bulk copy of the 16-byte
+// aligned window around it, placed at byte goff_k of the stage's gather area,
+// so column c of the chunk (start_k <= c < start_k + cols_k) is element
+// gbase_k + (c - start_k) of the area.
+struct SegTable {
+  int n;
+  int start[kMaxSeg], cols[kMaxSeg], gbase[kMaxSeg];
+  float scale[kMaxSeg];
+  int total;  // bytes of all windows
+};
+// Source windows, needed by the producer only.
+struct SegCopies {
+  unsigned long long lo[kMaxSeg];  // source window start (16-byte aligned)
+  int bytes[kMaxSeg], goff[kMaxSeg];
+};
+
+// w: descriptor words (8..15 seg_off, 16..19 seg_cols pairs, 20..27 seg_scale).
+template <typename G, typename Words>
+__device__ __forceinline__ void seg_table(const Words &w, const G *xs, const G *ts, SegTable &t,
+                                          SegCopies *cp = nullptr) {
+  const uint32_t flags = w[6];
+  t.n = static_cast<int>((flags >> 8) & 0xfu);
+  int start = 0, goff = 0;
 #pragma unroll
   for (int k = 0; k < kMaxSeg; k++) {
-    const int ck = static_cast<int>((w[16 + (k >> 1)] >> ((k & 1) * 16)) & 0xffffu);
-    if (k < nseg && c >= acc) {
-      sg = k;
-      start = acc;
-      off = static_cast<int>(w[8 + k]);
+    const int ck = k < t.n ? static_cast<int>((w[16 + (k >> 1)] >> ((k & 1) * 16)) & 0xffffu) : 0;
+    const G *src = ((flags >> (16 + k)) & 1u) ? ts : xs;
+    const unsigned long long a = reinterpret_cast<unsigned long long>(src + static_cast<int>(w[8 + k]));
+    const unsigned long long lo = a & ~15ull;
+    const unsigned long long hi = (a + static_cast<unsigned long long>(ck) * sizeof(G) + 15ull) & ~15ull;
+    const int bytes = ck > 0 ? static_cast<int>(hi - lo) : 0;
+    t.start[k] = start;
+    t.cols[k] = ck;
+    t.gbase[k] = (goff + static_cast<int>(a - lo)) / static_cast<int>(sizeof(G));
+    t.scale[k] = __uint_as_float(w[20 + k]);
+    if (cp) {
+      cp->lo[k] = lo;
+      cp->bytes[k] = bytes;
+      cp->goff[k] = goff;
     }
-    acc += ck;
+    start += ck;
+    goff += bytes;
   }
-  return sg;
+  t.total = goff;
 }
+
+// Words of a descriptor copied into shared memory.
+struct SmemWords {
+  const uint32_t *p;
+  __device__ __forceinline__ uint32_t operator[](int i) const { return p[i]; }
+};
 
 template <typename S>
 __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a) {
@@ -307,7 +333,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&full[s], 33);                 // lane-0 arrive(.expect_tx) + 32 cp.async arrivals
+      mbar_init(&full[s], 1);                  // lane-0 arrive.expect_tx; the bulk copies complete the tx
       mbar_init(&empty[s], kConsumerWarps);    // one arrival per consumer warp
     }
     mbar_init(redbar, kConsumerWarps);
@@ -346,43 +372,41 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
         const int ncols = static_cast<int>(w[2]);
         const int hpad = static_cast<int>(w[3]);
-        const uint32_t flags = w[6];
         unsigned char *st = stage0 + s * L::kStageSize;
-        G *gs = reinterpret_cast<G *>(st + L::kDataBytes);
+        unsigned char *garea = st + L::kDataBytes;
+        SegTable tab;
+        SegCopies cpy;
+        seg_table<G>(w, xs, ts, tab, &cpy);
+        const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
+                                                : static_cast<unsigned long long>(ncols);
+        const unsigned long long bytes = cols * hpad * es;
+        const bool good = ncols > 0 && ncols <= kMaxCols && bytes <= static_cast<unsigned long long>(kStageBytes) &&
+                          tab.total <= L::kGBytes;
+        const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
+                                       static_cast<unsigned long long>(data_off) * es;
+        const unsigned long long lo = src & ~15ull;
+        const unsigned long long hi = (src + bytes + 15ull) & ~15ull;
         if (lane == 0) {
           uint4 *dd = reinterpret_cast<uint4 *>(st + L::kDataBytes + L::kGBytes);
 #pragma unroll
           for (int q = 0; q < kChunkWords / 4; q++)
             dd[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-          const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
-                                                  : static_cast<unsigned long long>(ncols);
-          const unsigned long long bytes = cols * hpad * es;
-          if (ncols > 0 && bytes <= static_cast<unsigned long long>(kStageBytes)) {
-            const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
-                                           static_cast<unsigned long long>(data_off) * es;
-            const unsigned long long lo = src & ~15ull;
-            const unsigned long long hi = (src + bytes + 15ull) & ~15ull;
-            mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>(hi - lo));
-            bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
+          if (good) {
+            mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>(hi - lo) + static_cast<uint32_t>(tab.total));
           } else {
             if (ncols > 0) set_error(a.err, kErrBadChunk);
             mbar_arrive(&full[s]);
           }
         }
-        // gather the chunk's vector values
-        const int nseg = static_cast<int>((flags >> 8) & 0xfu);
-        const int gcols = ncols <= kMaxCols ? ncols : 0;
-        for (int c = lane; c < gcols; c += 32) {
-          int start, off;
-          const int sg = seg_of(w, nseg, c, start, off);
-          const G *src = ((flags >> (16 + sg)) & 1u) ? ts : xs;
-          const G *p = src + off + (c - start);
-          if (sizeof(G) == 8)
-            cp_async_8(gs + c, p);
-          else
-            cp_async_4(gs + c, p);
+        __syncwarp();
+        if (good) {
+          if (lane == 0) bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
+#pragma unroll
+          for (int k = 0; k < kMaxSeg; k++)
+            if (lane == k + 1 && cpy.bytes[k] > 0)
+              bulk_g2s(garea + cpy.goff[k], reinterpret_cast<const void *>(cpy.lo[k]),
+                       static_cast<uint32_t>(cpy.bytes[k]), &full[s]);
         }
-        cp_async_arrive_noinc(&full[s]);
         issued++;
       }
     }
@@ -426,6 +450,9 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
     const unsigned char *st = stage0 + s * L::kStageSize;
     const G *gs = reinterpret_cast<const G *>(st + L::kDataBytes);
     const Chunk &d = *reinterpret_cast<const Chunk *>(st + L::kDataBytes + L::kGBytes);
+    SegTable tab;
+    seg_table<G>(SmemWords{reinterpret_cast<const uint32_t *>(&d)}, static_cast<const G *>(a.xsrc),
+                 static_cast<const G *>(a.tsrc), tab);
     const uint32_t flags = d.flags;
     const int ncols = d.ncols;
     const int hpad = d.hpad;
@@ -443,10 +470,12 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
       if (active && ncols > 0 && ncols <= kMaxCols) {
         const int c0 = (cq * ncols) / Q, c1 = ((cq + 1) * ncols) / Q;
         const int soff = static_cast<int>((static_cast<unsigned long long>(d.data_off) * es) & 15ull);
-        G p[R];
-        chunk_dot<S, R>(st + soff, gs, hv, rv, c0, c1, p);
 #pragma unroll
-        for (int r = 0; r < R; r++) acc[r] += p[r];
+        for (int k = 0; k < kMaxSeg; k++) {
+          const int lo_c = max(c0, tab.start[k]), hi_c = min(c1, tab.start[k] + tab.cols[k]);
+          if (k < tab.n && lo_c < hi_c)
+            chunk_dot<S, R>(st + soff, gs + tab.gbase[k] - tab.start[k], hv, rv, lo_c, hi_c, acc);
+        }
       }
     } else {
       if (flags & kFirst) {
@@ -467,18 +496,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         const uint32_t sbase = smem_u32(st);  // BF16 chunks start 16-byte aligned (offset 0)
         const int nks = (ncols + 15) >> 4;
         const int mat = lane >> 3, mr = lane & 7;
-        // per-column BF16 block scale: segment ends and scales of this chunk
-        int send[kMaxSeg];
-        float sscl[kMaxSeg];
-        {
-          int acc_c = 0;
-#pragma unroll
-          for (int k = 0; k < kMaxSeg; k++) {
-            acc_c += k < nseg ? static_cast<int>(d.seg_cols[k]) : 0;
-            send[k] = k < nseg ? acc_c : 0x7fffffff;
-            sscl[k] = d.seg_scale[k];
-          }
-        }
+        (void)nseg;
         for (int ks = kp; ks < nks; ks += kparts) {
           // B fragment: lanes 0-3 hold the BF16-rounded vector (column 0),
           // lanes 4-7 the BF16-rounded remainder (column 1), others zero.
@@ -490,11 +508,15 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
               const int c = 16 * ks + 2 * tq + (e & 1) + (e >> 1) * 8;
               float x = 0.f;
               if (c < ncols) {
-                float sc = sscl[0];
+                float sc = tab.scale[0];
+                int gi = tab.gbase[0] + c;
 #pragma unroll
                 for (int k = 1; k < kMaxSeg; k++)
-                  if (c >= send[k - 1]) sc = sscl[k];
-                x = gs[c] * sc;
+                  if (k < tab.n && c >= tab.start[k]) {
+                    sc = tab.scale[k];
+                    gi = tab.gbase[k] + c - tab.start[k];
+                  }
+                x = gs[gi] * sc;
               }
               const float hi = __bfloat162float(__float2bfloat16_rn(x));
               v[e] = grp == 0 ? hi : x - hi;

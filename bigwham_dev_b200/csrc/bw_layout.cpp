@@ -70,7 +70,7 @@ int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 
 }  // namespace
 
-void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
+void build_operator(const Problem &p, bool tr, int grid, OperatorPlan &op) {
   const int64_t n_out = tr ? p.n_cols : p.n_rows;
   const int64_t n_in = tr ? p.n_rows : p.n_cols;
   op = OperatorPlan{};
@@ -112,13 +112,19 @@ void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
   op.t_len = t;
   if (t > INT32_MAX) fail("sum of ranks above 2^31-1");
   op.n_stacks = (int64_t)stacks.size();
+  grid = std::max(1, grid);
+  int64_t e1 = 0;  // phase-1 entries
+  for (size_t k = 0; k < nlr; k++) e1 += p.lr[k].r * eff_low(p, tr, k).n;
+  const int64_t cap1 = std::max<int64_t>(1, e1 / grid / kItemsPerCta);
   PhasePlan &p1 = op.ph[0];
   for (auto &kv : stacks) {
     const int64_t j0 = kv.first.first, n = kv.first.second;
     int64_t R = 0;
     for (int64_t k : kv.second) R += eff_low(p, tr, k).r;
-    // equal cuts of at most kHMax rows, multiples of kRowAlign except the last
-    const int64_t nit = (R + kHMax - 1) / kHMax;
+    // equal cuts of at most kHMax rows (fewer when n is wide, so no item holds
+    // more than cap1 entries; at least 16 rows), multiples of kRowAlign
+    const int64_t rmax = std::min<int64_t>(kHMax, std::max<int64_t>(16, (cap1 / n) / 16 * 16));
+    const int64_t nit = (R + rmax - 1) / rmax;
     const int64_t cut = align_up((R + nit - 1) / nit, kRowAlign);
     size_t bi = 0;      // block of the stack
     int64_t br = 0;     // next row inside that block
@@ -209,29 +215,43 @@ void build_operator(const Problem &p, bool tr, OperatorPlan &op) {
            std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
   }
 
-  // ---- phase 2 items: one per panel; FR slices first (they do not depend on t)
+  // ---- phase 2 items: one per panel (FR slices first: they do not depend on
+  // t); panels holding more than cap2 entries are cut into row parts
   PhasePlan &p2 = op.ph[1];
+  int64_t e2 = 0;
+  std::vector<int64_t> pw(npan, 0);
   for (size_t q = 0; q < npan; q++) {
-    Item it;
-    it.h = static_cast<int32_t>(pb[q + 1] - pb[q]);
-    it.hpad = static_cast<int32_t>(align_up(it.h, kRowAlign));
-    it.out_off = static_cast<int32_t>(pb[q]);
-    for (int pass = 0; pass < 2; pass++) {
-      for (const Cover &e : cov[q]) {
-        if (e.kind != pass) continue;
-        if (e.kind == 0) {
-          EffFull b = eff_full(p, tr, e.k);
-          it.segs.push_back({0, e.k, pb[q] - b.i0, b.n, 0, b.j0});
-          it.ncols += b.n;
-        } else {
-          EffLow b = eff_low(p, tr, e.k);
-          if (b.r == 0) continue;
-          it.segs.push_back({1, e.k, pb[q] - b.i0, b.r, 1, op.t_off[e.k]});
-          it.ncols += b.r;
+    for (const Cover &e : cov[q]) pw[q] += e.kind == 0 ? e.n : eff_low(p, tr, e.k).r;
+    e2 += pw[q] * (pb[q + 1] - pb[q]);
+  }
+  const int64_t cap2 = std::max<int64_t>(1, e2 / grid / kItemsPerCta);
+  for (size_t q = 0; q < npan; q++) {
+    const int64_t H = pb[q + 1] - pb[q];
+    int64_t parts = 1;
+    if (pw[q] > 0 && H * pw[q] > cap2) parts = std::min<int64_t>((H * pw[q] + cap2 - 1) / cap2, std::max<int64_t>(1, H / 16));
+    const int64_t cut = align_up((H + parts - 1) / parts, kRowAlign);
+    for (int64_t r0 = 0; r0 < H; r0 += cut) {
+      Item it;
+      it.h = static_cast<int32_t>(std::min<int64_t>(cut, H - r0));
+      it.hpad = static_cast<int32_t>(align_up(it.h, kRowAlign));
+      it.out_off = static_cast<int32_t>(pb[q] + r0);
+      for (int pass = 0; pass < 2; pass++) {
+        for (const Cover &e : cov[q]) {
+          if (e.kind != pass) continue;
+          if (e.kind == 0) {
+            EffFull b = eff_full(p, tr, e.k);
+            it.segs.push_back({0, e.k, pb[q] + r0 - b.i0, b.n, 0, b.j0});
+            it.ncols += b.n;
+          } else {
+            EffLow b = eff_low(p, tr, e.k);
+            if (b.r == 0) continue;
+            it.segs.push_back({1, e.k, pb[q] + r0 - b.i0, b.r, 1, op.t_off[e.k]});
+            it.ncols += b.r;
+          }
         }
       }
+      p2.items.push_back(std::move(it));
     }
-    p2.items.push_back(std::move(it));
   }
 }
 

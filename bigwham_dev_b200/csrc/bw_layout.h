@@ -37,6 +37,7 @@ constexpr int kMaxSeg = 8;           // gather segments per chunk (>= 8: any 8 c
 constexpr int kHMax = 512;           // max padded rows of one item
 constexpr int kRowAlign = 8;         // padded rows are a multiple of this
 constexpr int kItemAlign = 64;       // item start alignment, in elements
+constexpr int kItemsPerCta = 8;      // minimum items per CTA share (load balance)
 
 // Chunk flags
 constexpr uint32_t kFirst = 1u;      // first chunk of an item: reset accumulators
@@ -136,7 +137,9 @@ struct Problem {
 // Validates the pattern and builds the structural plan (items) of the operator
 // (transposed = true builds H^T from the same blocks).  Throws std::runtime_error
 // with a message on a malformed pattern.
-void build_operator(const Problem &p, bool transposed, OperatorPlan &op);
+// Items are cut so that none holds more than 1/kItemsPerCta of the average
+// per-CTA share of `grid` CTAs (static scheduling needs fine grains).
+void build_operator(const Problem &p, bool transposed, int grid, OperatorPlan &op);
 
 // Computes BF16 per-block scales (max |entry|, 1 if the block is zero) and the
 // per-t-entry scales, and checks that every entry is finite when check_finite.
