@@ -45,6 +45,7 @@ _SIGS = {
     "bw_timing_read": (C.c_int, [_P, _P, _P]),
     "bw_phase_bytes": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
     "bw_plan_tscale": (C.c_int, [_P, C.c_int, _P, _P]),
+    "bw_plan_gather": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
     "bw_destroy": (C.c_int, [_P]),
     "bw_version": (C.c_char_p, []),
 }

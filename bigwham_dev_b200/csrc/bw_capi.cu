@@ -49,12 +49,18 @@ int prec_index(int flags) {
   return -1;
 }
 
+// launches of one matvec: x gather, phase 1, G2 gather, phase 2
+constexpr int kTimedLaunches = 4;
+constexpr size_t kEv = kTimedLaunches + 1;
+
 struct DevPhase {
   void *data = nullptr;
   Chunk *chunks = nullptr;
   int32_t *cta = nullptr;
+  bw::GatherSeg *gsegs = nullptr;  // phase 2: runs that fill G2
   int64_t n_chunks = 0;
   int64_t n_elems = 0;
+  int64_t n_gsegs = 0;
 };
 
 }  // namespace
@@ -75,7 +81,7 @@ struct bw_hmat {
   std::vector<unsigned char> host_data[2][3][2];  // BW_PLAN_ONLY
   int32_t *d_perm0 = nullptr, *d_perm1 = nullptr;
   float *d_tscale[2] = {nullptr, nullptr};  // BF16 per-t-entry scales, per operator
-  void *d_xp = nullptr, *d_t = nullptr;
+  void *d_xp = nullptr, *d_t = nullptr, *d_g2 = nullptr;
   double *d_xh = nullptr, *d_yh = nullptr;
   int *d_err = nullptr;
   int *h_err = nullptr;    // pinned
@@ -88,22 +94,22 @@ struct bw_hmat {
   long long spin_limit = 2000000000LL;  // 2 s bound on every in-kernel wait
   // optional per-launch timing (bw_set_timing / bw_timing_read)
   bool timing = false;
-  std::vector<cudaEvent_t> ev_pool;     // 4 events per recorded matvec
+  std::vector<cudaEvent_t> ev_pool;     // kTimedLaunches + 1 events per recorded matvec
   size_t ev_used = 0;                   // matvecs recorded since the last read
 
   cudaEvent_t *timing_slot() {
     if (!timing) return nullptr;
     const size_t kMax = 200000;
     if (ev_used >= kMax) return nullptr;
-    if (4 * (ev_used + 1) > ev_pool.size()) {
-      const size_t grow = std::max<size_t>(64, ev_pool.size() / 4);
-      for (size_t i = 0; i < 4 * grow; i++) {
+    if (kEv * (ev_used + 1) > ev_pool.size()) {
+      const size_t grow = std::max<size_t>(64, ev_pool.size() / kEv);
+      for (size_t i = 0; i < kEv * grow; i++) {
         cudaEvent_t e;
         if (cudaEventCreate(&e) != cudaSuccess) throw CudaError("cudaEventCreate failed");
         ev_pool.push_back(e);
       }
     }
-    return &ev_pool[4 * ev_used++];
+    return &ev_pool[kEv * ev_used++];
   }
 
   void *dmalloc(size_t bytes) {
@@ -126,6 +132,7 @@ struct bw_hmat {
           cudaFree(ph.data);
           cudaFree(ph.chunks);
           cudaFree(ph.cta);
+          cudaFree(ph.gsegs);
           ph = DevPhase{};
         }
     cudaFree(d_perm0);
@@ -135,6 +142,7 @@ struct bw_hmat {
     d_tscale[0] = d_tscale[1] = nullptr;
     cudaFree(d_xp);
     cudaFree(d_t);
+    cudaFree(d_g2);
     cudaFree(d_xh);
     cudaFree(d_yh);
     cudaFree(d_err);
@@ -144,7 +152,7 @@ struct bw_hmat {
     ev_used = 0;
     if (stream) cudaStreamDestroy(stream);
     d_perm0 = d_perm1 = nullptr;
-    d_xp = d_t = nullptr;
+    d_xp = d_t = d_g2 = nullptr;
     d_xh = d_yh = nullptr;
     d_err = nullptr;
     h_err = nullptr;
@@ -189,6 +197,15 @@ template <typename S> void set_smem_attr() {
   if (dev < 64) done[dev] = true;
 }
 
+// Bytes of the phase-2 gather array G2 over the stored precisions and operators.
+int64_t g2_bytes(const bw_hmat *h, int mask, bool with_t) {
+  int64_t b = 0;
+  for (int o = 0; o < (with_t ? 2 : 1); o++)
+    for (int p = 0; p < 3; p++)
+      if (mask & (1 << p)) b = std::max<int64_t>(b, h->op[o].ph[1].cp[p].g_len * (p == 0 ? 8 : 4));
+  return b;
+}
+
 // Upload the data of one phase in pieces through two pinned staging buffers.
 void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   const bw::OperatorPlan &op = h->op[o];
@@ -198,6 +215,7 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   dp.n_elems = ph.n_elems[prec];
   const bw::ChunkPlan &cp = ph.cp[prec];
   dp.n_chunks = (int64_t)cp.chunks.size();
+  dp.n_gsegs = (int64_t)cp.gsegs.size();
   if (h->plan_only) {
     auto &buf = h->host_data[o][prec][phase];
     buf.assign((size_t)ph.n_elems[prec] * es, 0);
@@ -210,6 +228,11 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   if (!cp.chunks.empty())
     BW_CUDA(cudaMemcpy(dp.chunks, cp.chunks.data(), cp.chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
   BW_CUDA(cudaMemcpy(dp.cta, cp.cta_ptr.data(), cp.cta_ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  dp.n_gsegs = (int64_t)cp.gsegs.size();
+  if (dp.n_gsegs) {
+    dp.gsegs = static_cast<bw::GatherSeg *>(h->dmalloc(cp.gsegs.size() * sizeof(bw::GatherSeg)));
+    BW_CUDA(cudaMemcpy(dp.gsegs, cp.gsegs.data(), cp.gsegs.size() * sizeof(bw::GatherSeg), cudaMemcpyHostToDevice));
+  }
 
   const size_t kPiece = size_t(256) << 20;
   unsigned char *stage[2] = {nullptr, nullptr};
@@ -272,16 +295,20 @@ void compute_diagonal(bw_hmat *h) {
   }
 }
 
+// The four launches of one matvec: x gather (+ permutation), phase 1 (t),
+// G2 gather, phase 2 (y), with the given scratch vectors; `ev` (optional)
+// receives kTimedLaunches + 1 events around them.
 template <typename S>
-void launch_matvec(bw_hmat *h, int o, int prec, const double *x, double *y, bool permuted, cudaStream_t st) {
+void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y, bool permuted, cudaStream_t st,
+                        void *xp_buf, void *t_buf, void *g2_buf, cudaEvent_t *ev) {
   using G = typename bw::Store<S>::G;
   const bw::OperatorPlan &op = h->op[o];
   const int32_t *perm_in = permuted ? nullptr : (o == 0 ? h->d_perm1 : h->d_perm0);
   const int32_t *perm_out = permuted ? nullptr : (o == 0 ? h->d_perm0 : h->d_perm1);
   const int n_in = (int)op.n_in;
-  G *xp = static_cast<G *>(h->d_xp);
-  G *t = static_cast<G *>(h->d_t);
-  cudaEvent_t *ev = h->timing_slot();
+  G *xp = static_cast<G *>(xp_buf);
+  G *t = static_cast<G *>(t_buf);
+  G *g2 = static_cast<G *>(g2_buf);
   if (ev) BW_CUDA(cudaEventRecord(ev[0], st));
   if (n_in > 0) {
     bw::gather_x_kernel<G><<<(n_in + 255) / 256, 256, 0, st>>>(x, xp, perm_in, h->dof, n_in);
@@ -291,28 +318,39 @@ void launch_matvec(bw_hmat *h, int o, int prec, const double *x, double *y, bool
   set_smem_attr<S>();
   for (int phase = 0; phase < 2; phase++) {
     const DevPhase &dp = h->dev[o][prec][phase];
-    if (dp.n_chunks == 0) {
-      if (ev) BW_CUDA(cudaEventRecord(ev[2 + phase], st));
-      continue;
+    if (phase == 1) {
+      if (dp.n_gsegs > 0) {
+        const int per_block = 8;  // runs per 256-thread block (one warp each)
+        bw::gather_g2_kernel<G><<<(int)((dp.n_gsegs + per_block - 1) / per_block), 256, 0, st>>>(
+            dp.gsegs, (int)dp.n_gsegs, xp, t, g2);
+        BW_CUDA(cudaGetLastError());
+      }
+      if (ev) BW_CUDA(cudaEventRecord(ev[3], st));
     }
-    bw::StreamArgs a{};
-    a.data = dp.data;
-    a.chunks = dp.chunks;
-    a.cta_ptr = dp.cta;
-    a.xsrc = xp;
-    a.tsrc = t;
-    a.t_out = t;
-    a.t_scale = prec == 2 ? h->d_tscale[o] : nullptr;
-    a.y_out = y;
-    a.perm_out = perm_out;
-    a.dof = h->dof;
-    a.phase = phase + 1;
-    a.err = h->d_err;
-    a.spin_limit = h->spin_limit;
-    bw::stream_panels_kernel<S><<<h->grid, bw::kThreads, bw::SmemLayout<S>::kTotal, st>>>(a);
-    BW_CUDA(cudaGetLastError());
-    if (ev) BW_CUDA(cudaEventRecord(ev[2 + phase], st));
+    if (dp.n_chunks > 0) {
+      bw::StreamArgs a{};
+      a.data = dp.data;
+      a.chunks = dp.chunks;
+      a.cta_ptr = dp.cta;
+      a.gsrc = phase == 0 ? static_cast<const void *>(xp) : static_cast<const void *>(g2);
+      a.t_out = t;
+      a.t_scale = prec == 2 ? h->d_tscale[o] : nullptr;
+      a.y_out = y;
+      a.perm_out = perm_out;
+      a.dof = h->dof;
+      a.phase = phase + 1;
+      a.err = h->d_err;
+      a.spin_limit = h->spin_limit;
+      bw::stream_panels_kernel<S><<<h->grid, bw::kThreads, bw::SmemLayout<S>::kTotal, st>>>(a);
+      BW_CUDA(cudaGetLastError());
+    }
+    if (ev) BW_CUDA(cudaEventRecord(ev[phase == 0 ? 2 : 4], st));
   }
+}
+
+template <typename S>
+void launch_matvec(bw_hmat *h, int o, int prec, const double *x, double *y, bool permuted, cudaStream_t st) {
+  launch_matvec_impl<S>(h, o, prec, x, y, permuted, st, h->d_xp, h->d_t, h->d_g2, h->timing_slot());
 }
 
 // ----------------------------------------------------------------------------
@@ -347,43 +385,11 @@ void *static_scratch_ptr(int device) {
   return g_static_ptr[device];
 }
 
-// The three launches of one matvec with caller-provided scratch pointers
-// (same kernels and arguments as launch_matvec).
+// One matvec with its scratch vectors in the static array (no timing).
 template <typename S>
 void launch_matvec_on(bw_hmat *h, int o, int prec, const double *x, double *y, bool permuted, cudaStream_t st,
-                      void *xp_buf, void *t_buf) {
-  using G = typename bw::Store<S>::G;
-  const bw::OperatorPlan &op = h->op[o];
-  const int32_t *perm_in = permuted ? nullptr : (o == 0 ? h->d_perm1 : h->d_perm0);
-  const int32_t *perm_out = permuted ? nullptr : (o == 0 ? h->d_perm0 : h->d_perm1);
-  const int n_in = (int)op.n_in;
-  G *xp = static_cast<G *>(xp_buf);
-  G *t = static_cast<G *>(t_buf);
-  if (n_in > 0) {
-    bw::gather_x_kernel<G><<<(n_in + 255) / 256, 256, 0, st>>>(x, xp, perm_in, h->dof, n_in);
-    BW_CUDA(cudaGetLastError());
-  }
-  set_smem_attr<S>();
-  for (int phase = 0; phase < 2; phase++) {
-    const DevPhase &dp = h->dev[o][prec][phase];
-    if (dp.n_chunks == 0) continue;
-    bw::StreamArgs a{};
-    a.data = dp.data;
-    a.chunks = dp.chunks;
-    a.cta_ptr = dp.cta;
-    a.xsrc = xp;
-    a.tsrc = t;
-    a.t_out = t;
-    a.t_scale = prec == 2 ? h->d_tscale[o] : nullptr;
-    a.y_out = y;
-    a.perm_out = perm_out;
-    a.dof = h->dof;
-    a.phase = phase + 1;
-    a.err = h->d_err;
-    a.spin_limit = h->spin_limit;
-    bw::stream_panels_kernel<S><<<h->grid, bw::kThreads, bw::SmemLayout<S>::kTotal, st>>>(a);
-    BW_CUDA(cudaGetLastError());
-  }
+                      void *xp_buf, void *t_buf, void *g2_buf) {
+  launch_matvec_impl<S>(h, o, prec, x, y, permuted, st, xp_buf, t_buf, g2_buf, nullptr);
 }
 
 }  // namespace
@@ -510,7 +516,8 @@ int bw_finalize(bw_hmat *h, int flags) {
           if (mask & (1 << p))
             for (int ph = 0; ph < 2; ph++)
               need += h->op[o].ph[ph].n_elems[p] * bw::esize_of(p) +
-                      (int64_t)h->op[o].ph[ph].cp[p].chunks.size() * (int64_t)sizeof(Chunk);
+                      (int64_t)h->op[o].ph[ph].cp[p].chunks.size() * (int64_t)sizeof(Chunk) +
+                      (int64_t)h->op[o].ph[ph].cp[p].gsegs.size() * (int64_t)sizeof(bw::GatherSeg);
       if (h->dev_limit > 0 && need > h->dev_limit)
         throw OomError("layout needs " + std::to_string(need) + " device bytes, above the configured limit of " +
                        std::to_string(h->dev_limit));
@@ -531,6 +538,7 @@ int bw_finalize(bw_hmat *h, int flags) {
       // +16 bytes: the kernels stage vector segments in 16-byte aligned windows
       h->d_xp = h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8 + 16);
       h->d_t = h->dmalloc((size_t)std::max<int64_t>(1, h->sum_rank) * 8 + 16);
+      h->d_g2 = h->dmalloc((size_t)std::max<int64_t>(1, g2_bytes(h, mask, want_t)) + 16);
       h->d_xh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
       h->d_yh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
       h->d_err = static_cast<int *>(h->dmalloc(sizeof(int)));
@@ -605,11 +613,14 @@ int bw_matvec_static_scratch(bw_hmat *h, const double *x, double *y, int flags, 
       const char *xb = reinterpret_cast<const char *>(x), *yb = reinterpret_cast<const char *>(y);
       if (xb < yb + nout * 8 && yb < xb + nin * 8) throw std::invalid_argument("x and y overlap");
     }
-    // scratch: gathered x, then t at the next 256-byte boundary
+    // scratch: gathered x, t and the gather array G2, each at a 256-byte
+    // boundary with 16 bytes of slack (vector runs are staged in 16-byte
+    // aligned windows)
     const int64_t gsize = p == 0 ? 8 : 4;
-    // +16 bytes after each vector: segments are staged in 16-byte aligned windows
+    const int o_ = tr ? 1 : 0;
     const int64_t t_at = (nin * gsize + 16 + 255) / 256 * 256;
-    const int64_t need = t_at + h->sum_rank * gsize + 16;
+    const int64_t g2_at = (t_at + h->sum_rank * gsize + 16 + 255) / 256 * 256;
+    const int64_t need = g2_at + h->op[o_].ph[1].cp[p].g_len * gsize + 16;
     if (need > (int64_t)BW_STATIC_SCRATCH_BYTES)
       throw std::invalid_argument("this H-matrix needs " + std::to_string(need) +
                                   " bytes of scratch, above the static maximum of " +
@@ -621,11 +632,11 @@ int bw_matvec_static_scratch(bw_hmat *h, const double *x, double *y, int flags, 
     const bool perm = (flags & BW_PERMUTED) != 0;
     const int o = tr ? 1 : 0;
     if (p == 0)
-      launch_matvec_on<double>(h, o, 0, x, y, perm, st, base, base + t_at);
+      launch_matvec_on<double>(h, o, 0, x, y, perm, st, base, base + t_at, base + g2_at);
     else if (p == 1)
-      launch_matvec_on<float>(h, o, 1, x, y, perm, st, base, base + t_at);
+      launch_matvec_on<float>(h, o, 1, x, y, perm, st, base, base + t_at, base + g2_at);
     else
-      launch_matvec_on<bw::Bf16>(h, o, 2, x, y, perm, st, base, base + t_at);
+      launch_matvec_on<bw::Bf16>(h, o, 2, x, y, perm, st, base, base + t_at, base + g2_at);
     return BW_OK;
   });
 }
@@ -794,14 +805,14 @@ int bw_set_timing(bw_hmat *h, int enable) {
 int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs) {
   if (!h || !ms) return BW_ERR_ARG;
   return guarded(h, [&] {
-    ms[0] = ms[1] = ms[2] = 0.0;
+    for (int k = 0; k < kTimedLaunches; k++) ms[k] = 0.0;
     if (h->ev_used > 0) {
       BW_CUDA(cudaSetDevice(h->device));
-      BW_CUDA(cudaEventSynchronize(h->ev_pool[4 * h->ev_used - 1]));
+      BW_CUDA(cudaEventSynchronize(h->ev_pool[kEv * h->ev_used - 1]));
       for (size_t i = 0; i < h->ev_used; i++)
-        for (int k = 0; k < 3; k++) {
+        for (int k = 0; k < kTimedLaunches; k++) {
           float v = 0.0f;
-          BW_CUDA(cudaEventElapsedTime(&v, h->ev_pool[4 * i + k], h->ev_pool[4 * i + k + 1]));
+          BW_CUDA(cudaEventElapsedTime(&v, h->ev_pool[kEv * i + k], h->ev_pool[kEv * i + k + 1]));
           ms[k] += v;
         }
     }
@@ -827,6 +838,18 @@ int bw_phase_bytes(const bw_hmat *h, int precision, int transposed, int64_t *pha
   *phase1 = e[0] * es + 8 * h->op[o].n_in;
   *phase2 = e[1] * es + 8 * h->op[o].n_out;
   if (p == 2) *phase2 += 4 * ((int64_t)h->op[o].scale_fr.size() + 2 * (int64_t)h->op[o].scale_a.size());
+  return BW_OK;
+}
+
+int bw_plan_gather(const bw_hmat *h, int precision, int transposed, int64_t *n, int32_t *runs) {
+  if (!h || !n) return BW_ERR_ARG;
+  const int p = prec_index(precision);
+  if (p < 0 || !h->finalized || !(h->stored & (1 << p))) return BW_ERR_STATE;
+  const int o = transposed ? 1 : 0;
+  if (o == 1 && !h->has_t) return BW_ERR_UNSUPPORTED;
+  const std::vector<bw::GatherSeg> &g = h->op[o].ph[1].cp[p].gsegs;
+  *n = (int64_t)g.size();
+  if (runs) std::memcpy(runs, g.data(), g.size() * sizeof(bw::GatherSeg));
   return BW_OK;
 }
 

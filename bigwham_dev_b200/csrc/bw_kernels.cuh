@@ -2,10 +2,10 @@
 //
 // One persistent kernel per phase (see bw_layout.h).  Each CTA owns a fixed,
 // host-scheduled list of chunks.  Warp 0 is the producer: for every chunk it
-// stages the block data with one TMA bulk copy (cp.async.bulk of the 16-byte
-// aligned window around the chunk) and each of the chunk's <= 8 vector
-// segments (contiguous runs of x or t) with one more, into a ring of kStages
-// shared-memory stages; one mbarrier per stage counts the bytes.
+// stages the block data and the chunk's contiguous run of vector values with
+// two TMA bulk copies (cp.async.bulk of the 16-byte aligned windows around
+// them) into a ring of kStages shared-memory stages; one mbarrier per stage
+// counts the bytes, one more per stage returns it to the producer.
 // Warps 1..8 are consumers and own the item's output rows:
 //  * FP64 / FP32: each thread owns 2 (FP64) or 4 (FP32) adjacent rows and a
 //    contiguous range of the chunk's columns and accumulates with FMAs;
@@ -47,8 +47,7 @@ struct StreamArgs {
   const void *data;           // element array of the phase (storage type)
   const Chunk *chunks;        // ordered by CTA
   const int32_t *cta_ptr;     // grid + 1
-  const void *xsrc;           // gathered x (compute type), permuted order
-  const void *tsrc;           // t (compute type)
+  const void *gsrc;           // vector values: gathered x (phase 1) or G2 (phase 2), compute type
   void *t_out;                // phase-1 output (compute type)
   const float *t_scale;       // phase 1: per-t-entry output scale (BF16), or null
   double *y_out;              // phase-2 output
@@ -232,8 +231,8 @@ __device__ __forceinline__ void chunk_dot<float, 4>(const unsigned char *base, c
 template <typename S> struct SmemLayout {
   using G = typename Store<S>::G;
   static constexpr int kDataBytes = kStageBytes + 32;
-  // gather area: each segment lands 16-byte aligned with up to 15 bytes of slack each side
-  static constexpr int kGBytes = kMaxCols * (int)sizeof(G) + kMaxSeg * 32;
+  // vector window: the chunk's run of values with up to 15 bytes of slack each side
+  static constexpr int kGBytes = kMaxCols * (int)sizeof(G) + 32;
   static constexpr int kStageSize = kDataBytes + kGBytes + (int)sizeof(Chunk);
   static constexpr int kRedPer = red_per_buf<G>();
   static constexpr int kRedBytes = 2 * kRedPer * (int)sizeof(G);
@@ -264,59 +263,6 @@ __device__ __forceinline__ void load_desc(const Chunk *chunks, int idx, int end,
   }
 }
 
-// Gather layout of a chunk's segments.  Segment k is the contiguous run
-// src_k[0 .. cols_k) of x or t; it is staged by one bulk copy of the 16-byte
-// aligned window around it, placed at byte goff_k of the stage's gather area,
-// so column c of the chunk (start_k <= c < start_k + cols_k) is element
-// gbase_k + (c - start_k) of the area.
-struct SegTable {
-  int n;
-  int start[kMaxSeg], cols[kMaxSeg], gbase[kMaxSeg];
-  float scale[kMaxSeg];
-  int total;  // bytes of all windows
-};
-// Source windows, needed by the producer only.
-struct SegCopies {
-  unsigned long long lo[kMaxSeg];  // source window start (16-byte aligned)
-  int bytes[kMaxSeg], goff[kMaxSeg];
-};
-
-// w: descriptor words (8..15 seg_off, 16..19 seg_cols pairs, 20..27 seg_scale).
-template <typename G, typename Words>
-__device__ __forceinline__ void seg_table(const Words &w, const G *xs, const G *ts, SegTable &t,
-                                          SegCopies *cp = nullptr) {
-  const uint32_t flags = w[6];
-  t.n = static_cast<int>((flags >> 8) & 0xfu);
-  int start = 0, goff = 0;
-#pragma unroll
-  for (int k = 0; k < kMaxSeg; k++) {
-    const int ck = k < t.n ? static_cast<int>((w[16 + (k >> 1)] >> ((k & 1) * 16)) & 0xffffu) : 0;
-    const G *src = ((flags >> (16 + k)) & 1u) ? ts : xs;
-    const unsigned long long a = reinterpret_cast<unsigned long long>(src + static_cast<int>(w[8 + k]));
-    const unsigned long long lo = a & ~15ull;
-    const unsigned long long hi = (a + static_cast<unsigned long long>(ck) * sizeof(G) + 15ull) & ~15ull;
-    const int bytes = ck > 0 ? static_cast<int>(hi - lo) : 0;
-    t.start[k] = start;
-    t.cols[k] = ck;
-    t.gbase[k] = (goff + static_cast<int>(a - lo)) / static_cast<int>(sizeof(G));
-    t.scale[k] = __uint_as_float(w[20 + k]);
-    if (cp) {
-      cp->lo[k] = lo;
-      cp->bytes[k] = bytes;
-      cp->goff[k] = goff;
-    }
-    start += ck;
-    goff += bytes;
-  }
-  t.total = goff;
-}
-
-// Words of a descriptor copied into shared memory.
-struct SmemWords {
-  const uint32_t *p;
-  __device__ __forceinline__ uint32_t operator[](int i) const { return p[i]; }
-};
-
 template <typename S>
 __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a) {
   using G = typename Store<S>::G;
@@ -333,7 +279,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&full[s], 1);                  // lane-0 arrive.expect_tx; the bulk copies complete the tx
+      mbar_init(&full[s], 1);                  // lane-0 arrive.expect_tx; the two bulk copies complete the tx
       mbar_init(&empty[s], kConsumerWarps);    // one arrival per consumer warp
     }
     mbar_init(redbar, kConsumerWarps);
@@ -347,8 +293,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
   if (warp == 0) {
     // ------------------------------------------------------------------ producer
     const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
-    const G *xs = static_cast<const G *>(a.xsrc);
-    const G *ts = static_cast<const G *>(a.tsrc);
+    const unsigned char *gvec = static_cast<const unsigned char *>(a.gsrc);
     DescRegs cur, nxt;
     load_desc(a.chunks, cb + lane, ce, nxt);
     bool ok = true;
@@ -369,43 +314,34 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         uint32_t w[kChunkWords];
 #pragma unroll
         for (int q = 0; q < kChunkWords; q++) w[q] = __shfl_sync(0xffffffffu, cur.w[q], k);
-        const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
-        const int ncols = static_cast<int>(w[2]);
-        const int hpad = static_cast<int>(w[3]);
-        unsigned char *st = stage0 + s * L::kStageSize;
-        unsigned char *garea = st + L::kDataBytes;
-        SegTable tab;
-        SegCopies cpy;
-        seg_table<G>(w, xs, ts, tab, &cpy);
-        const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
-                                                : static_cast<unsigned long long>(ncols);
-        const unsigned long long bytes = cols * hpad * es;
-        const bool good = ncols > 0 && ncols <= kMaxCols && bytes <= static_cast<unsigned long long>(kStageBytes) &&
-                          tab.total <= L::kGBytes;
-        const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
-                                       static_cast<unsigned long long>(data_off) * es;
-        const unsigned long long lo = src & ~15ull;
-        const unsigned long long hi = (src + bytes + 15ull) & ~15ull;
         if (lane == 0) {
+          const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
+          const int ncols = static_cast<int>(w[2]);
+          const int hpad = static_cast<int>(w[3]);
+          const int g_off = static_cast<int>(w[7]);
+          unsigned char *st = stage0 + s * L::kStageSize;
           uint4 *dd = reinterpret_cast<uint4 *>(st + L::kDataBytes + L::kGBytes);
 #pragma unroll
           for (int q = 0; q < kChunkWords / 4; q++)
             dd[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-          if (good) {
-            mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>(hi - lo) + static_cast<uint32_t>(tab.total));
+          const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
+                                                  : static_cast<unsigned long long>(ncols);
+          const unsigned long long bytes = cols * hpad * es;
+          if (ncols > 0 && ncols <= kMaxCols && bytes <= static_cast<unsigned long long>(kStageBytes)) {
+            const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
+                                           static_cast<unsigned long long>(data_off) * es;
+            const unsigned long long lo = src & ~15ull, hi = (src + bytes + 15ull) & ~15ull;
+            const unsigned long long gs = reinterpret_cast<unsigned long long>(gvec) +
+                                          static_cast<unsigned long long>(g_off) * sizeof(G);
+            const unsigned long long glo = gs & ~15ull, ghi = (gs + ncols * sizeof(G) + 15ull) & ~15ull;
+            mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>((hi - lo) + (ghi - glo)));
+            bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
+            bulk_g2s(st + L::kDataBytes, reinterpret_cast<const void *>(glo), static_cast<uint32_t>(ghi - glo),
+                     &full[s]);
           } else {
             if (ncols > 0) set_error(a.err, kErrBadChunk);
             mbar_arrive(&full[s]);
           }
-        }
-        __syncwarp();
-        if (good) {
-          if (lane == 0) bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
-#pragma unroll
-          for (int k = 0; k < kMaxSeg; k++)
-            if (lane == k + 1 && cpy.bytes[k] > 0)
-              bulk_g2s(garea + cpy.goff[k], reinterpret_cast<const void *>(cpy.lo[k]),
-                       static_cast<uint32_t>(cpy.bytes[k]), &full[s]);
         }
         issued++;
       }
@@ -448,11 +384,12 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
       return;
     }
     const unsigned char *st = stage0 + s * L::kStageSize;
-    const G *gs = reinterpret_cast<const G *>(st + L::kDataBytes);
     const Chunk &d = *reinterpret_cast<const Chunk *>(st + L::kDataBytes + L::kGBytes);
-    SegTable tab;
-    seg_table<G>(SmemWords{reinterpret_cast<const uint32_t *>(&d)}, static_cast<const G *>(a.xsrc),
-                 static_cast<const G *>(a.tsrc), tab);
+    // the vector window starts at the 16-byte boundary below gsrc + g_off
+    const G *gs = reinterpret_cast<const G *>(
+        st + L::kDataBytes +
+        ((reinterpret_cast<unsigned long long>(a.gsrc) + static_cast<unsigned long long>(d.g_off) * sizeof(G)) &
+         15ull));
     const uint32_t flags = d.flags;
     const int ncols = d.ncols;
     const int hpad = d.hpad;
@@ -470,12 +407,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
       if (active && ncols > 0 && ncols <= kMaxCols) {
         const int c0 = (cq * ncols) / Q, c1 = ((cq + 1) * ncols) / Q;
         const int soff = static_cast<int>((static_cast<unsigned long long>(d.data_off) * es) & 15ull);
-#pragma unroll
-        for (int k = 0; k < kMaxSeg; k++) {
-          const int lo_c = max(c0, tab.start[k]), hi_c = min(c1, tab.start[k] + tab.cols[k]);
-          if (k < tab.n && lo_c < hi_c)
-            chunk_dot<S, R>(st + soff, gs + tab.gbase[k] - tab.start[k], hv, rv, lo_c, hi_c, acc);
-        }
+        chunk_dot<S, R>(st + soff, gs, hv, rv, c0, c1, acc);
       }
     } else {
       if (flags & kFirst) {
@@ -491,12 +423,10 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
           for (int q = 0; q < 4; q++) tacc[j][q] = 0.f;
       }
       if (wact && ncols > 0 && ncols <= kMaxCols) {
-        const int nseg = static_cast<int>((flags >> 8) & 0xfu);
         const int grp = lane >> 2, tq = lane & 3;
         const uint32_t sbase = smem_u32(st);  // BF16 chunks start 16-byte aligned (offset 0)
         const int nks = (ncols + 15) >> 4;
         const int mat = lane >> 3, mr = lane & 7;
-        (void)nseg;
         for (int ks = kp; ks < nks; ks += kparts) {
           // B fragment: lanes 0-3 hold the BF16-rounded vector (column 0),
           // lanes 4-7 the BF16-rounded remainder (column 1), others zero.
@@ -506,18 +436,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
 #pragma unroll
             for (int e = 0; e < 4; e++) {
               const int c = 16 * ks + 2 * tq + (e & 1) + (e >> 1) * 8;
-              float x = 0.f;
-              if (c < ncols) {
-                float sc = tab.scale[0];
-                int gi = tab.gbase[0] + c;
-#pragma unroll
-                for (int k = 1; k < kMaxSeg; k++)
-                  if (k < tab.n && c >= tab.start[k]) {
-                    sc = tab.scale[k];
-                    gi = tab.gbase[k] + c - tab.start[k];
-                  }
-                x = gs[gi] * sc;
-              }
+              const float x = c < ncols ? gs[c] : 0.f;
               const float hi = __bfloat162float(__float2bfloat16_rn(x));
               v[e] = grp == 0 ? hi : x - hi;
             }
@@ -601,6 +520,20 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
       items++;
     }
   }
+}
+
+// G2[dst + c] = scale * src[src_off + c] for every run (src: gathered x or t):
+// the phase-2 vector values laid out chunk by chunk.  One warp per run.
+template <typename G>
+__global__ void gather_g2_kernel(const GatherSeg *__restrict__ runs, int n_runs, const G *__restrict__ xp,
+                                 const G *__restrict__ t, G *__restrict__ g2) {
+  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= n_runs) return;
+  const GatherSeg gsg = runs[r];
+  const int cols = static_cast<int>(gsg.cols_src & 0x7fffffffu);
+  const G *src = (gsg.cols_src >> 31) ? t : xp;
+  const G sc = static_cast<G>(gsg.scale);
+  for (int c = threadIdx.x & 31; c < cols; c += 32) g2[gsg.dst + c] = sc * src[gsg.src_off + c];
 }
 
 // x (FP64, caller's ordering) -> gathered copy in the compute type, permuted

@@ -313,8 +313,10 @@ float seg_scale(const OperatorPlan &op, const Segment &s, int prec) {
   return 1.0f;  // LR A slices and B stacks: the scales are folded into t (t_scale)
 }
 
-// Chunks of one item for one precision.
-void chunk_item(const OperatorPlan &op, const Item &it, int prec, std::vector<Chunk> &out) {
+// Chunks of one item for one precision; phase-2 chunks also get their slice of
+// the gather array (g_len grows) and the runs that fill it.
+void chunk_item(const OperatorPlan &op, const Item &it, int prec, int phase, std::vector<Chunk> &out,
+                std::vector<GatherSeg> &gsegs, int64_t &g_len) {
   const int es = esize_of(prec);
   const bool tiled = prec == 2;
   int64_t cap;
@@ -322,22 +324,12 @@ void chunk_item(const OperatorPlan &op, const Item &it, int prec, std::vector<Ch
     cap = std::min<int64_t>(kMaxCols, (kStageBytes / (8 * int64_t(it.hpad) * es)) * 8);
   else
     cap = std::max<int64_t>(1, std::min<int64_t>(kMaxCols, kStageBytes / (int64_t(it.hpad) * es)));
-  // column -> segment map of the item
   std::vector<int64_t> seg_start(it.segs.size() + 1, 0);
   for (size_t s = 0; s < it.segs.size(); s++) seg_start[s + 1] = seg_start[s] + it.segs[s].ncols;
   int64_t c0 = 0;
-  size_t s_at = 0;  // segment containing column c0
+  size_t s_at = 0;  // first segment that may overlap column c0
   do {
-    int64_t take = std::min<int64_t>(cap, it.ncols - c0);
-    // at most kMaxSeg segment pieces
-    while (s_at < it.segs.size() && seg_start[s_at + 1] <= c0) s_at++;
-    if (s_at + kMaxSeg < it.segs.size()) {
-      const int64_t lim = seg_start[s_at + kMaxSeg] - c0;  // columns covered by kMaxSeg pieces
-      if (lim < take) take = lim;
-    }
-    // tiled chunks start on 8-column groups: cut at a multiple of 8 unless it is the item's end
-    if (tiled && c0 + take < it.ncols) take = (take / 8) * 8;
-    if (it.ncols > 0 && take <= 0) throw std::runtime_error("internal: empty chunk");
+    const int64_t take = std::min<int64_t>(cap, it.ncols - c0);
     Chunk ch;
     std::memset(&ch, 0, sizeof ch);
     ch.data_off = it.off[prec] + (tiled ? (c0 / 8) * 8 * int64_t(it.hpad) : c0 * int64_t(it.hpad));
@@ -345,20 +337,27 @@ void chunk_item(const OperatorPlan &op, const Item &it, int prec, std::vector<Ch
     ch.hpad = it.hpad;
     ch.rows = it.h;
     ch.out_off = it.out_off;
-    int ns = 0;
-    for (size_t s = s_at; s < it.segs.size() && seg_start[s] < c0 + take; s++) {
-      const int64_t a = std::max<int64_t>(c0, seg_start[s]), b = std::min<int64_t>(c0 + take, seg_start[s + 1]);
-      if (b <= a) continue;
-      if (ns >= kMaxSeg) throw std::runtime_error("internal: too many segments in a chunk");
-      const Segment &sg = it.segs[s];
-      ch.seg_off[ns] = static_cast<int32_t>(sg.src_off + (a - seg_start[s]));
-      ch.seg_cols[ns] = static_cast<uint16_t>(b - a);
-      ch.seg_scale[ns] = seg_scale(op, sg, prec);
-      if (sg.src) ch.flags |= 1u << (16 + ns);
-      ns++;
+    if (phase == 0) {
+      ch.g_off = it.segs.empty() ? 0 : static_cast<int32_t>(it.segs[0].src_off + c0);
+    } else {
+      const int64_t g = (g_len + 3) / 4 * 4;  // 16-byte aligned slice in FP32, 32 in FP64
+      if (g + take > INT32_MAX) throw std::runtime_error("gather array above 2^31 entries");
+      ch.g_off = static_cast<int32_t>(g);
+      g_len = g + take;
+      while (s_at < it.segs.size() && seg_start[s_at + 1] <= c0) s_at++;
+      for (size_t s = s_at; s < it.segs.size() && seg_start[s] < c0 + take; s++) {
+        const int64_t a = std::max<int64_t>(c0, seg_start[s]), b = std::min<int64_t>(c0 + take, seg_start[s + 1]);
+        if (b <= a) continue;
+        const Segment &sg = it.segs[s];
+        GatherSeg gs;
+        gs.dst = static_cast<int32_t>(g + (a - c0));
+        gs.src_off = static_cast<int32_t>(sg.src_off + (a - seg_start[s]));
+        gs.cols_src = static_cast<uint32_t>(b - a) | (sg.src ? 0x80000000u : 0u);
+        gs.scale = seg_scale(op, sg, prec);
+        gsegs.push_back(gs);
+      }
     }
-    ch.flags |= uint32_t(ns) << 8;
-    if (out.empty() || (out.back().flags & kLast)) ch.flags |= kFirst;
+    if (out.empty()) ch.flags |= kFirst;
     c0 += take;
     if (c0 >= it.ncols) ch.flags |= kLast;
     out.push_back(ch);
@@ -373,6 +372,7 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
   const int es = esize_of(prec);
   for (int phase = 0; phase < 2; phase++) {
     PhasePlan &ph = op.ph[phase];
+    ChunkPlan &cp = ph.cp[prec];
     // data layout of this precision
     int64_t off = 0;
     for (Item &it : ph.items) {
@@ -381,14 +381,17 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
     }
     ph.n_elems[prec] = off + kItemAlign;  // slack so 16-byte rounded copies stay inside
     std::vector<std::vector<Chunk>> per_item(ph.items.size());
-    for (size_t q = 0; q < ph.items.size(); q++) chunk_item(op, ph.items[q], prec, per_item[q]);
+    cp.gsegs.clear();
+    cp.g_len = 0;
+    for (size_t q = 0; q < ph.items.size(); q++)
+      chunk_item(op, ph.items[q], prec, phase, per_item[q], cp.gsegs, cp.g_len);
     // LPT: items by decreasing cost onto the least-loaded CTA.  Cost is the
-    // bytes streamed plus a fixed per-chunk overhead (descriptor, gather,
-    // barrier round trip) expressed in bytes.
+    // bytes streamed plus a fixed per-chunk overhead (descriptor, barrier round
+    // trip) expressed in bytes.
     const int64_t n = (int64_t)ph.items.size();
     std::vector<int64_t> cost(n);
     for (int64_t q = 0; q < n; q++)
-      cost[q] = item_elems(prec, ph.items[q].hpad, ph.items[q].ncols) * es + 2048 * (int64_t)per_item[q].size();
+      cost[q] = item_elems(prec, ph.items[q].hpad, ph.items[q].ncols) * es + 1024 * (int64_t)per_item[q].size();
     std::vector<int64_t> order(n);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
@@ -403,7 +406,6 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
       s.first += cost[q];
       heap.push(s);
     }
-    ChunkPlan &cp = ph.cp[prec];
     cp.chunks.clear();
     cp.cta_ptr.assign(grid + 1, 0);
     for (int c = 0; c < grid; c++) {

@@ -20,9 +20,8 @@
 // BF16 items are stored as 8x8 tiles (column group, then row group, then
 // 8 columns x 8 contiguous rows) so that tensor-core fragment loads from shared
 // memory are 128-byte contiguous.  An item is cut into chunks of at most
-// kStageBytes; a chunk is what one TMA bulk copy stages into shared memory,
-// and carries up to kMaxSeg "gather segments" that say where the vector values
-// of its columns come from (x or t) and which BF16 block scale applies.
+// kStageBytes; a chunk is what one TMA bulk copy stages into shared memory
+// (plus one more for its contiguous run of vector values).
 #pragma once
 
 #include <cstdint>
@@ -33,7 +32,6 @@ namespace bw {
 
 constexpr int kStageBytes = 32768;   // bytes of block data per pipeline stage
 constexpr int kMaxCols = 512;        // columns per chunk (size of a stage's gather buffer)
-constexpr int kMaxSeg = 8;           // gather segments per chunk (>= 8: any 8 columns fit one chunk)
 constexpr int kHMax = 512;           // max padded rows of one item
 constexpr int kRowAlign = 8;         // padded rows are a multiple of this
 constexpr int kItemAlign = 64;       // item start alignment, in elements
@@ -42,24 +40,33 @@ constexpr int kItemsPerCta = 8;      // minimum items per CTA share (load balanc
 // Chunk flags
 constexpr uint32_t kFirst = 1u;      // first chunk of an item: reset accumulators
 constexpr uint32_t kLast = 2u;       // last chunk of an item: reduce and write the output
-// bits 8..11: number of segments; bits 16..23: source of segment k (0 = x, 1 = t)
 
-// One chunk descriptor, 112 bytes (28 words), read by the producer warp and
-// copied into shared memory for the consumer warps.
+// One chunk descriptor, 32 bytes, read by the producer warp and copied into
+// shared memory for the consumer warps.  The vector values of the chunk's
+// columns are the contiguous run gsrc[g_off .. g_off + ncols), where gsrc is
+// the gathered x for phase 1 (stacked B rows multiply one slice of x) and the
+// per-matvec gather array G2 for phase 2.
 struct alignas(16) Chunk {
-  int64_t data_off;           // element offset of the chunk's first column in the data array
-  int32_t ncols;              // columns in this chunk
-  int32_t hpad;               // padded row count of the item (multiple of 8)
-  int32_t rows;               // rows of the item to write (<= hpad)
-  int32_t out_off;            // first output index: t offset (phase 1) or row (phase 2)
-  uint32_t flags;             // kFirst | kLast | nseg << 8 | src bits << 16
-  uint32_t reserved0;
-  int32_t seg_off[kMaxSeg];   // element offset of each segment in its source vector
-  uint16_t seg_cols[kMaxSeg]; // columns of each segment
-  float seg_scale[kMaxSeg];   // multiplies the vector values of the segment (BF16 block scale)
+  int64_t data_off;  // element offset of the chunk's first column in the data array
+  int32_t ncols;     // columns in this chunk
+  int32_t hpad;      // padded row count of the item (multiple of 8)
+  int32_t rows;      // rows of the item to write (<= hpad)
+  int32_t out_off;   // first output index: t offset (phase 1) or row (phase 2)
+  uint32_t flags;    // kFirst | kLast
+  int32_t g_off;     // first vector value in the phase's gather source
 };
-static_assert(sizeof(Chunk) == 112, "chunk descriptor must be 112 bytes");
+static_assert(sizeof(Chunk) == 32, "chunk descriptor must be 32 bytes");
 constexpr int kChunkWords = sizeof(Chunk) / 4;
+
+// One run of G2: G2[dst .. dst + cols) = scale * src[src_off .. src_off + cols)
+// with src = x (gathered) or t.  Built once per matvec before phase 2.
+struct GatherSeg {
+  int32_t dst;
+  int32_t src_off;
+  uint32_t cols_src;  // cols | src << 31
+  float scale;        // BF16: the full block's scale; 1 elsewhere
+};
+static_assert(sizeof(GatherSeg) == 16, "gather segment must be 16 bytes");
 
 // A read-only view of a column-major block (or of its transpose).
 struct View {
@@ -103,10 +110,13 @@ struct Item {
   std::vector<RowPiece> pieces;  // phase 1 only
 };
 
-// Per precision: chunk list ordered by CTA, and the CTA ranges.
+// Per precision: chunk list ordered by CTA, the CTA ranges, and (phase 2)
+// the runs that fill the gather array G2 of g_len values.
 struct ChunkPlan {
   std::vector<Chunk> chunks;
   std::vector<int32_t> cta_ptr;  // grid + 1
+  std::vector<GatherSeg> gsegs;  // phase 2 only
+  int64_t g_len = 0;
 };
 
 struct PhasePlan {

@@ -221,7 +221,7 @@ class HmatGpu:
         f = _prec_flag(precision)
         A.check(self._lib.bw_plan_export(self._h, f, phase, int(transposed), C.byref(nc), None, C.byref(ne), None,
                                          C.byref(nt), None), self._h)
-        chunks = np.zeros((nc.value, 28), np.int32)
+        chunks = np.zeros((nc.value, 8), np.int32)
         cta = np.zeros(nt.value, np.int32)
         data = np.zeros(ne.value) if with_data else None
         A.check(self._lib.bw_plan_export(self._h, f, phase, int(transposed), C.byref(nc), chunks.ctypes.data,
@@ -234,9 +234,9 @@ class HmatGpu:
         A.check(self._lib.bw_set_timing(self._h, int(enable)), self._h)
 
     def timing_read(self):
-        """Summed durations (ms) of the (x gather, phase 1, phase 2) launches
-        recorded since the last read, and the number of matvecs recorded."""
-        ms = (C.c_double * 3)()
+        """Summed durations (ms) of the (x gather, phase 1, G2 gather, phase 2)
+        launches recorded since the last read, and the number of matvecs."""
+        ms = (C.c_double * 4)()
         n = C.c_int64()
         A.check(self._lib.bw_timing_read(self._h, ms, C.byref(n)), self._h)
         return list(ms), int(n.value)

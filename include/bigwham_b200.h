@@ -109,8 +109,10 @@ int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream);
  * caller passes x and y; the scratch vectors live in a fixed device array of
  * BW_STATIC_SCRATCH_BYTES (16 MiB) compiled into the library, which every GPU
  * that loads the library holds until the process exits.  H-matrices needing
- * more scratch than that (8 or 4 bytes per input plus per low-rank rank
- * column, e.g. ~15.3 MB for FP64 at 196,608 DoF) are rejected with BW_ERR_ARG.
+ * more scratch than that are rejected with BW_ERR_ARG: 8 bytes (FP64) or 4
+ * (FP32, BF16) per input, per low-rank rank column and per column of every row
+ * panel (the phase-2 gather array), e.g. about 12 MB in FP32 at 49,152 DoF and
+ * 42 MB at 196,608 DoF.
  * The first call on a device looks the array's address up (once per device);
  * make that first call before any stream capture.  Every call overwrites the
  * scratch before reading it, so nothing in it needs to start at zero, and the
@@ -163,7 +165,7 @@ int bw_set_device_limit(bw_hmat *h, int64_t bytes);
 
 /* Host view of the built plan for one precision and phase (1: low-rank B
  * stage, 2: row panels), for inspection and testing.  Any output pointer may be
- * NULL; counts are always written.  chunks: n_chunks x 28 int32 words in the
+ * NULL; counts are always written.  chunks: n_chunks x 8 int32 words in the
  * layout of bw::Chunk (bigwham_dev_b200/csrc/bw_layout.h); data: n_elems values
  * converted to double, in the precision's layout (column-major items for FP64 /
  * FP32, 8x8 tiles for BF16; BF16 values divided by their block scale);
@@ -172,10 +174,10 @@ int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, i
                    int32_t *chunks, int64_t *n_elems, double *data, int64_t *n_cta, int32_t *cta_ptr);
 
 /* Per-launch timing for benchmarks.  With timing enabled every bw_matvec
- * records CUDA events on its stream around its three launches (x gather,
- * phase 1, phase 2).  bw_timing_read waits for the last recorded event, writes
- * the summed durations in milliseconds of the three launch kinds into ms[0..2]
- * and the number of recorded matvecs, and clears the record. */
+ * records CUDA events on its stream around its four launches (x gather,
+ * phase 1, G2 gather, phase 2).  bw_timing_read waits for the last recorded
+ * event, writes the summed durations in milliseconds of the four launch kinds
+ * into ms[0..3] and the number of recorded matvecs, and clears the record. */
 int bw_set_timing(bw_hmat *h, int enable);
 int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs);
 
@@ -183,6 +185,10 @@ int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs);
  * low-rank B factors (+ x, + t written), phase 2 reads the full blocks and the
  * A factors (+ y written).  Stored entries only: padding is not counted. */
 int bw_phase_bytes(const bw_hmat *h, int precision, int transposed, int64_t *phase1, int64_t *phase2);
+
+/* Runs that fill the phase-2 gather array (4 int32 words each: dst, src_off,
+ * cols | src << 31, scale bits), for inspection and testing. */
+int bw_plan_gather(const bw_hmat *h, int precision, int transposed, int64_t *n, int32_t *runs);
 
 /* Per-t-entry output scales of phase 1 (BF16: scale(A) * scale(B) of the
  * entry's low-rank block; 1 elsewhere), for inspection and testing. */

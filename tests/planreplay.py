@@ -1,31 +1,24 @@
 """Numpy replay of a host-only plan (test helper).
 
 Walks the chunk list exactly as the streaming kernel does (per CTA, per
-chunk: partial = D[:, cols] @ (g * segment scale), accumulated over the chunks
-of an item and written at its last chunk, phase-1 outputs times the per-t
-scale) so the layout, the chunking and the LPT schedule can be checked on a
-machine without a GPU.
+chunk: partial = D[:, cols] @ g[g_off : g_off + ncols], accumulated over the
+chunks of an item and written at its last chunk, phase-1 outputs times the
+per-t scale), with the phase-2 gather array G2 rebuilt from its runs, so the
+layout, the chunking and the LPT schedule can be checked on a machine without
+a GPU.
 """
+import ctypes as C
+
 import numpy as np
 
 K_FIRST, K_LAST = 1, 2
-WORDS = 28
+WORDS = 8
 
 
 def decode(w):
     w = np.asarray(w, dtype=np.int64) & 0xFFFFFFFF
-    data_off = int(w[0] | (w[1] << 32))
-    flags = int(w[6])
-    nseg = (flags >> 8) & 0xF
-    cols = []
-    for k in range(8):
-        word = int(w[16 + k // 2])
-        cols.append((word >> (16 * (k % 2))) & 0xFFFF)
-    scales = np.array(w[20:28], dtype=np.uint32).view(np.float32)
-    segs = [(int(np.int32(np.uint32(w[8 + k]))), cols[k], (flags >> (16 + k)) & 1, float(scales[k]))
-            for k in range(nseg)]
-    return dict(data_off=data_off, ncols=int(w[2]), hpad=int(w[3]), rows=int(w[4]), out_off=int(w[5]),
-                flags=flags, segs=segs)
+    return dict(data_off=int(w[0] | (w[1] << 32)), ncols=int(w[2]), hpad=int(w[3]), rows=int(w[4]),
+                out_off=int(w[5]), flags=int(w[6]), g_off=int(np.int32(np.uint32(w[7]))))
 
 
 def chunk_matrix(data, d, tiled):
@@ -35,11 +28,10 @@ def chunk_matrix(data, d, tiled):
         return data[d["data_off"]:d["data_off"] + nc * hp].reshape(nc, hp).T
     ng = (nc + 7) // 8
     t = data[d["data_off"]:d["data_off"] + ng * 8 * hp].reshape(ng, hp // 8, 8, 8)  # [cgroup, rgroup, c%8, r%8]
-    M = t.transpose(1, 3, 0, 2).reshape(hp, ng * 8)
-    return M[:, :nc]
+    return t.transpose(1, 3, 0, 2).reshape(hp, ng * 8)[:, :nc]
 
 
-def run_phase(plan, xsrc, tsrc, out, tiled=False, t_scale=None):
+def run_phase(plan, gsrc, out, tiled=False, t_scale=None):
     chunks, cta, data = plan["chunks"], plan["cta_ptr"], plan["data"]
     for b in range(len(cta) - 1):
         acc = None
@@ -48,10 +40,7 @@ def run_phase(plan, xsrc, tsrc, out, tiled=False, t_scale=None):
             if d["flags"] & K_FIRST:
                 acc = np.zeros(d["hpad"])
             if d["ncols"]:
-                D = chunk_matrix(data, d, tiled)
-                g = np.concatenate([(tsrc if src else xsrc)[off:off + n] * sc for off, n, src, sc in d["segs"]])
-                assert g.size == d["ncols"]
-                acc += D @ g
+                acc += chunk_matrix(data, d, tiled) @ gsrc[d["g_off"]:d["g_off"] + d["ncols"]]
             if d["flags"] & K_LAST:
                 r = acc[:d["rows"]]
                 if t_scale is not None:
@@ -60,10 +49,29 @@ def run_phase(plan, xsrc, tsrc, out, tiled=False, t_scale=None):
     return out
 
 
+def gather_runs(h, precision, transposed):
+    from bigwham_dev_b200 import _capi as A
+
+    n = C.c_int64()
+    f = A.PRECISIONS[precision]
+    A.check(A.lib().bw_plan_gather(h._h, f, int(transposed), C.byref(n), None), h._h)
+    runs = np.zeros((n.value, 4), np.int32)
+    A.check(A.lib().bw_plan_gather(h._h, f, int(transposed), C.byref(n), runs.ctypes.data), h._h)
+    return runs
+
+
+def build_g2(runs, x, t):
+    cols = (runs[:, 2].view(np.uint32) & 0x7FFFFFFF).astype(np.int64)
+    src = runs[:, 2].view(np.uint32) >> 31
+    scale = runs[:, 3].view(np.float32).astype(np.float64)
+    g2 = np.zeros(int((runs[:, 0] + cols).max()) if len(runs) else 0)
+    for (dst, off), c, s, sc in zip(runs[:, :2].astype(np.int64), cols, src, scale):
+        g2[dst:dst + c] = sc * (t if s else x)[off:off + c]
+    return g2
+
+
 def replay(h, x_perm, precision="fp64", transposed=False):
     """y (permuted ordering) = H x_perm, replaying h's plan (h finalized with plan_only)."""
-    import ctypes as C
-
     from bigwham_dev_b200 import _capi as A
 
     p1 = h.plan_export(precision, 1, transposed)
@@ -76,10 +84,9 @@ def replay(h, x_perm, precision="fp64", transposed=False):
         buf = (C.c_float * n.value)()
         A.check(A.lib().bw_plan_tscale(h._h, int(transposed), C.byref(n), buf), h._h)
         ts = np.frombuffer(buf, dtype=np.float32).astype(np.float64)
-    info = h.info()
-    t = np.zeros(max(1, info["sum_rank"]))
-    run_phase(p1, x_perm, t, t, tiled, ts)
-    n_out = h.n_cols if transposed else h.n_rows
-    y = np.full(n_out, np.nan)
-    run_phase(p2, x_perm, t, y, tiled)
+    t = np.zeros(max(1, h.info()["sum_rank"]))
+    run_phase(p1, x_perm, t, tiled, ts)
+    g2 = build_g2(gather_runs(h, precision, transposed), x_perm, t)
+    y = np.full(h.n_cols if transposed else h.n_rows, np.nan)
+    run_phase(p2, g2, y, tiled)
     return y

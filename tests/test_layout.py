@@ -5,7 +5,7 @@ rejected with the documented status codes."""
 import numpy as np
 import pytest
 from conftest import rel
-from planreplay import decode, replay
+from planreplay import decode, gather_runs, replay
 
 from bigwham_dev_b200 import BigWhamError, HmatGpu
 from bigwham_dev_b200 import _capi as A
@@ -53,16 +53,20 @@ def test_plan_structure(golden):
                 assert d["hpad"] % 8 == 0 and d["rows"] <= d["hpad"] <= 512
                 cols = (d["ncols"] + 7) // 8 * 8 if prec == "bf16" else d["ncols"]
                 assert cols * d["hpad"] * es <= 32768 and d["ncols"] <= 512
-                assert sum(n for _, n, _, _ in d["segs"]) == d["ncols"]
                 assert (d["data_off"] * es) % 16 == 0  # every chunk starts 16-byte aligned
-                if prec == "bf16":
-                    assert d["data_off"] % (8 * d["hpad"]) % 64 == 0
-                else:
-                    assert all(sc == 1.0 for _, _, _, sc in d["segs"])
+                if phase == 2:
+                    assert d["g_off"] % 4 == 0  # 16-byte aligned slice of the gather array
                 # chunks of one item are consecutive: FIRST opens, LAST closes
                 assert bool(d["flags"] & 1) != open_item
                 open_item = not (d["flags"] & 2)
             assert not open_item
+        # the gather runs tile the phase-2 slices exactly
+        runs = gather_runs(h, prec, False)
+        cols = (runs[:, 2].view(np.uint32) & 0x7FFFFFFF)
+        if prec != "bf16":
+            assert np.all(runs[:, 3].view(np.float32) == 1.0)
+        p2 = h.plan_export(prec, 2, with_data=False)
+        assert int(cols.sum()) == sum(decode(w)["ncols"] for w in p2["chunks"])
 
 
 def test_lpt_balance_on_many_items():
