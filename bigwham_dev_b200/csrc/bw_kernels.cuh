@@ -424,19 +424,33 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
       }
       if (wact && ncols > 0 && ncols <= kMaxCols) {
         const int grp = lane >> 2, tq = lane & 3;
-        const uint32_t sbase = smem_u32(st);  // BF16 chunks start 16-byte aligned (offset 0)
         const int nks = (ncols + 15) >> 4;
-        const int mat = lane >> 3, mr = lane & 7;
-        for (int ks = kp; ks < nks; ks += kparts) {
+        // ldmatrix.x4.trans: lane l addresses row (l & 7) of 8x8 matrix l >> 3;
+        // matrix bit 0 = second 8-row group, bit 1 = second 8-column group.
+        // Byte offset of (column group kg, row group rg, row r) in the tiled
+        // chunk: 2 * (kg * 8 * hpad + rg * 64 + r * 8).
+        const int mat = lane >> 3;
+        const uint32_t kstep_bytes = 32u * static_cast<uint32_t>(hpad);  // 16 columns
+        const uint32_t lane_base = smem_u32(st) + 2u * static_cast<uint32_t>((mat >> 1) * 8 * hpad +
+                                                                              (mat & 1) * 64 + (lane & 7) * 8);
+        const uint32_t back_k = (mat & 2) ? 16u * static_cast<uint32_t>(hpad) : 0u;  // to group 2ks if absent
+        const uint32_t back_m = (mat & 1) ? 128u : 0u;                               // to group 2mt if absent
+        // K-steps are dealt round-robin, rotated every chunk so the warps
+        // share the remainder evenly over a stream of chunks.
+        const int rot = i % kparts;
+        int ks = kp - rot;
+        if (ks < 0) ks += kparts;
+        for (; ks < nks; ks += kparts) {
           // B fragment: lanes 0-3 hold the BF16-rounded vector (column 0),
           // lanes 4-7 the BF16-rounded remainder (column 1), others zero.
           uint32_t b0 = 0, b1 = 0;
           if (grp < 2) {
+            const int c = 16 * ks + 2 * tq;
             float v[4];
 #pragma unroll
             for (int e = 0; e < 4; e++) {
-              const int c = 16 * ks + 2 * tq + (e & 1) + (e >> 1) * 8;
-              const float x = c < ncols ? gs[c] : 0.f;
+              const int ce = c + (e & 1) + (e >> 1) * 8;
+              const float x = ce < ncols ? gs[ce] : 0.f;
               const float hi = __bfloat162float(__float2bfloat16_rn(x));
               v[e] = grp == 0 ? hi : x - hi;
             }
@@ -444,20 +458,14 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
             b1 = pack_bf16x2(v[2], v[3]);
           }
           const bool k2 = 16 * ks + 8 < ncols;  // second 8-column group present
+          const uint32_t kaddr = lane_base + static_cast<uint32_t>(ks) * kstep_bytes - (k2 ? 0u : back_k);
 #pragma unroll
           for (int j = 0; j < 8; j++) {
             const int mt = mg * 8 + j;
             if (mt < nMt) {
               const bool m2 = mt * 16 + 8 < hpad;  // second 8-row group present
-              int kg = 2 * ks + (mat >> 1), rg = 2 * mt + (mat & 1);
-              const bool valid = (!(mat & 2) || k2) && (!(mat & 1) || m2);
-              if (!valid) {
-                kg = 2 * ks;
-                rg = 2 * mt;
-              }
-              const uint32_t addr = sbase + 2u * static_cast<uint32_t>(kg * 8 * hpad + rg * 64 + mr * 8);
               uint32_t a0, a1, a2, a3;
-              ldmatrix_x4_trans(addr, a0, a1, a2, a3);
+              ldmatrix_x4_trans(kaddr + 256u * static_cast<uint32_t>(mt) - (m2 ? 0u : back_m), a0, a1, a2, a3);
               if (!m2) {
                 a1 = 0;
                 a3 = 0;
