@@ -36,6 +36,7 @@ constexpr int kThreads = 32 + kConsumers;
 // Partial sums per reduction buffer: Q * hpad <= 2 * kConsumers (FP64, 2 rows
 // per thread), <= 4 * kConsumers (FP32, 4 rows), kparts * hpad <= 1024 (BF16).
 template <typename G> constexpr int red_per_buf() { return sizeof(G) == 8 ? 2 * kConsumers : 1024; }
+static_assert(kHMax <= 2 * kConsumers, "each consumer thread writes at most two output rows of an item");
 
 // error words
 constexpr int kErrTimeoutEmpty = 0x101;
@@ -360,6 +361,8 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
   const int ct = threadIdx.x - 32;
   const int cw = warp - 1;
   uint32_t items = 0;
+  float pre_scale[2] = {1.f, 1.f};
+  long long pre_dst[2] = {0, 0};
   // FMA path state
   constexpr int R = kTensor ? 1 : Store<S>::kRows;
   int hv = 1, Q = 1, rv = 0, cq = 0;
@@ -394,6 +397,24 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
     const int ncols = d.ncols;
     const int hpad = d.hpad;
     const int rows = d.rows, out_off = d.out_off;
+    if (flags & kFirst) {
+      // Per-row output data of the item (BF16 t scale, or the permuted y
+      // index), loaded now so the latency is hidden behind the item's chunks.
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int r = ct + q * kConsumers;
+        pre_scale[q] = 1.f;
+        pre_dst[q] = out_off + r;
+        if (r < rows) {
+          if (a.phase == 1) {
+            if (a.t_scale) pre_scale[q] = a.t_scale[out_off + r];
+          } else if (a.perm_out) {
+            const int row = out_off + r;
+            pre_dst[q] = static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof);
+          }
+        }
+      }
+    }
     if constexpr (!kTensor) {
       if (flags & kFirst) {
         hv = hpad / R;
@@ -512,17 +533,16 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         if (lane == 0) set_error(a.err, kErrTimeoutReduce);
         return;
       }
-      for (int r = ct; r < rows; r += kConsumers) {
-        G sum = 0;
-        for (int q = 0; q < nred; q++) sum += rb[q * hpad + r];
-        if (a.phase == 1) {
-          if (a.t_scale) sum *= a.t_scale[out_off + r];
-          static_cast<G *>(a.t_out)[out_off + r] = sum;
-        } else {
-          const int row = out_off + r;
-          long long dst = row;
-          if (a.perm_out) dst = static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof);
-          a.y_out[dst] = static_cast<double>(sum);
+#pragma unroll
+      for (int q2 = 0; q2 < 2; q2++) {
+        const int r = ct + q2 * kConsumers;
+        if (r < rows) {
+          G sum = 0;
+          for (int q = 0; q < nred; q++) sum += rb[q * hpad + r];
+          if (a.phase == 1)
+            static_cast<G *>(a.t_out)[out_off + r] = sum * static_cast<G>(pre_scale[q2]);
+          else
+            a.y_out[pre_dst[q2]] = static_cast<double>(sum);
         }
       }
       items++;
