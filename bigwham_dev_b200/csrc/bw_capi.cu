@@ -197,6 +197,16 @@ template <typename S> void set_smem_attr() {
   if (dev < 64) done[dev] = true;
 }
 
+int64_t align256(int64_t v) { return (v + 255) / 256 * 256; }
+
+// Bytes of the gathered-x region for a precision: the G values (+16 bytes,
+// vector runs are staged in 16-byte aligned windows) and, for BF16, a second
+// array of packed hi/lo words at the next 256-byte boundary.
+int64_t xp_region_bytes(int prec, int64_t nin) {
+  if (prec == 2) return align256(4 * nin + 16) + 4 * nin + 16;
+  return nin * (prec == 0 ? 8 : 4) + 16;
+}
+
 // Bytes of the phase-2 gather array G2 over the stored precisions and operators.
 int64_t g2_bytes(const bw_hmat *h, int mask, bool with_t) {
   int64_t b = 0;
@@ -306,12 +316,16 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
   const int32_t *perm_in = permuted ? nullptr : (o == 0 ? h->d_perm1 : h->d_perm0);
   const int32_t *perm_out = permuted ? nullptr : (o == 0 ? h->d_perm0 : h->d_perm1);
   const int n_in = (int)op.n_in;
+  constexpr bool kPacked = bw::Store<S>::kRows == 0;  // tensor-core path takes pack_hilo vectors
   G *xp = static_cast<G *>(xp_buf);
+  // BF16: the packed copy of x sits after the FP32 one in the same region
+  uint32_t *xpk = kPacked ? reinterpret_cast<uint32_t *>(static_cast<unsigned char *>(xp_buf) +
+                                                         align256(4 * (int64_t)n_in + 16))
+                          : nullptr;
   G *t = static_cast<G *>(t_buf);
-  G *g2 = static_cast<G *>(g2_buf);
   if (ev) BW_CUDA(cudaEventRecord(ev[0], st));
   if (n_in > 0) {
-    bw::gather_x_kernel<G><<<(n_in + 255) / 256, 256, 0, st>>>(x, xp, perm_in, h->dof, n_in);
+    bw::gather_x_kernel<G><<<(n_in + 255) / 256, 256, 0, st>>>(x, xp, xpk, perm_in, h->dof, n_in);
     BW_CUDA(cudaGetLastError());
   }
   if (ev) BW_CUDA(cudaEventRecord(ev[1], st));
@@ -321,8 +335,8 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
     if (phase == 1) {
       if (dp.n_gsegs > 0) {
         const int per_block = 8;  // runs per 256-thread block (one warp each)
-        bw::gather_g2_kernel<G><<<(int)((dp.n_gsegs + per_block - 1) / per_block), 256, 0, st>>>(
-            dp.gsegs, (int)dp.n_gsegs, xp, t, g2);
+        bw::gather_g2_kernel<G, kPacked><<<(int)((dp.n_gsegs + per_block - 1) / per_block), 256, 0, st>>>(
+            dp.gsegs, (int)dp.n_gsegs, xp, t, g2_buf);
         BW_CUDA(cudaGetLastError());
       }
       if (ev) BW_CUDA(cudaEventRecord(ev[3], st));
@@ -332,7 +346,8 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
       a.data = dp.data;
       a.chunks = dp.chunks;
       a.cta_ptr = dp.cta;
-      a.gsrc = phase == 0 ? static_cast<const void *>(xp) : static_cast<const void *>(g2);
+      a.gsrc = phase == 0 ? (kPacked ? static_cast<const void *>(xpk) : static_cast<const void *>(xp))
+                          : static_cast<const void *>(g2_buf);
       a.t_out = t;
       a.t_scale = prec == 2 ? h->d_tscale[o] : nullptr;
       a.y_out = y;
@@ -536,7 +551,7 @@ int bw_finalize(bw_hmat *h, int flags) {
           BW_CUDA(cudaMemcpy(h->d_tscale[o], ts.data(), ts.size() * 4, cudaMemcpyHostToDevice));
         }
       // +16 bytes: the kernels stage vector segments in 16-byte aligned windows
-      h->d_xp = h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8 + 16);
+      h->d_xp = h->dmalloc((size_t)std::max({xp_region_bytes(0, nmax), xp_region_bytes(2, nmax), (int64_t)1}));
       h->d_t = h->dmalloc((size_t)std::max<int64_t>(1, h->sum_rank) * 8 + 16);
       h->d_g2 = h->dmalloc((size_t)std::max<int64_t>(1, g2_bytes(h, mask, want_t)) + 16);
       h->d_xh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
@@ -618,7 +633,7 @@ int bw_matvec_static_scratch(bw_hmat *h, const double *x, double *y, int flags, 
     // aligned windows)
     const int64_t gsize = p == 0 ? 8 : 4;
     const int o_ = tr ? 1 : 0;
-    const int64_t t_at = (nin * gsize + 16 + 255) / 256 * 256;
+    const int64_t t_at = align256(xp_region_bytes(p, nin));
     const int64_t g2_at = (t_at + h->sum_rank * gsize + 16 + 255) / 256 * 256;
     const int64_t need = g2_at + h->op[o_].ph[1].cp[p].g_len * gsize + 16;
     if (need > (int64_t)BW_STATIC_SCRATCH_BYTES)

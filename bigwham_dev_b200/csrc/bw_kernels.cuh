@@ -463,20 +463,17 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         if (ks < 0) ks += kparts;
         for (; ks < nks; ks += kparts) {
           // B fragment: lanes 0-3 hold the BF16-rounded vector (column 0),
-          // lanes 4-7 the BF16-rounded remainder (column 1), others zero.
+          // lanes 4-7 the BF16-rounded remainder (column 1), others zero;
+          // the vector arrives as pack_hilo words.
           uint32_t b0 = 0, b1 = 0;
           if (grp < 2) {
+            const uint32_t *gw = reinterpret_cast<const uint32_t *>(gs);
             const int c = 16 * ks + 2 * tq;
-            float v[4];
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-              const int ce = c + (e & 1) + (e >> 1) * 8;
-              const float x = ce < ncols ? gs[ce] : 0.f;
-              const float hi = __bfloat162float(__float2bfloat16_rn(x));
-              v[e] = grp == 0 ? hi : x - hi;
-            }
-            b0 = pack_bf16x2(v[0], v[1]);
-            b1 = pack_bf16x2(v[2], v[3]);
+            const uint32_t w0 = c < ncols ? gw[c] : 0u, w1 = c + 1 < ncols ? gw[c + 1] : 0u;
+            const uint32_t w2 = c + 8 < ncols ? gw[c + 8] : 0u, w3 = c + 9 < ncols ? gw[c + 9] : 0u;
+            const uint32_t sel = grp == 0 ? 0x5410u : 0x7632u;  // low halves (hi) or high halves (lo)
+            b0 = __byte_perm(w0, w1, sel);
+            b1 = __byte_perm(w2, w3, sel);
           }
           const bool k2 = 16 * ks + 8 < ncols;  // second 8-column group present
           const uint32_t kaddr = lane_base + static_cast<uint32_t>(ks) * kstep_bytes - (k2 ? 0u : back_k);
@@ -550,30 +547,48 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
   }
 }
 
+// BF16 path: a vector value v is handed to the tensor cores as two BF16
+// numbers, hi = bf16(v) and lo = bf16(v - hi), packed in one word (hi in the
+// low half), so the consumers build mma B fragments with a byte permute.
+__device__ __forceinline__ uint32_t pack_hilo(float v) {
+  const float hi = __bfloat162float(__float2bfloat16_rn(v));
+  return pack_bf16x2(hi, v - hi);
+}
+
 // G2[dst + c] = scale * src[src_off + c] for every run (src: gathered x or t):
 // the phase-2 vector values laid out chunk by chunk.  One warp per run.
-template <typename G>
+// kPacked: store pack_hilo(value) words (BF16 path) instead of G values.
+template <typename G, bool kPacked>
 __global__ void gather_g2_kernel(const GatherSeg *__restrict__ runs, int n_runs, const G *__restrict__ xp,
-                                 const G *__restrict__ t, G *__restrict__ g2) {
+                                 const G *__restrict__ t, void *__restrict__ g2) {
   const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (r >= n_runs) return;
   const GatherSeg gsg = runs[r];
   const int cols = static_cast<int>(gsg.cols_src & 0x7fffffffu);
   const G *src = (gsg.cols_src >> 31) ? t : xp;
   const G sc = static_cast<G>(gsg.scale);
-  for (int c = threadIdx.x & 31; c < cols; c += 32) g2[gsg.dst + c] = sc * src[gsg.src_off + c];
+  for (int c = threadIdx.x & 31; c < cols; c += 32) {
+    const G v = sc * src[gsg.src_off + c];
+    if constexpr (kPacked)
+      static_cast<uint32_t *>(g2)[gsg.dst + c] = pack_hilo(static_cast<float>(v));
+    else
+      static_cast<G *>(g2)[gsg.dst + c] = v;
+  }
 }
 
 // x (FP64, caller's ordering) -> gathered copy in the compute type, permuted
 // order: xp[dof*i + j] = x[dof*perm[i] + j] (Hmat::matvecOriginal,
 // src/hmat/hmatrix/hmat.cc:586-593), or a plain cast when perm is null.
+// xpk (BF16 path, else null) receives the same values as pack_hilo words.
 template <typename G>
-__global__ void gather_x_kernel(const double *__restrict__ x, G *__restrict__ xp, const int32_t *__restrict__ perm,
-                                int dof, int n) {
+__global__ void gather_x_kernel(const double *__restrict__ x, G *__restrict__ xp, uint32_t *__restrict__ xpk,
+                                const int32_t *__restrict__ perm, int dof, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int src = perm ? dof * perm[i / dof] + (i % dof) : i;
-  xp[i] = static_cast<G>(x[src]);
+  const G v = static_cast<G>(x[src]);
+  xp[i] = v;
+  if (xpk) xpk[i] = pack_hilo(static_cast<float>(v));
 }
 
 }  // namespace bw
