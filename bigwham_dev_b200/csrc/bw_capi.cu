@@ -356,7 +356,7 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
       a.phase = phase + 1;
       a.err = h->d_err;
       a.spin_limit = h->spin_limit;
-      bw::stream_panels_kernel<S><<<h->grid, bw::kThreads, bw::SmemLayout<S>::kTotal, st>>>(a);
+      bw::stream_panels_kernel<S><<<h->grid, bw::threads_of<S>(), bw::SmemLayout<S>::kTotal, st>>>(a);
       BW_CUDA(cudaGetLastError());
     }
     if (ev) BW_CUDA(cudaEventRecord(ev[phase == 0 ? 2 : 4], st));

@@ -30,13 +30,6 @@
 namespace bw {
 
 constexpr int kStages = 6;
-constexpr int kConsumerWarps = 8;
-constexpr int kConsumers = 32 * kConsumerWarps;
-constexpr int kThreads = 32 + kConsumers;
-// Partial sums per reduction buffer: Q * hpad <= 2 * kConsumers (FP64, 2 rows
-// per thread), <= 4 * kConsumers (FP32, 4 rows), kparts * hpad <= 1024 (BF16).
-template <typename G> constexpr int red_per_buf() { return sizeof(G) == 8 ? 2 * kConsumers : 1024; }
-static_assert(kHMax <= 2 * kConsumers, "each consumer thread writes at most two output rows of an item");
 
 // error words
 constexpr int kErrTimeoutEmpty = 0x101;
@@ -138,21 +131,33 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
 struct Bf16 {};  // storage tag: 16-bit brain float, 8x8-tiled items
 
 template <typename S> struct Store;
+// kWarps: consumer warps per CTA (the BF16 path is latency-bound and gets
+// more warps; the FMA paths already stream at the HBM roofline with 8).
+// kRed: partial sums per reduction buffer, Q * hpad <= kRows * consumers
+// (FMA paths) or kparts * hpad <= 16 * 128 (tensor path).
 template <> struct Store<double> {
   using G = double;   // compute / gather type
   static constexpr int kEsize = 8;
   static constexpr int kRows = 2;  // rows per consumer thread
+  static constexpr int kWarps = 8;
+  static constexpr int kRed = 2 * 32 * kWarps;
 };
 template <> struct Store<float> {
   using G = float;
   static constexpr int kEsize = 4;
   static constexpr int kRows = 4;
+  static constexpr int kWarps = 8;
+  static constexpr int kRed = 4 * 32 * kWarps;
 };
 template <> struct Store<Bf16> {
   using G = float;
   static constexpr int kEsize = 2;
   static constexpr int kRows = 0;  // tensor-core path
+  static constexpr int kWarps = 16;
+  static constexpr int kRed = 2048;
 };
+template <typename S> __host__ __device__ constexpr int consumers_of() { return 32 * Store<S>::kWarps; }
+template <typename S> __host__ __device__ constexpr int threads_of() { return 32 + consumers_of<S>(); }
 
 // Adds the partial sums of R adjacent rows over columns [c0, c1) of a
 // column-major chunk to o; the vector value of column c is g[c].
@@ -235,7 +240,8 @@ template <typename S> struct SmemLayout {
   // vector window: the chunk's run of values with up to 15 bytes of slack each side
   static constexpr int kGBytes = kMaxCols * (int)sizeof(G) + 32;
   static constexpr int kStageSize = kDataBytes + kGBytes + (int)sizeof(Chunk);
-  static constexpr int kRedPer = red_per_buf<G>();
+  static constexpr int kRedPer = Store<S>::kRed;
+  static_assert(kHMax <= 2 * consumers_of<S>(), "each consumer thread writes at most two output rows of an item");
   static constexpr int kRedBytes = 2 * kRedPer * (int)sizeof(G);
   static constexpr int kBarBytes = (2 * kStages + 1) * 8;
   static constexpr int kTotal = kStages * kStageSize + kRedBytes + kBarBytes;
@@ -265,11 +271,13 @@ __device__ __forceinline__ void load_desc(const Chunk *chunks, int idx, int end,
 }
 
 template <typename S>
-__global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a) {
+__global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(StreamArgs a) {
   using G = typename Store<S>::G;
   using L = SmemLayout<S>;
   constexpr int es = Store<S>::kEsize;
   constexpr bool kTensor = Store<S>::kRows == 0;
+  constexpr int kConsumerWarps = Store<S>::kWarps;
+  constexpr int kConsumers = consumers_of<S>();
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char *stage0 = smem;
   G *red = reinterpret_cast<G *>(smem + kStages * L::kStageSize);
@@ -372,6 +380,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
   for (int r = 0; r < R; r++) acc[r] = 0;
   // tensor path state
   int nMt = 1, kparts = 1, mg = 0, kp = 0;
+  int rot = 0;  // rotation of the K-step deal: chunk index within the item, mod kparts
   bool wact = false;
   float tacc[kTensor ? 8 : 1][4];
 #pragma unroll
@@ -438,6 +447,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         mg = cw / kparts;
         kp = cw % kparts;
         wact = mg < mgroups;
+        rot = 0;
 #pragma unroll
         for (int j = 0; j < 8; j++)
 #pragma unroll
@@ -457,8 +467,9 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         const uint32_t back_k = (mat & 2) ? 16u * static_cast<uint32_t>(hpad) : 0u;  // to group 2ks if absent
         const uint32_t back_m = (mat & 1) ? 128u : 0u;                               // to group 2mt if absent
         // K-steps are dealt round-robin, rotated every chunk so the warps
-        // share the remainder evenly over a stream of chunks.
-        const int rot = i % kparts;
+        // share the remainder evenly over the item's chunks (the rotation
+        // depends only on the chunk's place in its item: results do not
+        // depend on the schedule).
         int ks = kp - rot;
         if (ks < 0) ks += kparts;
         for (; ks < nks; ks += kparts) {
@@ -498,6 +509,7 @@ __global__ void __launch_bounds__(kThreads, 1) stream_panels_kernel(StreamArgs a
         }
       }
     }
+    if constexpr (kTensor) rot = rot + 1 == kparts ? 0 : rot + 1;
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     if (flags & kLast) {

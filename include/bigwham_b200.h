@@ -99,7 +99,7 @@ int bw_finalize(bw_hmat *h, int flags);
 int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream);
 
 /* Bytes of device memory reserved by bw_matvec_static_scratch (per device). */
-#define BW_STATIC_SCRATCH_BYTES (16u << 20)
+#define BW_STATIC_SCRATCH_BYTES (64u << 20)
 
 /* y = H x like bw_matvec, but without any device allocation, ever: for callers
  * that cannot let a library call cudaMalloc -- a process whose device memory
@@ -107,12 +107,13 @@ int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream);
  * reserved the card up front), or a latency-critical path where cudaMalloc /
  * cudaFree are not allowed because they can synchronize the device.  The
  * caller passes x and y; the scratch vectors live in a fixed device array of
- * BW_STATIC_SCRATCH_BYTES (16 MiB) compiled into the library, which every GPU
+ * BW_STATIC_SCRATCH_BYTES (64 MiB) compiled into the library, which every GPU
  * that loads the library holds until the process exits.  H-matrices needing
  * more scratch than that are rejected with BW_ERR_ARG: 8 bytes (FP64) or 4
  * (FP32, BF16) per input, per low-rank rank column and per column of every row
- * panel (the phase-2 gather array), e.g. about 12 MB in FP32 at 49,152 DoF and
- * 42 MB at 196,608 DoF.
+ * panel (the phase-2 gather array).  For the 3DR0-H square crack that is
+ * 14 MB (FP64) or 7 MB (FP32, BF16) at 12,288 DoF and 40 MB or 20 MB at
+ * 49,152 DoF; the 196,608-DoF matrix needs more and is rejected.
  * The first call on a device looks the array's address up (once per device);
  * make that first call before any stream capture.  Every call overwrites the
  * scratch before reading it, so nothing in it needs to start at zero, and the

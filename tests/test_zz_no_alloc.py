@@ -1,7 +1,7 @@
 """bw_matvec_static_scratch: the matvec for callers that cannot let a library
 allocate device memory (their memory belongs to another allocator, or
 cudaMalloc/cudaFree's possible device-wide synchronization is not allowed on
-their path).  Its scratch lives in a fixed 16 MiB device array compiled into
+their path).  Its scratch lives in a fixed 64 MiB device array compiled into
 the library instead of memory allocated per handle.
 
 Checked through the C ABI against bw_matvec on the same handle, two calls in a
@@ -55,8 +55,8 @@ def test_static_scratch_rejects_oversize():
     import torch
 
     # one rank-1 block over n x n: the gathered input alone (8 bytes per input
-    # in FP64) exceeds the 16 MiB static scratch
-    n = 2_200_000
+    # in FP64) exceeds the 64 MiB static scratch
+    n = 9_000_000
     h = HmatGpu(1, n, n, np.arange(n), np.arange(n), device=0)
     h.add_lowrank(0, 0, np.ones((n, 1)), np.ones((1, n)))
     h.finalize(precisions=("fp64",))
