@@ -263,7 +263,17 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
       while (qe < nit && (item_start(qe + 1) - item_start(q)) * es <= (int64_t)kPiece) qe++;
       const int64_t e0 = item_start(q), e1 = item_start(qe);
       const size_t bytes = (size_t)(e1 - e0) * es;
-      if (bytes > kPiece) throw std::runtime_error("item larger than the staging piece");
+      if (bytes > kPiece) {
+        // a single item larger than the staging piece: fill a one-off host
+        // buffer and copy it synchronously
+        std::vector<unsigned char> big(bytes, 0);
+        bw::fill_items(h->prob, o == 1, op, phase, prec, q, qe, e0, big.data());
+        BW_CUDA(cudaStreamSynchronize(h->stream));
+        BW_CUDA(cudaMemcpy(static_cast<unsigned char *>(dp.data) + (size_t)e0 * es, big.data(), bytes,
+                           cudaMemcpyHostToDevice));
+        q = qe;
+        continue;
+      }
       if (used[which]) BW_CUDA(cudaEventSynchronize(ev[which]));
       std::memset(stage[which], 0, bytes);
       bw::fill_items(h->prob, o == 1, op, phase, prec, q, qe, e0, stage[which]);
