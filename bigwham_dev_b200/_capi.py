@@ -27,6 +27,9 @@ _P = C.c_void_p
 _I64 = C.c_int64
 _SIGS = {
     "bw_create": (C.c_int, [C.c_int, _I64, _I64, _P, _P, C.c_int, C.POINTER(_P)]),
+    "bw_create_batch": (C.c_int, [C.c_int, C.c_int, _P, _P, _P, _P, C.c_int, C.POINTER(_P)]),
+    "bw_batch_offsets": (C.c_int, [_P, C.c_int, _P, _P]),
+    "bw_batch_count": (C.c_int, [_P]),
     "bw_add_full": (C.c_int, [_P, _I64, _I64, _I64, _I64, _P, _I64]),
     "bw_add_lowrank": (C.c_int, [_P, _I64, _I64, _I64, _I64, _I64, _P, _I64, _P, _I64]),
     "bw_finalize": (C.c_int, [_P, C.c_int]),

@@ -70,6 +70,7 @@ struct bw_hmat {
   int dof = 1;
   int64_t n_rows = 0, n_cols = 0;
   std::vector<int64_t> perm0, perm1;
+  std::vector<int64_t> row_off, col_off;  // member k: rows [row_off[k], row_off[k+1]) (bw_create_batch)
   bw::Problem prob;
   bool finalized = false;
   bool plan_only = false;
@@ -423,8 +424,22 @@ extern "C" {
 
 const char *bw_version(void) { return "bigwham_b200 0.1 (sm_100a)"; }
 
+int bw_batch_offsets(const bw_hmat *h, int member, int64_t *row0, int64_t *col0) {
+  if (!h || member < 0 || member + 1 >= (int)h->row_off.size()) return BW_ERR_ARG;
+  if (row0) *row0 = h->row_off[(size_t)member];
+  if (col0) *col0 = h->col_off[(size_t)member];
+  return BW_OK;
+}
+
+int bw_batch_count(const bw_hmat *h) { return h ? (int)h->row_off.size() - 1 : 0; }
+
 int bw_create(int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0, const int64_t *perm1, int device,
               bw_hmat **out) {
+  return bw_create_batch(dof, 1, &n_rows, &n_cols, &perm0, &perm1, device, out);
+}
+
+int bw_create_batch(int dof, int count, const int64_t *n_rows_k, const int64_t *n_cols_k,
+                    const int64_t *const *perm0_k, const int64_t *const *perm1_k, int device, bw_hmat **out) {
   if (!out) return BW_ERR_ARG;
   *out = nullptr;
   auto fail = [](const std::string &m, int code) {
@@ -432,16 +447,39 @@ int bw_create(int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0, con
     g_last_create_error = m;
     return code;
   };
-  if (dof < 1 || n_rows < 0 || n_cols < 0 || n_rows % dof || n_cols % dof)
-    return fail("bad sizes: n_rows and n_cols must be non-negative multiples of dof >= 1", BW_ERR_ARG);
-  if (n_rows > INT32_MAX || n_cols > INT32_MAX) return fail("sizes above 2^31-1 are not supported", BW_ERR_ARG);
-  if ((n_rows && !perm0) || (n_cols && !perm1)) return fail("null permutation", BW_ERR_ARG);
+  if (count < 1 || !n_rows_k || !n_cols_k || !perm0_k || !perm1_k) return fail("bad member list", BW_ERR_ARG);
+  if (dof < 1) return fail("bad sizes: dof must be >= 1", BW_ERR_ARG);
   std::unique_ptr<bw_hmat> h(new bw_hmat);
+  // Members are laid along the diagonal of one block-diagonal H-matrix: member
+  // k's rows and columns start at the sums of the earlier members' sizes, and
+  // its permutations are shifted by the earlier members' point counts.
+  int64_t n_rows = 0, n_cols = 0;
+  for (int k = 0; k < count; k++) {
+    const int64_t m = n_rows_k[k], n = n_cols_k[k];
+    if (m < 0 || n < 0 || m % dof || n % dof)
+      return fail("bad sizes: n_rows and n_cols must be non-negative multiples of dof >= 1", BW_ERR_ARG);
+    if ((m && !perm0_k[k]) || (n && !perm1_k[k])) return fail("null permutation", BW_ERR_ARG);
+    if (m > INT32_MAX - n_rows || n > INT32_MAX - n_cols) return fail("sizes above 2^31-1 are not supported", BW_ERR_ARG);
+    h->row_off.push_back(n_rows);
+    h->col_off.push_back(n_cols);
+    for (int64_t i = 0; i < m / dof; i++) {
+      const int64_t v = perm0_k[k][i];
+      if (v < 0 || v >= m / dof) return fail("permutation is not a permutation of 0..n-1", BW_ERR_ARG);
+      h->perm0.push_back(v + n_rows / dof);
+    }
+    for (int64_t i = 0; i < n / dof; i++) {
+      const int64_t v = perm1_k[k][i];
+      if (v < 0 || v >= n / dof) return fail("permutation is not a permutation of 0..n-1", BW_ERR_ARG);
+      h->perm1.push_back(v + n_cols / dof);
+    }
+    n_rows += m;
+    n_cols += n;
+  }
+  h->row_off.push_back(n_rows);
+  h->col_off.push_back(n_cols);
   h->dof = dof;
   h->n_rows = n_rows;
   h->n_cols = n_cols;
-  h->perm0.assign(perm0, perm0 + n_rows / dof);
-  h->perm1.assign(perm1, perm1 + n_cols / dof);
   for (auto *pv : {&h->perm0, &h->perm1}) {
     const int64_t np = (int64_t)pv->size();
     std::vector<char> seen((size_t)np, 0);
@@ -453,6 +491,10 @@ int bw_create(int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0, con
   h->prob.dof = dof;
   h->prob.n_rows = n_rows;
   h->prob.n_cols = n_cols;
+  if (count > 1) {
+    h->prob.row_off = h->row_off;
+    h->prob.col_off = h->col_off;
+  }
   h->device = device;
   if (device >= 0) {
     int ndev = 0;

@@ -152,8 +152,16 @@ void build_operator(const Problem &p, bool tr, int grid, OperatorPlan &op) {
     }
   }
 
+  // batch members along the output and input axes (one member if none given)
+  std::vector<int64_t> out_off{0, n_out}, in_off{0, n_in};
+  if (!p.row_off.empty()) {
+    out_off = tr ? p.col_off : p.row_off;
+    in_off = tr ? p.row_off : p.col_off;
+  }
+
   // ---- row panels: finest partition of [0, n_out) by block row boundaries
-  std::vector<int64_t> bounds{0, n_out};
+  // (and member boundaries)
+  std::vector<int64_t> bounds(out_off.begin(), out_off.end());
   for (size_t k = 0; k < nfr; k++) {
     EffFull b = eff_full(p, tr, k);
     bounds.push_back(b.i0);
@@ -197,12 +205,18 @@ void build_operator(const Problem &p, bool tr, int grid, OperatorPlan &op) {
     for (size_t q = first_panel(b.i0); q < npan && pb[q] < b.i0 + b.m; q++)
       cov[q].push_back({1, (int64_t)k, b.j0, b.n});
   }
-  // coverage: the column intervals of each panel must tile [0, n_in) exactly
+  // coverage: the column intervals of each panel must tile its member's
+  // columns [in_off[k], in_off[k+1]) exactly ([0, n_in) for one member)
   for (size_t q = 0; q < npan; q++) {
     auto &c = cov[q];
     std::sort(c.begin(), c.end(), [](const Cover &a, const Cover &b) { return a.j0 < b.j0; });
-    int64_t at = 0;
+    const size_t mk = static_cast<size_t>(std::upper_bound(out_off.begin(), out_off.end(), pb[q]) - out_off.begin()) - 1;
+    const int64_t lo = in_off[mk], hi = in_off[mk + 1];
+    int64_t at = lo;
     for (const Cover &e : c) {
+      if (e.j0 < lo || e.j0 + e.n > hi)
+        fail("a block in rows [" + std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) +
+             ") reaches outside its batch member's columns");
       if (e.j0 < at)
         fail("blocks overlap in rows [" + std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
       if (e.j0 > at)
@@ -210,8 +224,8 @@ void build_operator(const Problem &p, bool tr, int grid, OperatorPlan &op) {
              std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
       at = e.j0 + e.n;
     }
-    if (at != n_in)
-      fail("columns [" + std::to_string(at) + ", " + std::to_string(n_in) + ") not covered in rows [" +
+    if (at != hi)
+      fail("columns [" + std::to_string(at) + ", " + std::to_string(hi) + ") not covered in rows [" +
            std::to_string(pb[q]) + ", " + std::to_string(pb[q + 1]) + ")");
   }
 

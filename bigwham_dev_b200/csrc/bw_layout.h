@@ -142,6 +142,10 @@ struct Problem {
   int64_t n_rows = 0, n_cols = 0;
   std::vector<FullBlock> fr;
   std::vector<LowRankBlock> lr;
+  // Batch members (block-diagonal problem): member k owns rows
+  // [row_off[k], row_off[k+1]) and columns [col_off[k], col_off[k+1]); blocks
+  // must tile each member's diagonal block.  Empty: one member.
+  std::vector<int64_t> row_off, col_off;
 };
 
 // Validates the pattern and builds the structural plan (items) of the operator

@@ -75,12 +75,13 @@ class HmatGpu:
                                          Amat.ctypes.data, max(1, Amat.shape[0]), Bmat.ctypes.data,
                                          max(1, Bmat.shape[0])), self._h)
 
-    def add_flat(self, fr, lr, fr_data, lr_data) -> None:
+    def add_flat(self, fr, lr, fr_data, lr_data, row0: int = 0, col0: int = 0) -> None:
         """Register all blocks from flat arrays laid out like the reference's
         block containers: FR blocks back to back (column-major), and per LR
         block A (m x r) then B (r x n).  fr rows: (i0, j0, iend, jend) and lr
         rows (i0, j0, iend, jend, r) in collocation-point units (HPattern,
-        h_pattern.h:21-33).  Zero-copy: the arrays are borrowed until finalize."""
+        h_pattern.h:21-33), shifted by the scalar offsets row0 / col0 (a batch
+        member's place).  Zero-copy: the arrays are borrowed until finalize."""
         d = self.dof
         fr = np.asarray(fr, dtype=np.int64).reshape(-1, 4)
         lr = np.asarray(lr, dtype=np.int64).reshape(-1, 5)
@@ -93,7 +94,8 @@ class HmatGpu:
             m, n = int(i1 - i0) * d, int(j1 - j0) * d
             if (o + m * n) > fr_data.size:
                 raise ValueError("fr_data shorter than the pattern says")
-            A.check(self._lib.bw_add_full(self._h, int(i0) * d, int(j0) * d, m, n, base + 8 * o, m), self._h)
+            A.check(self._lib.bw_add_full(self._h, row0 + int(i0) * d, col0 + int(j0) * d, m, n, base + 8 * o, m),
+                    self._h)
             o += m * n
         base = lr_data.ctypes.data
         o = 0
@@ -101,7 +103,8 @@ class HmatGpu:
             m, n, r = int(i1 - i0) * d, int(j1 - j0) * d, int(r)
             if (o + r * (m + n)) > lr_data.size:
                 raise ValueError("lr_data shorter than the pattern says")
-            A.check(self._lib.bw_add_lowrank(self._h, int(i0) * d, int(j0) * d, m, n, r, base + 8 * o, max(1, m),
+            A.check(self._lib.bw_add_lowrank(self._h, row0 + int(i0) * d, col0 + int(j0) * d, m, n, r, base + 8 * o,
+                                             max(1, m),
                                              base + 8 * (o + m * r), max(1, r)), self._h)
             o += r * (m + n)
 
@@ -131,6 +134,44 @@ class HmatGpu:
         h = cls(dof, n_rows, n_cols, perm0, perm1, device)
         h.add_flat(fr, lr, fr_data, lr_data)
         return h.finalize(**kw)
+
+    @classmethod
+    def batch(cls, members, device: int = 0, **kw) -> "HmatGpu":
+        """One handle for several independent H-matrices of the same dof
+        (bw_create_batch): the block-diagonal H-matrix of the members, applied
+        by one matvec.  members: objects with the fields of a flat block list
+        (dof, n_rows, n_cols, fr, lr, fr_data, lr_data, perm0, perm1).  x and y
+        hold the members' vectors back to back; ``row_offsets`` /
+        ``col_offsets`` (count + 1 entries) give where each starts."""
+        members = list(members)
+        if not members:
+            raise ValueError("empty batch")
+        dof = int(members[0].dof)
+        if any(int(m.dof) != dof for m in members):
+            raise ValueError("all members of a batch must have the same dof")
+        p0 = [np.ascontiguousarray(m.perm0, dtype=np.int64) for m in members]
+        p1 = [np.ascontiguousarray(m.perm1, dtype=np.int64) for m in members]
+        nr = np.array([int(m.n_rows) for m in members], dtype=np.int64)
+        nc = np.array([int(m.n_cols) for m in members], dtype=np.int64)
+        pp0 = (C.c_void_p * len(members))(*[a.ctypes.data for a in p0])
+        pp1 = (C.c_void_p * len(members))(*[a.ctypes.data for a in p1])
+        self = cls.__new__(cls)
+        self._lib = A.lib()
+        self.dof, self.n_rows, self.n_cols, self.device = dof, int(nr.sum()), int(nc.sum()), int(device)
+        h = C.c_void_p()
+        A.check(self._lib.bw_create_batch(dof, len(members), nr.ctypes.data, nc.ctypes.data, pp0, pp1, self.device,
+                                          C.byref(h)), None)
+        self._h = h
+        self._keep = []
+        self._finalized = False
+        self.precisions = ()
+        self.has_transpose = False
+        self.row_offsets = np.concatenate([[0], np.cumsum(nr)])
+        self.col_offsets = np.concatenate([[0], np.cumsum(nc)])
+        for k, m in enumerate(members):
+            self.add_flat(m.fr, m.lr, m.fr_data, m.lr_data, row0=int(self.row_offsets[k]),
+                          col0=int(self.col_offsets[k]))
+        return self.finalize(**kw)
 
     # ------------------------------------------------------------------ application
     @property

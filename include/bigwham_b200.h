@@ -66,6 +66,24 @@ enum {
 int bw_create(int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0, const int64_t *perm1, int device,
               bw_hmat **out);
 
+/* Create one handle for `count` independent H-matrices with the same dof
+ * ("members"); one bw_matvec then applies all of them in the same four
+ * launches.  The handle is the block-diagonal H-matrix diag(H_0, ..., H_{count-1}):
+ * member k's rows and columns start at the sums of the earlier members'
+ * n_rows / n_cols (bw_batch_offsets), its blocks are added with bw_add_full /
+ * bw_add_lowrank at those offsets, and x / y are the members' vectors back to
+ * back.  perm0[k], perm1[k]: member k's own permutations, as for bw_create.
+ * No reference counterpart (the reference applies one Hmat per call). */
+int bw_create_batch(int dof, int count, const int64_t *n_rows, const int64_t *n_cols, const int64_t *const *perm0,
+                    const int64_t *const *perm1, int device, bw_hmat **out);
+
+/* First scalar row and column of member k of a bw_create_batch handle (a
+ * bw_create handle has the one member 0 at (0, 0)). */
+int bw_batch_offsets(const bw_hmat *h, int member, int64_t *row0, int64_t *col0);
+
+/* Number of members (1 for a bw_create handle, 0 for NULL). */
+int bw_batch_count(const bw_hmat *h);
+
 /* Register a full-rank block: rows [i0, i0+m), cols [j0, j0+n), column-major
  * with leading dimension lda >= m.  The pointer is BORROWED until bw_finalize
  * returns (no copy is made before then).
