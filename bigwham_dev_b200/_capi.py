@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libbigwham_b200.so")
 
 BW_OK, BW_ERR_ARG, BW_ERR_STATE, BW_ERR_OOM, BW_ERR_CUDA, BW_ERR_DEVICE, BW_ERR_UNSUPPORTED = range(7)
 BW_FP64, BW_FP32, BW_BF16 = 1, 2, 4
-BW_STORE_TRANSPOSE, BW_NO_FINITE_CHECK, BW_PLAN_ONLY = 16, 32, 64
+BW_STORE_TRANSPOSE, BW_NO_FINITE_CHECK, BW_PLAN_ONLY, BW_STORE_MATMAT = 16, 32, 64, 128
 BW_PERMUTED, BW_TRANSPOSE = 256, 512
 
 STATUS_NAMES = {BW_ERR_ARG: "BW_ERR_ARG", BW_ERR_STATE: "BW_ERR_STATE", BW_ERR_OOM: "BW_ERR_OOM",
@@ -48,6 +48,7 @@ _SIGS = {
     "bw_timing_read": (C.c_int, [_P, _P, _P]),
     "bw_phase_bytes": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
     "bw_plan_tscale": (C.c_int, [_P, C.c_int, _P, _P]),
+    "bw_mm_plan_export": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "bw_plan_gather": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
     "bw_destroy": (C.c_int, [_P]),
     "bw_version": (C.c_char_p, []),

@@ -33,6 +33,8 @@ def _apply_columns(op, x: torch.Tensor, precision: str, transpose: bool, permute
         y = torch.empty(nout, dtype=torch.float64, device=x.device)
         op.matvec(xd.contiguous(), precision, transpose=transpose, permuted=permuted, out=y)
         return y
+    if hasattr(op, "matmat"):  # one call: the tensor-core path where the handle has it
+        return op.matmat(xd, precision, permuted=permuted, transpose=transpose)
     xt = xd.t().contiguous()  # (k, n): each right-hand side contiguous
     yt = torch.empty(xt.shape[0], nout, dtype=torch.float64, device=x.device)
     for k in range(xt.shape[0]):

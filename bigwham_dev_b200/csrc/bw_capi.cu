@@ -12,6 +12,7 @@
 
 #include "bigwham_b200.h"
 #include "bw_kernels.cuh"
+#include "bw_mm_kernels.cuh"
 #include "bw_layout.h"
 
 namespace {
@@ -63,6 +64,14 @@ struct DevPhase {
   int64_t n_gsegs = 0;
 };
 
+// Device data of one matmat phase (bw::MmPlan).
+struct DevMm {
+  uint16_t *data = nullptr;
+  bw::MmChunk *chunks = nullptr;
+  int32_t *cta = nullptr;
+  int64_t n_chunks = 0;
+};
+
 }  // namespace
 
 struct bw_hmat {
@@ -80,6 +89,11 @@ struct bw_hmat {
   bw::OperatorPlan op[2];  // forward, transposed
   DevPhase dev[2][3][2];   // [operator][precision][phase]
   std::vector<unsigned char> host_data[2][3][2];  // BW_PLAN_ONLY
+  bool has_mm = false;     // matmat layout stored (BW_STORE_MATMAT)
+  bw::MmPlan mm[2];        // forward, transposed
+  DevMm dmm[2][2];         // [operator][phase]
+  std::vector<uint16_t> mm_host[2][2];  // BW_PLAN_ONLY
+  uint16_t *d_xt = nullptr, *d_t8 = nullptr;  // matmat operands (8x8 BF16 tiles, bw::kMmRhs columns)
   int32_t *d_perm0 = nullptr, *d_perm1 = nullptr;
   float *d_tscale[2] = {nullptr, nullptr};  // BF16 per-t-entry scales, per operator
   void *d_xp = nullptr, *d_t = nullptr, *d_g2 = nullptr;
@@ -136,6 +150,16 @@ struct bw_hmat {
           cudaFree(ph.gsegs);
           ph = DevPhase{};
         }
+    for (auto &o : dmm)
+      for (auto &ph : o) {
+        cudaFree(ph.data);
+        cudaFree(ph.chunks);
+        cudaFree(ph.cta);
+        ph = DevMm{};
+      }
+    cudaFree(d_xt);
+    cudaFree(d_t8);
+    d_xt = d_t8 = nullptr;
     cudaFree(d_perm0);
     cudaFree(d_perm1);
     cudaFree(d_tscale[0]);
@@ -217,6 +241,70 @@ int64_t g2_bytes(const bw_hmat *h, int mask, bool with_t) {
   return b;
 }
 
+// Copies an array of `n_elems` elements of `es` bytes to `dev`, built on the
+// host in pieces of whole items through two pinned staging buffers:
+// item_start(q) is the first element of item q (item_start(nit) = end of the
+// last item), fill(q0, q1, e0, dst) writes items [q0, q1) into zeroed dst whose
+// first element is element e0.  The slack after the last item is zeroed.
+template <typename StartF, typename FillF>
+void staged_upload(bw_hmat *h, void *dev, int64_t n_elems, int es, int64_t nit, StartF item_start, FillF fill) {
+  const size_t kPiece = size_t(256) << 20;
+  unsigned char *stage[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  BW_CUDA(cudaMallocHost(&stage[0], kPiece));
+  BW_CUDA(cudaMallocHost(&stage[1], kPiece));
+  BW_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  BW_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  bool used[2] = {false, false};
+  try {
+    int64_t q = 0;
+    int which = 0;
+    while (q < nit) {
+      // grow the piece while it fits (at least one item)
+      int64_t qe = q + 1;
+      while (qe < nit && (item_start(qe + 1) - item_start(q)) * es <= (int64_t)kPiece) qe++;
+      const int64_t e0 = item_start(q), e1 = item_start(qe);
+      const size_t bytes = (size_t)(e1 - e0) * es;
+      if (bytes > kPiece) {
+        // a single item larger than the staging piece: fill a one-off host
+        // buffer and copy it synchronously
+        std::vector<unsigned char> big(bytes, 0);
+        fill(q, qe, e0, big.data());
+        BW_CUDA(cudaStreamSynchronize(h->stream));
+        BW_CUDA(cudaMemcpy(static_cast<unsigned char *>(dev) + (size_t)e0 * es, big.data(), bytes,
+                           cudaMemcpyHostToDevice));
+        q = qe;
+        continue;
+      }
+      if (used[which]) BW_CUDA(cudaEventSynchronize(ev[which]));
+      std::memset(stage[which], 0, bytes);
+      fill(q, qe, e0, stage[which]);
+      BW_CUDA(cudaMemcpyAsync(static_cast<unsigned char *>(dev) + (size_t)e0 * es, stage[which], bytes,
+                              cudaMemcpyHostToDevice, h->stream));
+      BW_CUDA(cudaEventRecord(ev[which], h->stream));
+      used[which] = true;
+      which ^= 1;
+      q = qe;
+    }
+    // tail slack
+    const int64_t tail0 = item_start(nit);
+    BW_CUDA(cudaMemsetAsync(static_cast<unsigned char *>(dev) + (size_t)tail0 * es, 0,
+                            (size_t)(n_elems - tail0) * es, h->stream));
+    BW_CUDA(cudaStreamSynchronize(h->stream));
+  } catch (...) {
+    cudaStreamSynchronize(h->stream);
+    cudaFreeHost(stage[0]);
+    cudaFreeHost(stage[1]);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    throw;
+  }
+  cudaFreeHost(stage[0]);
+  cudaFreeHost(stage[1]);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+}
+
 // Upload the data of one phase in pieces through two pinned staging buffers.
 void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   const bw::OperatorPlan &op = h->op[o];
@@ -245,63 +333,38 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
     BW_CUDA(cudaMemcpy(dp.gsegs, cp.gsegs.data(), cp.gsegs.size() * sizeof(bw::GatherSeg), cudaMemcpyHostToDevice));
   }
 
-  const size_t kPiece = size_t(256) << 20;
-  unsigned char *stage[2] = {nullptr, nullptr};
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  BW_CUDA(cudaMallocHost(&stage[0], kPiece));
-  BW_CUDA(cudaMallocHost(&stage[1], kPiece));
-  BW_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-  BW_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
-  bool used[2] = {false, false};
-  try {
-    const int64_t nit = (int64_t)ph.items.size();
-    auto item_start = [&](int64_t q) { return q < nit ? ph.items[q].off[prec] : ph.n_elems[prec]; };
-    int64_t q = 0;
-    int which = 0;
-    while (q < nit) {
-      // grow the piece while it fits (at least one item)
-      int64_t qe = q + 1;
-      while (qe < nit && (item_start(qe + 1) - item_start(q)) * es <= (int64_t)kPiece) qe++;
-      const int64_t e0 = item_start(q), e1 = item_start(qe);
-      const size_t bytes = (size_t)(e1 - e0) * es;
-      if (bytes > kPiece) {
-        // a single item larger than the staging piece: fill a one-off host
-        // buffer and copy it synchronously
-        std::vector<unsigned char> big(bytes, 0);
-        bw::fill_items(h->prob, o == 1, op, phase, prec, q, qe, e0, big.data());
-        BW_CUDA(cudaStreamSynchronize(h->stream));
-        BW_CUDA(cudaMemcpy(static_cast<unsigned char *>(dp.data) + (size_t)e0 * es, big.data(), bytes,
-                           cudaMemcpyHostToDevice));
-        q = qe;
-        continue;
-      }
-      if (used[which]) BW_CUDA(cudaEventSynchronize(ev[which]));
-      std::memset(stage[which], 0, bytes);
-      bw::fill_items(h->prob, o == 1, op, phase, prec, q, qe, e0, stage[which]);
-      BW_CUDA(cudaMemcpyAsync(static_cast<unsigned char *>(dp.data) + (size_t)e0 * es, stage[which], bytes,
-                              cudaMemcpyHostToDevice, h->stream));
-      BW_CUDA(cudaEventRecord(ev[which], h->stream));
-      used[which] = true;
-      which ^= 1;
-      q = qe;
-    }
-    // tail slack
-    const int64_t tail0 = item_start(nit);
-    BW_CUDA(cudaMemsetAsync(static_cast<unsigned char *>(dp.data) + (size_t)tail0 * es, 0,
-                            (size_t)(ph.n_elems[prec] - tail0) * es, h->stream));
-    BW_CUDA(cudaStreamSynchronize(h->stream));
-  } catch (...) {
-    cudaStreamSynchronize(h->stream);
-    cudaFreeHost(stage[0]);
-    cudaFreeHost(stage[1]);
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
-    throw;
+  const int64_t nit = (int64_t)ph.items.size();
+  staged_upload(
+      h, dp.data, ph.n_elems[prec], es, nit,
+      [&](int64_t q) { return q < nit ? ph.items[q].off[prec] : ph.n_elems[prec]; },
+      [&](int64_t q0, int64_t q1, int64_t e0, void *dst) {
+        bw::fill_items(h->prob, o == 1, op, phase, prec, q0, q1, e0, dst);
+      });
+}
+
+// Upload one phase of the matmat layout (plan, chunks and BF16 data).
+void upload_mm_phase(bw_hmat *h, int o, int phase) {
+  const bw::MmPhase &ph = h->mm[o].ph[phase];
+  const int64_t nit = (int64_t)ph.items.size();
+  if (h->plan_only) {
+    auto &buf = h->mm_host[o][phase];
+    buf.assign((size_t)ph.n_elems, 0);
+    bw::fill_mm_items(h->prob, o == 1, h->mm[o], phase, 0, nit, 0, buf.data());
+    return;
   }
-  cudaFreeHost(stage[0]);
-  cudaFreeHost(stage[1]);
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
+  DevMm &dm = h->dmm[o][phase];
+  dm.n_chunks = (int64_t)ph.chunks.size();
+  dm.data = static_cast<uint16_t *>(h->dmalloc((size_t)ph.n_elems * 2));
+  dm.chunks = static_cast<bw::MmChunk *>(h->dmalloc(std::max<size_t>(1, ph.chunks.size()) * sizeof(bw::MmChunk)));
+  dm.cta = static_cast<int32_t *>(h->dmalloc(ph.cta_ptr.size() * sizeof(int32_t)));
+  if (!ph.chunks.empty())
+    BW_CUDA(cudaMemcpy(dm.chunks, ph.chunks.data(), ph.chunks.size() * sizeof(bw::MmChunk), cudaMemcpyHostToDevice));
+  BW_CUDA(cudaMemcpy(dm.cta, ph.cta_ptr.data(), ph.cta_ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  staged_upload(
+      h, dm.data, ph.n_elems, 2, nit, [&](int64_t q) { return q < nit ? ph.items[q].off : ph.n_elems; },
+      [&](int64_t q0, int64_t q1, int64_t e0, void *dst) {
+        bw::fill_mm_items(h->prob, o == 1, h->mm[o], phase, q0, q1, e0, static_cast<uint16_t *>(dst));
+      });
 }
 
 void compute_diagonal(bw_hmat *h) {
@@ -409,6 +472,57 @@ void *static_scratch_ptr(int device) {
     g_static_ptr[device] = p;
   }
   return g_static_ptr[device];
+}
+
+// Rows of the matmat operand X: the largest input size rounded up to a tile
+// row, plus two tile rows that the widened windows of the last columns reach.
+int64_t mm_xt_rows(const bw_hmat *h) { return (std::max(h->n_rows, h->n_cols) + 7) / 8 * 8 + 16; }
+
+// Y[:, 0:nrhs] = op X[:, 0:nrhs] on the tensor cores, in passes of kMmRhs
+// right-hand sides: X gather (+ permutation) into 8x8 BF16 tiles, phase 1
+// (T8 = stacked B factors x X), phase 2 (row panels -> Y).
+void launch_matmat_tc(bw_hmat *h, int o, const double *X, int64_t ldx, double *Y, int64_t ldy, int nrhs, bool permuted,
+                      cudaStream_t st) {
+  static bool attr_done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64 || !attr_done[dev]) {
+    BW_CUDA(cudaFuncSetAttribute(bw::mm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bw::kMmSmem));
+    if (dev < 64) attr_done[dev] = true;
+  }
+  const bw::MmPlan &mm = h->mm[o];
+  const int32_t *perm_in = permuted ? nullptr : (o == 0 ? h->d_perm1 : h->d_perm0);
+  const int32_t *perm_out = permuted ? nullptr : (o == 0 ? h->d_perm0 : h->d_perm1);
+  const int n_in = (int)mm.n_in;
+  const int n_pad = (n_in + 7) / 8 * 8;
+  for (int c0 = 0; c0 < nrhs; c0 += bw::kMmRhs) {
+    const int nr = std::min(bw::kMmRhs, nrhs - c0);
+    if (n_pad > 0) {
+      bw::gather_xt_kernel<<<(n_pad + 63) / 64, 256, 0, st>>>(X + (int64_t)c0 * ldx, ldx, nr, h->d_xt, perm_in,
+                                                               h->dof, n_in, n_pad);
+      BW_CUDA(cudaGetLastError());
+    }
+    for (int phase = 0; phase < 2; phase++) {
+      const DevMm &dm = h->dmm[o][phase];
+      if (dm.n_chunks == 0) continue;
+      bw::MmArgs a{};
+      a.data = dm.data;
+      a.chunks = dm.chunks;
+      a.cta_ptr = dm.cta;
+      a.xt = h->d_xt;
+      a.t8 = h->d_t8;
+      a.y = Y + (int64_t)c0 * ldy;
+      a.ldy = ldy;
+      a.perm_out = perm_out;
+      a.dof = h->dof;
+      a.nrhs = nr;
+      a.phase = phase + 1;
+      a.err = h->d_err;
+      a.spin_limit = h->spin_limit;
+      bw::mm_stream_kernel<<<h->grid, bw::kMmThreads, bw::kMmSmem, st>>>(a);
+      BW_CUDA(cudaGetLastError());
+    }
+  }
 }
 
 // One matvec with its scratch vectors in the static array (no timing).
@@ -558,6 +672,7 @@ int bw_finalize(bw_hmat *h, int flags) {
     if (h->device >= 0) BW_CUDA(cudaSetDevice(h->device));
     const bool want_t = (flags & BW_STORE_TRANSPOSE) != 0;
     const bool check = (flags & BW_NO_FINITE_CHECK) == 0;
+    const bool want_mm = (flags & BW_STORE_MATMAT) != 0;
     // statistics
     h->entries = 0;
     h->sum_rank = 0;
@@ -573,6 +688,7 @@ int bw_finalize(bw_hmat *h, int flags) {
       bw::compute_scales(h->prob, o == 1, check && o == 0, h->op[o]);
       for (int p = 0; p < 3; p++)
         if (mask & (1 << p)) bw::build_chunks(h->prob, o == 1, p, h->grid, h->op[o]);
+      if (want_mm) bw::build_mm_plan(h->prob, o == 1, h->grid, h->op[o], h->mm[o]);
     }
     compute_diagonal(h);
     if (!h->plan_only) {
@@ -585,6 +701,15 @@ int bw_finalize(bw_hmat *h, int flags) {
               need += h->op[o].ph[ph].n_elems[p] * bw::esize_of(p) +
                       (int64_t)h->op[o].ph[ph].cp[p].chunks.size() * (int64_t)sizeof(Chunk) +
                       (int64_t)h->op[o].ph[ph].cp[p].gsegs.size() * (int64_t)sizeof(bw::GatherSeg);
+      int64_t t8_rows = 0;
+      if (want_mm) {
+        for (int o = 0; o < (want_t ? 2 : 1); o++) {
+          for (int ph = 0; ph < 2; ph++)
+            need += h->mm[o].ph[ph].n_elems * 2 + (int64_t)h->mm[o].ph[ph].chunks.size() * (int64_t)sizeof(bw::MmChunk);
+          t8_rows = std::max<int64_t>(t8_rows, h->mm[o].t8_len);
+        }
+        need += (mm_xt_rows(h) + t8_rows + 16) * 2 * bw::kMmRhs;
+      }
       if (h->dev_limit > 0 && need > h->dev_limit)
         throw OomError("layout needs " + std::to_string(need) + " device bytes, above the configured limit of " +
                        std::to_string(h->dev_limit));
@@ -608,6 +733,13 @@ int bw_finalize(bw_hmat *h, int flags) {
       h->d_g2 = h->dmalloc((size_t)std::max<int64_t>(1, g2_bytes(h, mask, want_t)) + 16);
       h->d_xh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
       h->d_yh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
+      if (want_mm) {
+        const size_t xb = (size_t)mm_xt_rows(h) * 2 * bw::kMmRhs, tb = (size_t)(t8_rows + 16) * 2 * bw::kMmRhs;
+        h->d_xt = static_cast<uint16_t *>(h->dmalloc(xb));
+        h->d_t8 = static_cast<uint16_t *>(h->dmalloc(tb));
+        BW_CUDA(cudaMemset(h->d_xt, 0, xb));
+        BW_CUDA(cudaMemset(h->d_t8, 0, tb));
+      }
       h->d_err = static_cast<int *>(h->dmalloc(sizeof(int)));
       BW_CUDA(cudaMemset(h->d_err, 0, sizeof(int)));
       BW_CUDA(cudaMallocHost(&h->h_err, sizeof(int)));
@@ -617,6 +749,10 @@ int bw_finalize(bw_hmat *h, int flags) {
       for (int p = 0; p < 3; p++)
         if (mask & (1 << p))
           for (int ph = 0; ph < 2; ph++) upload_phase(h, o, p, ph);
+    if (want_mm)
+      for (int o = 0; o < (want_t ? 2 : 1); o++)
+        for (int ph = 0; ph < 2; ph++) upload_mm_phase(h, o, ph);
+    h->has_mm = want_mm;
     h->stored = mask;
     h->has_t = want_t;
     h->finalized = true;
@@ -763,9 +899,46 @@ int bw_matmat(bw_hmat *h, const double *X, int64_t ldx, double *Y, int64_t ldy, 
     h->err = "leading dimension too small";
     return BW_ERR_ARG;
   }
+  const int o = tr ? 1 : 0;
+  if ((flags & BW_BF16) && h->has_mm && (o == 0 || h->has_t) && nrhs > 0) {
+    // tensor-core path: BF16 matmat layout, kMmRhs right-hand sides per pass
+    return guarded(h, [&] {
+      if (!h->finalized || h->plan_only) throw StateError("bw_matmat needs a finalized handle with device data");
+      if ((flags & (BW_FP64 | BW_FP32)) != 0) throw std::invalid_argument("flags must name exactly one precision");
+      if ((nin && !X) || (nout && !Y)) throw std::invalid_argument("null matrix");
+      if (X && Y) {
+        const char *xb = reinterpret_cast<const char *>(X), *yb = reinterpret_cast<const char *>(Y);
+        const int64_t xe = ((int64_t)(nrhs - 1) * ldx + nin) * 8, ye = ((int64_t)(nrhs - 1) * ldy + nout) * 8;
+        if (xb < yb + ye && yb < xb + xe) throw std::invalid_argument("X and Y overlap");
+      }
+      BW_CUDA(cudaSetDevice(h->device));
+      launch_matmat_tc(h, o, X, ldx, Y, ldy, nrhs, (flags & BW_PERMUTED) != 0, static_cast<cudaStream_t>(stream));
+      return BW_OK;
+    });
+  }
   for (int k = 0; k < nrhs; k++) {
     int rc = bw_matvec(h, X + k * ldx, Y + k * ldy, flags, stream);
     if (rc != BW_OK) return rc;
+  }
+  return BW_OK;
+}
+
+int bw_mm_plan_export(const bw_hmat *h, int phase, int transposed, int64_t *n_chunks, int32_t *chunks,
+                      int64_t *n_elems, uint16_t *data, int64_t *n_cta, int32_t *cta_ptr, int64_t *t8_len) {
+  if (!h || phase < 1 || phase > 2) return BW_ERR_ARG;
+  if (!h->finalized || !h->has_mm) return BW_ERR_STATE;
+  const int o = transposed ? 1 : 0;
+  if (o == 1 && !h->has_t) return BW_ERR_UNSUPPORTED;
+  const bw::MmPhase &ph = h->mm[o].ph[phase - 1];
+  if (n_chunks) *n_chunks = (int64_t)ph.chunks.size();
+  if (n_elems) *n_elems = ph.n_elems;
+  if (n_cta) *n_cta = (int64_t)ph.cta_ptr.size();
+  if (t8_len) *t8_len = h->mm[o].t8_len;
+  if (chunks) std::memcpy(chunks, ph.chunks.data(), ph.chunks.size() * sizeof(bw::MmChunk));
+  if (cta_ptr) std::memcpy(cta_ptr, ph.cta_ptr.data(), ph.cta_ptr.size() * sizeof(int32_t));
+  if (data) {
+    if (!h->plan_only) return BW_ERR_STATE;
+    std::memcpy(data, h->mm_host[o][phase - 1].data(), (size_t)ph.n_elems * 2);
   }
   return BW_OK;
 }

@@ -475,4 +475,225 @@ void fill_items(const Problem &p, bool tr, const OperatorPlan &op, int phase, in
   }
 }
 
+// ---------------------------------------------------------------------------- matmat plan
+
+namespace {
+
+// Chunks of one matmat item: at most kMmMaxCols columns and kMmStageBytes of
+// block data + operand rows, multiples of 16 columns, at most kMmMaxRuns runs.
+void mm_chunk_item(const MmItem &it, std::vector<MmChunk> &out) {
+  const int64_t per_col = 2 * int64_t(it.hpad) + 2 * int64_t(kMmRhs);
+  const int64_t cap = std::max<int64_t>(16, std::min<int64_t>(kMmMaxCols, (kMmStageBytes / per_col) / 16 * 16));
+  std::vector<int64_t> seg_start(it.segs.size() + 1, 0);
+  for (size_t s = 0; s < it.segs.size(); s++) seg_start[s + 1] = seg_start[s] + it.segs[s].ncols;
+  int64_t c0 = 0;
+  size_t s_at = 0;
+  while (c0 < it.ncols) {
+    while (s_at < it.segs.size() && seg_start[s_at + 1] <= c0) s_at++;
+    MmChunk ch;
+    std::memset(&ch, 0, sizeof ch);
+    // runs until the column cap or the run cap; the chunk must end on a
+    // multiple of 16 columns, so a fourth run may be cut short
+    int64_t end = std::min<int64_t>(c0 + cap, it.ncols);
+    int nr = 0;
+    for (size_t s = s_at; s < it.segs.size() && seg_start[s] < end; s++) {
+      if (nr == kMmMaxRuns) {
+        end = seg_start[s];
+        break;
+      }
+      nr++;
+    }
+    end = c0 + (end - c0) / 16 * 16;
+    if (end <= c0) end = std::min<int64_t>(c0 + 16, it.ncols);  // segments of 8: the run cap bends to fit 16 columns
+    nr = 0;
+    for (size_t s = s_at; s < it.segs.size() && seg_start[s] < end; s++) {
+      const int64_t a = std::max<int64_t>(c0, seg_start[s]), b = std::min<int64_t>(end, seg_start[s + 1]);
+      if (b <= a) continue;
+      if (nr == kMmMaxRuns) throw std::runtime_error("matmat chunk needs more than the run cap");
+      const MmSeg &sg = it.segs[s];
+      ch.run[nr].src = static_cast<uint32_t>(sg.src_row + (a - seg_start[s])) | (sg.src ? 0x80000000u : 0u);
+      ch.run[nr].rows = static_cast<uint32_t>(b - a);
+      nr++;
+    }
+    ch.data_off = it.off + (c0 / 8) * 8 * int64_t(it.hpad);
+    ch.kc = static_cast<int32_t>(end - c0);
+    ch.hpad = it.hpad;
+    ch.rows = it.h;
+    ch.out_off = it.out_off;
+    ch.flags = static_cast<uint32_t>(nr) << 8;
+    if (c0 == 0) ch.flags |= kFirst;
+    if (end >= it.ncols) ch.flags |= kLast;
+    out.push_back(ch);
+    c0 = end;
+  }
+}
+
+}  // namespace
+
+void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, MmPlan &mm) {
+  mm = MmPlan{};
+  mm.n_in = op.n_in;
+  mm.n_out = op.n_out;
+  const size_t nlr = p.lr.size();
+  grid = std::max(1, grid);
+  // stacks per column cluster (the matvec's phase-1 grouping), T8 numbering
+  std::map<std::pair<int64_t, int64_t>, std::vector<int64_t>> stacks;
+  for (size_t k = 0; k < nlr; k++) {
+    EffLow b = eff_low(p, tr, k);
+    if (b.r > 0) stacks[{b.j0, b.n}].push_back((int64_t)k);
+  }
+  mm.t8_off.assign(nlr, 0);
+  int64_t t8 = 0;
+  for (auto &kv : stacks) {
+    MmStack st{kv.first.first, kv.first.second, kv.second, t8};
+    for (int64_t k : kv.second) {
+      mm.t8_off[k] = t8;
+      t8 += align_up(eff_low(p, tr, k).r, 8);
+    }
+    mm.stacks.push_back(std::move(st));
+  }
+  mm.t8_len = t8;
+  if (t8 + 16 > INT32_MAX) fail("padded sum of ranks above 2^31");
+  // phase 1: each stack's rows cut into items of at most kHMax rows
+  int64_t e1 = 0;
+  std::vector<int64_t> wcols(mm.stacks.size()), rows8(mm.stacks.size());
+  for (size_t s = 0; s < mm.stacks.size(); s++) {
+    const MmStack &st = mm.stacks[s];
+    const int64_t j0a = st.j0 / 8 * 8;
+    wcols[s] = align_up(st.j0 + st.n - j0a, 16);
+    int64_t R8 = 0;
+    for (int64_t k : st.blocks) R8 += align_up(eff_low(p, tr, k).r, 8);
+    rows8[s] = R8;
+    e1 += R8 * wcols[s];
+  }
+  const int64_t cap1 = std::max<int64_t>(1, e1 / grid / kItemsPerCta);
+  MmPhase &p1 = mm.ph[0];
+  for (size_t s = 0; s < mm.stacks.size(); s++) {
+    const MmStack &st = mm.stacks[s];
+    const int64_t W = wcols[s], R8 = rows8[s];
+    const int64_t rmax = std::min<int64_t>(kHMax, std::max<int64_t>(16, (cap1 / W) / 16 * 16));
+    const int64_t nit = (R8 + rmax - 1) / rmax;
+    const int64_t cut = align_up((R8 + nit - 1) / nit, 8);
+    for (int64_t r0 = 0; r0 < R8; r0 += cut) {
+      MmItem it;
+      it.h = static_cast<int32_t>(std::min<int64_t>(cut, R8 - r0));
+      it.hpad = it.h;
+      it.out_off = static_cast<int32_t>(st.t8_base + r0);
+      it.ncols = W;
+      it.stack = (int64_t)s;
+      it.srow0 = r0;
+      const int64_t j0a = st.j0 / 8 * 8;
+      it.segs.push_back({2, -1, 0, st.j0 - j0a, st.n, W, 0, j0a});
+      p1.items.push_back(std::move(it));
+    }
+  }
+  // phase 2: the matvec's row-panel items on widened windows
+  MmPhase &p2 = mm.ph[1];
+  for (const Item &src : op.ph[1].items) {
+    MmItem it;
+    it.h = src.h;
+    it.hpad = src.hpad;
+    it.out_off = src.out_off;
+    for (const Segment &sg : src.segs) {
+      MmSeg m{};
+      m.kind = sg.kind;
+      m.block = sg.block;
+      m.row0 = sg.row0;
+      if (sg.kind == 0) {
+        m.src = 0;
+        m.src_row = sg.src_off / 8 * 8;
+        m.lead = sg.src_off - m.src_row;
+        m.width = sg.ncols;
+      } else {
+        m.src = 1;
+        m.src_row = mm.t8_off[sg.block];
+        m.lead = 0;
+        m.width = sg.ncols;  // the rank
+      }
+      m.ncols = align_up(m.lead + m.width, 8);
+      it.ncols += m.ncols;
+      it.segs.push_back(m);
+    }
+    if (it.ncols % 16) {  // one more tile row of the last operand window (zero columns)
+      it.segs.back().ncols += 8;
+      it.ncols += 8;
+    }
+    p2.items.push_back(std::move(it));
+  }
+  // data offsets, chunks, LPT schedule (cost: block bytes + operand bytes + a per-chunk overhead)
+  for (int phase = 0; phase < 2; phase++) {
+    MmPhase &ph = mm.ph[phase];
+    int64_t off = 0;
+    for (MmItem &it : ph.items) {
+      it.off = off;
+      off = align_up(off + it.ncols * int64_t(it.hpad), kItemAlign);
+    }
+    ph.n_elems = off + kItemAlign;
+    std::vector<std::vector<MmChunk>> per_item(ph.items.size());
+    std::vector<int64_t> cost(ph.items.size(), 0);
+    for (size_t q = 0; q < ph.items.size(); q++) {
+      mm_chunk_item(ph.items[q], per_item[q]);
+      for (const MmChunk &c : per_item[q]) cost[q] += int64_t(c.kc) * (2 * c.hpad + 2 * kMmRhs) + 1024;
+    }
+    std::vector<int64_t> order(ph.items.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+    using Slot = std::pair<int64_t, int>;
+    std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
+    for (int c = 0; c < grid; c++) heap.push({0, c});
+    std::vector<std::vector<int64_t>> bins(grid);
+    for (int64_t q : order) {
+      Slot s = heap.top();
+      heap.pop();
+      bins[s.second].push_back(q);
+      s.first += cost[q];
+      heap.push(s);
+    }
+    ph.chunks.clear();
+    ph.cta_ptr.assign(grid + 1, 0);
+    for (int c = 0; c < grid; c++) {
+      ph.cta_ptr[c] = static_cast<int32_t>(ph.chunks.size());
+      for (int64_t q : bins[c]) ph.chunks.insert(ph.chunks.end(), per_item[q].begin(), per_item[q].end());
+    }
+    ph.cta_ptr[grid] = static_cast<int32_t>(ph.chunks.size());
+    if (ph.chunks.size() > (size_t)INT32_MAX) fail("too many matmat chunks");
+  }
+}
+
+void fill_mm_items(const Problem &p, bool tr, const MmPlan &mm, int phase, int64_t i_begin, int64_t i_end,
+                   int64_t base, uint16_t *dst) {
+  const MmPhase &ph = mm.ph[phase];
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t q = i_begin; q < i_end; q++) {
+    const MmItem &it = ph.items[q];
+    uint16_t *d = dst + (it.off - base);
+    if (phase == 0) {
+      // stack rows [srow0, srow0 + h): block rows, then zero rows up to the
+      // block's padded rank; columns: the window [j0a, j0a + ncols)
+      const MmStack &st = mm.stacks[it.stack];
+      const MmSeg &sg = it.segs[0];
+      int64_t sb = 0;  // stack row of the current block's first row
+      for (int64_t k : st.blocks) {
+        const EffLow b = eff_low(p, tr, k);
+        const int64_t r8 = align_up(b.r, 8);
+        const int64_t lo = std::max<int64_t>(sb, it.srow0), hi = std::min<int64_t>(sb + b.r, it.srow0 + it.h);
+        for (int64_t s = lo; s < hi; s++)
+          for (int64_t c = 0; c < sg.width; c++)
+            d[item_index(2, it.hpad, s - it.srow0, sg.lead + c)] = to_bf16(static_cast<float>(b.B.at(s - sb, c)));
+        sb += r8;
+        if (sb >= it.srow0 + it.h) break;
+      }
+      continue;
+    }
+    int64_t col = 0;
+    for (const MmSeg &s : it.segs) {
+      const View v = s.kind == 0 ? eff_full(p, tr, s.block).a : eff_low(p, tr, s.block).A;
+      for (int64_t c = 0; c < s.width; c++)
+        for (int64_t i = 0; i < it.h; i++)
+          d[item_index(2, it.hpad, i, col + s.lead + c)] = to_bf16(static_cast<float>(v.at(s.row0 + i, c)));
+      col += s.ncols;
+    }
+  }
+}
+
 }  // namespace bw

@@ -185,4 +185,99 @@ int esize_of(int prec);
 uint16_t to_bf16(float f);
 float from_bf16(uint16_t b);
 
+// ----------------------------------------------------------------------------
+// Multi-right-hand-side layout: Y = H X on the tcgen05 tensor cores.
+//
+// The same two phases as the matvec, but every chunk is a small GEMM
+// D(rows x 64) += A(rows x kc) * B(kc x 64):
+//  * A is the chunk's block data in BF16 8x8 tiles (the layout above);
+//  * B is a run of rows of an 8x8-tiled BF16 operand with kMmRhs columns.
+//    That operand is X (the gathered right-hand sides) in phase 1 and for
+//    full-rank slices, and T8 (the phase-1 products) for low-rank slices.
+//  * The 8x8 tiles are the MN-major, no-swizzle canonical operand layout of
+//    tcgen05.mma.
+// Runs of operand rows must start on an 8-row tile boundary, so:
+//  * every column segment of an item is widened to the 8-aligned window of
+//    operand rows around it, with zeros in the widened columns;
+//  * T8 numbers the products of each low-rank block from an 8-aligned
+//    offset, its rank rounded up to a multiple of 8 with zero rows;
+//  * items are padded to a multiple of 16 columns (one MMA K-step).
+// The phases:
+//  * phase 1: stacks of B factors per column cluster, as for the matvec, with
+//    rows on T8's numbering;
+//  * phase 2: row panels, with FR and A slices on their widened windows.
+// Block data is stored unscaled: BF16 has FP32's exponent range, so a
+// per-block scale would leave every rounded mantissa unchanged.
+constexpr int kMmRhs = 64;             // right-hand sides per pass (MMA N)
+constexpr int kMmStageBytes = 49152;   // block data + operand rows of one pipeline stage
+constexpr int kMmMaxRuns = 4;          // operand runs per chunk (a chunk ends early to keep this)
+constexpr int kMmMaxCols = 512;        // columns per chunk
+
+struct MmRun {
+  uint32_t src;   // first operand row (multiple of 8) | operand << 31 (0: X, 1: T8)
+  uint32_t rows;  // operand rows (multiple of 8)
+};
+// One chunk descriptor, 64 bytes, with its operand runs inline.
+struct alignas(16) MmChunk {
+  int64_t data_off;  // element offset of the chunk's first column group
+  int32_t kc;        // columns (multiple of 16); the runs cover exactly kc operand rows
+  int32_t hpad;      // rows of the item's tiles (multiple of 8, <= kHMax)
+  int32_t rows;      // rows of the item to write
+  int32_t out_off;   // first output row: T8 row (phase 1) or y row (phase 2)
+  uint32_t flags;    // kFirst | kLast | (number of runs << 8)
+  uint32_t pad_;
+  MmRun run[kMmMaxRuns];
+};
+static_assert(sizeof(MmChunk) == 64, "matmat chunk descriptor must be 64 bytes");
+constexpr int kMmChunkWords = sizeof(MmChunk) / 4;
+
+// Column segment of a matmat item: operand rows [src_row, src_row + ncols),
+// the block's real columns at [lead, lead + width) of the window.
+struct MmSeg {
+  int kind;          // 0: FR slice, 1: LR A slice, 2: LR B stack
+  int64_t block;     // kinds 0, 1
+  int64_t row0;      // first row of the block in this item (kinds 0, 1)
+  int64_t lead, width, ncols;
+  int src;           // 0: X, 1: T8
+  int64_t src_row;
+};
+
+struct MmStack {
+  int64_t j0, n;                // column cluster
+  std::vector<int64_t> blocks;  // low-rank blocks, in T8 order
+  int64_t t8_base;              // T8 row of the stack's first row
+};
+
+struct MmItem {
+  int64_t off = 0;               // element offset in the phase's data array
+  int32_t h = 0, hpad = 0, out_off = 0;
+  int64_t ncols = 0;             // multiple of 16
+  std::vector<MmSeg> segs;
+  int64_t stack = -1, srow0 = 0;  // phase 1: stack and its first row in this item
+};
+
+struct MmPhase {
+  std::vector<MmItem> items;
+  int64_t n_elems = 0;
+  std::vector<MmChunk> chunks;   // ordered by CTA
+  std::vector<int32_t> cta_ptr;  // grid + 1
+};
+
+struct MmPlan {
+  int64_t n_in = 0, n_out = 0;
+  int64_t t8_len = 0;              // rows of T8 (multiple of 8)
+  std::vector<int64_t> t8_off;     // per low-rank block
+  std::vector<MmStack> stacks;
+  MmPhase ph[2];
+};
+
+// Builds the matmat plan of the operator (transposed: H^T) from the problem
+// and the operator's matvec plan (its row panels are reused).
+void build_mm_plan(const Problem &p, bool transposed, int grid, const OperatorPlan &op, MmPlan &mm);
+
+// Writes the BF16 data of items [i_begin, i_end) of one matmat phase into dst
+// (dst[0] is element `base` of the phase's array; dst must be zeroed).
+void fill_mm_items(const Problem &p, bool transposed, const MmPlan &mm, int phase, int64_t i_begin, int64_t i_end,
+                   int64_t base, uint16_t *dst);
+
 }  // namespace bw

@@ -43,6 +43,9 @@ class HmatGpu:
     device: CUDA ordinal, or -1 for a host-only plan (``finalize(plan_only=True)``).
     """
 
+    has_matmat = False
+    _plan_only = False
+
     def __init__(self, dof: int, n_rows: int, n_cols: int, perm0, perm1, device: int = 0):
         self._lib = A.lib()
         self.dof, self.n_rows, self.n_cols, self.device = int(dof), int(n_rows), int(n_cols), int(device)
@@ -109,7 +112,10 @@ class HmatGpu:
             o += r * (m + n)
 
     def finalize(self, precisions=("fp64",), transpose: bool = False, check_finite: bool = True,
-                 plan_only: bool = False, device_limit: int | None = None) -> "HmatGpu":
+                 plan_only: bool = False, device_limit: int | None = None, matmat: bool = False) -> "HmatGpu":
+        """Lay the blocks out on the device.  precisions: storage copies for
+        matvec ("fp64", "fp32", "bf16"); transpose: also H^T; matmat: also the
+        BF16 layout of the tensor-core multi-right-hand-side product."""
         flags = 0
         for p in precisions:
             flags |= _prec_flag(p)
@@ -119,6 +125,8 @@ class HmatGpu:
             flags |= A.BW_NO_FINITE_CHECK
         if plan_only:
             flags |= A.BW_PLAN_ONLY
+        if matmat:
+            flags |= A.BW_STORE_MATMAT
         if device_limit is not None:
             A.check(self._lib.bw_set_device_limit(self._h, int(device_limit)), self._h)
         st = self._lib.bw_finalize(self._h, flags)
@@ -127,6 +135,8 @@ class HmatGpu:
         self._finalized = True
         self.precisions = tuple(precisions)
         self.has_transpose = bool(transpose)
+        self.has_matmat = bool(matmat)
+        self._plan_only = bool(plan_only)
         return self
 
     @classmethod
@@ -231,9 +241,53 @@ class HmatGpu:
         self.sync(0)
 
     def matmat_ptr(self, X_ptr: int, ldx: int, Y_ptr: int, ldy: int, nrhs: int, precision="fp64",
-                   stream: int = 0) -> None:
+                   stream: int = 0, permuted: bool = False, transpose: bool = False) -> None:
         A.check(self._lib.bw_matmat(self._h, int(X_ptr), int(ldx), int(Y_ptr), int(ldy), int(nrhs),
-                                    _prec_flag(precision), int(stream)), self._h)
+                                    self._flags(precision, permuted, transpose), int(stream)), self._h)
+
+    def matmat(self, X, precision="fp64", permuted: bool = False, transpose: bool = False, out=None, stream=None):
+        """Y = H X (H^T X) for a CUDA float64 tensor X of shape (n, k),
+        stream-ordered on `stream` (default: the current torch stream).
+        X and Y are column-major (each right-hand side contiguous); X is copied
+        to that layout when it is not.  "bf16" on a handle finalized with
+        matmat=True runs on the tensor cores, 64 right-hand sides per pass;
+        everything else applies one matvec per column."""
+        import torch
+
+        nin, nout = (self.n_rows, self.n_cols) if transpose else (self.n_cols, self.n_rows)
+        if not (isinstance(X, torch.Tensor) and X.is_cuda and X.dtype == torch.float64 and X.dim() == 2):
+            raise TypeError("X must be a 2-D float64 CUDA tensor")
+        if X.shape[0] != nin:
+            raise ValueError(f"X must have {nin} rows")
+        k = X.shape[1]
+        if X.stride(0) != 1 or (k > 1 and X.stride(1) < nin):
+            X = X.t().contiguous().t()
+        if out is None:
+            out = torch.empty(k, nout, dtype=torch.float64, device=X.device).t()
+        elif out.shape != (nout, k) or out.stride(0) != 1 or (k > 1 and out.stride(1) < nout):
+            raise ValueError(f"out must be a column-major ({nout}, {k}) tensor")
+        if stream is None:
+            stream = torch.cuda.current_stream(X.device)
+        sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        ldx = X.stride(1) if k > 1 else nin
+        ldy = out.stride(1) if k > 1 else nout
+        self.matmat_ptr(X.data_ptr(), ldx, out.data_ptr(), ldy, k, precision, sp, permuted, transpose)
+        return out
+
+    def mm_plan_export(self, phase: int, transposed: bool = False) -> dict:
+        """Host view of the matmat plan of one phase (finalize(matmat=True)):
+        chunk words (n, 16), cta offsets, T8 rows, and (plan-only handles) the
+        raw BF16 data words."""
+        nch, nel, ncta, t8 = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        A.check(self._lib.bw_mm_plan_export(self._h, phase, int(transposed), C.byref(nch), None, C.byref(nel), None,
+                                            C.byref(ncta), None, C.byref(t8)), self._h)
+        chunks = np.zeros((nch.value, 16), np.int32)
+        cta = np.zeros(ncta.value, np.int32)
+        data = np.zeros(nel.value, np.uint16) if self._plan_only else None
+        A.check(self._lib.bw_mm_plan_export(self._h, phase, int(transposed), None, chunks.ctypes.data, None,
+                                            data.ctypes.data if data is not None else None, None, cta.ctypes.data,
+                                            None), self._h)
+        return {"chunks": chunks, "cta_ptr": cta, "data": data, "t8_len": t8.value}
 
     def sync(self, stream=0) -> None:
         sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)

@@ -45,7 +45,9 @@ enum {
   BW_BF16 = 4,            /* BF16 blocks with a per-block FP32 scale, FP32 accumulation */
   BW_STORE_TRANSPOSE = 16,/* bw_finalize: also lay out H^T for bw_matvec(..., BW_TRANSPOSE) */
   BW_NO_FINITE_CHECK = 32,/* bw_finalize: skip the non-finite entry check */
-  BW_PLAN_ONLY = 64       /* bw_finalize: build the host plan only (no device); for inspection */
+  BW_PLAN_ONLY = 64,      /* bw_finalize: build the host plan only (no device); for inspection */
+  BW_STORE_MATMAT = 128   /* bw_finalize: also store the BF16 matmat layout, so bw_matmat(..., BW_BF16)
+                             runs on the tcgen05 tensor cores (64 right-hand sides per pass) */
 };
 
 /* matvec flags (OR with exactly one of BW_FP64 / BW_FP32 / BW_BF16) */
@@ -148,8 +150,13 @@ int bw_matvec_static_scratch(bw_hmat *h, const double *x, double *y, int flags, 
 int bw_matvec_host(bw_hmat *h, const double *x, double *y, int flags);
 
 /* Y = H X for nrhs right-hand sides on DEVICE pointers; X is n_cols x nrhs
- * (column stride ldx), Y is n_rows x nrhs (column stride ldy), FP64.
- * No reference counterpart. */
+ * (column stride ldx), Y is n_rows x nrhs (column stride ldy), FP64 in and out.
+ * With BW_BF16 on a handle finalized with BW_STORE_MATMAT this runs on the
+ * tensor cores:
+ *  - X is rounded to BF16, products accumulate in FP32;
+ *  - 64 right-hand sides per pass of 3 launches.
+ * Otherwise it is one bw_matvec per column.  BW_PERMUTED and BW_TRANSPOSE
+ * apply as for bw_matvec.  No reference counterpart. */
 int bw_matmat(bw_hmat *h, const double *X, int64_t ldx, double *Y, int64_t ldy, int nrhs, int flags,
               void *stream);
 
@@ -181,6 +188,16 @@ int bw_last_error(const bw_hmat *h, char *buf, size_t len);
 /* Cap on the device bytes bw_finalize may allocate (0 = no cap).  Exceeding it
  * makes bw_finalize return BW_ERR_OOM before allocating. */
 int bw_set_device_limit(bw_hmat *h, int64_t bytes);
+
+/* Host view of the matmat plan (BW_STORE_MATMAT) for one phase:
+ *  - chunks: n_chunks x 16 int32 words in the layout of bw::MmChunk
+ *    (bigwham_dev_b200/csrc/bw_layout.h);
+ *  - data: n_elems raw BF16 words in 8x8 tiles (BW_PLAN_ONLY handles only);
+ *  - cta_ptr: grid+1 offsets;
+ *  - t8_len: rows of the low-rank product array T8.
+ * Any output pointer may be NULL. */
+int bw_mm_plan_export(const bw_hmat *h, int phase, int transposed, int64_t *n_chunks, int32_t *chunks,
+                      int64_t *n_elems, uint16_t *data, int64_t *n_cta, int32_t *cta_ptr, int64_t *t8_len);
 
 /* Host view of the built plan for one precision and phase (1: low-rank B
  * stage, 2: row panels), for inspection and testing.  Any output pointer may be

@@ -90,3 +90,59 @@ def replay(h, x_perm, precision="fp64", transposed=False):
     y = np.full(h.n_cols if transposed else h.n_rows, np.nan)
     run_phase(p2, g2, y, tiled)
     return y
+
+
+# --------------------------------------------------------------------------- matmat plan
+def mm_tile(data, off, hpad, kc):
+    """(hpad x kc) float64 matrix of a chunk stored in 8x8 BF16 tiles:
+    element (i, c) at off + (c/8)*8*hpad + (i/8)*64 + (c%8)*8 + i%8."""
+    words = data[off:off + kc * hpad].astype(np.uint32) << 16
+    t = words.view(np.float32).astype(np.float64)
+    # axes of the flat array: column group, row group, column in group, row in group
+    t = t.reshape(kc // 8, hpad // 8, 8, 8)
+    return t.transpose(1, 3, 0, 2).reshape(hpad, kc)
+
+
+def _bf16(a):
+    u = np.ascontiguousarray(a, dtype=np.float64).astype(np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def mm_replay(h, X_perm, transposed=False, check=None, round_operands=False):
+    """Walks the matmat plan of a BW_PLAN_ONLY handle as the tensor-core kernel
+    does, in float64: returns Y (permuted ordering, n_out x k).  With the
+    operands kept exact the structure, not the rounding, is under test;
+    round_operands=True rounds X and the phase-1 products T8 to BF16 as the
+    kernel does.  check(chunk_words) is called on every chunk."""
+    k = X_perm.shape[1]
+    if k > 64:  # passes of 64 right-hand sides, as the kernel runs them
+        return np.concatenate([mm_replay(h, X_perm[:, c:c + 64], transposed, check, round_operands)
+                               for c in range(0, k, 64)], axis=1)
+    n_in, n_out = (h.n_rows, h.n_cols) if transposed else (h.n_cols, h.n_rows)
+    p1, p2 = h.mm_plan_export(1, transposed), h.mm_plan_export(2, transposed)
+    ops = [np.zeros(((n_in + 7) // 8 * 8 + 16, 64)), np.zeros((p1["t8_len"] + 16, 64))]
+    ops[0][:n_in, :k] = _bf16(X_perm) if round_operands else X_perm
+    Y = np.zeros((n_out, k))
+    for phase, pl in ((1, p1), (2, p2)):
+        acc = None
+        for w in pl["chunks"]:
+            if check is not None:
+                check(w)
+            off = int(np.uint32(w[0])) | (int(np.uint32(w[1])) << 32)
+            kc, hpad, rows, out_off, flags = int(w[2]), int(w[3]), int(w[4]), int(w[5]), int(np.uint32(w[6]))
+            nr = (flags >> 8) & 0xFF
+            B = []
+            for r in range(nr):
+                src, nrow = int(np.uint32(w[8 + 2 * r])), int(w[9 + 2 * r])
+                B.append(ops[src >> 31][(src & 0x7FFFFFFF):(src & 0x7FFFFFFF) + nrow])
+            B = np.concatenate(B, axis=0)
+            if flags & 1:
+                acc = np.zeros((hpad, 64))
+            acc += mm_tile(pl["data"], off, hpad, kc) @ B
+            if flags & 2:
+                if phase == 1:
+                    ops[1][out_off:out_off + rows] = _bf16(acc[:rows]) if round_operands else acc[:rows]
+                else:
+                    Y[out_off:out_off + rows] = acc[:rows, :k]
+    return Y
