@@ -475,8 +475,8 @@ void *static_scratch_ptr(int device) {
 }
 
 // Rows of the matmat operand X: the largest input size rounded up to a tile
-// row, plus two tile rows that the widened windows of the last columns reach.
-int64_t mm_xt_rows(const bw_hmat *h) { return (std::max(h->n_rows, h->n_cols) + 7) / 8 * 8 + 16; }
+// row, plus the zero rows that the widened windows of the last columns reach.
+int64_t mm_xt_rows(const bw_hmat *h) { return (std::max(h->n_rows, h->n_cols) + 7) / 8 * 8 + bw::kMmPadRows; }
 
 // Y[:, 0:nrhs] = op X[:, 0:nrhs] on the tensor cores, in passes of kMmRhs
 // right-hand sides: X gather (+ permutation) into 8x8 BF16 tiles, phase 1
@@ -708,7 +708,7 @@ int bw_finalize(bw_hmat *h, int flags) {
             need += h->mm[o].ph[ph].n_elems * 2 + (int64_t)h->mm[o].ph[ph].chunks.size() * (int64_t)sizeof(bw::MmChunk);
           t8_rows = std::max<int64_t>(t8_rows, h->mm[o].t8_len);
         }
-        need += (mm_xt_rows(h) + t8_rows + 16) * 2 * bw::kMmRhs;
+        need += (mm_xt_rows(h) + t8_rows + bw::kMmPadRows) * 2 * bw::kMmRhs;
       }
       if (h->dev_limit > 0 && need > h->dev_limit)
         throw OomError("layout needs " + std::to_string(need) + " device bytes, above the configured limit of " +
@@ -734,7 +734,7 @@ int bw_finalize(bw_hmat *h, int flags) {
       h->d_xh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
       h->d_yh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
       if (want_mm) {
-        const size_t xb = (size_t)mm_xt_rows(h) * 2 * bw::kMmRhs, tb = (size_t)(t8_rows + 16) * 2 * bw::kMmRhs;
+        const size_t xb = (size_t)mm_xt_rows(h) * 2 * bw::kMmRhs, tb = (size_t)(t8_rows + bw::kMmPadRows) * 2 * bw::kMmRhs;
         h->d_xt = static_cast<uint16_t *>(h->dmalloc(xb));
         h->d_t8 = static_cast<uint16_t *>(h->dmalloc(tb));
         BW_CUDA(cudaMemset(h->d_xt, 0, xb));

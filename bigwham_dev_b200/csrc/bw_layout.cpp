@@ -553,14 +553,14 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
     mm.stacks.push_back(std::move(st));
   }
   mm.t8_len = t8;
-  if (t8 + 16 > INT32_MAX) fail("padded sum of ranks above 2^31");
+  if (t8 + kMmPadRows > INT32_MAX) fail("padded sum of ranks above 2^31");
   // phase 1: each stack's rows cut into items of at most kHMax rows
   int64_t e1 = 0;
   std::vector<int64_t> wcols(mm.stacks.size()), rows8(mm.stacks.size());
   for (size_t s = 0; s < mm.stacks.size(); s++) {
     const MmStack &st = mm.stacks[s];
     const int64_t j0a = st.j0 / 8 * 8;
-    wcols[s] = align_up(st.j0 + st.n - j0a, 16);
+    wcols[s] = std::max<int64_t>(kMmMinCols, align_up(st.j0 + st.n - j0a, 16));
     int64_t R8 = 0;
     for (int64_t k : st.blocks) R8 += align_up(eff_low(p, tr, k).r, 8);
     rows8[s] = R8;
@@ -571,7 +571,7 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
   for (size_t s = 0; s < mm.stacks.size(); s++) {
     const MmStack &st = mm.stacks[s];
     const int64_t W = wcols[s], R8 = rows8[s];
-    const int64_t rmax = std::min<int64_t>(kHMax, std::max<int64_t>(16, (cap1 / W) / 16 * 16));
+    const int64_t rmax = std::min<int64_t>(kMmHMax, std::max<int64_t>(16, (cap1 / W) / 16 * 16));
     const int64_t nit = (R8 + rmax - 1) / rmax;
     const int64_t cut = align_up((R8 + nit - 1) / nit, 8);
     for (int64_t r0 = 0; r0 < R8; r0 += cut) {
@@ -587,38 +587,46 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
       p1.items.push_back(std::move(it));
     }
   }
-  // phase 2: the matvec's row-panel items on widened windows
+  // phase 2: the matvec's row-panel items on widened windows, cut into parts
+  // of at most kMmHMax rows
   MmPhase &p2 = mm.ph[1];
+  auto window = [&](const Segment &sg, int64_t r0) {
+    MmSeg m{};
+    m.kind = sg.kind;
+    m.block = sg.block;
+    m.row0 = sg.row0 + r0;
+    if (sg.kind == 0) {
+      m.src = 0;
+      m.src_row = sg.src_off / 8 * 8;
+      m.lead = sg.src_off - m.src_row;
+    } else {
+      m.src = 1;
+      m.src_row = mm.t8_off[sg.block];
+      m.lead = 0;
+    }
+    m.width = sg.ncols;  // the block's columns, or its rank
+    m.ncols = align_up(m.lead + m.width, 8);
+    return m;
+  };
   for (const Item &src : op.ph[1].items) {
-    MmItem it;
-    it.h = src.h;
-    it.hpad = src.hpad;
-    it.out_off = src.out_off;
-    for (const Segment &sg : src.segs) {
-      MmSeg m{};
-      m.kind = sg.kind;
-      m.block = sg.block;
-      m.row0 = sg.row0;
-      if (sg.kind == 0) {
-        m.src = 0;
-        m.src_row = sg.src_off / 8 * 8;
-        m.lead = sg.src_off - m.src_row;
-        m.width = sg.ncols;
-      } else {
-        m.src = 1;
-        m.src_row = mm.t8_off[sg.block];
-        m.lead = 0;
-        m.width = sg.ncols;  // the rank
+    const int64_t parts = (src.hpad + kMmHMax - 1) / kMmHMax;
+    const int64_t cut = align_up((src.h + parts - 1) / parts, 8);
+    for (int64_t r0 = 0; r0 < src.h; r0 += cut) {
+      MmItem it;
+      it.h = static_cast<int32_t>(std::min<int64_t>(cut, src.h - r0));
+      it.hpad = static_cast<int32_t>(align_up(it.h, 8));
+      it.out_off = static_cast<int32_t>(src.out_off + r0);
+      for (const Segment &sg : src.segs) {
+        it.segs.push_back(window(sg, r0));
+        it.ncols += it.segs.back().ncols;
       }
-      m.ncols = align_up(m.lead + m.width, 8);
-      it.ncols += m.ncols;
-      it.segs.push_back(m);
+      // a multiple of 16 columns, at least kMmMinCols: more tile rows of the
+      // last operand window (zero columns)
+      const int64_t want = std::max<int64_t>(kMmMinCols, align_up(it.ncols, 16));
+      it.segs.back().ncols += want - it.ncols;
+      it.ncols = want;
+      p2.items.push_back(std::move(it));
     }
-    if (it.ncols % 16) {  // one more tile row of the last operand window (zero columns)
-      it.segs.back().ncols += 8;
-      it.ncols += 8;
-    }
-    p2.items.push_back(std::move(it));
   }
   // data offsets, chunks, LPT schedule (cost: block bytes + operand bytes + a per-chunk overhead)
   for (int phase = 0; phase < 2; phase++) {

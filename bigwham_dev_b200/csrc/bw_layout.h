@@ -201,7 +201,9 @@ float from_bf16(uint16_t b);
 //    operand rows around it, with zeros in the widened columns;
 //  * T8 numbers the products of each low-rank block from an 8-aligned
 //    offset, its rank rounded up to a multiple of 8 with zero rows;
-//  * items are padded to a multiple of 16 columns (one MMA K-step).
+//  * items are padded to a multiple of 16 columns (one MMA K-step) and to at
+//    least 32 (the K-steps of an item alternate between two MMA issuers);
+//  * items have at most 256 rows (two M = 128 tiles).
 // The phases:
 //  * phase 1: stacks of B factors per column cluster, as for the matvec, with
 //    rows on T8's numbering;
@@ -212,6 +214,9 @@ constexpr int kMmRhs = 64;             // right-hand sides per pass (MMA N)
 constexpr int kMmStageBytes = 49152;   // block data + operand rows of one pipeline stage
 constexpr int kMmMaxRuns = 4;          // operand runs per chunk (a chunk ends early to keep this)
 constexpr int kMmMaxCols = 512;        // columns per chunk
+constexpr int kMmHMax = 256;           // rows per item (two M = 128 tiles)
+constexpr int kMmMinCols = 32;         // columns per item (two K-steps: one per MMA issuer)
+constexpr int kMmPadRows = 32;         // zero operand rows after X and T8 that widened windows may reach
 
 struct MmRun {
   uint32_t src;   // first operand row (multiple of 8) | operand << 31 (0: X, 1: T8)

@@ -2,23 +2,28 @@
 // the 5th-generation tensor cores (tcgen05, sm_100a).
 //
 // One persistent kernel per phase, one CTA per SM, with four roles:
-//  * warp 0, producer: for every chunk, two or more bulk copies (cp.async.bulk)
-//    into a ring of kMmStages shared-memory stages, counted in bytes on the
-//    stage's `full` mbarrier:
+//  * warps 0 and 1, producers (even and odd chunks, so that the issue of
+//    their copies overlaps): for every chunk, two or more bulk copies
+//    (cp.async.bulk) into a ring of kMmStages shared-memory stages, counted in
+//    bytes on the stage's `full` mbarrier:
 //      - the chunk's block data (8x8 BF16 tiles);
 //      - its runs of operand rows (8x8 BF16 tiles of X or T8, 64 columns).
-//  * warp 1, MMA issuer: allocates 512 TMEM columns (two accumulator buffers
-//    of up to 4 m-tiles x 64 columns).  Per chunk, one thread issues
-//    tcgen05.mma.cta_group::1.kind::f16, M = 128, N = 64, K = 16, for every
-//    (K-step, m-tile).
+//  * warps 2 and 3, MMA issuers: warp 2 allocates 512 TMEM columns (two
+//    accumulator buffers x two issuers x two m-tiles x 64 columns).  One
+//    thread per issuer issues tcgen05.mma.cta_group::1.kind::f16, M = 128,
+//    N = 64, K = 16.
+//      - The K-steps of an item alternate between the issuers (split-K into
+//        two accumulators): one thread issues an MMA at most every ~80
+//        cycles, two keep the N = 64 tensor pipe fed.
 //      - A and B are read from shared memory through MN-major, no-swizzle
 //        descriptors.
-//      - The chunk's stage is released by tcgen05.commit on its `empty` barrier.
-//      - At an item's last chunk, a second commit signals `accfull`.
-//  * warps 2-5, epilogue: each reads its 32-lane quarter of the finished
-//    accumulators with tcgen05.ld, then writes T8 (BF16 tiles, phase 1) or
-//    y (FP64, caller's ordering through the row permutation, phase 2).  It
-//    then hands the buffer back on `accempty`.
+//      - Each issuer releases a chunk's stage with tcgen05.commit on its
+//        `empty` barrier (two arrivals), and at an item's last chunk signals
+//        `accfull` (two arrivals).
+//  * warps 4-7, epilogue: each reads its 32-lane quarter of both issuers'
+//    finished accumulators with tcgen05.ld and adds them.  It then writes T8
+//    (BF16 tiles, phase 1) or y (FP64, caller's ordering through the row
+//    permutation, phase 2), and hands the buffer back on `accempty`.
 // Items alternate between the two accumulator buffers, so the epilogue of one
 // item overlaps the MMAs of the next.  Every wait is bounded; on a timeout the
 // kernel records an error word, lets copies and MMAs in flight finish, frees
@@ -38,12 +43,12 @@ namespace bw {
 constexpr int kMmStages = 4;
 constexpr int kMmSlack = 2048;      // an M = 128 read of a chunk of fewer rows reaches up to 2 KB past it
 constexpr int kMmStageSize = kMmStageBytes + kMmSlack;
-constexpr int kMmThreads = 192;     // producer, MMA issuer, 4 epilogue warps
-constexpr int kMmTmemCols = 512;    // 2 buffers x 4 m-tiles x 64 columns
-constexpr int kMmBarBytes = (2 * kMmStages + 4 + 1) * 8 + 16;
+constexpr int kMmThreads = 256;     // 2 producers, 2 MMA issuers, 4 epilogue warps
+constexpr int kMmTmemCols = 512;    // 2 buffers x 2 issuers x 2 m-tiles x 64 columns
+constexpr int kMmBarBytes = (2 * kMmStages + 4 + 2) * 8 + 16;
 constexpr int kMmSmem = kMmStages * kMmStageSize + kMmStages * (int)sizeof(MmChunk) + kMmBarBytes;
 static_assert(kMmSmem <= 232448, "shared memory above the 227 KB per-CTA limit");
-static_assert(kHMax <= 4 * 128, "an item's rows must fit 4 m-tiles of 128");
+static_assert(kMmHMax <= 2 * 128, "an item's rows must fit 2 m-tiles of 128");
 
 constexpr int kErrMmTimeout = 0x201;
 constexpr int kErrMmBadChunk = 0x202;
@@ -130,27 +135,28 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
   uint64_t *empty = full + kMmStages;
   uint64_t *accfull = empty + kMmStages;   // [2]
   uint64_t *accempty = accfull + 2;        // [2]
-  uint64_t *drained = accempty + 2;        // MMA completion before TMEM is freed
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drained + 1);
+  uint64_t *drained = accempty + 2;        // [2] per issuer: MMA completion before TMEM is freed
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drained + 2);
   volatile int *abort = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kMmStages; s++) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+      mbar_init(&empty[s], 2);     // one commit per MMA issuer
     }
     for (int b = 0; b < 2; b++) {
-      mbar_init(&accfull[b], 1);
-      mbar_init(&accempty[b], 4);
+      mbar_init(&accfull[b], 2);   // one commit per MMA issuer
+      mbar_init(&accempty[b], 4);  // one arrival per epilogue warp
     }
-    mbar_init(drained, 1);
+    mbar_init(&drained[0], 1);
+    mbar_init(&drained[1], 1);
     *abort = 0;
     fence_barrier_init();
   }
   const int cb = a.cta_ptr[blockIdx.x], ce = a.cta_ptr[blockIdx.x + 1];
   if (cb >= ce) return;  // uniform across the CTA: nothing allocated yet
-  if (warp == 1) {
+  if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kMmTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -160,18 +166,21 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 0) {
-    // ------------------------------------------------------------------ producer
+  if (warp < 2) {
+    // ------------------------------------------------------------------ producers
+    // producer `warp` stages the chunks i (CTA-relative) with i % 2 == warp;
+    // its lane k holds the descriptor of the k-th such chunk of a batch of 32
     const unsigned char *gdata = reinterpret_cast<const unsigned char *>(a.data);
     const unsigned char *gx = reinterpret_cast<const unsigned char *>(a.xt);
     const unsigned char *gt = reinterpret_cast<const unsigned char *>(a.t8);
     int issued = 0;
     bool ok = true;
-    for (int bb = cb; bb < ce && ok; bb += 32) {
-      // lane k holds the descriptor of chunk bb + k
+    const int nch = ce - cb;
+    for (int i0 = warp; i0 < nch && ok; i0 += 64) {
       uint32_t dw[kMmChunkWords];
-      if (bb + lane < ce) {
-        const uint4 *p = reinterpret_cast<const uint4 *>(a.chunks + bb + lane);
+      const int mine = i0 + 2 * lane;
+      if (mine < nch) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(a.chunks + cb + mine);
 #pragma unroll
         for (int q = 0; q < kMmChunkWords / 4; q++) {
           const uint4 v = __ldg(p + q);
@@ -184,12 +193,12 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
 #pragma unroll
         for (int q = 0; q < kMmChunkWords; q++) dw[q] = 0;
       }
-      const int nb = min(32, ce - bb);
+      const int nb = min(32, (nch - i0 + 1) / 2);
       for (int k = 0; k < nb; k++) {
-        const int i = bb + k - cb;
+        const int i = i0 + 2 * k;
         const int s = i % kMmStages;
         const uint32_t use = static_cast<uint32_t>(i / kMmStages);
-        // lane k holds chunk k's descriptor and issues it; the others wait
+        // lane k holds chunk i's descriptor and issues it; the others wait
         bool waited = true;
         if (lane == k) {
           waited = mm_wait(&empty[s], (use & 1u) ^ 1u, a.spin_limit, abort);
@@ -217,7 +226,7 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
             if (r < nr) run_rows += w[8 + 2 * r + 1];
           const uint32_t dbytes = static_cast<uint32_t>(kc) * static_cast<uint32_t>(hpad) * 2u;
           const uint32_t bbytes = static_cast<uint32_t>(kc) * (2u * kMmRhs);
-          const bool good = kc > 0 && kc <= kMmMaxCols && (kc & 15) == 0 && hpad > 0 && hpad <= kHMax &&
+          const bool good = kc > 0 && kc <= kMmMaxCols && (kc & 15) == 0 && hpad > 0 && hpad <= kMmHMax &&
                             (hpad & 7) == 0 && nr > 0 && nr <= kMmMaxRuns && run_rows == static_cast<uint32_t>(kc) &&
                             dbytes + bbytes <= static_cast<uint32_t>(kMmStageBytes);
           unsigned char *st = smem + s * kMmStageSize;
@@ -238,7 +247,7 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
             bulk_g2s(st + bbytes, gdata + static_cast<unsigned long long>(data_off) * 2ull, dbytes, &full[s]);
           } else {
             set_error(a.err, kErrMmBadChunk);
-            sd->kc = 0;  // the MMA issuer skips the chunk
+            sd->kc = 0;  // the MMA issuers skip the chunk
             mbar_arrive(&full[s]);
           }
         }
@@ -247,15 +256,20 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
       }
     }
     if (!ok) {
-      for (int i = max(0, issued - kMmStages); i < issued; i++) {
+      // let this producer's copies in flight land before the CTA can exit
+      for (int j = max(0, issued - kMmStages / 2); j < issued; j++) {
+        const int i = warp + 2 * j;
         const int s = i % kMmStages;
         mbar_wait(&full[s], static_cast<uint32_t>(i / kMmStages) & 1u, a.spin_limit);
       }
     }
-  } else if (warp == 1) {
-    // ------------------------------------------------------------------ MMA issuer
+  } else if (warp < 4) {
+    // ------------------------------------------------------------------ MMA issuers
+    const uint32_t q = static_cast<uint32_t>(warp - 2);  // takes the item's K-steps of parity q
     const uint32_t idesc = umma_idesc_bf16(128, kMmRhs);
     uint32_t items = 0;
+    int kg = 0;          // K-steps of the current item before this chunk
+    bool started = false;  // this issuer's accumulator of the current item holds a product
     bool ok = true;
     for (int i = 0; i < ce - cb && ok; i++) {
       const int s = i % kMmStages;
@@ -273,32 +287,40 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
           ok = false;
           break;
         }
+        kg = 0;
+        started = false;
       }
       tc_fence_after();
-      if (lane == 0 && kc > 0) {
-        // descriptors of K-step 0; each K-step moves A by 2 * lbo_a bytes and
-        // B by 2 * lbo_b bytes, i.e. the start-address field by that / 16
-        const int nM = (hpad + 127) >> 7, nks = kc >> 4;
+      const int nks = kc >> 4;
+      const int ks0 = (static_cast<int>(q) - kg) & 1;  // first K-step of this chunk with the issuer's parity
+      if (lane == 0 && kc > 0 && ks0 < nks) {
+        // descriptors of K-step ks0; each of this issuer's K-steps moves A by
+        // 4 * lbo_a bytes and B by 4 * lbo_b bytes (two K-steps), i.e. the
+        // start-address field by that / 16
+        const int nM = (hpad + 127) >> 7;
         const uint32_t sb = smem_u32(smem + s * kMmStageSize);
         const uint32_t sa = sb + static_cast<uint32_t>(kc) * (2u * kMmRhs);
         const uint32_t lbo_a = 16u * static_cast<uint32_t>(hpad), lbo_b = 16u * kMmRhs;
-        const uint64_t a0 = umma_desc(sa, lbo_a, 128u), b0 = umma_desc(sb, lbo_b, 128u);
+        const uint64_t a0 = umma_desc(sa + static_cast<uint32_t>(ks0) * 2u * lbo_a, lbo_a, 128u);
+        const uint64_t b0 = umma_desc(sb + static_cast<uint32_t>(ks0) * 2u * lbo_b, lbo_b, 128u);
         const uint32_t a_hi = static_cast<uint32_t>(a0 >> 32), b_hi = static_cast<uint32_t>(b0 >> 32);
-        const uint32_t a_step = (2u * lbo_a) >> 4, b_step = (2u * lbo_b) >> 4;
-        const uint32_t acc0 = (flags & kFirst) ? 0u : 1u;
+        const uint32_t a_step = (4u * lbo_a) >> 4, b_step = (4u * lbo_b) >> 4;
+        const uint32_t acc0 = started ? 1u : 0u;
         for (int mt = 0; mt < nM; mt++) {
-          const uint32_t d = tmem + buf * 256u + static_cast<uint32_t>(mt) * kMmRhs;
+          const uint32_t dt = tmem + buf * 256u + q * 128u + static_cast<uint32_t>(mt) * kMmRhs;
           uint32_t a_lo = static_cast<uint32_t>(a0) + static_cast<uint32_t>(mt) * (2048u >> 4);
           uint32_t b_lo = static_cast<uint32_t>(b0);
-          umma_bf16(d, a_lo, a_hi, b_lo, b_hi, idesc, acc0);
+          umma_bf16(dt, a_lo, a_hi, b_lo, b_hi, idesc, acc0);
 #pragma unroll 4
-          for (int ks = 1; ks < nks; ks++) {
+          for (int ks = ks0 + 2; ks < nks; ks += 2) {
             a_lo += a_step;
             b_lo += b_step;
-            umma_bf16(d, a_lo, a_hi, b_lo, b_hi, idesc, 1u);
+            umma_bf16(dt, a_lo, a_hi, b_lo, b_hi, idesc, 1u);
           }
         }
       }
+      if (ks0 < nks) started = true;
+      kg += nks;
       __syncwarp();
       if (lane == 0) {
         umma_commit(&empty[s]);
@@ -312,9 +334,9 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
       *abort = 1;
     }
     // every MMA issued so far completes before the TMEM is freed
-    if (lane == 0) umma_commit(drained);
+    if (lane == 0) umma_commit(&drained[q]);
     __syncwarp();
-    mbar_wait(drained, 0u, a.spin_limit);
+    mbar_wait(&drained[q], 0u, a.spin_limit);
   } else {
     // ------------------------------------------------------------------ epilogue
     const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
@@ -358,11 +380,14 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
           }
 #pragma unroll 1
           for (int c0 = 0; c0 < kMmRhs; c0 += 16) {
-            float v[16];
-            tmem_ld16(tmem + (static_cast<uint32_t>(quarter * 32) << 16) + buf * 256u +
-                          static_cast<uint32_t>(mt) * kMmRhs + static_cast<uint32_t>(c0),
-                      v);
+            float v[16], v2[16];
+            const uint32_t ta = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + buf * 256u +
+                                static_cast<uint32_t>(mt) * kMmRhs + static_cast<uint32_t>(c0);
+            tmem_ld16(ta, v);
+            tmem_ld16(ta + 128u, v2);  // the second issuer's accumulator
             if (!live) continue;
+#pragma unroll
+            for (int k2 = 0; k2 < 16; k2++) v[k2] += v2[k2];
             if (a.phase == 1) {
               const long long r8 = static_cast<long long>(ioff) + row;
 #pragma unroll
@@ -392,7 +417,7 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 1) {
+  if (warp == 2) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMmTmemCols));
   }

@@ -121,7 +121,7 @@ def mm_replay(h, X_perm, transposed=False, check=None, round_operands=False):
                                for c in range(0, k, 64)], axis=1)
     n_in, n_out = (h.n_rows, h.n_cols) if transposed else (h.n_cols, h.n_rows)
     p1, p2 = h.mm_plan_export(1, transposed), h.mm_plan_export(2, transposed)
-    ops = [np.zeros(((n_in + 7) // 8 * 8 + 16, 64)), np.zeros((p1["t8_len"] + 16, 64))]
+    ops = [np.zeros(((n_in + 7) // 8 * 8 + 32, 64)), np.zeros((p1["t8_len"] + 32, 64))]
     ops[0][:n_in, :k] = _bf16(X_perm) if round_operands else X_perm
     Y = np.zeros((n_out, k))
     for phase, pl in ((1, p1), (2, p2)):

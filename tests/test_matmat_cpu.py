@@ -14,7 +14,8 @@ the kernel's limits:
   * kc a multiple of 16 and at most 512;
   * at most 4 runs, each 8-aligned and 8-row multiple, covering exactly kc rows;
   * block data + operand rows within one 48 KB stage;
-  * hpad a multiple of 8 and at most 512.
+  * hpad a multiple of 8 and at most 256;
+  * every item at least 32 columns (a K-step for each MMA issuer).
 """
 import numpy as np
 import pytest
@@ -44,7 +45,9 @@ def check_chunk(w):
     kc, hpad = int(w[2]), int(w[3])
     nr = (int(np.uint32(w[6])) >> 8) & 0xFF
     assert 0 < kc <= 512 and kc % 16 == 0
-    assert 0 < hpad <= 512 and hpad % 8 == 0
+    assert 0 < hpad <= 256 and hpad % 8 == 0
+    if (int(np.uint32(w[6])) & 3) == 3:  # an item of one chunk still has a K-step for each of the two MMA issuers
+        assert kc >= 32
     assert 1 <= nr <= 4
     rows = [int(w[9 + 2 * r]) for r in range(nr)]
     srcs = [int(np.uint32(w[8 + 2 * r])) & 0x7FFFFFFF for r in range(nr)]
