@@ -197,7 +197,7 @@ def build_hmatrix(a, world, rank, local):
         info["host_build_s"] = round(time.time() - t0, 2)
         t0 = time.time()
         io.use_cuda = True
-        h = io.attach_gpu(precs, transpose=False)
+        h = io.attach_gpu(precs, transpose=False, matmat=a.matmat)
         info["upload_s"] = round(time.time() - t0, 2)
         info["compression"] = io.get_compression_ratio()
         return io, h, info
@@ -232,7 +232,7 @@ def build_hmatrix(a, world, rank, local):
     arr = {k: np.load(os.path.join(d, k + ".bin"), mmap_mode="r") for k in keys}
     t0 = time.time()
     h = HmatGpu.from_flat(meta["dof"], meta["n_rows"], meta["n_cols"], arr["fr"], arr["lr"], arr["fr_data"],
-                          arr["lr_data"], arr["perm0"], arr["perm1"], device=local, precisions=precs)
+                          arr["lr_data"], arr["perm0"], arr["perm1"], device=local, precisions=precs, matmat=a.matmat)
     info["upload_s"] = round(time.time() - t0, 2)
     barrier(world)
     if rank == 0:
@@ -241,6 +241,108 @@ def build_hmatrix(a, world, rank, local):
         os.unlink(os.path.join(d, "meta.json"))
         os.rmdir(d)
     return None, h, info
+
+
+def _events_ms(fn, steps):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def time_matmat(a, h, dev, peak, ms_bf16_matvec):
+    """H X for 64 right-hand sides on the tensor cores (BF16 matmat layout):
+    3 launches per product (X gather, phase 1, phase 2)."""
+    import torch
+
+    k = 64
+    X = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, (h.n_cols, k))).to(dev).t().contiguous().t()
+    Y = torch.empty(k, h.n_rows, dtype=torch.float64, device=dev).t()
+    for _ in range(a.warmup):
+        h.matmat(X, "bf16", out=Y)
+    steps = max(3, min(a.steps, 50))
+    ms = _events_ms(lambda: h.matmat(X, "bf16", out=Y), steps)
+    errs = []
+    for j in (0, k - 1):
+        y64 = h.matvec(X[:, j].contiguous(), "fp64")
+        errs.append(float(torch.linalg.vector_norm(Y[:, j] - y64) / torch.linalg.vector_norm(y64)))
+    block = 0
+    for phase in (1, 2):
+        c = h.mm_plan_export(phase)["chunks"].astype(np.int64)
+        block += int((c[:, 2] * c[:, 3] * 2).sum())
+    return {"workload": "3DR0-H 256x256, 64 right-hand sides ~U(-1,1) seed 5, BF16 blocks and X, FP32 accumulate "
+                        "(tcgen05, TMEM accumulators)",
+            "steps": steps, "ms_per_matmat": ms, "rhs_per_s": k / (ms * 1e-3),
+            "per_rhs_speedup_vs_bf16_matvec": ms_bf16_matvec * k / ms, "block_bytes": block,
+            "block_gbs": block / (ms * 1e-3) / 1e9, "roofline_frac_of_measured_hbm": block / (ms * 1e-3) / 1e9 / peak,
+            "rel_err_vs_fp64_gpu_columns_0_63": errs, "launches_per_matmat": 3}
+
+
+def time_batch(a, dev):
+    """48 independent 2DS0-H straight cracks on [-1,1], segment counts
+    log-uniform in [256, 16,384] (seed 3), leaf 32, eta 3, eps 1e-5, built by
+    the reference's host code: one batched matvec (4 launches for all 48)
+    against 48 separate handles (4 launches each)."""
+    import torch
+    from types import SimpleNamespace
+
+    from bigwham_dev_b200 import HmatGpu
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+    from bigwham_dev_b200.meshes import straight_crack_2d
+
+    rng = np.random.default_rng(3)
+    sizes = np.round(np.exp(rng.uniform(np.log(256), np.log(16384), 48))).astype(int)
+    t0 = time.time()
+    members = []
+    for n in sizes:
+        coor, conn = straight_crack_2d(int(n))
+        io = BigWhamIOGpu(coor, conn, "2DS0-H", PROPS, os.cpu_count() or 1, useCuda=False)
+        io.build_hierarchical_matrix(LEAF, ETA, EPS)
+        members.append(SimpleNamespace(**io.export_blocks()))
+        io.close()
+    build_s = time.time() - t0
+    precs = ("fp64", "bf16")
+    hb = HmatGpu.batch(members, device=dev.index or 0, precisions=precs)
+    hs = [HmatGpu.from_flat(m.dof, m.n_rows, m.n_cols, m.fr, m.lr, m.fr_data, m.lr_data, m.perm0, m.perm1,
+                            device=dev.index or 0, precisions=precs) for m in members]
+    x = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, hb.n_cols)).to(dev)
+    y = torch.empty(hb.n_rows, dtype=torch.float64, device=dev)
+    xs = [x[int(hb.col_offsets[k]):int(hb.col_offsets[k + 1])].contiguous() for k in range(len(hs))]
+    ys = [torch.empty(hs[k].n_rows, dtype=torch.float64, device=dev) for k in range(len(hs))]
+    out = {"workload": "48 x 2DS0-H straight cracks, segments log-uniform in [256, 16384] seed 3 "
+                       f"({int(sizes.sum()):,} segments, {hb.n_rows:,} DoF in total), x~U(-1,1) seed 0",
+           "host_build_s": round(build_s, 2)}
+    steps = max(3, min(a.steps, 50))
+    for p in precs:
+        for _ in range(a.warmup):
+            hb.matvec(x, p, out=y)
+            for k in range(len(hs)):
+                hs[k].matvec(xs[k], p, out=ys[k])
+        ms_b = _events_ms(lambda: hb.matvec(x, p, out=y), steps)
+
+        def separate():
+            for k in range(len(hs)):
+                hs[k].matvec(xs[k], p, out=ys[k])
+
+        ms_s = _events_ms(separate, steps)
+        yb = y.clone()
+        separate()
+        diff = max(float(torch.linalg.vector_norm(yb[int(hb.row_offsets[k]):int(hb.row_offsets[k + 1])] - ys[k]) /
+                         torch.linalg.vector_norm(ys[k])) for k in range(len(hs)))
+        out[p] = {"ms_per_batched_matvec": ms_b, "batches_per_s": 1e3 / ms_b, "ms_48_separate_handles": ms_s,
+                  "speedup_batched_vs_separate": ms_s / ms_b, "algorithmic_bytes": hb.algorithmic_bytes(p),
+                  "batched_gbs": hb.algorithmic_bytes(p) / (ms_b * 1e-3) / 1e9,
+                  "max_member_rel_diff_batched_vs_separate": diff, "launches": {"batched": 4, "separate": 4 * len(hs)}}
+    hb.close()
+    for h in hs:
+        h.close()
+    return out
 
 
 def cpu_baseline(a, x_host, y_fp64):
@@ -282,6 +384,8 @@ def run_ours(a):
 
     world, rank, local = dist_setup(a.gpus)
     torch.cuda.set_device(local)
+    if world > 1:  # the matmat and batch lines run on one GPU only
+        a.matmat, a.no_batch = False, True
     io, h, setup = build_hmatrix(a, world, rank, local)
     dev = torch.device("cuda", local)
     n_in, n_out = h.n_cols, h.n_rows
@@ -345,6 +449,11 @@ def run_ours(a):
     y64 = yref if "fp64" in ys else None
     errs = {p: float(np.linalg.norm(ys[p].cpu().numpy() - yref) / np.linalg.norm(yref)) for p in ys if p != "fp64"}
     errs["e2e_bf16_vs_device_bf16"] = float(np.linalg.norm(y_e2e - ys["bf16"].cpu().numpy()) / np.linalg.norm(yref))
+    extra = {}
+    if world == 1 and a.matmat:
+        extra["matmat_64rhs"] = time_matmat(a, h, dev, peak, res["bf16"]["ms_per_step"])
+    if world == 1 and not a.no_batch:
+        extra["batched_2ds0_48"] = time_batch(a, dev)
     if rank != 0:
         return 0
     cpu, parity = (None, None)
@@ -379,6 +488,7 @@ def run_ours(a):
         "speedup_fp32_vs_fp64": res["fp32"]["value"] / res["fp64"]["value"] if {"fp32", "fp64"} <= set(res) else None,
         "rel_err_vs_fp64_gpu": errs,
         "fp64_gpu_vs_reference_rel_err": parity,
+        **extra,
     }
     print(json.dumps(out))
     if world > 1:
@@ -398,6 +508,9 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precisions", default="fp64,fp32,bf16",
                     help="storage precisions to upload and time (comma list; must include bf16, the headline)")
+    ap.add_argument("--no-matmat", dest="matmat", action="store_false",
+                    help="skip the 64-right-hand-side tensor-core matmat line (N = 1 only)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 48 x 2DS0 batched line (N = 1 only)")
     ap.add_argument("--cpu-budget-s", type=float, default=10.0)
     ap.add_argument("--ref-budget-s", type=float, default=60.0)
     a = ap.parse_args(argv)

@@ -113,16 +113,20 @@ class BigWhamIOGpu:
         if self.use_cuda:
             self.attach_gpu(self._precisions, self._transpose)
 
-    def attach_gpu(self, precisions=("fp64",), transpose: bool = False, release_host: bool = True) -> HmatGpu:
+    def attach_gpu(self, precisions=("fp64",), transpose: bool = False, release_host: bool = True,
+                   matmat: bool = False) -> HmatGpu:
         flags = 0
         for p in precisions:
             flags |= _prec_flag(p)
         if transpose:
             flags |= A.BW_STORE_TRANSPOSE
+        if matmat:
+            flags |= A.BW_STORE_MATMAT
         _check(self._L.bwh_attach_gpu(self._h, self.device, flags, int(release_host)))
         h = self._L.bwh_gpu_handle(self._h)
         self.gpu = HmatGpu._borrow(h, self.get_dof(), self.matrix_size(0), self.matrix_size(1), precisions,
                                    transpose, owner=self)
+        self.gpu.has_matmat = bool(matmat)
         self.set_precision(precisions[0] if "fp64" not in precisions else "fp64")
         return self.gpu
 
