@@ -111,6 +111,7 @@ def _ref():
         lib.ref_matvec_perm.argtypes = [C.c_void_p, _f64p, _f64p]
         lib.ref_diagonal.argtypes = [C.c_void_p, _f64p]
         lib.ref_collocation_points.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ref_dense_rows.argtypes = [C.c_void_p, C.c_char_p, _f64p, _i64p, C.c_int64, _f64p]
         lib.ref_collocation_points.restype = C.c_int64
         lib.ref_destroy.argtypes = [C.c_void_p]
         _ref_lib = lib
@@ -161,6 +162,19 @@ class RefHmat:
 
     def compression(self) -> float:
         return _ref().ref_compression(self._h)
+
+    def dense_rows(self, kernel: str, properties, points):
+        """Rows of the dense FP64 operator (exact kernel, no H-matrix
+        approximation) for the given collocation points, original ordering:
+        (len(points) * dof, n_cols)."""
+        lib = _ref()
+        pts = np.ascontiguousarray(points, dtype=np.int64)
+        props = np.ascontiguousarray(properties, dtype=np.float64)
+        out = np.empty((pts.size * self.dof, self.shape[1]))
+        rc = lib.ref_dense_rows(self._h, kernel.encode(), props, pts, pts.size, out)
+        if rc != 0:
+            raise RuntimeError(f"ref_dense_rows failed ({rc})")
+        return out
 
     def collocation_points(self):
         lib = _ref()

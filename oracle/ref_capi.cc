@@ -16,6 +16,15 @@
 #include <vector>
 
 #include "cblas.h"
+#include "core/bie_kernel.h"
+#include "core/elastic_properties.h"
+#include "elasticity/bie_elastostatic.h"
+#include "elasticity/fullspace_iso_2d_segment/bie_elastostatic_segment_0_influence.h"
+#include "elasticity/fullspace_iso_3d_rectangle/bie_elastostatic_rectangle_0_influence.h"
+#include "elasticity/fullspace_iso_3d_triangle/bie_elastostatic_triangle_0_influence.h"
+#include "elements/rectangle.h"
+#include "elements/segment.h"
+#include "elements/triangle.h"
 #include "io/bigwham_io.h"
 
 #ifdef BIGWHAM_OPENMP
@@ -143,6 +152,59 @@ int ref_diagonal(void *h, double *d) {
   H(h)->io->GetDiagonal(v);
   std::memcpy(d, v.data(), sizeof(double) * v.size());
   return 0;
+}
+
+// Rows of the DENSE FP64 operator (no H-matrix approximation) for the given
+// collocation points, in the original ordering: out is (npts * dof) x
+// (n_points * dof), row-major; row q*dof + a, column j*dof + b holds the
+// influence of source point j's component b on receiver point points[q]'s
+// component a.  The kernel is built as BigWhamIO builds it for the same
+// kernel string (src/io/bigwham_io.cc:130-290) and evaluated entry by entry as
+// the reference's BieMatrixGenerator::set does (src/hmat/bie_matrix_generator.h:
+// 96-147), over the handle's own mesh.  Kernels: 2DS0-H, 3DR0-H, 3DT0-H.
+int ref_dense_rows(void *h, const char *kernel, const double *props, const int64_t *points, int64_t npts,
+                   double *out) {
+  try {
+    const std::shared_ptr<bigwham::Mesh> mesh = H(h)->io->GetSourceMeshPtr();
+    bigwham::ElasticProperties elas(props[0], props[1]);
+    std::shared_ptr<bigwham::BieKernel<double>> ker;
+    const std::string k(kernel);
+    if (k == "2DS0-H")
+      ker = std::make_shared<bigwham::BieElastostatic<bigwham::Segment<0>, bigwham::Segment<0>,
+                                                      bigwham::ElasticKernelType::H>>(elas, 2);
+    else if (k == "3DR0-H")
+      ker = std::make_shared<bigwham::BieElastostatic<bigwham::Rectangle<0>, bigwham::Rectangle<0>,
+                                                      bigwham::ElasticKernelType::H>>(elas, 3);
+    else if (k == "3DT0-H")
+      ker = std::make_shared<bigwham::BieElastostatic<bigwham::Triangle<0>, bigwham::Triangle<0>,
+                                                      bigwham::ElasticKernelType::H>>(elas, 3);
+    else
+      return 1;
+    const int dof = (int)ker->dof_dimension();
+    const int64_t np = mesh->num_collocation_points();
+    const int64_t ncols = np * dof;
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t q = 0; q < npts; q++) {
+      const int64_t i = points[q];
+      if (i < 0 || i >= np) {
+#pragma omp atomic write
+        bad = 1;
+        continue;
+      }
+      const auto re = mesh->GetElement(mesh->GetElementId(i));
+      const il::int_t ir = mesh->GetElementCollocationId(i);
+      for (int64_t j = 0; j < np; j++) {
+        const auto se = mesh->GetElement(mesh->GetElementId(j));
+        const std::vector<double> st = ker->influence(*se, mesh->GetElementCollocationId(j), *re, ir);
+        for (int b = 0; b < dof; b++)
+          for (int a = 0; a < dof; a++) out[(q * dof + a) * ncols + j * dof + b] = st[b * dof + a];
+      }
+    }
+    return bad ? 2 : 0;
+  } catch (...) {
+    return 3;
+  }
 }
 
 // Collocation points, flattened row-major (n_points x spatial_dim).

@@ -76,3 +76,37 @@ def test_restatement_matches_live_reference(kind):
     assert rel(oracle_matvec(arr, x, 4), R.matvec(x)) < 1e-13
     assert rel(oracle_matvec_perm(arr, x, 4), R.matvec_perm(x)) < 1e-13
     assert np.array_equal(oracle_diagonal(arr), R.diagonal())
+
+
+@needs_ref
+@pytest.mark.parametrize("kind", ["2ds0", "3dr0", "3dt0"])
+def test_dense_rows_equal_eta0_build(kind):
+    """ref_dense_rows (the exact kernel, evaluated as the reference's matrix
+    generator does) against an eta = 0 build of the reference, whose blocks are
+    all full rank: the same entries, bitwise."""
+    from bigwham_dev_b200.meshes import penny_crack_3d
+
+    if kind == "2ds0":
+        coor, conn = straight_crack_2d(300)
+        kern, props = "2DS0-H", [1.0, 0.25]
+    elif kind == "3dr0":
+        coor, conn = square_crack_3d(9)
+        kern, props = "3DR0-H", [1.0, 0.25]
+    else:
+        coor, conn = penny_crack_3d(0.2, seed=2)
+        kern, props = "3DT0-H", [1.0, 0.2]
+    R = RefHmat(kern, coor, conn, props, 16, 0.0, 1e-4, n_threads=4)
+    arr = R.arrays()
+    assert arr.lr.shape[0] == 0
+    D = np.zeros((arr.n_rows, arr.n_cols))
+    for i0, j0, a in arr.fr_blocks():
+        D[i0:i0 + a.shape[0], j0:j0 + a.shape[1]] = a
+    d = arr.dof
+    rp = (d * arr.perm0[:, None] + np.arange(d)[None, :]).ravel()
+    cp = (d * arr.perm1[:, None] + np.arange(d)[None, :]).ravel()
+    Do = np.zeros_like(D)
+    Do[np.ix_(rp, cp)] = D
+    pts = np.random.default_rng(0).choice(arr.n_rows // d, size=7, replace=False)
+    rows = R.dense_rows(kern, props, pts)
+    want = Do[(d * pts[:, None] + np.arange(d)[None, :]).ravel()]
+    assert np.array_equal(rows, want)
