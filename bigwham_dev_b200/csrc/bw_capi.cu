@@ -57,9 +57,11 @@ constexpr size_t kEv = kTimedLaunches + 1;
 struct DevPhase {
   void *data = nullptr;
   Chunk *chunks = nullptr;
-  int32_t *cta = nullptr;
+  int32_t *items = nullptr;        // chunk ranges of the items, in the order CTAs take them
+  int *queue = nullptr;            // [next item, CTAs done], zero between launches
   bw::GatherSeg *gsegs = nullptr;  // phase 2: runs that fill G2
   int64_t n_chunks = 0;
+  int64_t n_items = 0;
   int64_t n_elems = 0;
   int64_t n_gsegs = 0;
 };
@@ -146,7 +148,8 @@ struct bw_hmat {
         for (auto &ph : p) {
           cudaFree(ph.data);
           cudaFree(ph.chunks);
-          cudaFree(ph.cta);
+          cudaFree(ph.items);
+          cudaFree(ph.queue);
           cudaFree(ph.gsegs);
           ph = DevPhase{};
         }
@@ -323,10 +326,13 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   }
   dp.data = h->dmalloc((size_t)ph.n_elems[prec] * es);
   dp.chunks = static_cast<Chunk *>(h->dmalloc(std::max<size_t>(1, cp.chunks.size()) * sizeof(Chunk)));
-  dp.cta = static_cast<int32_t *>(h->dmalloc(cp.cta_ptr.size() * sizeof(int32_t)));
+  dp.n_items = (int64_t)cp.item_ptr.size() - 1;
+  dp.items = static_cast<int32_t *>(h->dmalloc(cp.item_ptr.size() * sizeof(int32_t)));
+  dp.queue = static_cast<int *>(h->dmalloc(2 * sizeof(int)));
+  BW_CUDA(cudaMemset(dp.queue, 0, 2 * sizeof(int)));
   if (!cp.chunks.empty())
     BW_CUDA(cudaMemcpy(dp.chunks, cp.chunks.data(), cp.chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
-  BW_CUDA(cudaMemcpy(dp.cta, cp.cta_ptr.data(), cp.cta_ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  BW_CUDA(cudaMemcpy(dp.items, cp.item_ptr.data(), cp.item_ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   dp.n_gsegs = (int64_t)cp.gsegs.size();
   if (dp.n_gsegs) {
     dp.gsegs = static_cast<bw::GatherSeg *>(h->dmalloc(cp.gsegs.size() * sizeof(bw::GatherSeg)));
@@ -419,7 +425,9 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
       bw::StreamArgs a{};
       a.data = dp.data;
       a.chunks = dp.chunks;
-      a.cta_ptr = dp.cta;
+      a.item_ptr = dp.items;
+      a.n_items = (int)dp.n_items;
+      a.queue = dp.queue;
       a.gsrc = phase == 0 ? (kPacked ? static_cast<const void *>(xpk) : static_cast<const void *>(xp))
                           : static_cast<const void *>(g2_buf);
       a.t_out = t;
@@ -1007,7 +1015,7 @@ int bw_last_error(const bw_hmat *h, char *buf, size_t len) {
 }
 
 int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_chunks, int32_t *chunks,
-                   int64_t *n_elems, double *data, int64_t *n_cta, int32_t *cta_ptr) {
+                   int64_t *n_elems, double *data, int64_t *n_item_ptr, int32_t *item_ptr) {
   if (!h || phase < 1 || phase > 2) return BW_ERR_ARG;
   const int p = prec_index(precision);
   if (p < 0 || !h->finalized || !(h->stored & (1 << p))) return BW_ERR_STATE;
@@ -1017,9 +1025,9 @@ int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, i
   const bw::ChunkPlan &cp = ph.cp[p];
   if (n_chunks) *n_chunks = (int64_t)cp.chunks.size();
   if (n_elems) *n_elems = ph.n_elems[p];
-  if (n_cta) *n_cta = (int64_t)cp.cta_ptr.size();
+  if (n_item_ptr) *n_item_ptr = (int64_t)cp.item_ptr.size();
   if (chunks) std::memcpy(chunks, cp.chunks.data(), cp.chunks.size() * sizeof(Chunk));  // kChunkWords int32 each
-  if (cta_ptr) std::memcpy(cta_ptr, cp.cta_ptr.data(), cp.cta_ptr.size() * sizeof(int32_t));
+  if (item_ptr) std::memcpy(item_ptr, cp.item_ptr.data(), cp.item_ptr.size() * sizeof(int32_t));
   if (data) {
     if (!h->plan_only) return BW_ERR_STATE;
     const auto &buf = h->host_data[o][p][phase - 1];

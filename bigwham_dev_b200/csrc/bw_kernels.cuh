@@ -1,7 +1,9 @@
 // Device code of the streamed H-matrix matvec (sm_100a).
 //
-// One persistent kernel per phase (see bw_layout.h).  Each CTA owns a fixed,
-// host-scheduled list of chunks.  Warp 0 is the producer: for every chunk it
+// One persistent kernel per phase (see bw_layout.h).  The CTAs take items
+// (longest first) from a queue in device memory, one atomicAdd per item, so a
+// CTA that finishes early takes more work; an item's result does not depend on
+// the CTA that computes it.  Warp 0 is the producer: for every chunk it
 // stages the block data and the chunk's contiguous run of vector values with
 // two TMA bulk copies (cp.async.bulk of the 16-byte aligned windows around
 // them) into a ring of kStages shared-memory stages; one mbarrier per stage
@@ -39,8 +41,10 @@ constexpr int kErrBadChunk = 0x104;
 
 struct StreamArgs {
   const void *data;           // element array of the phase (storage type)
-  const Chunk *chunks;        // ordered by CTA
-  const int32_t *cta_ptr;     // grid + 1
+  const Chunk *chunks;        // item by item
+  const int32_t *item_ptr;    // chunk ranges of the items, longest first (n_items + 1)
+  int n_items;
+  int *queue;                 // [next item, CTAs done]: zero at launch, reset to zero by the last CTA
   const void *gsrc;           // vector values: gathered x (phase 1) or G2 (phase 2), compute type
   void *t_out;                // phase-1 output (compute type)
   const float *t_scale;       // phase 1: per-t-entry output scale (BF16), or null
@@ -296,63 +300,83 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
   }
   __syncthreads();
 
-  const int cb = a.cta_ptr[blockIdx.x], ce = a.cta_ptr[blockIdx.x + 1];
-  if (cb >= ce) return;
-
   if (warp == 0) {
     // ------------------------------------------------------------------ producer
     const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
     const unsigned char *gvec = static_cast<const unsigned char *>(a.gsrc);
-    DescRegs cur, nxt;
-    load_desc(a.chunks, cb + lane, ce, nxt);
     bool ok = true;
-    int issued = 0;
-    for (int bb = cb; bb < ce && ok; bb += 32) {
-      cur = nxt;
-      load_desc(a.chunks, bb + 32 + lane, ce, nxt);
-      const int nb = min(32, ce - bb);
-      for (int k = 0; k < nb; k++) {
-        const int i = bb + k - cb;
-        const int s = i % kStages;
-        const uint32_t use = static_cast<uint32_t>(i / kStages);
-        if (!mbar_wait(&empty[s], (use & 1u) ^ 1u, a.spin_limit)) {
-          if (lane == 0) set_error(a.err, kErrTimeoutEmpty);
-          ok = false;
-          break;
-        }
-        uint32_t w[kChunkWords];
-#pragma unroll
-        for (int q = 0; q < kChunkWords; q++) w[q] = __shfl_sync(0xffffffffu, cur.w[q], k);
-        if (lane == 0) {
-          const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
-          const int ncols = static_cast<int>(w[2]);
-          const int hpad = static_cast<int>(w[3]);
-          const int g_off = static_cast<int>(w[7]);
-          unsigned char *st = stage0 + s * L::kStageSize;
-          uint4 *dd = reinterpret_cast<uint4 *>(st + L::kDataBytes + L::kGBytes);
-#pragma unroll
-          for (int q = 0; q < kChunkWords / 4; q++)
-            dd[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-          const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
-                                                  : static_cast<unsigned long long>(ncols);
-          const unsigned long long bytes = cols * hpad * es;
-          if (ncols > 0 && ncols <= kMaxCols && bytes <= static_cast<unsigned long long>(kStageBytes)) {
-            const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
-                                           static_cast<unsigned long long>(data_off) * es;
-            const unsigned long long lo = src & ~15ull, hi = (src + bytes + 15ull) & ~15ull;
-            const unsigned long long gs = reinterpret_cast<unsigned long long>(gvec) +
-                                          static_cast<unsigned long long>(g_off) * sizeof(G);
-            const unsigned long long glo = gs & ~15ull, ghi = (gs + ncols * sizeof(G) + 15ull) & ~15ull;
-            mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>((hi - lo) + (ghi - glo)));
-            bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
-            bulk_g2s(st + L::kDataBytes, reinterpret_cast<const void *>(glo), static_cast<uint32_t>(ghi - glo),
-                     &full[s]);
-          } else {
-            if (ncols > 0) set_error(a.err, kErrBadChunk);
-            mbar_arrive(&full[s]);
+    int issued = 0;  // chunks staged so far by this CTA (stage = issued % kStages)
+    // the item to stage now and the next one, fetched one item ahead
+    int cur = 0;
+    if (lane == 0) cur = atomicAdd(&a.queue[0], 1);
+    cur = __shfl_sync(0xffffffffu, cur, 0);
+    while (cur < a.n_items && ok) {
+      int nxt = 0;
+      if (lane == 0) nxt = atomicAdd(&a.queue[0], 1);
+      const int cb = a.item_ptr[cur], ce = a.item_ptr[cur + 1];
+      for (int bb = cb; bb < ce && ok; bb += 32) {
+        DescRegs cur_d;
+        load_desc(a.chunks, bb + lane, ce, cur_d);
+        const int nb = min(32, ce - bb);
+        for (int k = 0; k < nb; k++) {
+          const int s = issued % kStages;
+          const uint32_t use = static_cast<uint32_t>(issued / kStages);
+          if (!mbar_wait(&empty[s], (use & 1u) ^ 1u, a.spin_limit)) {
+            if (lane == 0) set_error(a.err, kErrTimeoutEmpty);
+            ok = false;
+            break;
           }
+          uint32_t w[kChunkWords];
+#pragma unroll
+          for (int q = 0; q < kChunkWords; q++) w[q] = __shfl_sync(0xffffffffu, cur_d.w[q], k);
+          if (lane == 0) {
+            const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
+            const int ncols = static_cast<int>(w[2]);
+            const int hpad = static_cast<int>(w[3]);
+            const int g_off = static_cast<int>(w[7]);
+            unsigned char *st = stage0 + s * L::kStageSize;
+            uint4 *dd = reinterpret_cast<uint4 *>(st + L::kDataBytes + L::kGBytes);
+#pragma unroll
+            for (int q = 0; q < kChunkWords / 4; q++)
+              dd[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+            const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
+                                                    : static_cast<unsigned long long>(ncols);
+            const unsigned long long bytes = cols * hpad * es;
+            if (ncols > 0 && ncols <= kMaxCols && bytes <= static_cast<unsigned long long>(kStageBytes)) {
+              const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
+                                             static_cast<unsigned long long>(data_off) * es;
+              const unsigned long long lo = src & ~15ull, hi = (src + bytes + 15ull) & ~15ull;
+              const unsigned long long gs = reinterpret_cast<unsigned long long>(gvec) +
+                                            static_cast<unsigned long long>(g_off) * sizeof(G);
+              const unsigned long long glo = gs & ~15ull, ghi = (gs + ncols * sizeof(G) + 15ull) & ~15ull;
+              mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>((hi - lo) + (ghi - glo)));
+              bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
+              bulk_g2s(st + L::kDataBytes, reinterpret_cast<const void *>(glo), static_cast<uint32_t>(ghi - glo),
+                       &full[s]);
+            } else {
+              if (ncols > 0) set_error(a.err, kErrBadChunk);
+              mbar_arrive(&full[s]);
+            }
+          }
+          issued++;
         }
-        issued++;
+      }
+      cur = __shfl_sync(0xffffffffu, nxt, 0);
+    }
+    if (ok) {
+      // end of work: a descriptor with kEnd alone, no data
+      const int s = issued % kStages;
+      const uint32_t use = static_cast<uint32_t>(issued / kStages);
+      if (mbar_wait(&empty[s], (use & 1u) ^ 1u, a.spin_limit)) {
+        if (lane == 0) {
+          uint4 *dd = reinterpret_cast<uint4 *>(stage0 + s * L::kStageSize + L::kDataBytes + L::kGBytes);
+          dd[0] = make_uint4(0, 0, 0, 0);
+          dd[1] = make_uint4(0, 0, kEnd, 0);
+          mbar_arrive(&full[s]);
+        }
+      } else {
+        if (lane == 0) set_error(a.err, kErrTimeoutEmpty);
+        ok = false;
       }
     }
     if (!ok) {
@@ -360,6 +384,16 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
       for (int i = max(0, issued - kStages); i < issued; i++) {
         const int s = i % kStages;
         mbar_wait(&full[s], static_cast<uint32_t>(i / kStages) & 1u, a.spin_limit);
+      }
+    }
+    // This CTA takes no more items.  The last CTA to get here returns the
+    // queue to zero for the next launch (every other CTA is done with it).
+    if (lane == 0) {
+      __threadfence();
+      if (atomicAdd(&a.queue[1], 1) == static_cast<int>(gridDim.x) - 1) {
+        a.queue[0] = 0;
+        a.queue[1] = 0;
+        __threadfence();
       }
     }
     return;
@@ -388,7 +422,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
 #pragma unroll
     for (int q = 0; q < 4; q++) tacc[j][q] = 0.f;
 
-  for (int i = 0; i < ce - cb; i++) {
+  for (int i = 0;; i++) {
     const int s = i % kStages;
     const uint32_t use = static_cast<uint32_t>(i / kStages);
     if (!mbar_wait(&full[s], use & 1u, a.spin_limit)) {
@@ -397,6 +431,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
     }
     const unsigned char *st = stage0 + s * L::kStageSize;
     const Chunk &d = *reinterpret_cast<const Chunk *>(st + L::kDataBytes + L::kGBytes);
+    if (d.flags & kEnd) return;  // the producer has no more items for this CTA
     // the vector window starts at the 16-byte boundary below gsrc + g_off
     const G *gs = reinterpret_cast<const G *>(
         st + L::kDataBytes +

@@ -383,6 +383,7 @@ void chunk_item(const OperatorPlan &op, const Item &it, int prec, int phase, std
 void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &op) {
   (void)p;
   (void)tr;
+  (void)grid;
   const int es = esize_of(prec);
   for (int phase = 0; phase < 2; phase++) {
     PhasePlan &ph = op.ph[phase];
@@ -399,9 +400,10 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
     cp.g_len = 0;
     for (size_t q = 0; q < ph.items.size(); q++)
       chunk_item(op, ph.items[q], prec, phase, per_item[q], cp.gsegs, cp.g_len);
-    // LPT: items by decreasing cost onto the least-loaded CTA.  Cost is the
-    // bytes streamed plus a fixed per-chunk overhead (descriptor, barrier round
-    // trip) expressed in bytes.
+    // Longest first: the CTAs take items from a queue in this order (greedy
+    // list scheduling; each CTA takes the next item when its producer is
+    // done with the previous one).  Cost is the bytes streamed plus a fixed
+    // per-chunk overhead (descriptor, barrier round trip) expressed in bytes.
     const int64_t n = (int64_t)ph.items.size();
     std::vector<int64_t> cost(n);
     for (int64_t q = 0; q < n; q++)
@@ -409,25 +411,13 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
     std::vector<int64_t> order(n);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
-    using Slot = std::pair<int64_t, int>;  // load, cta
-    std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
-    for (int c = 0; c < grid; c++) heap.push({0, c});
-    std::vector<std::vector<int64_t>> bins(grid);
-    for (int64_t q : order) {
-      Slot s = heap.top();
-      heap.pop();
-      bins[s.second].push_back(q);
-      s.first += cost[q];
-      heap.push(s);
-    }
     cp.chunks.clear();
-    cp.cta_ptr.assign(grid + 1, 0);
-    for (int c = 0; c < grid; c++) {
-      cp.cta_ptr[c] = static_cast<int32_t>(cp.chunks.size());
-      for (int64_t q : bins[c]) cp.chunks.insert(cp.chunks.end(), per_item[q].begin(), per_item[q].end());
+    cp.item_ptr.assign(1, 0);
+    for (int64_t q : order) {
+      cp.chunks.insert(cp.chunks.end(), per_item[q].begin(), per_item[q].end());
+      if (cp.chunks.size() > (size_t)INT32_MAX) fail("too many chunks");
+      cp.item_ptr.push_back(static_cast<int32_t>(cp.chunks.size()));
     }
-    cp.cta_ptr[grid] = static_cast<int32_t>(cp.chunks.size());
-    if (cp.chunks.size() > (size_t)INT32_MAX) fail("too many chunks");
   }
 }
 

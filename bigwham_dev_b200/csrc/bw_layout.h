@@ -40,6 +40,7 @@ constexpr int kItemsPerCta = 8;      // minimum items per CTA share (load balanc
 // Chunk flags
 constexpr uint32_t kFirst = 1u;      // first chunk of an item: reset accumulators
 constexpr uint32_t kLast = 2u;       // last chunk of an item: reduce and write the output
+constexpr uint32_t kEnd = 4u;        // no more chunks for this CTA (written by the producer, never stored)
 
 // One chunk descriptor, 32 bytes, read by the producer warp and copied into
 // shared memory for the consumer warps.  The vector values of the chunk's
@@ -110,12 +111,13 @@ struct Item {
   std::vector<RowPiece> pieces;  // phase 1 only
 };
 
-// Per precision: chunk list ordered by CTA, the CTA ranges, and (phase 2)
-// the runs that fill the gather array G2 of g_len values.
+// Per precision: the chunks item by item, items in the order the CTAs take
+// them (decreasing cost), the items' chunk ranges, and (phase 2) the runs that
+// fill the gather array G2 of g_len values.
 struct ChunkPlan {
   std::vector<Chunk> chunks;
-  std::vector<int32_t> cta_ptr;  // grid + 1
-  std::vector<GatherSeg> gsegs;  // phase 2 only
+  std::vector<int32_t> item_ptr;  // items + 1
+  std::vector<GatherSeg> gsegs;   // phase 2 only
   int64_t g_len = 0;
 };
 
@@ -160,8 +162,8 @@ void build_operator(const Problem &p, bool transposed, int grid, OperatorPlan &o
 void compute_scales(const Problem &p, bool transposed, bool check_finite, OperatorPlan &op);
 
 // Lays out every item for one precision (0 FP64, 1 FP32, 2 BF16), splits it
-// into chunks, and assigns items to `grid` CTAs (longest-processing-time
-// first, cost = bytes).
+// into chunks, and orders the items longest first (cost = bytes + a per-chunk
+// overhead): the kernel's CTAs take them in that order from a device queue.
 void build_chunks(const Problem &p, bool transposed, int prec, int grid, OperatorPlan &op);
 
 // Writes the data of items [i_begin, i_end) of one phase, converted to the

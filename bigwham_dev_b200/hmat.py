@@ -317,12 +317,12 @@ class HmatGpu:
         A.check(self._lib.bw_plan_export(self._h, f, phase, int(transposed), C.byref(nc), None, C.byref(ne), None,
                                          C.byref(nt), None), self._h)
         chunks = np.zeros((nc.value, 8), np.int32)
-        cta = np.zeros(nt.value, np.int32)
+        items = np.zeros(nt.value, np.int32)
         data = np.zeros(ne.value) if with_data else None
         A.check(self._lib.bw_plan_export(self._h, f, phase, int(transposed), C.byref(nc), chunks.ctypes.data,
                                          C.byref(ne), data.ctypes.data if with_data else None, C.byref(nt),
-                                         cta.ctypes.data), self._h)
-        return {"chunks": chunks, "cta_ptr": cta, "data": data}
+                                         items.ctypes.data), self._h)
+        return {"chunks": chunks, "item_ptr": items, "data": data}
 
     def set_timing(self, enable: bool = True) -> None:
         """Record CUDA events around each launch of every following matvec."""

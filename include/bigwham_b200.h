@@ -205,9 +205,11 @@ int bw_mm_plan_export(const bw_hmat *h, int phase, int transposed, int64_t *n_ch
  * layout of bw::Chunk (bigwham_dev_b200/csrc/bw_layout.h); data: n_elems values
  * converted to double, in the precision's layout (column-major items for FP64 /
  * FP32, 8x8 tiles for BF16; BF16 values divided by their block scale);
- * cta_ptr: grid+1 offsets.  Only valid on a handle finalized with BW_PLAN_ONLY. */
+ * item_ptr: the chunk ranges of the items (n_item_ptr = items + 1 offsets), in
+ * the order the kernel's CTAs take them (longest first).  data is only
+ * available on a handle finalized with BW_PLAN_ONLY. */
 int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_chunks,
-                   int32_t *chunks, int64_t *n_elems, double *data, int64_t *n_cta, int32_t *cta_ptr);
+                   int32_t *chunks, int64_t *n_elems, double *data, int64_t *n_item_ptr, int32_t *item_ptr);
 
 /* Per-launch timing for benchmarks.  With timing enabled every bw_matvec
  * records CUDA events on its stream around its four launches (x gather,

@@ -32,10 +32,10 @@ def chunk_matrix(data, d, tiled):
 
 
 def run_phase(plan, gsrc, out, tiled=False, t_scale=None):
-    chunks, cta, data = plan["chunks"], plan["cta_ptr"], plan["data"]
-    for b in range(len(cta) - 1):
+    chunks, items, data = plan["chunks"], plan["item_ptr"], plan["data"]
+    for b in range(len(items) - 1):
         acc = None
-        for i in range(cta[b], cta[b + 1]):
+        for i in range(items[b], items[b + 1]):
             d = decode(chunks[i])
             if d["flags"] & K_FIRST:
                 acc = np.zeros(d["hpad"])

@@ -45,8 +45,12 @@ def test_plan_structure(golden):
     for prec, es in (("fp64", 8), ("fp32", 4), ("bf16", 2)):
         for phase in (1, 2):
             p = h.plan_export(prec, phase, with_data=False)
-            cta = p["cta_ptr"]
-            assert cta[0] == 0 and np.all(np.diff(cta) >= 0) and cta[-1] == len(p["chunks"])
+            items = p["item_ptr"]
+            assert items[0] == 0 and np.all(np.diff(items) > 0) and items[-1] == len(p["chunks"])
+            # each item range opens with its first chunk and closes with its last
+            for b in range(len(items) - 1):
+                assert decode(p["chunks"][items[b]])["flags"] & 1
+                assert decode(p["chunks"][items[b + 1] - 1])["flags"] & 2
             open_item = False
             for w in p["chunks"]:
                 d = decode(w)
@@ -69,8 +73,9 @@ def test_plan_structure(golden):
         assert int(cols.sum()) == sum(decode(w)["ncols"] for w in p2["chunks"])
 
 
-def test_lpt_balance_on_many_items():
-    # 400 equal full blocks on a 20 x 20 block grid: 20 panels of equal cost
+def test_items_longest_first():
+    # 400 equal full blocks on a 20 x 20 block grid, plus a wider last block
+    # column: the items come out in non-increasing cost order
     dof, nb, bs = 1, 20, 24
     n = nb * bs
     rng = np.random.default_rng(0)
@@ -82,8 +87,10 @@ def test_lpt_balance_on_many_items():
             h.add_full(i * bs, j * bs, blocks[i, j])
     h.finalize(plan_only=True)
     p = h.plan_export("fp64", 2)
-    per_cta = np.diff(p["cta_ptr"])
-    assert per_cta.max() - per_cta[per_cta > 0].min() <= 2
+    items = p["item_ptr"]
+    cost = [sum(decode(w)["ncols"] * decode(w)["hpad"] * 8 + 1024 for w in p["chunks"][items[b]:items[b + 1]])
+            for b in range(len(items) - 1)]
+    assert all(a >= b for a, b in zip(cost, cost[1:]))
     D = np.block([[blocks[i, j] for j in range(nb)] for i in range(nb)])
     x = rng.standard_normal(n)
     assert rel(replay(h, x), D @ x) < 1e-14
