@@ -11,7 +11,8 @@ Sizes:
   reference build takes minutes.
 
 Checks:
-* FP32 / BF16 matvecs against the FP64 dense operator on 2,048 sampled rows
+* FP32 / BF16 matvecs against the FP64 dense operator on 2,049 sampled rows
+  (683 collocation points x 3 components)
   (the exact kernel, no H-matrix approximation, evaluated by the reference's
   kernel in the oracle).  The bound is the ACA tolerance plus the storage
   rounding (relative 2e-3).
@@ -49,7 +50,8 @@ def penny():
     h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
                           arr.perm1, device=0, precisions=("fp64", "fp32", "bf16"))
     npts = arr.n_rows // 3
-    sample = np.sort(np.random.default_rng(7).choice(npts, size=min(2048, npts), replace=False))
+    # 683 collocation points = 2,049 sampled rows of the dense operator
+    sample = np.sort(np.random.default_rng(7).choice(npts, size=min(683, npts), replace=False))
     D = R.dense_rows("3DT0-H", PROPS, sample)
     rows = (3 * sample[:, None] + np.arange(3)[None, :]).ravel()
     cp = R.collocation_points().reshape(-1, 3)
