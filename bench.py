@@ -187,8 +187,11 @@ def build_hmatrix(a, world, rank, local):
     from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
     from bigwham_dev_b200.meshes import square_crack_3d
 
+    from bigwham_dev_b200.tune import load_best
+
     precs = tuple(a.precisions)
-    info = {}
+    tuning = load_best(a.mesh, "bf16")  # committed autotuner result for this mesh, if any
+    info = {"tuning": tuning or "defaults"}
     coor, conn = square_crack_3d(a.mesh)
     if world == 1:
         t0 = time.time()
@@ -197,7 +200,7 @@ def build_hmatrix(a, world, rank, local):
         info["host_build_s"] = round(time.time() - t0, 2)
         t0 = time.time()
         io.use_cuda = True
-        h = io.attach_gpu(precs, transpose=False, matmat=a.matmat)
+        h = io.attach_gpu(precs, transpose=False, matmat=a.matmat, tuning=tuning)
         info["upload_s"] = round(time.time() - t0, 2)
         info["compression"] = io.get_compression_ratio()
         return io, h, info
@@ -232,7 +235,8 @@ def build_hmatrix(a, world, rank, local):
     arr = {k: np.load(os.path.join(d, k + ".bin"), mmap_mode="r") for k in keys}
     t0 = time.time()
     h = HmatGpu.from_flat(meta["dof"], meta["n_rows"], meta["n_cols"], arr["fr"], arr["lr"], arr["fr_data"],
-                          arr["lr_data"], arr["perm0"], arr["perm1"], device=local, precisions=precs, matmat=a.matmat)
+                          arr["lr_data"], arr["perm0"], arr["perm1"], device=local, precisions=precs, matmat=a.matmat,
+                          tuning=tuning)
     info["upload_s"] = round(time.time() - t0, 2)
     barrier(world)
     if rank == 0:

@@ -30,6 +30,7 @@ _SIGS = {
     "bw_create_batch": (C.c_int, [C.c_int, C.c_int, _P, _P, _P, _P, C.c_int, C.POINTER(_P)]),
     "bw_batch_offsets": (C.c_int, [_P, C.c_int, _P, _P]),
     "bw_batch_count": (C.c_int, [_P]),
+    "bw_set_tuning": (C.c_int, [_P, C.c_char_p, _I64]),
     "bw_add_full": (C.c_int, [_P, _I64, _I64, _I64, _I64, _P, _I64]),
     "bw_add_lowrank": (C.c_int, [_P, _I64, _I64, _I64, _I64, _I64, _P, _I64, _P, _I64]),
     "bw_finalize": (C.c_int, [_P, C.c_int]),

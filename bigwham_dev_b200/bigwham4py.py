@@ -35,6 +35,7 @@ _HSIGS = {
     "bwh_build": (C.c_int, [_P, C.c_int, C.c_double, C.c_double]),
     "bwh_attach_gpu": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
     "bwh_set_precision": (C.c_int, [_P, C.c_int]),
+    "bwh_set_tuning": (C.c_int, [_P, C.c_char_p, C.c_int64]),
     "bwh_matvec": (C.c_int, [_P, _P, _P]),
     "bwh_matvec_perm": (C.c_int, [_P, _P, _P]),
     "bwh_matvec_raw_ptr": (C.c_int, [_P, _P, _P]),
@@ -114,7 +115,9 @@ class BigWhamIOGpu:
             self.attach_gpu(self._precisions, self._transpose)
 
     def attach_gpu(self, precisions=("fp64",), transpose: bool = False, release_host: bool = True,
-                   matmat: bool = False) -> HmatGpu:
+                   matmat: bool = False, tuning: dict | None = None) -> HmatGpu:
+        for k, v in (tuning or {}).items():
+            _check(self._L.bwh_set_tuning(self._h, k.encode(), int(v)))
         flags = 0
         for p in precisions:
             flags |= _prec_flag(p)

@@ -555,6 +555,37 @@ int bw_batch_offsets(const bw_hmat *h, int member, int64_t *row0, int64_t *col0)
 
 int bw_batch_count(const bw_hmat *h) { return h ? (int)h->row_off.size() - 1 : 0; }
 
+int bw_set_tuning(bw_hmat *h, const char *key, int64_t value) {
+  if (!h || !key) return BW_ERR_ARG;
+  if (h->finalized) {
+    h->err = "bw_set_tuning after bw_finalize";
+    return BW_ERR_STATE;
+  }
+  const std::string k(key);
+  bw::Tuning &t = h->prob.tune;
+  if (k == "items_per_cta_phase1" || k == "items_per_cta_phase2" || k == "mm_items_per_cta") {
+    if (value < 1 || value > 256) {
+      h->err = k + " must be in [1, 256]";
+      return BW_ERR_ARG;
+    }
+    if (k == "mm_items_per_cta")
+      t.mm_items_per_cta = (int)value;
+    else
+      t.items_per_cta[k.back() - '1'] = (int)value;
+    return BW_OK;
+  }
+  if (k == "chunk_bytes") {
+    if (value < 4096 || value > bw::kStageBytes || value % 16) {
+      h->err = "chunk_bytes must be a multiple of 16 in [4096, " + std::to_string(bw::kStageBytes) + "]";
+      return BW_ERR_ARG;
+    }
+    t.chunk_bytes = (int)value;
+    return BW_OK;
+  }
+  h->err = "unknown tuning key " + k;
+  return BW_ERR_ARG;
+}
+
 int bw_create(int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0, const int64_t *perm1, int device,
               bw_hmat **out) {
   return bw_create_batch(dof, 1, &n_rows, &n_cols, &perm0, &perm1, device, out);

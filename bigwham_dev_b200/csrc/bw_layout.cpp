@@ -115,7 +115,7 @@ void build_operator(const Problem &p, bool tr, int grid, OperatorPlan &op) {
   grid = std::max(1, grid);
   int64_t e1 = 0;  // phase-1 entries
   for (size_t k = 0; k < nlr; k++) e1 += p.lr[k].r * eff_low(p, tr, k).n;
-  const int64_t cap1 = std::max<int64_t>(1, e1 / grid / kItemsPerCta);
+  const int64_t cap1 = std::max<int64_t>(1, e1 / grid / std::max(1, p.tune.items_per_cta[0]));
   PhasePlan &p1 = op.ph[0];
   for (auto &kv : stacks) {
     const int64_t j0 = kv.first.first, n = kv.first.second;
@@ -238,7 +238,7 @@ void build_operator(const Problem &p, bool tr, int grid, OperatorPlan &op) {
     for (const Cover &e : cov[q]) pw[q] += e.kind == 0 ? e.n : eff_low(p, tr, e.k).r;
     e2 += pw[q] * (pb[q + 1] - pb[q]);
   }
-  const int64_t cap2 = std::max<int64_t>(1, e2 / grid / kItemsPerCta);
+  const int64_t cap2 = std::max<int64_t>(1, e2 / grid / std::max(1, p.tune.items_per_cta[1]));
   for (size_t q = 0; q < npan; q++) {
     const int64_t H = pb[q + 1] - pb[q];
     int64_t parts = 1;
@@ -329,15 +329,15 @@ float seg_scale(const OperatorPlan &op, const Segment &s, int prec) {
 
 // Chunks of one item for one precision; phase-2 chunks also get their slice of
 // the gather array (g_len grows) and the runs that fill it.
-void chunk_item(const OperatorPlan &op, const Item &it, int prec, int phase, std::vector<Chunk> &out,
+void chunk_item(const OperatorPlan &op, const Item &it, int prec, int phase, int chunk_bytes, std::vector<Chunk> &out,
                 std::vector<GatherSeg> &gsegs, int64_t &g_len) {
   const int es = esize_of(prec);
   const bool tiled = prec == 2;
   int64_t cap;
   if (tiled)
-    cap = std::min<int64_t>(kMaxCols, (kStageBytes / (8 * int64_t(it.hpad) * es)) * 8);
+    cap = std::max<int64_t>(8, std::min<int64_t>(kMaxCols, (chunk_bytes / (8 * int64_t(it.hpad) * es)) * 8));
   else
-    cap = std::max<int64_t>(1, std::min<int64_t>(kMaxCols, kStageBytes / (int64_t(it.hpad) * es)));
+    cap = std::max<int64_t>(1, std::min<int64_t>(kMaxCols, chunk_bytes / (int64_t(it.hpad) * es)));
   std::vector<int64_t> seg_start(it.segs.size() + 1, 0);
   for (size_t s = 0; s < it.segs.size(); s++) seg_start[s + 1] = seg_start[s] + it.segs[s].ncols;
   int64_t c0 = 0;
@@ -381,7 +381,6 @@ void chunk_item(const OperatorPlan &op, const Item &it, int prec, int phase, std
 }  // namespace
 
 void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &op) {
-  (void)p;
   (void)tr;
   (void)grid;
   const int es = esize_of(prec);
@@ -399,7 +398,7 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
     cp.gsegs.clear();
     cp.g_len = 0;
     for (size_t q = 0; q < ph.items.size(); q++)
-      chunk_item(op, ph.items[q], prec, phase, per_item[q], cp.gsegs, cp.g_len);
+      chunk_item(op, ph.items[q], prec, phase, p.tune.chunk_bytes, per_item[q], cp.gsegs, cp.g_len);
     // Longest first: the CTAs take items from a queue in this order (greedy
     // list scheduling; each CTA takes the next item when its producer is
     // done with the previous one).  Cost is the bytes streamed plus a fixed
@@ -556,7 +555,7 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
     rows8[s] = R8;
     e1 += R8 * wcols[s];
   }
-  const int64_t cap1 = std::max<int64_t>(1, e1 / grid / kItemsPerCta);
+  const int64_t cap1 = std::max<int64_t>(1, e1 / grid / std::max(1, p.tune.mm_items_per_cta));
   MmPhase &p1 = mm.ph[0];
   for (size_t s = 0; s < mm.stacks.size(); s++) {
     const MmStack &st = mm.stacks[s];

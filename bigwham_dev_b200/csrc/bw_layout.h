@@ -139,7 +139,16 @@ struct OperatorPlan {
   int64_t n_stacks = 0;
 };
 
+// Plan parameters a tuner may change (bw_set_tuning); the defaults are the
+// compiled-in choices.
+struct Tuning {
+  int items_per_cta[2] = {kItemsPerCta, kItemsPerCta};  // per phase: items per CTA share (granularity)
+  int chunk_bytes = kStageBytes;                        // block data per chunk (<= kStageBytes)
+  int mm_items_per_cta = kItemsPerCta;                  // matmat phase 1
+};
+
 struct Problem {
+  Tuning tune;
   int dof = 1;
   int64_t n_rows = 0, n_cols = 0;
   std::vector<FullBlock> fr;

@@ -111,11 +111,22 @@ class HmatGpu:
                                              base + 8 * (o + m * r), max(1, r)), self._h)
             o += r * (m + n)
 
+    def set_tuning(self, **kw) -> "HmatGpu":
+        """Plan parameters (bw_set_tuning), before finalize: items_per_cta_phase1,
+        items_per_cta_phase2, chunk_bytes, mm_items_per_cta."""
+        for k, v in kw.items():
+            A.check(self._lib.bw_set_tuning(self._h, k.encode(), int(v)), self._h)
+        return self
+
     def finalize(self, precisions=("fp64",), transpose: bool = False, check_finite: bool = True,
-                 plan_only: bool = False, device_limit: int | None = None, matmat: bool = False) -> "HmatGpu":
+                 plan_only: bool = False, device_limit: int | None = None, matmat: bool = False,
+                 tuning: dict | None = None) -> "HmatGpu":
         """Lay the blocks out on the device.  precisions: storage copies for
         matvec ("fp64", "fp32", "bf16"); transpose: also H^T; matmat: also the
-        BF16 layout of the tensor-core multi-right-hand-side product."""
+        BF16 layout of the tensor-core multi-right-hand-side product; tuning:
+        plan parameters (set_tuning)."""
+        if tuning:
+            self.set_tuning(**tuning)
         flags = 0
         for p in precisions:
             flags |= _prec_flag(p)

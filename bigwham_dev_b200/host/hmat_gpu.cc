@@ -13,7 +13,8 @@ void HmatGpu::check(int status, const char *what) const {
   throw std::runtime_error(std::string("bigwham_b200: ") + what + " failed (" + std::to_string(status) + "): " + buf);
 }
 
-HmatGpu::HmatGpu(const std::shared_ptr<bigwham::Hmat<double>> &cpu, int device, int storage) {
+HmatGpu::HmatGpu(const std::shared_ptr<bigwham::Hmat<double>> &cpu, int device, int storage,
+                 const std::vector<std::pair<std::string, int64_t>> &tuning) {
   if (!cpu || !cpu->isBuilt()) throw std::runtime_error("bigwham_b200: HmatGpu needs a built Hmat");
   // Base-class state read through the public getters (hmat.h:108-121).
   hr_ = cpu->get_hr();
@@ -43,6 +44,7 @@ HmatGpu::HmatGpu(const std::shared_ptr<bigwham::Hmat<double>> &cpu, int device, 
     throw std::runtime_error(std::string("bigwham_b200: bw_create failed: ") + buf);
   }
   try {
+    for (const auto &kv : tuning) check(bw_set_tuning(h_, kv.first.c_str(), kv.second), "bw_set_tuning");
     const bigwham::HPattern &pat = hr_->pattern_;
     // FR blocks (hmat.cc:315-353 builds them; pattern rows 1..4 in points)
     for (il::int_t k = 0; k < pat.n_FRB; k++) {

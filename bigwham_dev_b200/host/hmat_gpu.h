@@ -15,6 +15,9 @@
 #pragma once
 
 #include <memory>
+#include <string>
+#include <utility>
+#include <vector>
 #include <vector>
 
 #include "bigwham_b200.h"
@@ -26,7 +29,9 @@ class HmatGpu : public bigwham::Hmat<double> {
  public:
   // storage: BW_FP64 | BW_FP32 | BW_BF16 (+ BW_STORE_TRANSPOSE).  Throws
   // std::runtime_error when the upload fails.
-  HmatGpu(const std::shared_ptr<bigwham::Hmat<double>> &cpu, int device, int storage);
+  // tuning: plan parameters passed to bw_set_tuning before bw_finalize.
+  HmatGpu(const std::shared_ptr<bigwham::Hmat<double>> &cpu, int device, int storage,
+          const std::vector<std::pair<std::string, int64_t>> &tuning = {});
   ~HmatGpu() override;
   HmatGpu(const HmatGpu &) = delete;
   HmatGpu &operator=(const HmatGpu &) = delete;

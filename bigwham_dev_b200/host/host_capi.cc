@@ -17,6 +17,7 @@
 struct bwh_io {
   std::unique_ptr<BigWhamIO> io;
   std::shared_ptr<bigwham_b200::HmatGpu> gpu;
+  std::vector<std::pair<std::string, int64_t>> tuning;  // for the next bwh_attach_gpu
 };
 
 namespace {
@@ -74,12 +75,18 @@ int bwh_attach_gpu(bwh_io *h, int device, int storage, int release_host) {
   return guarded([&] {
     if (!h->io->is_built()) return fail("bwh_attach_gpu before bwh_build");
     auto cpu = h->io->getHmat();
-    auto gpu = std::make_shared<bigwham_b200::HmatGpu>(cpu, device, storage);
+    auto gpu = std::make_shared<bigwham_b200::HmatGpu>(cpu, device, storage, h->tuning);
     h->io->setHmat(gpu);
     h->gpu = gpu;
     if (release_host) cpu->hmatMemFree();
     return 0;
   });
+}
+
+int bwh_set_tuning(bwh_io *h, const char *key, int64_t value) {
+  if (!h || !key) return fail("null argument");
+  h->tuning.emplace_back(key, value);
+  return 0;
 }
 
 int bwh_set_precision(bwh_io *h, int p) {

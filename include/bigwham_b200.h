@@ -86,6 +86,17 @@ int bw_batch_offsets(const bw_hmat *h, int member, int64_t *row0, int64_t *col0)
 /* Number of members (1 for a bw_create handle, 0 for NULL). */
 int bw_batch_count(const bw_hmat *h);
 
+/* Plan parameters, set before bw_finalize (bigwham_dev_b200/tune.py sweeps
+ * them on a GPU and commits the best per workload):
+ *   "items_per_cta_phase1", "items_per_cta_phase2": items per CTA share
+ *       (granularity of the work queue), 1..256, default 8;
+ *   "chunk_bytes": block data per chunk, 4096..32768, multiple of 16,
+ *       default 32768;
+ *   "mm_items_per_cta": granularity of the matmat's phase 1, default 8.
+ * Results do not depend on them (each item is reduced in a fixed order).
+ * BW_ERR_ARG for an unknown key or a value out of range. */
+int bw_set_tuning(bw_hmat *h, const char *key, int64_t value);
+
 /* Register a full-rank block: rows [i0, i0+m), cols [j0, j0+n), column-major
  * with leading dimension lda >= m.  The pointer is BORROWED until bw_finalize
  * returns (no copy is made before then).

@@ -43,6 +43,10 @@ int bwh_attach_gpu(bwh_io *io, int device, int storage, int release_host);
 /* Precision of the reference-facing matvec calls (one of BW_FP64, BW_FP32, BW_BF16). */
 int bwh_set_precision(bwh_io *io, int precision);
 
+/* Plan parameter for the next bwh_attach_gpu (passed to bw_set_tuning; an
+ * unknown key or a bad value makes bwh_attach_gpu fail). */
+int bwh_set_tuning(bwh_io *io, const char *key, int64_t value);
+
 /* BigWhamIO::MatVec(il::ArrayView) -- host arrays, original ordering. */
 int bwh_matvec(bwh_io *io, const double *x, double *y);
 /* BigWhamIO::MatVecPerm -- host arrays, permuted ordering. */

@@ -170,3 +170,35 @@ def test_tall_panels_and_high_rank_are_split():
     D = np.concatenate([F, Al @ Bl], axis=1)
     assert rel(replay(h, x), D @ x) < 1e-13
     assert rel(replay(h, x, transposed=True), D.T @ x) < 1e-13
+
+
+def test_tuning_changes_the_plan_not_the_result(golden):
+    arr, ex = golden
+    x = np.random.default_rng(3).uniform(-1, 1, arr.n_cols)
+    ref = oracle_matvec_perm(arr, x, 1)
+    sizes = set()
+    for tuning in ({}, {"items_per_cta_phase1": 32, "items_per_cta_phase2": 2, "chunk_bytes": 4096},
+                   {"items_per_cta_phase1": 1, "chunk_bytes": 16384}):
+        h = HmatGpu(arr.dof, arr.n_rows, arr.n_cols, arr.perm0, arr.perm1, device=-1)
+        h.add_flat(arr.fr, arr.lr, arr.fr_data, arr.lr_data)
+        h.finalize(plan_only=True, precisions=("fp64", "bf16"), tuning=tuning)
+        assert rel(replay(h, x, "fp64"), ref) < 1e-14
+        p = h.plan_export("fp64", 2, with_data=False)
+        sizes.add(len(p["chunks"]))
+        if tuning.get("chunk_bytes"):
+            assert max(decode(w)["ncols"] * decode(w)["hpad"] * 8 for w in p["chunks"]) <= max(
+                tuning["chunk_bytes"], 8 * max(decode(w)["hpad"] for w in p["chunks"]))
+    assert len(sizes) > 1
+
+
+def test_tuning_rejects_bad_values():
+    h = _simple()
+    for k, v in (("chunk_bytes", 1000), ("chunk_bytes", 65536), ("items_per_cta_phase1", 0), ("nope", 1)):
+        with pytest.raises(BigWhamError) as e:
+            h.set_tuning(**{k: v})
+        assert e.value.status == A.BW_ERR_ARG
+    h.add_full(0, 0, np.ones((8, 8)))
+    h.finalize(plan_only=True)
+    with pytest.raises(BigWhamError) as e:
+        h.set_tuning(chunk_bytes=8192)
+    assert e.value.status == A.BW_ERR_STATE
