@@ -70,8 +70,10 @@ struct DevPhase {
 struct DevMm {
   uint16_t *data = nullptr;
   bw::MmChunk *chunks = nullptr;
-  int32_t *cta = nullptr;
+  int32_t *items = nullptr;  // chunk ranges of the items, longest first
+  int *queue = nullptr;      // [next item, CTAs done], zero between launches
   int64_t n_chunks = 0;
+  int64_t n_items = 0;
 };
 
 }  // namespace
@@ -157,7 +159,8 @@ struct bw_hmat {
       for (auto &ph : o) {
         cudaFree(ph.data);
         cudaFree(ph.chunks);
-        cudaFree(ph.cta);
+        cudaFree(ph.items);
+        cudaFree(ph.queue);
         ph = DevMm{};
       }
     cudaFree(d_xt);
@@ -362,10 +365,13 @@ void upload_mm_phase(bw_hmat *h, int o, int phase) {
   dm.n_chunks = (int64_t)ph.chunks.size();
   dm.data = static_cast<uint16_t *>(h->dmalloc((size_t)ph.n_elems * 2));
   dm.chunks = static_cast<bw::MmChunk *>(h->dmalloc(std::max<size_t>(1, ph.chunks.size()) * sizeof(bw::MmChunk)));
-  dm.cta = static_cast<int32_t *>(h->dmalloc(ph.cta_ptr.size() * sizeof(int32_t)));
+  dm.n_items = (int64_t)ph.item_ptr.size() - 1;
+  dm.items = static_cast<int32_t *>(h->dmalloc(ph.item_ptr.size() * sizeof(int32_t)));
+  dm.queue = static_cast<int *>(h->dmalloc(2 * sizeof(int)));
+  BW_CUDA(cudaMemset(dm.queue, 0, 2 * sizeof(int)));
   if (!ph.chunks.empty())
     BW_CUDA(cudaMemcpy(dm.chunks, ph.chunks.data(), ph.chunks.size() * sizeof(bw::MmChunk), cudaMemcpyHostToDevice));
-  BW_CUDA(cudaMemcpy(dm.cta, ph.cta_ptr.data(), ph.cta_ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  BW_CUDA(cudaMemcpy(dm.items, ph.item_ptr.data(), ph.item_ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   staged_upload(
       h, dm.data, ph.n_elems, 2, nit, [&](int64_t q) { return q < nit ? ph.items[q].off : ph.n_elems; },
       [&](int64_t q0, int64_t q1, int64_t e0, void *dst) {
@@ -516,7 +522,9 @@ void launch_matmat_tc(bw_hmat *h, int o, const double *X, int64_t ldx, double *Y
       bw::MmArgs a{};
       a.data = dm.data;
       a.chunks = dm.chunks;
-      a.cta_ptr = dm.cta;
+      a.item_ptr = dm.items;
+      a.n_items = (int)dm.n_items;
+      a.queue = dm.queue;
       a.xt = h->d_xt;
       a.t8 = h->d_t8;
       a.y = Y + (int64_t)c0 * ldy;
@@ -963,7 +971,7 @@ int bw_matmat(bw_hmat *h, const double *X, int64_t ldx, double *Y, int64_t ldy, 
 }
 
 int bw_mm_plan_export(const bw_hmat *h, int phase, int transposed, int64_t *n_chunks, int32_t *chunks,
-                      int64_t *n_elems, uint16_t *data, int64_t *n_cta, int32_t *cta_ptr, int64_t *t8_len) {
+                      int64_t *n_elems, uint16_t *data, int64_t *n_item_ptr, int32_t *item_ptr, int64_t *t8_len) {
   if (!h || phase < 1 || phase > 2) return BW_ERR_ARG;
   if (!h->finalized || !h->has_mm) return BW_ERR_STATE;
   const int o = transposed ? 1 : 0;
@@ -971,10 +979,10 @@ int bw_mm_plan_export(const bw_hmat *h, int phase, int transposed, int64_t *n_ch
   const bw::MmPhase &ph = h->mm[o].ph[phase - 1];
   if (n_chunks) *n_chunks = (int64_t)ph.chunks.size();
   if (n_elems) *n_elems = ph.n_elems;
-  if (n_cta) *n_cta = (int64_t)ph.cta_ptr.size();
+  if (n_item_ptr) *n_item_ptr = (int64_t)ph.item_ptr.size();
   if (t8_len) *t8_len = h->mm[o].t8_len;
   if (chunks) std::memcpy(chunks, ph.chunks.data(), ph.chunks.size() * sizeof(bw::MmChunk));
-  if (cta_ptr) std::memcpy(cta_ptr, ph.cta_ptr.data(), ph.cta_ptr.size() * sizeof(int32_t));
+  if (item_ptr) std::memcpy(item_ptr, ph.item_ptr.data(), ph.item_ptr.size() * sizeof(int32_t));
   if (data) {
     if (!h->plan_only) return BW_ERR_STATE;
     std::memcpy(data, h->mm_host[o][phase - 1].data(), (size_t)ph.n_elems * 2);

@@ -617,7 +617,7 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
       p2.items.push_back(std::move(it));
     }
   }
-  // data offsets, chunks, LPT schedule (cost: block bytes + operand bytes + a per-chunk overhead)
+  // data offsets, chunks, items longest first (cost: block bytes + operand bytes + a per-chunk overhead)
   for (int phase = 0; phase < 2; phase++) {
     MmPhase &ph = mm.ph[phase];
     int64_t off = 0;
@@ -635,25 +635,13 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
     std::vector<int64_t> order(ph.items.size());
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
-    using Slot = std::pair<int64_t, int>;
-    std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
-    for (int c = 0; c < grid; c++) heap.push({0, c});
-    std::vector<std::vector<int64_t>> bins(grid);
-    for (int64_t q : order) {
-      Slot s = heap.top();
-      heap.pop();
-      bins[s.second].push_back(q);
-      s.first += cost[q];
-      heap.push(s);
-    }
     ph.chunks.clear();
-    ph.cta_ptr.assign(grid + 1, 0);
-    for (int c = 0; c < grid; c++) {
-      ph.cta_ptr[c] = static_cast<int32_t>(ph.chunks.size());
-      for (int64_t q : bins[c]) ph.chunks.insert(ph.chunks.end(), per_item[q].begin(), per_item[q].end());
+    ph.item_ptr.assign(1, 0);
+    for (int64_t q : order) {
+      ph.chunks.insert(ph.chunks.end(), per_item[q].begin(), per_item[q].end());
+      if (ph.chunks.size() > (size_t)INT32_MAX) fail("too many matmat chunks");
+      ph.item_ptr.push_back(static_cast<int32_t>(ph.chunks.size()));
     }
-    ph.cta_ptr[grid] = static_cast<int32_t>(ph.chunks.size());
-    if (ph.chunks.size() > (size_t)INT32_MAX) fail("too many matmat chunks");
   }
 }
 

@@ -275,8 +275,8 @@ struct MmItem {
 struct MmPhase {
   std::vector<MmItem> items;
   int64_t n_elems = 0;
-  std::vector<MmChunk> chunks;   // ordered by CTA
-  std::vector<int32_t> cta_ptr;  // grid + 1
+  std::vector<MmChunk> chunks;    // item by item
+  std::vector<int32_t> item_ptr;  // chunk ranges of the items, longest first (items + 1)
 };
 
 struct MmPlan {

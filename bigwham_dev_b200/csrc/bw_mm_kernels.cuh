@@ -1,14 +1,18 @@
 // Device code of the H-matmat Y = H X (up to 64 right-hand sides per pass) on
 // the 5th-generation tensor cores (tcgen05, sm_100a).
 //
-// One persistent kernel per phase, one CTA per SM, with four roles:
-//  * warps 0 and 1, producers (even and odd chunks, so that the issue of
-//    their copies overlaps): for every chunk, two or more bulk copies
-//    (cp.async.bulk) into a ring of kMmStages shared-memory stages, counted in
-//    bytes on the stage's `full` mbarrier:
+// One persistent kernel per phase, one CTA per SM.  The CTAs take items
+// (longest first) from a queue in device memory, one atomicAdd per item; an
+// item's result does not depend on the CTA that computes it.  Four roles:
+//  * warp 0, producer: takes items from the queue and, for every chunk,
+//    issues two or more bulk copies (cp.async.bulk) into a ring of kMmStages
+//    shared-memory stages, counted in bytes on the stage's `full` mbarrier:
 //      - the chunk's block data (8x8 BF16 tiles);
 //      - its runs of operand rows (8x8 BF16 tiles of X or T8, 64 columns).
-//  * warps 2 and 3, MMA issuers: warp 2 allocates 512 TMEM columns (two
+//    It announces each item (rows, output offset) to the epilogue in a small
+//    ring in shared memory, and ends with a kEnd descriptor and an end entry
+//    in that ring.
+//  * warps 1 and 2, MMA issuers: warp 1 allocates 512 TMEM columns (two
 //    accumulator buffers x two issuers x two m-tiles x 64 columns).  One
 //    thread per issuer issues tcgen05.mma.cta_group::1.kind::f16, M = 128,
 //    N = 64, K = 16.
@@ -20,7 +24,7 @@
 //      - Each issuer releases a chunk's stage with tcgen05.commit on its
 //        `empty` barrier (two arrivals), and at an item's last chunk signals
 //        `accfull` (two arrivals).
-//  * warps 4-7, epilogue: each reads its 32-lane quarter of both issuers'
+//  * warps 3-6, epilogue: each reads its 32-lane quarter of both issuers'
 //    finished accumulators with tcgen05.ld and adds them.  It then writes T8
 //    (BF16 tiles, phase 1) or y (FP64, caller's ordering through the row
 //    permutation, phase 2), and hands the buffer back on `accempty`.
@@ -43,10 +47,12 @@ namespace bw {
 constexpr int kMmStages = 4;
 constexpr int kMmSlack = 2048;      // an M = 128 read of a chunk of fewer rows reaches up to 2 KB past it
 constexpr int kMmStageSize = kMmStageBytes + kMmSlack;
-constexpr int kMmThreads = 256;     // 2 producers, 2 MMA issuers, 4 epilogue warps
+constexpr int kMmThreads = 224;     // producer, 2 MMA issuers, 4 epilogue warps
 constexpr int kMmTmemCols = 512;    // 2 buffers x 2 issuers x 2 m-tiles x 64 columns
+constexpr int kMmRing = 16;         // item announcements in flight (the producer runs at most ~6 items ahead)
 constexpr int kMmBarBytes = (2 * kMmStages + 4 + 2) * 8 + 16;
-constexpr int kMmSmem = kMmStages * kMmStageSize + kMmStages * (int)sizeof(MmChunk) + kMmBarBytes;
+constexpr int kMmSmem =
+    kMmStages * kMmStageSize + kMmStages * (int)sizeof(MmChunk) + kMmRing * 16 + kMmBarBytes;
 static_assert(kMmSmem <= 232448, "shared memory above the 227 KB per-CTA limit");
 static_assert(kMmHMax <= 2 * 128, "an item's rows must fit 2 m-tiles of 128");
 
@@ -55,8 +61,10 @@ constexpr int kErrMmBadChunk = 0x202;
 
 struct MmArgs {
   const uint16_t *data;       // BF16 tiles of the phase
-  const MmChunk *chunks;      // ordered by CTA
-  const int32_t *cta_ptr;     // grid + 1
+  const MmChunk *chunks;      // item by item
+  const int32_t *item_ptr;    // chunk ranges of the items, longest first (n_items + 1)
+  int n_items;
+  int *queue;                 // [next item, CTAs done]: zero at launch, reset to zero by the last CTA
   const uint16_t *xt;         // operand 0: X in 8x8 tiles, kMmRhs columns
   uint16_t *t8;               // operand 1 (phase 2) / output (phase 1): T8 in 8x8 tiles
   double *y;                  // phase-2 output, column-major, leading dimension ldy
@@ -127,11 +135,21 @@ __device__ __forceinline__ bool mm_wait(uint64_t *bar, uint32_t parity, long lon
   return true;
 }
 
+// Item announcement, producer -> epilogue: written field by field, seq last.
+struct MmItemInfo {
+  int rows;      // rows to write; -1: no more items
+  int out_off;
+  int hpad;
+  int seq;       // 1 + the item's place in this CTA's sequence
+};
+
 __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
   extern __shared__ __align__(128) unsigned char mm_smem[];
   unsigned char *smem = mm_smem;
   MmChunk *sdesc = reinterpret_cast<MmChunk *>(smem + kMmStages * kMmStageSize);
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + kMmStages * kMmStageSize + kMmStages * sizeof(MmChunk));
+  volatile MmItemInfo *ring = reinterpret_cast<volatile MmItemInfo *>(sdesc + kMmStages);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + kMmStages * kMmStageSize + kMmStages * sizeof(MmChunk) +
+                                                kMmRing * sizeof(MmItemInfo));
   uint64_t *empty = full + kMmStages;
   uint64_t *accfull = empty + kMmStages;   // [2]
   uint64_t *accempty = accfull + 2;        // [2]
@@ -151,12 +169,11 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
     }
     mbar_init(&drained[0], 1);
     mbar_init(&drained[1], 1);
+    for (int r = 0; r < kMmRing; r++) ring[r].seq = 0;
     *abort = 0;
     fence_barrier_init();
   }
-  const int cb = a.cta_ptr[blockIdx.x], ce = a.cta_ptr[blockIdx.x + 1];
-  if (cb >= ce) return;  // uniform across the CTA: nothing allocated yet
-  if (warp == 2) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kMmTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -166,112 +183,162 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp < 2) {
-    // ------------------------------------------------------------------ producers
-    // producer `warp` stages the chunks i (CTA-relative) with i % 2 == warp;
-    // its lane k holds the descriptor of the k-th such chunk of a batch of 32
+  if (warp == 0) {
+    // ------------------------------------------------------------------ producer
     const unsigned char *gdata = reinterpret_cast<const unsigned char *>(a.data);
     const unsigned char *gx = reinterpret_cast<const unsigned char *>(a.xt);
     const unsigned char *gt = reinterpret_cast<const unsigned char *>(a.t8);
-    int issued = 0;
+    int issued = 0;  // chunks staged by this CTA (stage = issued % kMmStages)
+    int nitems = 0;  // items announced
     bool ok = true;
-    const int nch = ce - cb;
-    for (int i0 = warp; i0 < nch && ok; i0 += 64) {
-      uint32_t dw[kMmChunkWords];
-      const int mine = i0 + 2 * lane;
-      if (mine < nch) {
-        const uint4 *p = reinterpret_cast<const uint4 *>(a.chunks + cb + mine);
+    int cur = 0;
+    if (lane == 0) cur = atomicAdd(&a.queue[0], 1);
+    cur = __shfl_sync(0xffffffffu, cur, 0);
+    while (cur < a.n_items && ok) {
+      int nxt = 0;
+      if (lane == 0) nxt = atomicAdd(&a.queue[0], 1);  // the next item, fetched one item ahead
+      const int cb = a.item_ptr[cur], ce = a.item_ptr[cur + 1];
+      for (int bb = cb; bb < ce && ok; bb += 32) {
+        // lane k holds the descriptor of chunk bb + k
+        uint32_t dw[kMmChunkWords];
+        if (bb + lane < ce) {
+          const uint4 *p = reinterpret_cast<const uint4 *>(a.chunks + bb + lane);
 #pragma unroll
-        for (int q = 0; q < kMmChunkWords / 4; q++) {
-          const uint4 v = __ldg(p + q);
-          dw[4 * q] = v.x;
-          dw[4 * q + 1] = v.y;
-          dw[4 * q + 2] = v.z;
-          dw[4 * q + 3] = v.w;
+          for (int q = 0; q < kMmChunkWords / 4; q++) {
+            const uint4 v = __ldg(p + q);
+            dw[4 * q] = v.x;
+            dw[4 * q + 1] = v.y;
+            dw[4 * q + 2] = v.z;
+            dw[4 * q + 3] = v.w;
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < kMmChunkWords; q++) dw[q] = 0;
+        }
+        if (bb == cb && lane == 0) {
+          // announce the item to the epilogue
+          volatile MmItemInfo &e = ring[nitems % kMmRing];
+          e.rows = static_cast<int>(dw[4]);
+          e.out_off = static_cast<int>(dw[5]);
+          e.hpad = static_cast<int>(dw[3]);
+          __threadfence_block();
+          e.seq = nitems + 1;
+        }
+        if (bb == cb) nitems++;
+        const int nb = min(32, ce - bb);
+        for (int k = 0; k < nb; k++) {
+          const int s = issued % kMmStages;
+          const uint32_t use = static_cast<uint32_t>(issued / kMmStages);
+          // lane k holds chunk k's descriptor and issues it; the others wait
+          bool waited = true;
+          if (lane == k) {
+            waited = mm_wait(&empty[s], (use & 1u) ^ 1u, a.spin_limit, abort);
+            if (!waited) {
+              set_error(a.err, kErrMmTimeout);
+              *abort = 1;
+            }
+          }
+          if (!__shfl_sync(0xffffffffu, waited ? 1 : 0, k)) {
+            ok = false;
+            break;
+          }
+          const uint32_t(&w)[kMmChunkWords] = dw;
+          if (lane == k) {
+            MmChunk *sd = sdesc + s;
+            uint4 *sdw = reinterpret_cast<uint4 *>(sd);
+#pragma unroll
+            for (int q = 0; q < kMmChunkWords / 4; q++)
+              sdw[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+            const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
+            const int kc = static_cast<int>(w[2]), hpad = static_cast<int>(w[3]);
+            const int nr = static_cast<int>((w[6] >> 8) & 0xffu);
+            uint32_t run_rows = 0;
+#pragma unroll
+            for (int r = 0; r < kMmMaxRuns; r++)
+              if (r < nr) run_rows += w[8 + 2 * r + 1];
+            const uint32_t dbytes = static_cast<uint32_t>(kc) * static_cast<uint32_t>(hpad) * 2u;
+            const uint32_t bbytes = static_cast<uint32_t>(kc) * (2u * kMmRhs);
+            const bool good = kc > 0 && kc <= kMmMaxCols && (kc & 15) == 0 && hpad > 0 && hpad <= kMmHMax &&
+                              (hpad & 7) == 0 && nr > 0 && nr <= kMmMaxRuns &&
+                              run_rows == static_cast<uint32_t>(kc) &&
+                              dbytes + bbytes <= static_cast<uint32_t>(kMmStageBytes);
+            unsigned char *st = smem + s * kMmStageSize;
+            if (good) {
+              mbar_arrive_expect_tx(&full[s], dbytes + bbytes);
+              // operand rows first (stage offset 0), block data after them
+              uint32_t dst = 0;
+#pragma unroll
+              for (int r = 0; r < kMmMaxRuns; r++) {
+                if (r < nr) {
+                  const uint32_t src = w[8 + 2 * r], rows = w[8 + 2 * r + 1];
+                  const unsigned char *base = (src >> 31) ? gt : gx;
+                  bulk_g2s(st + dst, base + static_cast<unsigned long long>(src & 0x7fffffffu) * (2u * kMmRhs),
+                           rows * (2u * kMmRhs), &full[s]);
+                  dst += rows * (2u * kMmRhs);
+                }
+              }
+              bulk_g2s(st + bbytes, gdata + static_cast<unsigned long long>(data_off) * 2ull, dbytes, &full[s]);
+            } else {
+              set_error(a.err, kErrMmBadChunk);
+              sd->kc = 0;  // the MMA issuers skip the chunk
+              sd->flags &= ~kEnd;
+              mbar_arrive(&full[s]);
+            }
+          }
+          __syncwarp();
+          issued++;
+        }
+      }
+      cur = __shfl_sync(0xffffffffu, nxt, 0);
+    }
+    if (ok) {
+      // end of work: the issuers get a kEnd descriptor, the epilogue an end entry
+      const int s = issued % kMmStages;
+      const uint32_t use = static_cast<uint32_t>(issued / kMmStages);
+      if (mm_wait(&empty[s], (use & 1u) ^ 1u, a.spin_limit, abort)) {
+        if (lane == 0) {
+          sdesc[s].kc = 0;
+          sdesc[s].flags = kEnd;
+          mbar_arrive(&full[s]);
+          volatile MmItemInfo &e = ring[nitems % kMmRing];
+          e.rows = -1;
+          __threadfence_block();
+          e.seq = nitems + 1;
         }
       } else {
-#pragma unroll
-        for (int q = 0; q < kMmChunkWords; q++) dw[q] = 0;
-      }
-      const int nb = min(32, (nch - i0 + 1) / 2);
-      for (int k = 0; k < nb; k++) {
-        const int i = i0 + 2 * k;
-        const int s = i % kMmStages;
-        const uint32_t use = static_cast<uint32_t>(i / kMmStages);
-        // lane k holds chunk i's descriptor and issues it; the others wait
-        bool waited = true;
-        if (lane == k) {
-          waited = mm_wait(&empty[s], (use & 1u) ^ 1u, a.spin_limit, abort);
-          if (!waited) {
-            set_error(a.err, kErrMmTimeout);
-            *abort = 1;
-          }
+        if (lane == 0) {
+          set_error(a.err, kErrMmTimeout);
+          *abort = 1;
         }
-        if (!__shfl_sync(0xffffffffu, waited ? 1 : 0, k)) {
-          ok = false;
-          break;
-        }
-        const uint32_t(&w)[kMmChunkWords] = dw;
-        if (lane == k) {
-          MmChunk *sd = sdesc + s;
-          uint4 *sdw = reinterpret_cast<uint4 *>(sd);
-#pragma unroll
-          for (int q = 0; q < kMmChunkWords / 4; q++) sdw[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-          const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
-          const int kc = static_cast<int>(w[2]), hpad = static_cast<int>(w[3]);
-          const int nr = static_cast<int>((w[6] >> 8) & 0xffu);
-          uint32_t run_rows = 0;
-#pragma unroll
-          for (int r = 0; r < kMmMaxRuns; r++)
-            if (r < nr) run_rows += w[8 + 2 * r + 1];
-          const uint32_t dbytes = static_cast<uint32_t>(kc) * static_cast<uint32_t>(hpad) * 2u;
-          const uint32_t bbytes = static_cast<uint32_t>(kc) * (2u * kMmRhs);
-          const bool good = kc > 0 && kc <= kMmMaxCols && (kc & 15) == 0 && hpad > 0 && hpad <= kMmHMax &&
-                            (hpad & 7) == 0 && nr > 0 && nr <= kMmMaxRuns && run_rows == static_cast<uint32_t>(kc) &&
-                            dbytes + bbytes <= static_cast<uint32_t>(kMmStageBytes);
-          unsigned char *st = smem + s * kMmStageSize;
-          if (good) {
-            mbar_arrive_expect_tx(&full[s], dbytes + bbytes);
-            // operand rows first (stage offset 0), block data after them
-            uint32_t dst = 0;
-#pragma unroll
-            for (int r = 0; r < kMmMaxRuns; r++) {
-              if (r < nr) {
-                const uint32_t src = w[8 + 2 * r], rows = w[8 + 2 * r + 1];
-                const unsigned char *base = (src >> 31) ? gt : gx;
-                bulk_g2s(st + dst, base + static_cast<unsigned long long>(src & 0x7fffffffu) * (2u * kMmRhs),
-                         rows * (2u * kMmRhs), &full[s]);
-                dst += rows * (2u * kMmRhs);
-              }
-            }
-            bulk_g2s(st + bbytes, gdata + static_cast<unsigned long long>(data_off) * 2ull, dbytes, &full[s]);
-          } else {
-            set_error(a.err, kErrMmBadChunk);
-            sd->kc = 0;  // the MMA issuers skip the chunk
-            mbar_arrive(&full[s]);
-          }
-        }
-        __syncwarp();
-        issued++;
+        ok = false;
       }
     }
     if (!ok) {
-      // let this producer's copies in flight land before the CTA can exit
-      for (int j = max(0, issued - kMmStages / 2); j < issued; j++) {
-        const int i = warp + 2 * j;
+      // let the copies in flight land before the CTA can exit
+      for (int i = max(0, issued - kMmStages); i < issued; i++) {
         const int s = i % kMmStages;
         mbar_wait(&full[s], static_cast<uint32_t>(i / kMmStages) & 1u, a.spin_limit);
       }
     }
-  } else if (warp < 4) {
+    // This CTA takes no more items.  The last CTA to get here returns the
+    // queue to zero for the next launch (every other CTA is done with it).
+    if (lane == 0) {
+      __threadfence();
+      if (atomicAdd(&a.queue[1], 1) == static_cast<int>(gridDim.x) - 1) {
+        a.queue[0] = 0;
+        a.queue[1] = 0;
+        __threadfence();
+      }
+    }
+  } else if (warp < 3) {
     // ------------------------------------------------------------------ MMA issuers
-    const uint32_t q = static_cast<uint32_t>(warp - 2);  // takes the item's K-steps of parity q
+    const uint32_t q = static_cast<uint32_t>(warp - 1);  // takes the item's K-steps of parity q
     const uint32_t idesc = umma_idesc_bf16(128, kMmRhs);
     uint32_t items = 0;
-    int kg = 0;          // K-steps of the current item before this chunk
+    int kg = 0;            // K-steps of the current item before this chunk
     bool started = false;  // this issuer's accumulator of the current item holds a product
     bool ok = true;
-    for (int i = 0; i < ce - cb && ok; i++) {
+    for (int i = 0;; i++) {
       const int s = i % kMmStages;
       const uint32_t use = static_cast<uint32_t>(i / kMmStages);
       if (!mm_wait(&full[s], use & 1u, a.spin_limit, abort)) {
@@ -281,6 +348,7 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
       const MmChunk &d = sdesc[s];
       const int kc = d.kc, hpad = d.hpad;
       const uint32_t flags = d.flags;
+      if (flags & kEnd) break;
       const uint32_t buf = items & 1u;
       if (flags & kFirst) {
         if (!mm_wait(&accempty[buf], ((items >> 1) & 1u) ^ 1u, a.spin_limit, abort)) {
@@ -340,84 +408,83 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
   } else {
     // ------------------------------------------------------------------ epilogue
     const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
-    uint32_t items = 0;
-    for (int bb = cb; bb < ce; bb += 32) {
-      const int idx = bb + lane;
-      uint32_t f = 0;
-      int rows = 0, out_off = 0, hpad = 0;
-      if (idx < ce) {
-        f = __ldg(&a.chunks[idx].flags);
-        rows = __ldg(&a.chunks[idx].rows);
-        out_off = __ldg(&a.chunks[idx].out_off);
-        hpad = __ldg(&a.chunks[idx].hpad);
-      }
-      unsigned lastmask = __ballot_sync(0xffffffffu, (f & kLast) != 0);
-      bool ok = true;
-      while (lastmask) {
-        const int k = __ffs(lastmask) - 1;
-        lastmask &= lastmask - 1;
-        const int irows = __shfl_sync(0xffffffffu, rows, k);
-        const int ioff = __shfl_sync(0xffffffffu, out_off, k);
-        const int ihpad = __shfl_sync(0xffffffffu, hpad, k);
-        const uint32_t buf = items & 1u;
-        if (!mm_wait(&accfull[buf], (items >> 1) & 1u, a.spin_limit, abort)) {
-          if (lane == 0) {
-            set_error(a.err, kErrMmTimeout);
-            *abort = 1;
-          }
-          ok = false;
-          break;
+    for (uint32_t items = 0;; items++) {
+      // the item's announcement (bounded wait on the ring entry)
+      volatile MmItemInfo &e = ring[items % kMmRing];
+      bool seen = e.seq == static_cast<int>(items + 1);
+      if (!seen) {
+        const unsigned long long t0 = global_ns();
+        unsigned n = 0;
+        while (!(seen = e.seq == static_cast<int>(items + 1))) {
+          if ((++n & 63u) == 0 && (*abort || global_ns() - t0 > static_cast<unsigned long long>(a.spin_limit)))
+            break;
         }
-        tc_fence_after();
-        const int nM = (ihpad + 127) >> 7;
-        for (int mt = 0; mt < nM; mt++) {
-          const int row = mt * 128 + quarter * 32 + lane;
-          const bool live = row < irows;
-          long long dst = 0;
-          if (live && a.phase == 2) {
-            const int orow = ioff + row;
-            dst = a.perm_out ? static_cast<long long>(a.dof) * a.perm_out[orow / a.dof] + (orow % a.dof) : orow;
-          }
+      }
+      if (!seen) {
+        if (lane == 0) {
+          set_error(a.err, kErrMmTimeout);
+          *abort = 1;
+        }
+        break;
+      }
+      __threadfence_block();
+      const int irows = e.rows, ioff = e.out_off, ihpad = e.hpad;
+      if (irows < 0) break;  // no more items
+      const uint32_t buf = items & 1u;
+      if (!mm_wait(&accfull[buf], (items >> 1) & 1u, a.spin_limit, abort)) {
+        if (lane == 0) {
+          set_error(a.err, kErrMmTimeout);
+          *abort = 1;
+        }
+        break;
+      }
+      tc_fence_after();
+      const int nM = (ihpad + 127) >> 7;
+      for (int mt = 0; mt < nM; mt++) {
+        const int row = mt * 128 + quarter * 32 + lane;
+        const bool live = row < irows;
+        long long dst = 0;
+        if (live && a.phase == 2) {
+          const int orow = ioff + row;
+          dst = a.perm_out ? static_cast<long long>(a.dof) * a.perm_out[orow / a.dof] + (orow % a.dof) : orow;
+        }
 #pragma unroll 1
-          for (int c0 = 0; c0 < kMmRhs; c0 += 16) {
-            float v[16], v2[16];
-            const uint32_t ta = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + buf * 256u +
-                                static_cast<uint32_t>(mt) * kMmRhs + static_cast<uint32_t>(c0);
-            tmem_ld16(ta, v);
-            tmem_ld16(ta + 128u, v2);  // the second issuer's accumulator
-            if (!live) continue;
+        for (int c0 = 0; c0 < kMmRhs; c0 += 16) {
+          float v[16], v2[16];
+          const uint32_t ta = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + buf * 256u +
+                              static_cast<uint32_t>(mt) * kMmRhs + static_cast<uint32_t>(c0);
+          tmem_ld16(ta, v);
+          tmem_ld16(ta + 128u, v2);  // the second issuer's accumulator
+          if (!live) continue;
 #pragma unroll
-            for (int k2 = 0; k2 < 16; k2++) v[k2] += v2[k2];
-            if (a.phase == 1) {
-              const long long r8 = static_cast<long long>(ioff) + row;
+          for (int k2 = 0; k2 < 16; k2++) v[k2] += v2[k2];
+          if (a.phase == 1) {
+            const long long r8 = static_cast<long long>(ioff) + row;
 #pragma unroll
-              for (int g = 0; g < 2; g++) {
-                uint4 pk;
-                pk.x = pack_bf16x2(v[8 * g + 0], v[8 * g + 1]);
-                pk.y = pack_bf16x2(v[8 * g + 2], v[8 * g + 3]);
-                pk.z = pack_bf16x2(v[8 * g + 4], v[8 * g + 5]);
-                pk.w = pack_bf16x2(v[8 * g + 6], v[8 * g + 7]);
-                const long long e = (r8 >> 3) * (8 * kMmRhs) + ((c0 >> 3) + g) * 64 + (r8 & 7) * 8;
-                *reinterpret_cast<uint4 *>(a.t8 + e) = pk;
-              }
-            } else {
-#pragma unroll
-              for (int q = 0; q < 16; q++)
-                if (c0 + q < a.nrhs) a.y[static_cast<long long>(c0 + q) * a.ldy + dst] = static_cast<double>(v[q]);
+            for (int g = 0; g < 2; g++) {
+              uint4 pk;
+              pk.x = pack_bf16x2(v[8 * g + 0], v[8 * g + 1]);
+              pk.y = pack_bf16x2(v[8 * g + 2], v[8 * g + 3]);
+              pk.z = pack_bf16x2(v[8 * g + 4], v[8 * g + 5]);
+              pk.w = pack_bf16x2(v[8 * g + 6], v[8 * g + 7]);
+              const long long e8 = (r8 >> 3) * (8 * kMmRhs) + ((c0 >> 3) + g) * 64 + (r8 & 7) * 8;
+              *reinterpret_cast<uint4 *>(a.t8 + e8) = pk;
             }
+          } else {
+#pragma unroll
+            for (int k2 = 0; k2 < 16; k2++)
+              if (c0 + k2 < a.nrhs) a.y[static_cast<long long>(c0 + k2) * a.ldy + dst] = static_cast<double>(v[k2]);
           }
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&accempty[buf]);
-        items++;
       }
-      if (!ok) break;
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accempty[buf]);
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 2) {
+  if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMmTmemCols));
   }

@@ -298,7 +298,7 @@ class HmatGpu:
         A.check(self._lib.bw_mm_plan_export(self._h, phase, int(transposed), None, chunks.ctypes.data, None,
                                             data.ctypes.data if data is not None else None, None, cta.ctypes.data,
                                             None), self._h)
-        return {"chunks": chunks, "cta_ptr": cta, "data": data, "t8_len": t8.value}
+        return {"chunks": chunks, "item_ptr": cta, "data": data, "t8_len": t8.value}
 
     def sync(self, stream=0) -> None:
         sp = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)

@@ -204,11 +204,12 @@ int bw_set_device_limit(bw_hmat *h, int64_t bytes);
  *  - chunks: n_chunks x 16 int32 words in the layout of bw::MmChunk
  *    (bigwham_dev_b200/csrc/bw_layout.h);
  *  - data: n_elems raw BF16 words in 8x8 tiles (BW_PLAN_ONLY handles only);
- *  - cta_ptr: grid+1 offsets;
+ *  - item_ptr: the chunk ranges of the items (n_item_ptr = items + 1), in the
+ *    order the kernel's CTAs take them (longest first);
  *  - t8_len: rows of the low-rank product array T8.
  * Any output pointer may be NULL. */
 int bw_mm_plan_export(const bw_hmat *h, int phase, int transposed, int64_t *n_chunks, int32_t *chunks,
-                      int64_t *n_elems, uint16_t *data, int64_t *n_cta, int32_t *cta_ptr, int64_t *t8_len);
+                      int64_t *n_elems, uint16_t *data, int64_t *n_item_ptr, int32_t *item_ptr, int64_t *t8_len);
 
 /* Host view of the built plan for one precision and phase (1: low-rank B
  * stage, 2: row panels), for inspection and testing.  Any output pointer may be
