@@ -103,7 +103,7 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -112,7 +112,7 @@ def dist_setup(n_gpus):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=None)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=900), device_id=None)
     return world, rank, local
 
 
@@ -123,15 +123,53 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(v, world):
+def max_over_ranks(v, world, device="cuda"):
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+BLOCK_KEYS = ("fr", "lr", "fr_data", "lr_data", "perm0", "perm1")
+
+
+def shared_blocks(world, rank, tag, build):
+    """Replicas share one H-matrix build: rank 0 runs build(alloc) -> the
+    export dict (BigWhamIOGpu.export_blocks) with its arrays placed by `alloc`
+    in /dev/shm, then every rank maps them.  Returns (meta, arrays, release);
+    release() (all ranks, after their upload) removes the files."""
+    d = os.path.join("/dev/shm", f"bw_blocks_{tag}")
+    if rank == 0:
+        os.makedirs(d, exist_ok=True)
+        names = iter(BLOCK_KEYS)
+
+        def alloc(shape, dtype):
+            return np.lib.format.open_memmap(os.path.join(d, next(names) + ".bin"), mode="w+", dtype=dtype,
+                                             shape=shape)
+
+        ex = build(alloc)
+        for k in BLOCK_KEYS:
+            ex[k].flush()
+        with open(os.path.join(d, "meta.json"), "w") as f:
+            json.dump({"dof": ex["dof"], "n_rows": ex["n_rows"], "n_cols": ex["n_cols"]}, f)
+    barrier(world)
+    with open(os.path.join(d, "meta.json")) as f:
+        meta = json.load(f)
+    arr = {k: np.load(os.path.join(d, k + ".bin"), mmap_mode="r") for k in BLOCK_KEYS}
+
+    def release():
+        barrier(world)
+        if rank == 0:
+            for k in BLOCK_KEYS:
+                os.unlink(os.path.join(d, k + ".bin"))
+            os.unlink(os.path.join(d, "meta.json"))
+            os.rmdir(d)
+
+    return meta, arr, release
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -206,44 +244,23 @@ def build_hmatrix(a, world, rank, local):
         return io, h, info
     # replicas: one build, shared through /dev/shm
     tag = os.environ.get("TORCHELASTIC_RUN_ID", "bench") + f"_{a.mesh}"
-    d = os.path.join("/dev/shm", f"bw_blocks_{tag}")
-    keys = ("fr", "lr", "fr_data", "lr_data", "perm0", "perm1")
-    if rank == 0:
+
+    def build(alloc):
         t0 = time.time()
         io = BigWhamIOGpu(coor, conn, "3DR0-H", PROPS, os.cpu_count() or 1, useCuda=False, device=local)
         io.build_hierarchical_matrix(LEAF, ETA, EPS)
-        os.makedirs(d, exist_ok=True)
-        alloc_paths = {}
-
-        def alloc(shape, dtype, _n=[0]):
-            name = keys[_n[0]]
-            _n[0] += 1
-            path = os.path.join(d, name + ".bin")
-            alloc_paths[name] = (path, shape, np.dtype(dtype).str)
-            return np.lib.format.open_memmap(path, mode="w+", dtype=dtype, shape=shape)
-
         ex = io.export_blocks(alloc)
-        for k in keys:
-            ex[k].flush()
-        with open(os.path.join(d, "meta.json"), "w") as f:
-            json.dump({"dof": ex["dof"], "n_rows": ex["n_rows"], "n_cols": ex["n_cols"]}, f)
         info["host_build_s"] = round(time.time() - t0, 2)
         io.close()
-    barrier(world)
-    with open(os.path.join(d, "meta.json")) as f:
-        meta = json.load(f)
-    arr = {k: np.load(os.path.join(d, k + ".bin"), mmap_mode="r") for k in keys}
+        return ex
+
+    meta, arr, release = shared_blocks(world, rank, tag, build)
     t0 = time.time()
     h = HmatGpu.from_flat(meta["dof"], meta["n_rows"], meta["n_cols"], arr["fr"], arr["lr"], arr["fr_data"],
                           arr["lr_data"], arr["perm0"], arr["perm1"], device=local, precisions=precs, matmat=a.matmat,
                           tuning=tuning)
     info["upload_s"] = round(time.time() - t0, 2)
-    barrier(world)
-    if rank == 0:
-        for k in keys:
-            os.unlink(os.path.join(d, k + ".bin"))
-        os.unlink(os.path.join(d, "meta.json"))
-        os.rmdir(d)
+    release()
     return None, h, info
 
 
