@@ -298,8 +298,8 @@ def time_matmat(a, h, dev, peak, ms_bf16_matvec):
     for phase in (1, 2):
         c = h.mm_plan_export(phase)["chunks"].astype(np.int64)
         block += int((c[:, 2] * c[:, 3] * 2).sum())
-    return {"workload": "3DR0-H 256x256, 64 right-hand sides ~U(-1,1) seed 5, BF16 blocks and X, FP32 accumulate "
-                        "(tcgen05, TMEM accumulators)",
+    return {"workload": f"3DR0-H {a.mesh}x{a.mesh}, 64 right-hand sides ~U(-1,1) seed 5, BF16 blocks and X, "
+                        "FP32 accumulate (tcgen05, TMEM accumulators)",
             "steps": steps, "ms_per_matmat": ms, "rhs_per_s": k / (ms * 1e-3),
             "per_rhs_speedup_vs_bf16_matvec": ms_bf16_matvec * k / ms, "block_bytes": block,
             "block_gbs": block / (ms * 1e-3) / 1e9, "roofline_frac_of_measured_hbm": block / (ms * 1e-3) / 1e9 / peak,

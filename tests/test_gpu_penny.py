@@ -65,7 +65,9 @@ def penny():
 def test_matvec_against_dense_rows(penny, prec):
     x = np.random.default_rng(11).uniform(-1, 1, penny["h"].n_cols)
     y = penny["h"].matvec(x, prec)
-    assert rel(y[penny["rows"]], penny["D"] @ x) < 2e-3
+    err = rel(y[penny["rows"]], penny["D"] @ x)
+    print(f"C3 h={H} n={penny['h'].n_rows} {prec} matvec vs dense rows: {err:.3e}")
+    assert err < 2e-3
 
 
 def test_refined_gmres_pressurised_penny(penny):
@@ -80,6 +82,8 @@ def test_refined_gmres_pressurised_penny(penny):
     for p in ("fp32", "bf16"):
         xr, inf = refine(ops["fp64"], ops[p], b, h.n_rows, minv=minv, tol=1e-8, inner_tol=1e-3, restart=50)
         assert inf.converged, (p, inf.residuals)
+        print(f"C3 refine {p}: outer {inf.outer}, inner iterations {inf.iterations}, "
+              f"rel err vs FP64 GMRES {rel(xr.cpu().numpy(), X):.2e}")
         r = torch.empty_like(b)
         ops["fp64"](xr, r)
         assert float(torch.linalg.vector_norm(b - r) / torch.linalg.vector_norm(b)) <= 1e-8
@@ -91,4 +95,6 @@ def test_refined_gmres_pressurised_penny(penny):
     inner = r <= 0.8
     w = 8 * (1 - PROPS[1] ** 2) / (np.pi * PROPS[0]) * np.sqrt(1 - r[inner] ** 2)
     wn = np.abs(X[2::3][inner])
+    print(f"C3 FP64 GMRES iterations {info.iterations}; dense-row residual {rel(penny['D'] @ X, penny['b'][penny['rows']]):.2e}; "
+          f"Sneddon rel diff {rel(wn, w):.2e}")
     assert rel(wn, w) < 0.03
