@@ -33,8 +33,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TUNING_DIR = os.path.join(HERE, "tuning")
-GRID = {"items_per_cta_phase1": [4, 8, 16, 32], "items_per_cta_phase2": [4, 8, 16],
-        "chunk_bytes": [16384, 24576, 32768]}
+GRID = {"items_per_cta_phase1": [1, 2, 4, 8], "items_per_cta_phase2": [2, 4, 8],
+        "chunk_bytes": [24576, 32768]}
 
 
 def tuning_path(mesh: int) -> str:
