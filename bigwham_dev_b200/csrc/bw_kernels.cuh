@@ -257,6 +257,57 @@ struct DescRegs {
   uint32_t w[kChunkWords];
 };
 
+// The producer warp's view of the work queue, pipelined so that no latency
+// lands on an item boundary:
+//  * `cur` is the item being staged, its chunk range [cb, ce) already loaded;
+//  * `nxt` is the next item, its range [ncb, nce) loading during `cur`;
+//  * lane 0 holds `pend`, the result of the atomicAdd for the item after
+//    that, issued one item earlier.
+// An index >= n_items means the queue is empty; no atomic is issued after
+// that, so the CTA touches queue[0] at most n_taken + 3 times.
+struct ItemQueue {
+  const int32_t *item_ptr;
+  int n_items;
+  int *queue;
+  int cur, cb, ce;
+  int nxt, ncb, nce;
+  int pend;  // lane 0 only
+
+  __device__ __forceinline__ void load_range(int it, int &b, int &e) const {
+    b = 0;
+    e = 0;
+    if (it < n_items) {
+      b = item_ptr[it];
+      e = item_ptr[it + 1];
+    }
+  }
+  __device__ __forceinline__ void init(const int32_t *ptr, int n, int *q, int lane) {
+    item_ptr = ptr;
+    n_items = n;
+    queue = q;
+    int i0 = 0, i1 = 0;
+    pend = n;
+    if (lane == 0) {
+      i0 = atomicAdd(&queue[0], 1);
+      i1 = i0 < n ? atomicAdd(&queue[0], 1) : n;
+      pend = i1 < n ? atomicAdd(&queue[0], 1) : n;
+    }
+    cur = __shfl_sync(0xffffffffu, i0, 0);
+    nxt = __shfl_sync(0xffffffffu, i1, 0);
+    load_range(cur, cb, ce);
+    load_range(nxt, ncb, nce);
+  }
+  __device__ __forceinline__ bool valid() const { return cur < n_items; }
+  __device__ __forceinline__ void advance(int lane) {
+    cur = nxt;
+    cb = ncb;
+    ce = nce;
+    nxt = __shfl_sync(0xffffffffu, pend, 0);
+    load_range(nxt, ncb, nce);
+    if (lane == 0) pend = nxt < n_items ? atomicAdd(&queue[0], 1) : n_items;
+  }
+};
+
 __device__ __forceinline__ void load_desc(const Chunk *chunks, int idx, int end, DescRegs &r) {
   if (idx < end) {
     const uint4 *p = reinterpret_cast<const uint4 *>(chunks + idx);
@@ -306,18 +357,20 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
     const unsigned char *gvec = static_cast<const unsigned char *>(a.gsrc);
     bool ok = true;
     int issued = 0;  // chunks staged so far by this CTA (stage = issued % kStages)
-    // the item to stage now and the next one, fetched one item ahead
-    int cur = 0;
-    if (lane == 0) cur = atomicAdd(&a.queue[0], 1);
-    cur = __shfl_sync(0xffffffffu, cur, 0);
-    while (cur < a.n_items && ok) {
-      int nxt = 0;
-      if (lane == 0) nxt = atomicAdd(&a.queue[0], 1);
-      const int cb = a.item_ptr[cur], ce = a.item_ptr[cur + 1];
-      for (int bb = cb; bb < ce && ok; bb += 32) {
-        DescRegs cur_d;
-        load_desc(a.chunks, bb + lane, ce, cur_d);
-        const int nb = min(32, ce - bb);
+    ItemQueue iq;
+    iq.init(a.item_ptr, a.n_items, a.queue, lane);
+    // batches of up to 32 chunks of one item; lane k holds chunk k's
+    // descriptor, and the next batch's descriptors load during this one
+    int bb = iq.cb;
+    DescRegs cur_d;
+    load_desc(a.chunks, bb + lane, iq.ce, cur_d);
+    while (iq.valid() && ok) {
+      const int be = min(bb + 32, iq.ce);
+      const bool same = be < iq.ce;
+      DescRegs nxt_d;
+      load_desc(a.chunks, (same ? be : iq.ncb) + lane, same ? iq.ce : iq.nce, nxt_d);
+      {
+        const int nb = be - bb;
         for (int k = 0; k < nb; k++) {
           const int s = issued % kStages;
           const uint32_t use = static_cast<uint32_t>(issued / kStages);
@@ -361,7 +414,13 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
           issued++;
         }
       }
-      cur = __shfl_sync(0xffffffffu, nxt, 0);
+      if (same) {
+        bb = be;
+      } else {
+        iq.advance(lane);
+        bb = iq.cb;
+      }
+      cur_d = nxt_d;
     }
     if (ok) {
       // end of work: a descriptor with kEnd alone, no data

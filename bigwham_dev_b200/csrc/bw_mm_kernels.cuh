@@ -191,32 +191,37 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
     int issued = 0;  // chunks staged by this CTA (stage = issued % kMmStages)
     int nitems = 0;  // items announced
     bool ok = true;
-    int cur = 0;
-    if (lane == 0) cur = atomicAdd(&a.queue[0], 1);
-    cur = __shfl_sync(0xffffffffu, cur, 0);
-    while (cur < a.n_items && ok) {
-      int nxt = 0;
-      if (lane == 0) nxt = atomicAdd(&a.queue[0], 1);  // the next item, fetched one item ahead
-      const int cb = a.item_ptr[cur], ce = a.item_ptr[cur + 1];
-      for (int bb = cb; bb < ce && ok; bb += 32) {
-        // lane k holds the descriptor of chunk bb + k
-        uint32_t dw[kMmChunkWords];
-        if (bb + lane < ce) {
-          const uint4 *p = reinterpret_cast<const uint4 *>(a.chunks + bb + lane);
+    ItemQueue iq;
+    iq.init(a.item_ptr, a.n_items, a.queue, lane);
+    // batches of up to 32 chunks of one item; lane k holds chunk k's
+    // descriptor, and the next batch's descriptors load during this one
+    auto load = [&](int from, int to, uint32_t (&dw)[kMmChunkWords]) {
+      if (from + lane < to) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(a.chunks + from + lane);
 #pragma unroll
-          for (int q = 0; q < kMmChunkWords / 4; q++) {
-            const uint4 v = __ldg(p + q);
-            dw[4 * q] = v.x;
-            dw[4 * q + 1] = v.y;
-            dw[4 * q + 2] = v.z;
-            dw[4 * q + 3] = v.w;
-          }
-        } else {
-#pragma unroll
-          for (int q = 0; q < kMmChunkWords; q++) dw[q] = 0;
+        for (int q = 0; q < kMmChunkWords / 4; q++) {
+          const uint4 v = __ldg(p + q);
+          dw[4 * q] = v.x;
+          dw[4 * q + 1] = v.y;
+          dw[4 * q + 2] = v.z;
+          dw[4 * q + 3] = v.w;
         }
-        if (bb == cb && lane == 0) {
-          // announce the item to the epilogue
+      } else {
+#pragma unroll
+        for (int q = 0; q < kMmChunkWords; q++) dw[q] = 0;
+      }
+    };
+    int bb = iq.cb;
+    uint32_t dw[kMmChunkWords];
+    load(bb, iq.ce, dw);
+    while (iq.valid() && ok) {
+      const int be = min(bb + 32, iq.ce);
+      const bool same = be < iq.ce;
+      uint32_t ndw[kMmChunkWords];
+      load(same ? be : iq.ncb, same ? iq.ce : iq.nce, ndw);
+      if (bb == iq.cb) {
+        // a new item: announce it to the epilogue (lane 0 holds its first chunk)
+        if (lane == 0) {
           volatile MmItemInfo &e = ring[nitems % kMmRing];
           e.rows = static_cast<int>(dw[4]);
           e.out_off = static_cast<int>(dw[5]);
@@ -224,8 +229,10 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
           __threadfence_block();
           e.seq = nitems + 1;
         }
-        if (bb == cb) nitems++;
-        const int nb = min(32, ce - bb);
+        nitems++;
+      }
+      {
+        const int nb = be - bb;
         for (int k = 0; k < nb; k++) {
           const int s = issued % kMmStages;
           const uint32_t use = static_cast<uint32_t>(issued / kMmStages);
@@ -289,7 +296,14 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
           issued++;
         }
       }
-      cur = __shfl_sync(0xffffffffu, nxt, 0);
+      if (same) {
+        bb = be;
+      } else {
+        iq.advance(lane);
+        bb = iq.cb;
+      }
+#pragma unroll
+      for (int q = 0; q < kMmChunkWords; q++) dw[q] = ndw[q];
     }
     if (ok) {
       // end of work: the issuers get a kEnd descriptor, the epilogue an end entry
