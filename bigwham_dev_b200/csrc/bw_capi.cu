@@ -579,6 +579,16 @@ int bw_batch_offsets(const bw_hmat *h, int member, int64_t *row0, int64_t *col0)
 
 int bw_batch_count(const bw_hmat *h) { return h ? (int)h->row_off.size() - 1 : 0; }
 
+int bw_set_wait_limit(bw_hmat *h, int64_t ns) {
+  if (!h) return BW_ERR_ARG;
+  if (ns < 1 || ns > 60000000000LL) {
+    h->err = "wait limit must be in [1 ns, 60 s]";
+    return BW_ERR_ARG;
+  }
+  h->spin_limit = ns;
+  return BW_OK;
+}
+
 int bw_set_tuning(bw_hmat *h, const char *key, int64_t value) {
   if (!h || !key) return BW_ERR_ARG;
   if (h->finalized) {

@@ -33,6 +33,11 @@ namespace bw {
 
 constexpr int kStages = 6;
 
+// Bound of the waits that only let work already issued finish (bulk copies
+// in flight, MMAs before TMEM is freed) after an error: independent of the
+// caller's wait limit, so that no CTA exits with work outstanding.
+constexpr long long kDrainLimitNs = 2000000000LL;
+
 // error words
 constexpr int kErrTimeoutEmpty = 0x101;
 constexpr int kErrTimeoutFull = 0x102;
@@ -442,7 +447,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
       // let the copies already in flight land before the CTA can exit
       for (int i = max(0, issued - kStages); i < issued; i++) {
         const int s = i % kStages;
-        mbar_wait(&full[s], static_cast<uint32_t>(i / kStages) & 1u, a.spin_limit);
+        mbar_wait(&full[s], static_cast<uint32_t>(i / kStages) & 1u, kDrainLimitNs);
       }
     }
     // This CTA takes no more items.  The last CTA to get here returns the

@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
       // let the copies in flight land before the CTA can exit
       for (int i = max(0, issued - kMmStages); i < issued; i++) {
         const int s = i % kMmStages;
-        mbar_wait(&full[s], static_cast<uint32_t>(i / kMmStages) & 1u, a.spin_limit);
+        mbar_wait(&full[s], static_cast<uint32_t>(i / kMmStages) & 1u, kDrainLimitNs);
       }
     }
     // This CTA takes no more items.  The last CTA to get here returns the
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
     // every MMA issued so far completes before the TMEM is freed
     if (lane == 0) umma_commit(&drained[q]);
     __syncwarp();
-    mbar_wait(&drained[q], 0u, a.spin_limit);
+    mbar_wait(&drained[q], 0u, kDrainLimitNs);
   } else {
     // ------------------------------------------------------------------ epilogue
     const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31

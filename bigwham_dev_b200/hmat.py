@@ -111,6 +111,10 @@ class HmatGpu:
                                              base + 8 * (o + m * r), max(1, r)), self._h)
             o += r * (m + n)
 
+    def set_wait_limit(self, ns: int) -> None:
+        """Bound of every in-kernel wait (bw_set_wait_limit); default 2 s."""
+        A.check(self._lib.bw_set_wait_limit(self._h, int(ns)), self._h)
+
     def set_tuning(self, **kw) -> "HmatGpu":
         """Plan parameters (bw_set_tuning), before finalize: items_per_cta_phase1,
         items_per_cta_phase2, chunk_bytes, mm_items_per_cta."""

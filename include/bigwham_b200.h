@@ -86,6 +86,15 @@ int bw_batch_offsets(const bw_hmat *h, int member, int64_t *row0, int64_t *col0)
 /* Number of members (1 for a bw_create handle, 0 for NULL). */
 int bw_batch_count(const bw_hmat *h);
 
+/* Bound (in ns, 1 ns .. 60 s, default 2 s) of every wait inside the kernels:
+ * a stage that never fills or empties, an item reduction that never completes.
+ * When a wait runs out the kernel writes an error word and returns; the
+ * cleanup waits (copies in flight, tensor-core work before its memory is
+ * freed) keep their own 2 s bound, so no work is left outstanding.  The next
+ * bw_sync on the stream reports BW_ERR_DEVICE and clears the word; the handle
+ * stays usable. */
+int bw_set_wait_limit(bw_hmat *h, int64_t ns);
+
 /* Plan parameters, set before bw_finalize (bigwham_dev_b200/tune.py sweeps
  * them on a GPU and commits the best per workload):
  *   "items_per_cta_phase1", "items_per_cta_phase2": items per CTA share
