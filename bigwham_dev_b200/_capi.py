@@ -32,6 +32,7 @@ _SIGS = {
     "bw_batch_count": (C.c_int, [_P]),
     "bw_set_tuning": (C.c_int, [_P, C.c_char_p, _I64]),
     "bw_set_wait_limit": (C.c_int, [_P, _I64]),
+    "bw_test_withhold_chunk": (C.c_int, [_P, C.c_int]),
     "bw_add_full": (C.c_int, [_P, _I64, _I64, _I64, _I64, _P, _I64]),
     "bw_add_lowrank": (C.c_int, [_P, _I64, _I64, _I64, _I64, _I64, _P, _I64, _P, _I64]),
     "bw_finalize": (C.c_int, [_P, C.c_int]),

@@ -112,6 +112,12 @@ struct bw_hmat {
   std::vector<double> diag_perm;
   std::string err;
   long long spin_limit = 2000000000LL;  // 2 s bound on every in-kernel wait
+  int withhold = -1;                    // bw_test_withhold_chunk: applies to the next streaming launch only
+  int take_withhold() {
+    const int w = withhold;
+    withhold = -1;
+    return w;
+  }
   // optional per-launch timing (bw_set_timing / bw_timing_read)
   bool timing = false;
   std::vector<cudaEvent_t> ev_pool;     // kTimedLaunches + 1 events per recorded matvec
@@ -460,6 +466,7 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
       a.phase = phase + 1;
       a.err = h->d_err;
       a.spin_limit = h->spin_limit;
+      a.withhold = h->take_withhold();
       bw::stream_panels_kernel<S><<<h->grid, bw::threads_of<S>(), bw::SmemLayout<S>::kTotal, st>>>(a);
       BW_CUDA(cudaGetLastError());
     }
@@ -551,6 +558,7 @@ void launch_matmat_tc(bw_hmat *h, int o, const double *X, int64_t ldx, double *Y
       a.phase = phase + 1;
       a.err = h->d_err;
       a.spin_limit = h->spin_limit;
+      a.withhold = h->take_withhold();
       bw::mm_stream_kernel<<<h->grid, bw::kMmThreads, bw::kMmSmem, st>>>(a);
       BW_CUDA(cudaGetLastError());
     }
@@ -586,6 +594,12 @@ int bw_set_wait_limit(bw_hmat *h, int64_t ns) {
     return BW_ERR_ARG;
   }
   h->spin_limit = ns;
+  return BW_OK;
+}
+
+int bw_test_withhold_chunk(bw_hmat *h, int index) {
+  if (!h || index < 0) return BW_ERR_ARG;
+  h->withhold = index;
   return BW_OK;
 }
 

@@ -59,6 +59,7 @@ struct StreamArgs {
   int phase;                  // 1 or 2
   int *err;
   long long spin_limit;       // bound of every wait, in nanoseconds
+  int withhold;               // test hook: CTA 0 never stages its chunk of this index (-1: none)
 };
 
 // ----------------------------------------------------------------------------- PTX helpers
@@ -387,7 +388,9 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
           uint32_t w[kChunkWords];
 #pragma unroll
           for (int q = 0; q < kChunkWords; q++) w[q] = __shfl_sync(0xffffffffu, cur_d.w[q], k);
-          if (lane == 0) {
+          // test hook: a withheld chunk is never staged, so its wait runs out
+          const bool held = blockIdx.x == 0 && issued == a.withhold;
+          if (lane == 0 && !held) {
             const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w[1]) << 32) | w[0]);
             const int ncols = static_cast<int>(w[2]);
             const int hpad = static_cast<int>(w[3]);
@@ -446,6 +449,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
     if (!ok) {
       // let the copies already in flight land before the CTA can exit
       for (int i = max(0, issued - kStages); i < issued; i++) {
+        if (blockIdx.x == 0 && i == a.withhold) continue;  // nothing in flight for it
         const int s = i % kStages;
         mbar_wait(&full[s], static_cast<uint32_t>(i / kStages) & 1u, kDrainLimitNs);
       }

@@ -75,6 +75,7 @@ struct MmArgs {
   int phase;                  // 1 or 2
   int *err;
   long long spin_limit;       // bound of every wait, in nanoseconds
+  int withhold;               // test hook: CTA 0 never stages its chunk of this index (-1: none)
 };
 
 // ----------------------------------------------------------------------------- tcgen05 helpers
@@ -250,7 +251,9 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
             break;
           }
           const uint32_t(&w)[kMmChunkWords] = dw;
-          if (lane == k) {
+          // test hook: a withheld chunk is never staged, so its wait runs out
+          const bool held = blockIdx.x == 0 && issued == a.withhold;
+          if (lane == k && !held) {
             MmChunk *sd = sdesc + s;
             uint4 *sdw = reinterpret_cast<uint4 *>(sd);
 #pragma unroll
@@ -330,6 +333,7 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
     if (!ok) {
       // let the copies in flight land before the CTA can exit
       for (int i = max(0, issued - kMmStages); i < issued; i++) {
+        if (blockIdx.x == 0 && i == a.withhold) continue;  // nothing in flight for it
         const int s = i % kMmStages;
         mbar_wait(&full[s], static_cast<uint32_t>(i / kMmStages) & 1u, kDrainLimitNs);
       }

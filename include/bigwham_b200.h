@@ -95,6 +95,13 @@ int bw_batch_count(const bw_hmat *h);
  * stays usable. */
 int bw_set_wait_limit(bw_hmat *h, int64_t ns);
 
+/* Test hook for the timeout path: in the next streaming launch (phase 1 of the
+ * next bw_matvec or bw_matmat), CTA 0 never stages its chunk number `index`.
+ * The wait for that chunk then runs out after the wait limit, the kernel
+ * reports it through the error word, and the result of that call is
+ * incomplete.  Nothing is left in flight: the chunk was never copied. */
+int bw_test_withhold_chunk(bw_hmat *h, int index);
+
 /* Plan parameters, set before bw_finalize (bigwham_dev_b200/tune.py sweeps
  * them on a GPU and commits the best per workload):
  *   "items_per_cta_phase1", "items_per_cta_phase2": items per CTA share

@@ -1,7 +1,8 @@
 """Failure detection on the GPU without faulting it (-m gpu).
 
-A wait limit of 1 ns (bw_set_wait_limit) makes the kernels' bounded waits run
-out: the consumers' first wait for data always spins.  Each timed-out kernel:
+bw_test_withhold_chunk makes CTA 0 of the next streaming launch skip staging
+one chunk: a barrier that nothing completes.  With a 20 ms wait limit
+(bw_set_wait_limit) the wait for it runs out.  The timed-out kernel:
 * writes an error word;
 * lets its bulk copies and tensor-core work finish (those waits keep a fixed
   2 s bound);
@@ -38,8 +39,9 @@ def test_timeout_reported_and_handle_recovers(handle):
     good = {p: h.matvec(x, p).clone() for p in ("fp64", "bf16")}
     good_mm = h.matmat(X, "bf16").clone()
     h.sync()
-    h.set_wait_limit(1)
+    h.set_wait_limit(20_000_000)
     for run in (lambda: h.matvec(x, "fp64"), lambda: h.matvec(x, "bf16"), lambda: h.matmat(X, "bf16")):
+        A.check(A.lib().bw_test_withhold_chunk(h._h, 1), h._h)
         run()
         with pytest.raises(BigWhamError) as e:
             h.sync()
