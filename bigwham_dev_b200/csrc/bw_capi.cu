@@ -442,7 +442,7 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
     const DevPhase &dp = h->dev[o][prec][phase];
     if (phase == 1) {
       if (dp.n_gsegs > 0) {
-        const int per_block = 8;  // runs per 256-thread block (one warp each)
+        const int per_block = 8 * bw::kG2Runs;  // runs per 256-thread block (kG2Runs per warp)
         bw::gather_g2_kernel<G, kPacked><<<(int)((dp.n_gsegs + per_block - 1) / per_block), 256, 0, st>>>(
             dp.gsegs, (int)dp.n_gsegs, xp, t, g2_buf);
         BW_CUDA(cudaGetLastError());

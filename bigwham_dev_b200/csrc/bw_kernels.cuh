@@ -671,23 +671,49 @@ __device__ __forceinline__ uint32_t pack_hilo(float v) {
 }
 
 // G2[dst + c] = scale * src[src_off + c] for every run (src: gathered x or t):
-// the phase-2 vector values laid out chunk by chunk.  One warp per run.
+// the phase-2 vector values laid out chunk by chunk.  Runs are short (tens of
+// values), so each warp takes kG2Runs of them at once: lanes 0..kG2Runs-1
+// fetch the run descriptors together, and every lane keeps one load per run
+// in flight per step, instead of one dependent chain per run.
 // kPacked: store pack_hilo(value) words (BF16 path) instead of G values.
+constexpr int kG2Runs = 4;
+
 template <typename G, bool kPacked>
 __global__ void gather_g2_kernel(const GatherSeg *__restrict__ runs, int n_runs, const G *__restrict__ xp,
                                  const G *__restrict__ t, void *__restrict__ g2) {
-  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (r >= n_runs) return;
-  const GatherSeg gsg = runs[r];
-  const int cols = static_cast<int>(gsg.cols_src & 0x7fffffffu);
-  const G *src = (gsg.cols_src >> 31) ? t : xp;
-  const G sc = static_cast<G>(gsg.scale);
-  for (int c = threadIdx.x & 31; c < cols; c += 32) {
-    const G v = sc * src[gsg.src_off + c];
-    if constexpr (kPacked)
-      static_cast<uint32_t *>(g2)[gsg.dst + c] = pack_hilo(static_cast<float>(v));
-    else
-      static_cast<G *>(g2)[gsg.dst + c] = v;
+  const int lane = threadIdx.x & 31;
+  const int r0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kG2Runs;
+  if (r0 >= n_runs) return;
+  GatherSeg mine{};
+  if (lane < kG2Runs && r0 + lane < n_runs) mine = runs[r0 + lane];  // cols = 0 past the end
+  int dst[kG2Runs], off[kG2Runs], cols[kG2Runs], from_t[kG2Runs];
+  float sc[kG2Runs];
+  int most = 0;
+#pragma unroll
+  for (int q = 0; q < kG2Runs; q++) {
+    dst[q] = __shfl_sync(0xffffffffu, mine.dst, q);
+    off[q] = __shfl_sync(0xffffffffu, mine.src_off, q);
+    const uint32_t cs = __shfl_sync(0xffffffffu, mine.cols_src, q);
+    cols[q] = static_cast<int>(cs & 0x7fffffffu);
+    from_t[q] = static_cast<int>(cs >> 31);
+    sc[q] = __shfl_sync(0xffffffffu, mine.scale, q);
+    most = max(most, cols[q]);
+  }
+  for (int c = lane; c < most; c += 32) {
+    G v[kG2Runs];
+#pragma unroll
+    for (int q = 0; q < kG2Runs; q++)
+      if (c < cols[q]) v[q] = (from_t[q] ? t : xp)[off[q] + c];
+#pragma unroll
+    for (int q = 0; q < kG2Runs; q++) {
+      if (c < cols[q]) {
+        const G w = static_cast<G>(sc[q]) * v[q];
+        if constexpr (kPacked)
+          static_cast<uint32_t *>(g2)[dst[q] + c] = pack_hilo(static_cast<float>(w));
+        else
+          static_cast<G *>(g2)[dst[q] + c] = w;
+      }
+    }
   }
 }
 
