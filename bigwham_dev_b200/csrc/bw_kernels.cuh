@@ -263,6 +263,10 @@ struct DescRegs {
   uint32_t w[kChunkWords];
 };
 
+template <int N> struct IntC {
+  static constexpr int value = N;
+};
+
 // The producer warp's view of the work queue, pipelined so that no latency
 // lands on an item boundary:
 //  * `cur` is the item being staged, its chunk range [cb, ce) already loaded;
@@ -575,27 +579,44 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
         // depend on the schedule).
         int ks = kp - rot;
         if (ks < 0) ks += kparts;
-        for (; ks < nks; ks += kparts) {
-          // B fragment: lanes 0-3 hold the BF16-rounded vector (column 0),
-          // lanes 4-7 the BF16-rounded remainder (column 1), others zero;
-          // the vector arrives as pack_hilo words.
-          uint32_t b0 = 0, b1 = 0;
-          if (grp < 2) {
-            const uint32_t *gw = reinterpret_cast<const uint32_t *>(gs);
-            const int c = 16 * ks + 2 * tq;
-            const uint32_t w0 = c < ncols ? gw[c] : 0u, w1 = c + 1 < ncols ? gw[c + 1] : 0u;
-            const uint32_t w2 = c + 8 < ncols ? gw[c + 8] : 0u, w3 = c + 9 < ncols ? gw[c + 9] : 0u;
-            const uint32_t sel = grp == 0 ? 0x5410u : 0x7632u;  // low halves (hi) or high halves (lo)
-            b0 = __byte_perm(w0, w1, sel);
-            b1 = __byte_perm(w2, w3, sel);
-          }
-          const bool k2 = 16 * ks + 8 < ncols;  // second 8-column group present
-          const uint32_t kaddr = lane_base + static_cast<uint32_t>(ks) * kstep_bytes - (k2 ? 0u : back_k);
+        // the m-tile holding only 8 rows (hpad = 16k + 8), or -1
+        const int half_mt = (hpad & 15) ? (hpad >> 4) : -1;
+        // K-steps for kNJ active m-tiles of this warp: the tile count is a
+        // compile-time constant, so accumulators stay in registers and no
+        // slot is predicated off; full K-steps skip the bounds checks.
+        auto ksteps = [&](auto nj) {
+          constexpr int kNJ = decltype(nj)::value;
+          for (; ks < nks; ks += kparts) {
+            const bool full = 16 * ks + 16 <= ncols;
+            // B fragment: lanes 0-3 hold the BF16-rounded vector (column 0),
+            // lanes 4-7 the BF16-rounded remainder (column 1), others zero;
+            // the vector arrives as pack_hilo words.
+            uint32_t b0 = 0, b1 = 0;
+            if (grp < 2) {
+              const uint32_t *gw = reinterpret_cast<const uint32_t *>(gs);
+              const int c = 16 * ks + 2 * tq;
+              uint32_t w0, w1, w2, w3;
+              if (full) {
+                w0 = gw[c];
+                w1 = gw[c + 1];
+                w2 = gw[c + 8];
+                w3 = gw[c + 9];
+              } else {
+                w0 = c < ncols ? gw[c] : 0u;
+                w1 = c + 1 < ncols ? gw[c + 1] : 0u;
+                w2 = c + 8 < ncols ? gw[c + 8] : 0u;
+                w3 = c + 9 < ncols ? gw[c + 9] : 0u;
+              }
+              const uint32_t sel = grp == 0 ? 0x5410u : 0x7632u;  // low halves (hi) or high halves (lo)
+              b0 = __byte_perm(w0, w1, sel);
+              b1 = __byte_perm(w2, w3, sel);
+            }
+            const bool k2 = full || 16 * ks + 8 < ncols;  // second 8-column group present
+            const uint32_t kaddr = lane_base + static_cast<uint32_t>(ks) * kstep_bytes - (k2 ? 0u : back_k);
 #pragma unroll
-          for (int j = 0; j < 8; j++) {
-            const int mt = mg * 8 + j;
-            if (mt < nMt) {
-              const bool m2 = mt * 16 + 8 < hpad;  // second 8-row group present
+            for (int j = 0; j < kNJ; j++) {
+              const int mt = mg * 8 + j;
+              const bool m2 = mt != half_mt;  // second 8-row group present
               uint32_t a0, a1, a2, a3;
               ldmatrix_x4_trans(kaddr + 256u * static_cast<uint32_t>(mt) - (m2 ? 0u : back_m), a0, a1, a2, a3);
               if (!m2) {
@@ -609,6 +630,16 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
               mma_bf16_16816(tacc[j], a0, a1, a2, a3, b0, b1);
             }
           }
+        };
+        switch (min(8, nMt - mg * 8)) {
+          case 1: ksteps(IntC<1>{}); break;
+          case 2: ksteps(IntC<2>{}); break;
+          case 3: ksteps(IntC<3>{}); break;
+          case 4: ksteps(IntC<4>{}); break;
+          case 5: ksteps(IntC<5>{}); break;
+          case 6: ksteps(IntC<6>{}); break;
+          case 7: ksteps(IntC<7>{}); break;
+          default: ksteps(IntC<8>{}); break;
         }
       }
     }
