@@ -134,42 +134,22 @@ def max_over_ranks(v, world, device="cuda"):
     return float(t.item())
 
 
-BLOCK_KEYS = ("fr", "lr", "fr_data", "lr_data", "perm0", "perm1")
-
-
-def shared_blocks(world, rank, tag, build):
-    """Replicas share one H-matrix build: rank 0 runs build(alloc) -> the
-    export dict (BigWhamIOGpu.export_blocks) with its arrays placed by `alloc`
-    in /dev/shm, then every rank maps them.  Returns (meta, arrays, release);
-    release() (all ranks, after their upload) removes the files."""
-    d = os.path.join("/dev/shm", f"bw_blocks_{tag}")
-    if rank == 0:
-        os.makedirs(d, exist_ok=True)
-        names = iter(BLOCK_KEYS)
-
-        def alloc(shape, dtype):
-            return np.lib.format.open_memmap(os.path.join(d, next(names) + ".bin"), mode="w+", dtype=dtype,
-                                             shape=shape)
-
-        ex = build(alloc)
-        for k in BLOCK_KEYS:
-            ex[k].flush()
-        with open(os.path.join(d, "meta.json"), "w") as f:
-            json.dump({"dof": ex["dof"], "n_rows": ex["n_rows"], "n_cols": ex["n_cols"]}, f)
+def shared_block_file(world, rank, path, build, keep=False):
+    """Replicas share one H-matrix build through a block file: rank 0 runs
+    build(path), which writes it (BigWhamIOGpu.write_to_file), unless `path`
+    already exists; then every rank maps it (HmatGpu.from_file).  Returns
+    release(); release() (all ranks, after their upload) removes the file
+    unless keep."""
+    if rank == 0 and not os.path.exists(path):
+        build(path)
     barrier(world)
-    with open(os.path.join(d, "meta.json")) as f:
-        meta = json.load(f)
-    arr = {k: np.load(os.path.join(d, k + ".bin"), mmap_mode="r") for k in BLOCK_KEYS}
 
     def release():
         barrier(world)
-        if rank == 0:
-            for k in BLOCK_KEYS:
-                os.unlink(os.path.join(d, k + ".bin"))
-            os.unlink(os.path.join(d, "meta.json"))
-            os.rmdir(d)
+        if rank == 0 and not keep:
+            os.unlink(path)
 
-    return meta, arr, release
+    return release
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -232,33 +212,47 @@ def build_hmatrix(a, world, rank, local):
     info = {"tuning": tuning or "defaults"}
     coor, conn = square_crack_3d(a.mesh)
     if world == 1:
+        if a.block_file and os.path.exists(a.block_file):
+            # blocks saved by an earlier run: no host rebuild, e2e through HmatGpu.matvec(host arrays)
+            from bigwham_dev_b200 import blockfile
+
+            head = blockfile.info(a.block_file)
+            t0 = time.time()
+            h = HmatGpu.from_file(a.block_file, device=local, verify=True, precisions=precs, transpose=False,
+                                  matmat=a.matmat, tuning=tuning)
+            info["upload_s"] = round(time.time() - t0, 2)
+            info["block_file"] = f"{a.block_file} (read; host build skipped)"
+            info["compression"] = (head["fr_entries"] + head["lr_entries"]) / (head["n_rows"] * head["n_cols"])
+            return None, h, info
         t0 = time.time()
         io = BigWhamIOGpu(coor, conn, "3DR0-H", PROPS, os.cpu_count() or 1, useCuda=False, device=local)
         io.build_hierarchical_matrix(LEAF, ETA, EPS)
         info["host_build_s"] = round(time.time() - t0, 2)
+        if a.block_file:
+            io.write_to_file(a.block_file)
+            info["block_file"] = f"{a.block_file} (written)"
         t0 = time.time()
         io.use_cuda = True
         h = io.attach_gpu(precs, transpose=False, matmat=a.matmat, tuning=tuning)
         info["upload_s"] = round(time.time() - t0, 2)
         info["compression"] = io.get_compression_ratio()
         return io, h, info
-    # replicas: one build, shared through /dev/shm
+    # replicas: one build, shared as a block file (in /dev/shm unless --block-file names one)
     tag = os.environ.get("TORCHELASTIC_RUN_ID", "bench") + f"_{a.mesh}"
+    path = a.block_file or os.path.join("/dev/shm", f"bw_blocks_{tag}.bwb")
+    reused = os.path.exists(path)
 
-    def build(alloc):
+    def build(p):
         t0 = time.time()
         io = BigWhamIOGpu(coor, conn, "3DR0-H", PROPS, os.cpu_count() or 1, useCuda=False, device=local)
         io.build_hierarchical_matrix(LEAF, ETA, EPS)
-        ex = io.export_blocks(alloc)
+        io.write_to_file(p)
         info["host_build_s"] = round(time.time() - t0, 2)
         io.close()
-        return ex
 
-    meta, arr, release = shared_blocks(world, rank, tag, build)
+    release = shared_block_file(world, rank, path, build, keep=a.block_file is not None)
     t0 = time.time()
-    h = HmatGpu.from_flat(meta["dof"], meta["n_rows"], meta["n_cols"], arr["fr"], arr["lr"], arr["fr_data"],
-                          arr["lr_data"], arr["perm0"], arr["perm1"], device=local, precisions=precs, matmat=a.matmat,
-                          tuning=tuning)
+    h = HmatGpu.from_file(path, device=local, verify=reused, precisions=precs, matmat=a.matmat, tuning=tuning)
     info["upload_s"] = round(time.time() - t0, 2)
     release()
     return None, h, info
@@ -534,6 +528,9 @@ def main(argv=None):
     ap.add_argument("--no-matmat", dest="matmat", action="store_false",
                     help="skip the 64-right-hand-side tensor-core matmat line (N = 1 only)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 48 x 2DS0 batched line (N = 1 only)")
+    ap.add_argument("--block-file", default=None,
+                    help="block file of the H-matrix: read it when it exists (no host rebuild), else write it "
+                         "after the build")
     ap.add_argument("--cpu-budget-s", type=float, default=10.0)
     ap.add_argument("--ref-budget-s", type=float, default=60.0)
     a = ap.parse_args(argv)

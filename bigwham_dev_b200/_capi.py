@@ -12,13 +12,14 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libbigwham_b200.so")
 
-BW_OK, BW_ERR_ARG, BW_ERR_STATE, BW_ERR_OOM, BW_ERR_CUDA, BW_ERR_DEVICE, BW_ERR_UNSUPPORTED = range(7)
+BW_OK, BW_ERR_ARG, BW_ERR_STATE, BW_ERR_OOM, BW_ERR_CUDA, BW_ERR_DEVICE, BW_ERR_UNSUPPORTED, BW_ERR_IO = range(8)
 BW_FP64, BW_FP32, BW_BF16 = 1, 2, 4
 BW_STORE_TRANSPOSE, BW_NO_FINITE_CHECK, BW_PLAN_ONLY, BW_STORE_MATMAT = 16, 32, 64, 128
 BW_PERMUTED, BW_TRANSPOSE = 256, 512
 
 STATUS_NAMES = {BW_ERR_ARG: "BW_ERR_ARG", BW_ERR_STATE: "BW_ERR_STATE", BW_ERR_OOM: "BW_ERR_OOM",
-                BW_ERR_CUDA: "BW_ERR_CUDA", BW_ERR_DEVICE: "BW_ERR_DEVICE", BW_ERR_UNSUPPORTED: "BW_ERR_UNSUPPORTED"}
+                BW_ERR_CUDA: "BW_ERR_CUDA", BW_ERR_DEVICE: "BW_ERR_DEVICE", BW_ERR_UNSUPPORTED: "BW_ERR_UNSUPPORTED",
+                BW_ERR_IO: "BW_ERR_IO"}
 
 PRECISIONS = {"fp64": BW_FP64, "fp32": BW_FP32, "bf16": BW_BF16}
 
@@ -53,6 +54,12 @@ _SIGS = {
     "bw_plan_tscale": (C.c_int, [_P, C.c_int, _P, _P]),
     "bw_mm_plan_export": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "bw_plan_gather": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
+    "bw_file_write": (C.c_int, [C.c_char_p, C.c_int, _I64, _I64, _P, _P, _I64, _P, _P, _I64, _P, _P, _P]),
+    "bw_file_write_blocks": (C.c_int, [C.c_char_p, C.c_int, _I64, _I64, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, _P,
+                                       _P, _P, _P]),
+    "bw_file_info": (C.c_int, [C.c_char_p, _P]),
+    "bw_file_read": (C.c_int, [C.c_char_p, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "bw_create_from_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(_P)]),
     "bw_destroy": (C.c_int, [_P]),
     "bw_version": (C.c_char_p, []),
 }

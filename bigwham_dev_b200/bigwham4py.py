@@ -50,6 +50,7 @@ _HSIGS = {
     "bwh_n_blocks": (_I64, [_P, C.c_int]),
     "bwh_entries": (_I64, [_P, C.c_int]),
     "bwh_export": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "bwh_write_to_file": (C.c_int, [_P, C.c_char_p]),
     "bwh_gpu_handle": (_P, [_P]),
     "bwh_destroy": (C.c_int, [_P]),
     "bwh_last_error": (C.c_char_p, []),
@@ -210,6 +211,12 @@ class BigWhamIOGpu:
         _check(self._L.bwh_export(self._h, *(out[k].ctypes.data for k in
                                              ("fr", "lr", "fr_data", "lr_data", "perm0", "perm1"))))
         return out
+
+    def write_to_file(self, path) -> None:
+        """Save the built H-matrix as a block file (before attach_gpu): the
+        reference's Hmat::writeToFile (src/hmat/hmatrix/hmat.cc:749-835) without
+        HDF5.  Load it with HmatGpu.from_file or blockfile.read."""
+        _check(self._L.bwh_write_to_file(self._h, os.fsencode(os.fspath(path))))
 
     def close(self) -> None:
         if getattr(self, "_h", None):

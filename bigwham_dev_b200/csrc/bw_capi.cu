@@ -13,6 +13,7 @@
 #include "bigwham_b200.h"
 #include "bw_kernels.cuh"
 #include "bw_mm_kernels.cuh"
+#include "bw_file.h"
 #include "bw_layout.h"
 
 namespace {
@@ -113,6 +114,7 @@ struct bw_hmat {
   std::string err;
   long long spin_limit = 2000000000LL;  // 2 s bound on every in-kernel wait
   int withhold = -1;                    // bw_test_withhold_chunk: applies to the next streaming launch only
+  std::shared_ptr<void> borrowed;       // mapped block file the registered blocks point into (until finalize)
   int take_withhold() {
     const int w = withhold;
     withhold = -1;
@@ -855,6 +857,7 @@ int bw_finalize(bw_hmat *h, int flags) {
     h->prob.lr.clear();
     h->prob.fr.shrink_to_fit();
     h->prob.lr.shrink_to_fit();
+    h->borrowed.reset();
   }
   return rc;
 }
@@ -1197,6 +1200,222 @@ int bw_plan_tscale(const bw_hmat *h, int transposed, int64_t *n, float *out) {
   const std::vector<float> &ts = h->op[o].t_scale;
   *n = (int64_t)ts.size();
   if (out) std::memcpy(out, ts.data(), ts.size() * 4);
+  return BW_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int file_fail(const std::string &m, int code) {
+  std::lock_guard<std::mutex> g(g_err_mu);
+  g_last_create_error = m;
+  return code;
+}
+
+// Block-file entries have no handle: messages go where bw_create's do.
+template <typename F> int file_guarded(F &&f) {
+  try {
+    return f();
+  } catch (const std::invalid_argument &e) {
+    return file_fail(e.what(), BW_ERR_ARG);
+  } catch (const std::bad_alloc &) {
+    return file_fail("host allocation failed", BW_ERR_OOM);
+  } catch (const std::exception &e) {
+    return file_fail(e.what(), BW_ERR_IO);
+  }
+}
+
+// Block extent in scalar units from pattern coordinates in points; throws
+// unless 0 <= a0 < a1 <= limit.
+int64_t extent(int64_t a0, int64_t a1, int64_t limit, int64_t dof, const char *what, int64_t k) {
+  if (!(0 <= a0 && a0 < a1 && a1 <= limit))
+    throw std::invalid_argument(std::string(what) + " block " + std::to_string(k) + " lies outside the matrix");
+  return (a1 - a0) * dof;
+}
+
+// Copy in parallel (block data can be gigabytes).
+void par_copy(void *dst, const void *src, int64_t bytes) {
+  const int64_t step = int64_t(16) << 20;
+#pragma omp parallel for schedule(static)
+  for (int64_t o = 0; o < bytes; o += step)
+    std::memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, (size_t)std::min(step, bytes - o));
+}
+
+}  // namespace
+
+extern "C" {
+
+int bw_file_write(const char *path, int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0,
+                  const int64_t *perm1, int64_t n_fr, const int64_t *fr, const double *fr_data, int64_t n_lr,
+                  const int64_t *lr, const double *lr_data, const double *lr_error) {
+  return file_guarded([&] {
+    if (!path) throw std::invalid_argument("null path");
+    if (dof < 1 || n_rows < 0 || n_cols < 0 || n_fr < 0 || n_lr < 0)
+      throw std::invalid_argument("bad sizes or block counts");
+    if ((n_fr && (!fr || !fr_data)) || (n_lr && (!lr || !lr_data)))
+      throw std::invalid_argument("null pattern or block data");
+    const int64_t rp = n_rows / dof, cp = n_cols / dof;
+    std::vector<int64_t> frp(6 * n_fr), lrp(6 * n_lr), frl(n_fr), al(n_lr), bl(n_lr);
+    std::vector<const double *> frb(n_fr), ab(n_lr), bb(n_lr);
+    int64_t o = 0;
+    for (int64_t k = 0; k < n_fr; k++) {
+      const int64_t *c = fr + 4 * k;
+      const int64_t m = extent(c[0], c[2], rp, dof, "FR", k), n = extent(c[1], c[3], cp, dof, "FR", k);
+      int64_t *q = &frp[6 * k];
+      q[0] = k;
+      for (int i = 0; i < 4; i++) q[1 + i] = c[i];
+      q[5] = 0;
+      frb[k] = fr_data + o;
+      frl[k] = m;
+      o += m * n;
+    }
+    o = 0;
+    for (int64_t k = 0; k < n_lr; k++) {
+      const int64_t *c = lr + 5 * k;
+      const int64_t m = extent(c[0], c[2], rp, dof, "LR", k), n = extent(c[1], c[3], cp, dof, "LR", k), r = c[4];
+      if (r < 0) throw std::invalid_argument("LR block " + std::to_string(k) + " has a negative rank");
+      int64_t *q = &lrp[6 * k];
+      q[0] = k;
+      for (int i = 0; i < 5; i++) q[1 + i] = c[i];
+      ab[k] = lr_data + o;
+      al[k] = std::max<int64_t>(1, m);
+      bb[k] = lr_data + o + m * r;
+      bl[k] = std::max<int64_t>(1, r);
+      o += r * (m + n);
+    }
+    bw::FileBlocks b;
+    b.dof = dof;
+    b.n_rows = n_rows;
+    b.n_cols = n_cols;
+    b.perm0 = perm0;
+    b.perm1 = perm1;
+    b.n_fr = n_fr;
+    b.fr_pattern = frp.data();
+    b.fr = frb.data();
+    b.fr_ld = frl.data();
+    b.n_lr = n_lr;
+    b.lr_pattern = lrp.data();
+    b.lr_a = ab.data();
+    b.lr_a_ld = al.data();
+    b.lr_b = bb.data();
+    b.lr_b_ld = bl.data();
+    b.lr_error = lr_error;
+    bw::write_block_file(path, b);
+    return BW_OK;
+  });
+}
+
+int bw_file_write_blocks(const char *path, int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0,
+                         const int64_t *perm1, int64_t n_fr, const int64_t *fr_pattern, const double *const *fr,
+                         const int64_t *fr_ld, int64_t n_lr, const int64_t *lr_pattern, const double *const *lr_a,
+                         const int64_t *lr_a_ld, const double *const *lr_b, const int64_t *lr_b_ld,
+                         const double *lr_error) {
+  return file_guarded([&] {
+    if (!path) throw std::invalid_argument("null path");
+    bw::FileBlocks b;
+    b.dof = dof;
+    b.n_rows = n_rows;
+    b.n_cols = n_cols;
+    b.perm0 = perm0;
+    b.perm1 = perm1;
+    b.n_fr = n_fr;
+    b.fr_pattern = fr_pattern;
+    b.fr = fr;
+    b.fr_ld = fr_ld;
+    b.n_lr = n_lr;
+    b.lr_pattern = lr_pattern;
+    b.lr_a = lr_a;
+    b.lr_a_ld = lr_a_ld;
+    b.lr_b = lr_b;
+    b.lr_b_ld = lr_b_ld;
+    b.lr_error = lr_error;
+    bw::write_block_file(path, b);
+    return BW_OK;
+  });
+}
+
+int bw_file_info(const char *path, int64_t info[9]) {
+  return file_guarded([&] {
+    if (!path || !info) throw std::invalid_argument("null path or output");
+    auto f = bw::BlockFile::open(path, false);
+    const bw::FileHeader &h = f->header();
+    const int64_t v[9] = {h.dof,        h.n_rows,     h.n_cols, h.n_fr, h.n_lr, h.fr_entries,
+                          h.lr_entries, h.flags & 1, f->file_bytes()};
+    std::memcpy(info, v, sizeof v);
+    return BW_OK;
+  });
+}
+
+int bw_file_read(const char *path, int verify, int64_t *fr, int64_t *lr, double *fr_data, double *lr_data,
+                 int64_t *perm0, int64_t *perm1, double *lr_error, int64_t *fr_pattern, int64_t *lr_pattern) {
+  return file_guarded([&] {
+    if (!path) throw std::invalid_argument("null path");
+    auto f = bw::BlockFile::open(path, verify != 0);
+    const bw::FileHeader &h = f->header();
+    if ((h.n_fr && (!fr || !fr_data)) || (h.n_lr && (!lr || !lr_data)) || (h.n_rows && !perm0) ||
+        (h.n_cols && !perm1))
+      throw std::invalid_argument("null output array");
+    const int64_t *fp = f->fr_pattern(), *lp = f->lr_pattern();
+    for (int64_t k = 0; k < h.n_fr; k++)
+      for (int i = 0; i < 4; i++) fr[4 * k + i] = fp[6 * k + 1 + i];
+    for (int64_t k = 0; k < h.n_lr; k++)
+      for (int i = 0; i < 5; i++) lr[5 * k + i] = lp[6 * k + 1 + i];
+    if (fr_pattern) std::memcpy(fr_pattern, fp, (size_t)(48 * h.n_fr));
+    if (lr_pattern) std::memcpy(lr_pattern, lp, (size_t)(48 * h.n_lr));
+    if (h.n_rows) std::memcpy(perm0, f->perm0(), (size_t)(8 * (h.n_rows / h.dof)));
+    if (h.n_cols) std::memcpy(perm1, f->perm1(), (size_t)(8 * (h.n_cols / h.dof)));
+    if (lr_error) {
+      if (f->lr_error())
+        std::memcpy(lr_error, f->lr_error(), (size_t)(8 * h.n_lr));
+      else
+        std::fill(lr_error, lr_error + h.n_lr, 0.0);
+    }
+    par_copy(fr_data, f->fr_data(), 8 * h.fr_entries);
+    par_copy(lr_data, f->lr_data(), 8 * h.lr_entries);
+    return BW_OK;
+  });
+}
+
+int bw_create_from_file(const char *path, int device, int verify, bw_hmat **out) {
+  if (!out) return BW_ERR_ARG;
+  *out = nullptr;
+  std::shared_ptr<bw::BlockFile> f;
+  int rc = file_guarded([&] {
+    if (!path) throw std::invalid_argument("null path");
+    f = bw::BlockFile::open(path, verify != 0);
+    return BW_OK;
+  });
+  if (rc != BW_OK) return rc;
+  const bw::FileHeader &hd = f->header();
+  bw_hmat *h = nullptr;
+  rc = bw_create((int)hd.dof, hd.n_rows, hd.n_cols, f->perm0(), f->perm1(), device, &h);
+  if (rc != BW_OK) return rc;
+  const int64_t d = hd.dof;
+  const int64_t *fp = f->fr_pattern(), *lp = f->lr_pattern();
+  const double *fdat = f->fr_data(), *ldat = f->lr_data();
+  int64_t o = 0;
+  for (int64_t k = 0; k < hd.n_fr && rc == BW_OK; k++) {
+    const int64_t *c = fp + 6 * k;
+    const int64_t m = (c[3] - c[1]) * d, n = (c[4] - c[2]) * d;
+    rc = bw_add_full(h, c[1] * d, c[2] * d, m, n, fdat + o, m);
+    o += m * n;
+  }
+  o = 0;
+  for (int64_t k = 0; k < hd.n_lr && rc == BW_OK; k++) {
+    const int64_t *c = lp + 6 * k;
+    const int64_t m = (c[3] - c[1]) * d, n = (c[4] - c[2]) * d, r = c[5];
+    rc = bw_add_lowrank(h, c[1] * d, c[2] * d, m, n, r, ldat + o, std::max<int64_t>(1, m), ldat + o + m * r,
+                        std::max<int64_t>(1, r));
+    o += r * (m + n);
+  }
+  if (rc != BW_OK) {
+    file_fail(std::string(path) + ": " + h->err, rc);
+    bw_destroy(h);
+    return rc;
+  }
+  h->borrowed = f;
+  *out = h;
   return BW_OK;
 }
 

@@ -161,6 +161,30 @@ class HmatGpu:
         return h.finalize(**kw)
 
     @classmethod
+    def from_file(cls, path, device: int = 0, verify: bool = True, **kw) -> "HmatGpu":
+        """Handle from a block file (bw_create_from_file; written by
+        ``blockfile.write`` or ``BigWhamIOGpu.write_to_file``): the blocks are
+        registered straight from the mapped file and laid out by
+        ``finalize(**kw)``, with no H-matrix rebuild.  verify: check the block
+        data checksums first.  The counterpart of the reference's
+        ``Hmat(filename)`` constructor (src/hmat/hmatrix/hmat.cc:64-74)."""
+        from . import blockfile
+
+        head = blockfile.info(path)
+        self = cls.__new__(cls)
+        self._lib = A.lib()
+        self.dof, self.n_rows, self.n_cols, self.device = head["dof"], head["n_rows"], head["n_cols"], int(device)
+        h = C.c_void_p()
+        A.check(self._lib.bw_create_from_file(blockfile._path(path), self.device, int(bool(verify)), C.byref(h)),
+                None)
+        self._h = h
+        self._keep = []
+        self._finalized = False
+        self.precisions = ()
+        self.has_transpose = False
+        return self.finalize(**kw)
+
+    @classmethod
     def batch(cls, members, device: int = 0, **kw) -> "HmatGpu":
         """One handle for several independent H-matrices of the same dof
         (bw_create_batch): the block-diagonal H-matrix of the members, applied

@@ -35,7 +35,8 @@ enum {
   BW_ERR_OOM = 3,         /* device or host allocation failed, or above the configured limit */
   BW_ERR_CUDA = 4,        /* a CUDA runtime call failed */
   BW_ERR_DEVICE = 5,      /* a kernel reported an error word (e.g. a bounded wait ran out) */
-  BW_ERR_UNSUPPORTED = 6  /* precision or operation not stored / not available */
+  BW_ERR_UNSUPPORTED = 6, /* precision or operation not stored / not available */
+  BW_ERR_IO = 7           /* a block file could not be read or written, or failed its checks */
 };
 
 /* storage / precision flags */
@@ -259,6 +260,58 @@ int bw_plan_gather(const bw_hmat *h, int precision, int transposed, int64_t *n, 
 /* Per-t-entry output scales of phase 1 (BF16: scale(A) * scale(B) of the
  * entry's low-rank block; 1 elsewhere), for inspection and testing. */
 int bw_plan_tscale(const bw_hmat *h, int transposed, int64_t *n, float *out);
+
+/* ---- Block files ----------------------------------------------------------
+ * A built H-matrix on disk: dof, sizes, both permutations, the HPattern
+ * columns (spot, i0, j0, i_end, j_end, flag) of every block, the full-rank
+ * blocks, each low-rank block's A and B, and optionally the low-rank blocks'
+ * ACA error estimates, in a page-aligned binary with a checksum per section.
+ * The content of the reference's Hmat<T>::writeToFile / readFromFile
+ * (src/hmat/hmatrix/hmat.cc:749-935, declared hmat.h:100-101), which need
+ * HDF5; here the file is mapped, so a later run uploads the blocks without
+ * rebuilding the H-matrix.  Writers go through a temporary file renamed into
+ * place.  Errors: BW_ERR_ARG (inconsistent arguments), BW_ERR_IO (file cannot
+ * be read or written, is not a block file, is truncated, or fails a checksum);
+ * bw_last_error(NULL, ...) gives the message. */
+
+/* Write from the flat form of bwh_export: fr (n_fr x 4: i0, j0, i_end, j_end
+ * in points), lr (n_lr x 5: the same + rank in scalar columns), the FR blocks
+ * back to back and per LR block A then B (column-major, no padding).
+ * lr_error: n_lr values or NULL.  The HPattern spot of block k is stored as k. */
+int bw_file_write(const char *path, int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0,
+                  const int64_t *perm1, int64_t n_fr, const int64_t *fr, const double *fr_data, int64_t n_lr,
+                  const int64_t *lr, const double *lr_data, const double *lr_error);
+
+/* Write from per-block pointers, as an Hmat holds them: fr_pattern /
+ * lr_pattern are HPattern columns (n x 6, FRB_pattern / LRB_pattern of
+ * h_pattern.h:21-33 with LR flag = rank in scalar columns, hmat.cc:390); block
+ * k is column-major at fr[k] with leading dimension fr_ld[k] (>= its rows),
+ * its factors at lr_a[k] (ld lr_a_ld[k]) and lr_b[k] (ld lr_b_ld[k]). */
+int bw_file_write_blocks(const char *path, int dof, int64_t n_rows, int64_t n_cols, const int64_t *perm0,
+                         const int64_t *perm1, int64_t n_fr, const int64_t *fr_pattern, const double *const *fr,
+                         const int64_t *fr_ld, int64_t n_lr, const int64_t *lr_pattern, const double *const *lr_a,
+                         const int64_t *lr_a_ld, const double *const *lr_b, const int64_t *lr_b_ld,
+                         const double *lr_error);
+
+/* Header of a block file (the header checksum, section bounds, pattern and
+ * permutations are checked): info[0..8] = dof, n_rows, n_cols, n_fr, n_lr,
+ * FR entries, LR entries, 1 if ACA error estimates are stored, file bytes. */
+int bw_file_info(const char *path, int64_t info[9]);
+
+/* Copy a block file out in the flat form of bw_file_write (array sizes from
+ * bw_file_info); lr_error may be NULL (zeros are written when the file has
+ * none).  fr_pattern / lr_pattern (n x 6 HPattern columns) may be NULL.
+ * verify != 0 also checks the block data checksums. */
+int bw_file_read(const char *path, int verify, int64_t *fr, int64_t *lr, double *fr_data, double *lr_data,
+                 int64_t *perm0, int64_t *perm1, double *lr_error, int64_t *fr_pattern, int64_t *lr_pattern);
+
+/* Create a handle from a block file: bw_create with the file's sizes and
+ * permutations, then every block registered as bw_add_full / bw_add_lowrank
+ * would, borrowing the mapped file (no copy) until bw_finalize succeeds or the
+ * handle is destroyed.  Call bw_set_tuning / bw_set_device_limit and
+ * bw_finalize on it as usual.  verify != 0 checks the block data checksums
+ * first (one pass over the file). */
+int bw_create_from_file(const char *path, int device, int verify, bw_hmat **out);
 
 /* Release everything. */
 int bw_destroy(bw_hmat *h);

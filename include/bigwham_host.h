@@ -78,6 +78,13 @@ int64_t bwh_entries(const bwh_io *io, int kind);
 int bwh_export(const bwh_io *io, int64_t *fr, int64_t *lr, double *fr_data, double *lr_data, int64_t *perm0,
                int64_t *perm1);
 
+/* Save the built H-matrix as a block file (bw_file_write_blocks of
+ * include/bigwham_b200.h: pattern with its HPattern spots, permutations, every
+ * block and the ACA error estimates), before bwh_attach_gpu.  The content of
+ * the reference's Hmat::writeToFile (src/hmat/hmatrix/hmat.cc:749-835), which
+ * needs HDF5.  Load it with bw_create_from_file / HmatGpu.from_file. */
+int bwh_write_to_file(const bwh_io *io, const char *path);
+
 /* The device H-matrix after bwh_attach_gpu (owned by io), for the
  * extensions of include/bigwham_b200.h (precision choice, H^T, matmat). */
 struct bw_hmat *bwh_gpu_handle(bwh_io *io);

@@ -1,13 +1,13 @@
 """The N > 1 path of bench.py (replicas) on CPU: 2 processes over gloo.
 
 bench.py --gpus N runs N independent replicas.
-* Rank 0 builds the H-matrix once with the reference's host code and places
-  the exported blocks in /dev/shm.
-* Every rank maps them and lays out its own copy.
+* Rank 0 builds the H-matrix once with the reference's host code and writes
+  it as a block file (/dev/shm by default).
+* Every rank maps the file and lays out its own copy (HmatGpu.from_file).
 * Timings are reduced with a max over ranks.
 Here each rank lays the blocks out as a host plan and replays a matvec.  The
 two ranks must agree bitwise and match the oracle.  max_over_ranks must return
-the largest rank value, and the shared files must be gone afterwards.
+the largest rank value, and the shared file must be gone afterwards.
 """
 import os
 import socket
@@ -28,7 +28,7 @@ def _worker(rank, world, port, out_dir):
     import torch.distributed as dist
 
     import bench
-    from bigwham_dev_b200 import HmatGpu
+    from bigwham_dev_b200 import HmatGpu, blockfile
     from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
     from bigwham_dev_b200.meshes import square_crack_3d
     from oracle import HmatArrays, oracle_matvec_perm
@@ -37,30 +37,26 @@ def _worker(rank, world, port, out_dir):
     w, r, _ = bench.dist_setup(world, backend="gloo")
     coor, conn = square_crack_3d(12)
 
-    def build(alloc):
+    def build(path):
         io = BigWhamIOGpu(coor, conn, "3DR0-H", [1.0, 0.25], 2, useCuda=False)
         io.build_hierarchical_matrix(32, 3.0, 1e-5)
-        ex = io.export_blocks(alloc)
+        io.write_to_file(path)
         io.close()
-        return ex
 
-    tag = f"test_{port}"
-    meta, arr, release = bench.shared_blocks(w, r, tag, build)
-    h = HmatGpu(meta["dof"], meta["n_rows"], meta["n_cols"], arr["perm0"], arr["perm1"], device=-1)
-    h.add_flat(arr["fr"], arr["lr"], arr["fr_data"], arr["lr_data"])
-    h.finalize(plan_only=True, precisions=("fp64",))
-    x = np.random.default_rng(0).uniform(-1, 1, meta["n_cols"])
+    path = os.path.join(out_dir, f"blocks_{port}.bwb")
+    release = bench.shared_block_file(w, r, path, build)
+    h = HmatGpu.from_file(path, device=-1, plan_only=True, precisions=("fp64",))
+    ex = blockfile.read(path)
+    x = np.random.default_rng(0).uniform(-1, 1, ex["n_cols"])
     y = replay(h, x, "fp64")
-    flat = HmatArrays(meta["dof"], meta["n_rows"], meta["n_cols"], np.array(arr["fr"]), np.array(arr["lr"]),
-                      np.array(arr["fr_data"]), np.array(arr["lr_data"]), np.array(arr["perm0"]),
-                      np.array(arr["perm1"]))
+    flat = HmatArrays(ex["dof"], ex["n_rows"], ex["n_cols"], ex["fr"], ex["lr"], ex["fr_data"], ex["lr_data"],
+                      ex["perm0"], ex["perm1"])
     y_or = oracle_matvec_perm(flat, x, 1)
     release()
     m = bench.max_over_ranks(float(r + 1), w, device="cpu")
     np.save(os.path.join(out_dir, f"y{r}.npy"), y)
     np.save(os.path.join(out_dir, f"info{r}.npy"),
-            np.array([m, np.linalg.norm(y - y_or) / np.linalg.norm(y_or),
-                      float(os.path.exists(os.path.join("/dev/shm", f"bw_blocks_{tag}")))]))
+            np.array([m, np.linalg.norm(y - y_or) / np.linalg.norm(y_or), float(os.path.exists(path))]))
     dist.destroy_process_group()
 
 
