@@ -1353,8 +1353,7 @@ int bw_file_read(const char *path, int verify, int64_t *fr, int64_t *lr, double 
     if (!path) throw std::invalid_argument("null path");
     auto f = bw::BlockFile::open(path, verify != 0);
     const bw::FileHeader &h = f->header();
-    if ((h.n_fr && (!fr || !fr_data)) || (h.n_lr && (!lr || !lr_data)) || (h.n_rows && !perm0) ||
-        (h.n_cols && !perm1))
+    if ((h.n_fr && !fr) || (h.n_lr && !lr) || (h.n_rows && !perm0) || (h.n_cols && !perm1))
       throw std::invalid_argument("null output array");
     const int64_t *fp = f->fr_pattern(), *lp = f->lr_pattern();
     for (int64_t k = 0; k < h.n_fr; k++)
@@ -1371,8 +1370,8 @@ int bw_file_read(const char *path, int verify, int64_t *fr, int64_t *lr, double 
       else
         std::fill(lr_error, lr_error + h.n_lr, 0.0);
     }
-    par_copy(fr_data, f->fr_data(), 8 * h.fr_entries);
-    par_copy(lr_data, f->lr_data(), 8 * h.lr_entries);
+    if (fr_data) par_copy(fr_data, f->fr_data(), 8 * h.fr_entries);
+    if (lr_data) par_copy(lr_data, f->lr_data(), 8 * h.lr_entries);
     return BW_OK;
   });
 }

@@ -18,7 +18,6 @@
 #include <string>
 #include <utility>
 #include <vector>
-#include <vector>
 
 #include "bigwham_b200.h"
 #include "hmat/hmatrix/hmat.h"
@@ -31,6 +30,14 @@ class HmatGpu : public bigwham::Hmat<double> {
   // std::runtime_error when the upload fails.
   // tuning: plan parameters passed to bw_set_tuning before bw_finalize.
   HmatGpu(const std::shared_ptr<bigwham::Hmat<double>> &cpu, int device, int storage,
+          const std::vector<std::pair<std::string, int64_t>> &tuning = {});
+  // From a block file written by write_block_file (or bw_file_write): the
+  // counterpart of the reference's Hmat(filename) constructor
+  // (src/hmat/hmatrix/hmat.cc:64-74, readFromFile :837-935), without HDF5.
+  // The device blocks are uploaded straight from the mapped file (checksums
+  // verified); the pattern, permutations, FR blocks (for fullBlocksOriginal)
+  // and ACA error estimates are restored on the host.
+  HmatGpu(const std::string &filename, int device, int storage,
           const std::vector<std::pair<std::string, int64_t>> &tuning = {});
   ~HmatGpu() override;
   HmatGpu(const HmatGpu &) = delete;
@@ -59,5 +66,12 @@ class HmatGpu : public bigwham::Hmat<double> {
   int precision_ = BW_FP64;
   il::int_t entries_ = 0;
 };
+
+// Save a built Hmat as a block file: the content of the reference's
+// Hmat::writeToFile (src/hmat/hmatrix/hmat.cc:749-835), without HDF5
+// (bw_file_write_blocks; the file is written whole or not at all).  Works
+// for a CPU Hmat before it is replaced by an HmatGpu.  Throws
+// std::runtime_error on failure.
+void write_block_file(const bigwham::Hmat<double> &hmat, const std::string &filename);
 
 }  // namespace bigwham_b200

@@ -223,50 +223,7 @@ int bwh_write_to_file(const bwh_io *h, const char *path) {
   if (!h || !path) return fail("null argument");
   if (h->gpu) return fail("bwh_write_to_file must run before bwh_attach_gpu (the host blocks are released there)");
   return guarded([&] {
-    auto hm = h->io->getHmat();
-    const bigwham::HPattern &p = hm->pattern();
-    auto hr = hm->get_hr();
-    const auto &frs = hm->get_full_rank_blocks();
-    const auto &lrs = hm->get_low_rank_blocks();
-    const il::int_t dof = hm->get_dof_dimension();
-    std::vector<int64_t> frp(6 * p.n_FRB), lrp(6 * p.n_LRB), fld(p.n_FRB), ald(p.n_LRB), bld(p.n_LRB);
-    std::vector<const double *> fb(p.n_FRB), ab(p.n_LRB), bb(p.n_LRB);
-    std::vector<double> err(p.n_LRB);
-    for (il::int_t k = 0; k < p.n_FRB; k++) {
-      for (int r = 0; r < 6; r++) frp[6 * k + r] = p.FRB_pattern(r, k);
-      const il::Array2D<double> &a = *frs[(size_t)k];
-      if (a.size(0) != (p.FRB_pattern(3, k) - p.FRB_pattern(1, k)) * dof ||
-          a.size(1) != (p.FRB_pattern(4, k) - p.FRB_pattern(2, k)) * dof)
-        throw std::runtime_error("FR block " + std::to_string(k) + " disagrees with its pattern");
-      fb[k] = a.data();
-      fld[k] = std::max<il::int_t>(1, a.capacity(0));
-    }
-    for (il::int_t k = 0; k < p.n_LRB; k++) {
-      for (int r = 0; r < 6; r++) lrp[6 * k + r] = p.LRB_pattern(r, k);
-      const bigwham::LowRank<double> &lr = *lrs[(size_t)k];
-      const il::int_t rank = lr.A.size(1);
-      if (rank != p.LRB_pattern(5, k) || lr.B.size(0) != rank ||
-          lr.A.size(0) != (p.LRB_pattern(3, k) - p.LRB_pattern(1, k)) * dof ||
-          lr.B.size(1) != (p.LRB_pattern(4, k) - p.LRB_pattern(2, k)) * dof)
-        throw std::runtime_error("LR block " + std::to_string(k) + " disagrees with its pattern");
-      ab[k] = lr.A.data();
-      ald[k] = std::max<il::int_t>(1, lr.A.capacity(0));
-      bb[k] = lr.B.data();
-      bld[k] = std::max<il::int_t>(1, lr.B.capacity(0));
-      err[k] = lr.error_on_approximation;
-    }
-    std::vector<int64_t> p0(hr->permutation_0_.size()), p1(hr->permutation_1_.size());
-    for (size_t i = 0; i < p0.size(); i++) p0[i] = hr->permutation_0_[(il::int_t)i];
-    for (size_t i = 0; i < p1.size(); i++) p1[i] = hr->permutation_1_[(il::int_t)i];
-    const auto size = hm->get_size();
-    const int st = bw_file_write_blocks(path, (int)dof, size[0], size[1], p0.data(), p1.data(), p.n_FRB, frp.data(),
-                                        fb.data(), fld.data(), p.n_LRB, lrp.data(), ab.data(), ald.data(), bb.data(),
-                                        bld.data(), err.data());
-    if (st != BW_OK) {
-      char buf[512];
-      bw_last_error(nullptr, buf, sizeof buf);
-      return fail(std::string("bwh_write_to_file: ") + buf, st);
-    }
+    bigwham_b200::write_block_file(*h->io->getHmat(), path);
     return 0;
   });
 }

@@ -299,9 +299,10 @@ int bw_file_write_blocks(const char *path, int dof, int64_t n_rows, int64_t n_co
 int bw_file_info(const char *path, int64_t info[9]);
 
 /* Copy a block file out in the flat form of bw_file_write (array sizes from
- * bw_file_info); lr_error may be NULL (zeros are written when the file has
- * none).  fr_pattern / lr_pattern (n x 6 HPattern columns) may be NULL.
- * verify != 0 also checks the block data checksums. */
+ * bw_file_info).  fr_data / lr_data may be NULL to leave that block data in
+ * the file; lr_error may be NULL (zeros are written when the file has none);
+ * fr_pattern / lr_pattern (n x 6 HPattern columns) may be NULL.  verify != 0
+ * also checks the block data checksums. */
 int bw_file_read(const char *path, int verify, int64_t *fr, int64_t *lr, double *fr_data, double *lr_data,
                  int64_t *perm0, int64_t *perm1, double *lr_error, int64_t *fr_pattern, int64_t *lr_pattern);
 

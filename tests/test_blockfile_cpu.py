@@ -11,11 +11,15 @@ A block file holds what the reference's Hmat::writeToFile stores
   empty patterns;
 * corrupt, truncated, foreign and missing files, and inconsistent arguments,
   are rejected with BW_ERR_IO / BW_ERR_ARG, and a failed write leaves no file;
-* the header checksum follows the documented algorithm (a Python restatement).
+* the header checksum follows the documented algorithm (a Python restatement);
+* the C++ API (write_block_file, HmatGpu(filename)) restores the Hmat state
+  and BigWhamIO's queries bitwise (tests/cpp/hmat_file_check.cc, built from
+  the reference sources when they are present).
 """
 import ctypes as C
 import os
 import struct
+import subprocess
 
 import numpy as np
 import pytest
@@ -47,6 +51,21 @@ def crack(tmp_path_factory):
     nblk = io.n_blocks()
     io.close()
     return ex, str(path), nblk
+
+
+REF = os.environ.get("BIGWHAM_REF", "/root/reference")
+
+
+@needs_host
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src")), reason="reference sources not present")
+def test_cpp_file_constructor_restores_the_hmat(tmp_path):
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "bigwham_dev_b200", "host"), f"REF={REF}", "check"],
+                       capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    r = subprocess.run([os.path.join(ROOT, "_build", "hmat_file_check"), str(tmp_path / "c.bwb")],
+                       capture_output=True, text=True, timeout=300)
+    lines = r.stdout.strip().splitlines()
+    assert r.returncode == 0 and lines and lines[-1].startswith("ok "), r.stdout + r.stderr
 
 
 def _rel(a, b):
