@@ -53,7 +53,9 @@ class Gmres:
 
     op(x, y): writes op applied to x into y (both CUDA float64, length n),
     stream-ordered on the current torch stream; called at capture time.
-    minv: optional CUDA float64 vector, right Jacobi preconditioner (diag^-1).
+    minv: optional right preconditioner M^-1: a CUDA float64 vector (Jacobi,
+    diag^-1, applied elementwise) or a callable minv(x, out) with op's
+    conventions (e.g. precond.BlockJacobi).
     """
 
     def __init__(self, op, n: int, restart: int = 50, minv=None, device="cuda", use_graph: bool = True):
@@ -74,10 +76,7 @@ class Gmres:
         """m Arnoldi steps from V[0]; fills V and H (FP64)."""
         V, H, z, w = self.V, self.H, self.z, self.w
         for j in range(self.m):
-            if self.minv is not None:
-                self.torch.mul(V[j], self.minv, out=z)
-            else:
-                z.copy_(V[j])
+            self._precondition(V[j], z)
             self.op(z, w)
             Vj = V[:j + 1]
             h = Vj @ w
@@ -88,6 +87,14 @@ class Gmres:
             nrm = self.torch.linalg.vector_norm(w)
             H[j + 1, j] = nrm
             self.torch.div(w, nrm, out=V[j + 1])
+
+    def _precondition(self, v, out):
+        if self.minv is None:
+            out.copy_(v)
+        elif callable(self.minv):
+            self.minv(v, out)
+        else:
+            self.torch.mul(v, self.minv, out=out)
 
     def _run_cycle(self):
         torch = self.torch
@@ -138,9 +145,8 @@ class Gmres:
             info.iterations += self.m
             yt = torch.from_numpy(y).to(b.device)
             upd = self.V[:k].t() @ yt
-            if self.minv is not None:
-                upd.mul_(self.minv)
-            x.add_(upd)
+            self._precondition(upd, self.z)
+            x.add_(self.z)
             if res <= tol * bnorm and residual_op is None:
                 info.residuals.append(res / bnorm)
                 info.converged = True

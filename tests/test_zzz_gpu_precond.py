@@ -1,0 +1,57 @@
+"""Block-Jacobi preconditioner on the GPU (-m gpu).
+
+On every golden case:
+* applying M^-1 on the device (original ordering, FP64 inverses) equals the
+  host composition P1^T blockdiag(D_k^-1) P0 x to 1e-13;
+* GMRES(30) with M^-1 captured in the cycle's CUDA graph reaches a true
+  relative residual of 1e-10, in no more Arnoldi steps than with point
+  Jacobi (the reference's BEMatrix.H_jacobi_prec).
+"""
+import numpy as np
+import pytest
+from conftest import rel
+
+from bigwham_dev_b200 import HmatGpu
+from bigwham_dev_b200.precond import BlockJacobi, diagonal_blocks, inverted_blocks
+from bigwham_dev_b200.solve import Gmres
+
+pytestmark = pytest.mark.gpu
+
+
+def test_block_jacobi_apply_and_gmres(golden):
+    import torch
+
+    arr, _ = golden
+    flat = {"dof": arr.dof, "n_rows": arr.n_rows, "n_cols": arr.n_cols, "fr": arr.fr, "lr": arr.lr,
+            "fr_data": arr.fr_data, "lr_data": arr.lr_data, "perm0": arr.perm0, "perm1": arr.perm1}
+    n, d = arr.n_rows, arr.dof
+    h = HmatGpu.from_flat(arr.dof, n, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0, arr.perm1,
+                          device=0, precisions=("fp64",))
+    bj = BlockJacobi(flat, device=0)
+    rng = np.random.default_rng(12)
+    x = rng.uniform(-1, 1, n)
+    xp = x[(d * np.asarray(arr.perm0)[:, None] + np.arange(d)).ravel()]
+    yp = np.empty(n)
+    for s, Dinv in inverted_blocks(flat, diagonal_blocks(flat)):
+        yp[s:s + Dinv.shape[0]] = Dinv @ xp[s:s + Dinv.shape[0]]
+    want = np.empty(n)
+    want[(d * np.asarray(arr.perm1)[:, None] + np.arange(d)).ravel()] = yp
+    out = torch.empty(n, dtype=torch.float64, device="cuda")
+    bj(torch.from_numpy(x).cuda(), out)
+    torch.cuda.synchronize()
+    assert rel(out.cpu().numpy(), want) < 1e-13
+
+    def op(v, w):
+        h.matvec(v, "fp64", out=w)
+
+    b = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+    steps = {}
+    for name, minv in (("jacobi", torch.from_numpy(1.0 / h.diagonal()).cuda()), ("block", bj)):
+        sol, info = Gmres(op, n, restart=30, minv=minv).solve(b, tol=1e-10, maxiter=3000)
+        r = b - h.matvec(sol, "fp64")
+        torch.cuda.synchronize()
+        assert info.converged and float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b)) < 2e-10
+        steps[name] = info.iterations
+    assert steps["block"] <= steps["jacobi"], steps
+    h.sync()
+    bj.close()
