@@ -1,0 +1,51 @@
+"""Rectangular and irregular H-matrices through the layout (host plan).
+
+Hmat::matvec (src/hmat/hmatrix/hmat.cc:472-537) does not assume a square
+matrix: BigWhamIO's rectangular constructor (src/io/bigwham_io.h:85-96) pairs
+a source mesh with a different receiver mesh.  The reference's own CUDA path
+aborts on non-square matrices (hmat_cuda.cc:1358-1362); this backend lays
+them out like square ones.  Synthetic quadtree partitions (tests/synth.py)
+with n_rows != n_cols, dof 1-3, odd block shapes and ragged ranks; the
+replayed plan must match the oracle in FP64 (1e-14) for H and H^T, and the
+reduced precisions within their rounding bounds.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle_matvec_perm, oracle_rmatvec_perm
+from planreplay import replay
+from synth import synthetic_hmat
+
+from bigwham_dev_b200 import HmatGpu
+
+SHAPES = [(40, 25, 2), (17, 60, 3), (64, 64, 1), (1, 9, 3), (33, 1, 2)]
+TOL = {"fp64": 1e-14, "fp32": 2e-6, "bf16": 1e-2}
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("npr,npc,dof", SHAPES)
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "bf16"])
+def test_rectangular_plan_matches_the_oracle(npr, npc, dof, precision):
+    arr = synthetic_hmat(npr, npc, dof, seed=npr * 100 + npc)
+    h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
+                          arr.perm1, device=-1, plan_only=True, precisions=(precision,), transpose=True)
+    x = np.random.default_rng(2).uniform(-1, 1, arr.n_cols)
+    xr = np.random.default_rng(3).uniform(-1, 1, arr.n_rows)
+    assert _rel(replay(h, x, precision), oracle_matvec_perm(arr, x, 1)) < TOL[precision]
+    assert _rel(replay(h, xr, precision, True), oracle_rmatvec_perm(arr, xr, 1)) < TOL[precision]
+
+
+def test_dense_single_block_and_all_low_rank():
+    """Degenerate partitions: one full-rank block; only low-rank blocks."""
+    one = synthetic_hmat(5, 7, 3, seed=9, leaf=100)
+    assert len(one.fr) + len(one.lr) == 1
+    lr_only = synthetic_hmat(32, 24, 2, seed=4, leaf=4, stop=0.0, lr_share=1.0)
+    assert len(lr_only.fr) == 0 and len(lr_only.lr) > 10
+    for arr in (one, lr_only):
+        h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
+                              arr.perm1, device=-1, plan_only=True, precisions=("fp64",))
+        x = np.random.default_rng(5).uniform(-1, 1, arr.n_cols)
+        assert _rel(replay(h, x, "fp64"), oracle_matvec_perm(arr, x, 1)) < 1e-14
