@@ -114,8 +114,27 @@ def _ref():
         lib.ref_dense_rows.argtypes = [C.c_void_p, C.c_char_p, _f64p, _i64p, C.c_int64, _f64p]
         lib.ref_collocation_points.restype = C.c_int64
         lib.ref_destroy.argtypes = [C.c_void_p]
+        lib.ref_r0_stress.argtypes = [C.c_double] * 7 + [_f64p]
+        lib.ref_r0_displacement.argtypes = [C.c_double] * 6 + [_f64p]
         _ref_lib = lib
     return _ref_lib
+
+
+def ref_r0_stress(x, y, z, a, b, G, nu):
+    """The reference's StressesKernelR0: (3, 6) stresses (rows DD x, y, z;
+    columns xx, yy, zz, xy, xz, yz) at (x, y, z) in a rectangle's local frame."""
+    out = np.zeros(18)
+    if _ref().ref_r0_stress(x, y, z, a, b, G, nu, out) != 0:
+        raise RuntimeError("ref_r0_stress failed")
+    return out.reshape(3, 6)
+
+
+def ref_r0_displacement(x, y, z, a, b, nu):
+    """The reference's DisplacementKernelR0 as its 3 x 3 array."""
+    out = np.zeros(9)
+    if _ref().ref_r0_displacement(x, y, z, a, b, nu, out) != 0:
+        raise RuntimeError("ref_r0_displacement failed")
+    return out.reshape(3, 3)
 
 
 class RefHmat:

@@ -21,6 +21,7 @@
 #include "elasticity/bie_elastostatic.h"
 #include "elasticity/fullspace_iso_2d_segment/bie_elastostatic_segment_0_influence.h"
 #include "elasticity/fullspace_iso_3d_rectangle/bie_elastostatic_rectangle_0_influence.h"
+#include "elasticity/fullspace_iso_3d_rectangle/elastic_3dR0_element.h"
 #include "elasticity/fullspace_iso_3d_triangle/bie_elastostatic_triangle_0_influence.h"
 #include "elements/rectangle.h"
 #include "elements/segment.h"
@@ -215,5 +216,33 @@ int64_t ref_collocation_points(void *h, double *out) {
 }
 
 void ref_destroy(void *h) { delete H(h); }
+
+// The reference's rectangular (3DR0) point kernels, for checking a
+// restatement of them: stresses at (x, y, z) in the local frame of a
+// [-a, a] x [-b, b] rectangle at z = 0 carrying unit displacement
+// discontinuities (StressesKernelR0, elastic_3dR0_element.h), out[6 * dd + c]
+// with c = xx, yy, zz, xy, xz, yz; displacements (DisplacementKernelR0),
+// out[3 * i + j] = entry (i, j) of the reference's 3 x 3 array.
+int ref_r0_stress(double x, double y, double z, double a, double b, double G, double nu, double *out) {
+  try {
+    il::StaticArray2D<double, 3, 6> s = bigwham::StressesKernelR0(x, y, z, a, b, G, nu);
+    for (int i = 0; i < 3; i++)
+      for (int c = 0; c < 6; c++) out[6 * i + c] = s(i, c);
+    return 0;
+  } catch (...) {
+    return 3;
+  }
+}
+
+int ref_r0_displacement(double x, double y, double z, double a, double b, double nu, double *out) {
+  try {
+    il::Array2D<double> u = bigwham::DisplacementKernelR0(x, y, z, a, b, nu);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) out[3 * i + j] = u(i, j);
+    return 0;
+  } catch (...) {
+    return 3;
+  }
+}
 
 }  // extern "C"
