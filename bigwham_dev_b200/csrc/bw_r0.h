@@ -209,5 +209,39 @@ BW_HD void displacement(double x, double y, double z, double a, double b, double
   u[2][2] = c * (k1 * D.z - z * D.zz);
 }
 
+// Hypersingular (H) kernel entry between two rectangles: tractions at the
+// receiver's collocation point, in the receiver's local frame, due to unit
+// DDs of the source in the source's local frame; K[j][i] = traction j due to
+// DD i.  Frames as BigWham's elements hold them: rot is row-major with
+// local = rot * global; cp the collocation point (centroid), n_r the
+// receiver's unit normal, (a_s, b_s) the source's half sides along its local
+// x and y.  The steps are those of the reference's
+// BieElastostatic<Rectangle<0>, Rectangle<0>, H>::influence
+// (src/elasticity/fullspace_iso_3d_rectangle/
+// bie_elastostatic_rectangle_0_influence.h:29-125): stresses at the receiver
+// point in the source frame, traction on the receiver normal, rotated to
+// global and then to the receiver frame.
+BW_HD void influence_h(const double *cp_s, const double *rot_s, double a_s, double b_s, const double *cp_r,
+                       const double *rot_r, const double *n_r, double G, double nu, double K[3][3]) {
+  double d[3], dl[3], nl[3];
+  for (int k = 0; k < 3; k++) d[k] = cp_r[k] - cp_s[k];
+  for (int r = 0; r < 3; r++) {
+    dl[r] = rot_s[3 * r] * d[0] + rot_s[3 * r + 1] * d[1] + rot_s[3 * r + 2] * d[2];
+    nl[r] = rot_s[3 * r] * n_r[0] + rot_s[3 * r + 1] * n_r[1] + rot_s[3 * r + 2] * n_r[2];
+  }
+  double s[3][6];
+  stress(dl[0], dl[1], dl[2], a_s, b_s, G, nu, s);
+  for (int i = 0; i < 3; i++) {
+    // traction on nl in the source frame (symmetric tensor xx yy zz xy xz yz)
+    const double t0 = s[i][0] * nl[0] + s[i][3] * nl[1] + s[i][4] * nl[2];
+    const double t1 = s[i][3] * nl[0] + s[i][1] * nl[1] + s[i][5] * nl[2];
+    const double t2 = s[i][4] * nl[0] + s[i][5] * nl[1] + s[i][2] * nl[2];
+    // to global (rot_s^T) and to the receiver frame (rot_r)
+    double g[3];
+    for (int k = 0; k < 3; k++) g[k] = rot_s[k] * t0 + rot_s[3 + k] * t1 + rot_s[6 + k] * t2;
+    for (int j = 0; j < 3; j++) K[j][i] = rot_r[3 * j] * g[0] + rot_r[3 * j + 1] * g[1] + rot_r[3 * j + 2] * g[2];
+  }
+}
+
 }  // namespace r0
 }  // namespace bw

@@ -114,6 +114,7 @@ def _ref():
         lib.ref_dense_rows.argtypes = [C.c_void_p, C.c_char_p, _f64p, _i64p, C.c_int64, _f64p]
         lib.ref_collocation_points.restype = C.c_int64
         lib.ref_destroy.argtypes = [C.c_void_p]
+        lib.ref_element_frames.argtypes = [C.c_void_p, _f64p]
         lib.ref_r0_stress.argtypes = [C.c_double] * 7 + [_f64p]
         lib.ref_r0_displacement.argtypes = [C.c_double] * 6 + [_f64p]
         _ref_lib = lib
@@ -193,6 +194,17 @@ class RefHmat:
         rc = lib.ref_dense_rows(self._h, kernel.encode(), props, pts, pts.size, out)
         if rc != 0:
             raise RuntimeError(f"ref_dense_rows failed ({rc})")
+        return out
+
+    def element_frames(self):
+        """(n_elements, 15): collocation point, row-major rotation matrix
+        (local = R global) and unit normal of each element, from the
+        reference's element objects (3D meshes, one collocation point per
+        element)."""
+        n = self.shape[1] // self.dof
+        out = np.empty((n, 15))
+        if _ref().ref_element_frames(self._h, out) != 0:
+            raise RuntimeError("ref_element_frames failed")
         return out
 
     def collocation_points(self):

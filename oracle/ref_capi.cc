@@ -217,6 +217,29 @@ int64_t ref_collocation_points(void *h, double *out) {
 
 void ref_destroy(void *h) { delete H(h); }
 
+// Per element of the handle's (source) mesh, 15 values: collocation point
+// (3), rotation matrix row-major (9; local = R global, BoundaryElement::
+// ConvertToLocal) and unit normal (3), as the reference's elements hold them
+// (BigWhamIO::GetCollocationPoints / GetRotationMatrix / GetElementNormals,
+// src/io/bigwham_io.cc:985-1140).  One collocation point per element only.
+int ref_element_frames(void *h, double *out) {
+  try {
+    BigWhamIO &io = *H(h)->io;
+    const std::vector<double> cp = io.GetCollocationPoints(), rot = io.GetRotationMatrix(),
+                              nrm = io.GetElementNormals();
+    const size_t ne = nrm.size() / 3;
+    if (cp.size() != 3 * ne || rot.size() != 9 * ne) return 1;
+    for (size_t e = 0; e < ne; e++) {
+      for (int k = 0; k < 3; k++) out[15 * e + k] = cp[3 * e + k];
+      for (int k = 0; k < 9; k++) out[15 * e + 3 + k] = rot[9 * e + k];
+      for (int k = 0; k < 3; k++) out[15 * e + 12 + k] = nrm[3 * e + k];
+    }
+    return 0;
+  } catch (...) {
+    return 3;
+  }
+}
+
 // The reference's rectangular (3DR0) point kernels, for checking a
 // restatement of them: stresses at (x, y, z) in the local frame of a
 // [-a, a] x [-b, b] rectangle at z = 0 carrying unit displacement

@@ -18,4 +18,13 @@ void probe_r0_displacement(double x, double y, double z, double a, double b, dou
     for (int j = 0; j < 3; j++) out[3 * i + j] = u[i][j];
 }
 
+void probe_r0_influence(const double *frame_s, double a_s, double b_s, const double *frame_r, double G, double nu,
+                        double *out) {
+  // frame: collocation point (3), row-major rotation (9), normal (3)
+  double K[3][3];
+  bw::r0::influence_h(frame_s, frame_s + 3, a_s, b_s, frame_r, frame_r + 3, frame_r + 12, G, nu, K);
+  for (int j = 0; j < 3; j++)
+    for (int i = 0; i < 3; i++) out[3 * j + i] = K[j][i];
+}
+
 }  // extern "C"
