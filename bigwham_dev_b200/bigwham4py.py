@@ -51,6 +51,7 @@ _HSIGS = {
     "bwh_entries": (_I64, [_P, C.c_int]),
     "bwh_export": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "bwh_write_to_file": (C.c_int, [_P, C.c_char_p]),
+    "bwh_element_frames": (_I64, [_P, _P]),
     "bwh_gpu_handle": (_P, [_P]),
     "bwh_destroy": (C.c_int, [_P]),
     "bwh_last_error": (C.c_char_p, []),
@@ -97,6 +98,7 @@ class BigWhamIOGpu:
                             C.byref(h)))
         self._h = h
         self._L = L
+        self._coor, self._conn = coor, conn  # mesh, for element_records
         self.kernel = kernel
         self.use_cuda = bool(useCuda)
         self.device = int(device)
@@ -211,6 +213,23 @@ class BigWhamIOGpu:
         _check(self._L.bwh_export(self._h, *(out[k].ctypes.data for k in
                                              ("fr", "lr", "fr_data", "lr_data", "perm0", "perm1"))))
         return out
+
+    def element_records(self):
+        """(n_elements, 17) records of the device assembly (bw_r0_assemble_fr):
+        collocation point, rotation matrix (row-major, local = R global) and
+        unit normal from the reference's element objects, then the half sides
+        |v1 - v0| / 2 and |v3 - v0| / 2 of each quadrilateral (the reference's
+        get_a_and_b, elastic_3dR0_common.cc:443-468)."""
+        n = int(self._L.bwh_element_frames(self._h, None))
+        if n < 0:
+            _check(1)
+        fr = np.empty((n, 15))
+        self._L.bwh_element_frames(self._h, fr.ctypes.data)
+        v = np.asarray(self._coor, dtype=np.float64).reshape(-1, 3)[np.asarray(self._conn).reshape(n, -1)]
+        if v.shape[1] != 4:
+            raise ValueError("element records need quadrilateral (3DR0) elements")
+        ab = np.stack([np.linalg.norm(v[:, 1] - v[:, 0], axis=1), np.linalg.norm(v[:, 3] - v[:, 0], axis=1)], 1) / 2
+        return np.ascontiguousarray(np.hstack([fr, ab]))
 
     def write_to_file(self, path) -> None:
         """Save the built H-matrix as a block file (before attach_gpu): the

@@ -13,6 +13,7 @@
 #include "bigwham_b200.h"
 #include "bw_kernels.cuh"
 #include "bw_mm_kernels.cuh"
+#include "bw_assemble_kernels.cuh"
 #include "bw_file.h"
 #include "bw_layout.h"
 
@@ -1226,6 +1227,22 @@ template <typename F> int file_guarded(F &&f) {
   }
 }
 
+// Handle-less device entries: as file_guarded, with CUDA and allocation
+// failures reported as such.
+template <typename F> int device_guarded(F &&f) {
+  try {
+    return f();
+  } catch (const CudaError &e) {
+    return file_fail(e.what(), BW_ERR_CUDA);
+  } catch (const OomError &e) {
+    return file_fail(e.what(), BW_ERR_OOM);
+  } catch (const std::bad_alloc &) {
+    return file_fail("host allocation failed", BW_ERR_OOM);
+  } catch (const std::exception &e) {
+    return file_fail(e.what(), BW_ERR_ARG);
+  }
+}
+
 // Block extent in scalar units from pattern coordinates in points; throws
 // unless 0 <= a0 < a1 <= limit.
 int64_t extent(int64_t a0, int64_t a1, int64_t limit, int64_t dof, const char *what, int64_t k) {
@@ -1416,6 +1433,71 @@ int bw_create_from_file(const char *path, int device, int verify, bw_hmat **out)
   h->borrowed = f;
   *out = h;
   return BW_OK;
+}
+
+int bw_r0_assemble_fr(int device, int64_t n_elems, const double *records, double G, double nu, int64_t n_fr,
+                      const int64_t *fr, const int64_t *perm, int64_t n_points, double *out, int64_t out_len,
+                      void *stream) {
+  return device_guarded([&] {
+    if (!records || n_elems < 1 || n_fr < 0 || n_points < 1 || (n_fr && (!fr || !perm || !out)))
+      throw std::invalid_argument("bw_r0_assemble_fr: null or empty argument");
+    if (n_elems >= (int64_t(1) << 31) || n_points >= (int64_t(1) << 31))
+      throw std::invalid_argument("bw_r0_assemble_fr: more than 2^31 elements");
+    if (!(G > 0.0) || !(nu > -1.0 && nu < 0.5)) throw std::invalid_argument("bw_r0_assemble_fr: bad G or nu");
+    // every index the kernel reads or writes is checked here
+    std::vector<int32_t> p32(n_points);
+    for (int64_t i = 0; i < n_points; i++) {
+      if (perm[i] < 0 || perm[i] >= n_elems) throw std::invalid_argument("bw_r0_assemble_fr: perm out of range");
+      p32[i] = (int32_t)perm[i];
+    }
+    std::vector<bw::AsmBlock> blocks(n_fr);
+    std::vector<bw::AsmTile> tiles;
+    int64_t off = 0;
+    for (int64_t k = 0; k < n_fr; k++) {
+      const int64_t i0 = fr[4 * k], j0 = fr[4 * k + 1], i1 = fr[4 * k + 2], j1 = fr[4 * k + 3];
+      if (!(0 <= i0 && i0 < i1 && i1 <= n_points && 0 <= j0 && j0 < j1 && j1 <= n_points))
+        throw std::invalid_argument("bw_r0_assemble_fr: block " + std::to_string(k) + " outside the matrix");
+      blocks[k] = {off, (int)i0, (int)j0, (int)(i1 - i0), (int)(j1 - j0)};
+      for (int64_t ti = 0; ti < i1 - i0; ti += bw::kAsmTile)
+        for (int64_t tj = 0; tj < j1 - j0; tj += bw::kAsmTile) tiles.push_back({(int)k, (int)ti, (int)tj, 0});
+      off += 9 * (i1 - i0) * (j1 - j0);
+    }
+    if (off > out_len) throw std::invalid_argument("bw_r0_assemble_fr: out holds fewer than the blocks' entries");
+    if (tiles.empty()) return BW_OK;
+    BW_CUDA(cudaSetDevice(device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    void *d_rec = nullptr, *d_perm = nullptr, *d_blk = nullptr, *d_tile = nullptr;
+    auto release = [&] {
+      cudaFree(d_rec);
+      cudaFree(d_perm);
+      cudaFree(d_blk);
+      cudaFree(d_tile);
+    };
+    try {
+      const size_t rb = sizeof(double) * bw::r0::kFrameDoubles * (size_t)n_elems;
+      BW_CUDA(cudaMalloc(&d_rec, rb));
+      BW_CUDA(cudaMalloc(&d_perm, 4 * p32.size()));
+      BW_CUDA(cudaMalloc(&d_blk, sizeof(bw::AsmBlock) * blocks.size()));
+      BW_CUDA(cudaMalloc(&d_tile, sizeof(bw::AsmTile) * tiles.size()));
+      BW_CUDA(cudaMemcpyAsync(d_rec, records, rb, cudaMemcpyHostToDevice, st));
+      BW_CUDA(cudaMemcpyAsync(d_perm, p32.data(), 4 * p32.size(), cudaMemcpyHostToDevice, st));
+      BW_CUDA(cudaMemcpyAsync(d_blk, blocks.data(), sizeof(bw::AsmBlock) * blocks.size(), cudaMemcpyHostToDevice, st));
+      BW_CUDA(cudaMemcpyAsync(d_tile, tiles.data(), sizeof(bw::AsmTile) * tiles.size(), cudaMemcpyHostToDevice, st));
+      const long long nt = (long long)tiles.size();
+      const int grid = (int)std::min<long long>(nt, 148LL * 8);
+      bw::r0_fr_assemble_kernel<<<grid, bw::kAsmTile * bw::kAsmTile, 0, st>>>(
+          static_cast<const double *>(d_rec), static_cast<const int *>(d_perm),
+          static_cast<const bw::AsmBlock *>(d_blk), static_cast<const bw::AsmTile *>(d_tile), nt, G, nu, out);
+      BW_CUDA(cudaGetLastError());
+      BW_CUDA(cudaStreamSynchronize(st));
+    } catch (...) {
+      cudaStreamSynchronize(st);
+      release();
+      throw;
+    }
+    release();
+    return BW_OK;
+  });
 }
 
 int bw_destroy(bw_hmat *h) {

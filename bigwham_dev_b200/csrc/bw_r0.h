@@ -243,5 +243,21 @@ BW_HD void influence_h(const double *cp_s, const double *rot_s, double a_s, doub
   }
 }
 
+// Element record used by the assembly: collocation point (3), rotation
+// row-major (9), unit normal (3), half sides a, b.
+constexpr int kFrameDoubles = 17;
+
+// The 3 x 3 H-kernel entry of receiver element `rec` and source element
+// `src` (records as above), written column-major into a full-rank block of
+// leading dimension ld at (row0, col0): out[(col0 + i) * ld + row0 + j] =
+// traction j at the receiver due to DD i of the source.
+BW_HD void h_entry_into_block(const double *src, const double *rec, double G, double nu, double *out, long long ld,
+                              long long row0, long long col0) {
+  double K[3][3];
+  influence_h(src, src + 3, src[15], src[16], rec, rec + 3, rec + 12, G, nu, K);
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) out[(col0 + i) * ld + row0 + j] = K[j][i];
+}
+
 }  // namespace r0
 }  // namespace bw

@@ -219,6 +219,27 @@ int bwh_export(const bwh_io *h, int64_t *fr, int64_t *lr, double *fr_data, doubl
   });
 }
 
+int64_t bwh_element_frames(const bwh_io *h, double *out) {
+  if (!h) return fail("null handle"), -1;
+  int64_t n = -1;
+  const int rc = guarded([&] {
+    const std::vector<double> cp = h->io->GetCollocationPoints(), rot = h->io->GetRotationMatrix(),
+                              nrm = h->io->GetElementNormals();
+    const size_t ne = nrm.size() / 3;
+    if (h->io->spatial_dimension() != 3 || cp.size() != 3 * ne || rot.size() != 9 * ne)
+      return fail("bwh_element_frames: needs a 3D mesh with one collocation point per element");
+    n = (int64_t)ne;
+    if (out)
+      for (size_t e = 0; e < ne; e++) {
+        for (int k = 0; k < 3; k++) out[15 * e + k] = cp[3 * e + k];
+        for (int k = 0; k < 9; k++) out[15 * e + 3 + k] = rot[9 * e + k];
+        for (int k = 0; k < 3; k++) out[15 * e + 12 + k] = nrm[3 * e + k];
+      }
+    return 0;
+  });
+  return rc == 0 ? n : -1;
+}
+
 int bwh_write_to_file(const bwh_io *h, const char *path) {
   if (!h || !path) return fail("null argument");
   if (h->gpu) return fail("bwh_write_to_file must run before bwh_attach_gpu (the host blocks are released there)");

@@ -314,6 +314,24 @@ int bw_file_read(const char *path, int verify, int64_t *fr, int64_t *lr, double 
  * first (one pass over the file). */
 int bw_create_from_file(const char *path, int device, int verify, bw_hmat **out);
 
+/* ---- Device assembly (3DR0-H) ----------------------------------------------
+ * Full-rank blocks of a 3DR0-H H-matrix computed on the device: the work of
+ * the reference's Hmat::buildFR (src/hmat/hmatrix/hmat.cc:315-353) for the
+ * rectangle hypersingular kernel
+ * (src/elasticity/fullspace_iso_3d_rectangle/
+ * bie_elastostatic_rectangle_0_influence.h:29-125).
+ * records: n_elems x 17 doubles per element (collocation point, rotation
+ * matrix row-major with local = R global, unit normal, half sides a and b
+ * along the local x and y); G, nu: shear modulus and Poisson ratio; fr:
+ * n_fr x 4 blocks (i0, j0, i_end, j_end) in permuted points; perm: n_points
+ * values, permuted point -> element.  out (device, out_len doubles): the
+ * blocks back to back, column-major, as bw_add_full / bw_file_write take
+ * them.  Every index is checked on the host before the launch; returns once
+ * the blocks are written (stream-ordered, then synchronized). */
+int bw_r0_assemble_fr(int device, int64_t n_elems, const double *records, double G, double nu, int64_t n_fr,
+                      const int64_t *fr, const int64_t *perm, int64_t n_points, double *out, int64_t out_len,
+                      void *stream);
+
 /* Release everything. */
 int bw_destroy(bw_hmat *h);
 

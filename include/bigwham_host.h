@@ -64,6 +64,13 @@ double bwh_hmat_time(const bwh_io *io);
 int bwh_permutation(const bwh_io *io, int64_t *perm);
 /* GetCollocationPoints: returns the count; fills `out` when non-null. */
 int64_t bwh_collocation_points(const bwh_io *io, double *out);
+/* Per element of a 3D mesh with one collocation point per element, 15
+ * doubles: collocation point, rotation matrix row-major (local = R global)
+ * and unit normal, from the reference's element objects
+ * (GetCollocationPoints / GetRotationMatrix / GetElementNormals,
+ * src/io/bigwham_io.cc:985-1140).  Returns the element count; fills `out`
+ * when non-null; -1 for other meshes. */
+int64_t bwh_element_frames(const bwh_io *io, double *out);
 /* GetHPattern: 6 doubles per block; returns the count; fills `out` when non-null. */
 int64_t bwh_hpattern(const bwh_io *io, double *out);
 /* Block counts of the pattern: kind 0 full rank, 1 low rank. */

@@ -27,4 +27,22 @@ void probe_r0_influence(const double *frame_s, double a_s, double b_s, const dou
     for (int i = 0; i < 3; i++) out[3 * j + i] = K[j][i];
 }
 
+// Full-rank blocks of a 3DR0-H H-matrix assembled on the host with the same
+// entry function as the device kernel: fr (n_fr x 4, permuted points), perm
+// (permuted point -> element), frames (n_elems x 17); out: the blocks back to
+// back, column-major.
+void probe_r0_fr_blocks(const double *frames, double G, double nu, long long n_fr, const long long *fr,
+                        const long long *perm, double *out) {
+  long long off = 0;
+  for (long long k = 0; k < n_fr; k++) {
+    const long long i0 = fr[4 * k], j0 = fr[4 * k + 1], mp = fr[4 * k + 2] - i0, np_ = fr[4 * k + 3] - j0;
+    for (long long jj = 0; jj < np_; jj++)
+      for (long long ii = 0; ii < mp; ii++)
+        bw::r0::h_entry_into_block(frames + bw::r0::kFrameDoubles * perm[j0 + jj],
+                                   frames + bw::r0::kFrameDoubles * perm[i0 + ii], G, nu, out + off, 3 * mp, 3 * ii,
+                                   3 * jj);
+    off += 9 * mp * np_;
+  }
+}
+
 }  // extern "C"

@@ -52,8 +52,13 @@ def probe():
         lib.probe_r0_displacement(*a, o)
         return o.reshape(3, 3)
 
+    lib.probe_r0_fr_blocks.argtypes = [p, C.c_double, C.c_double, C.c_longlong,
+                                       np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS"),
+                                       np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS"), p]
+
     class Probe(tuple):
         influence = staticmethod(lib.probe_r0_influence)
+        fr_blocks = staticmethod(lib.probe_r0_fr_blocks)
 
     return Probe((stress, disp))
 
@@ -215,3 +220,74 @@ def test_h_kernel_entries_match_the_reference_operator(probe, mesh):
     scale = np.max(np.abs(dense))
     err = np.max(np.abs(mine - dense)) / scale
     assert err < (1e-13 if mesh == "planar" else 1e-12), err  # measured: 4e-16 and 2e-15
+
+
+def element_records(R, coor, conn):
+    """(n_elements, 17) records of the assembly: the reference's frames plus
+    the half sides |v1 - v0| / 2, |v3 - v0| / 2."""
+    v = coor[conn]
+    ab = np.stack([np.linalg.norm(v[:, 1] - v[:, 0], axis=1) / 2, np.linalg.norm(v[:, 3] - v[:, 0], axis=1) / 2], 1)
+    return np.ascontiguousarray(np.hstack([R.element_frames(), ab]))
+
+
+@pytest.mark.parametrize("mesh", ["planar", "cylinder"])
+def test_fr_blocks_assembled_like_the_reference(probe, mesh):
+    """The full-rank blocks of a built 3DR0-H H-matrix, assembled from its
+    pattern and permutation with the device kernel's entry function, equal
+    the reference's blocks (Hmat::buildFR, hmat.cc:315-353)."""
+    from bigwham_dev_b200.meshes import square_crack_3d
+    from oracle import RefHmat
+
+    E, nu = 1.0, 0.25
+    coor, conn = square_crack_3d(24) if mesh == "planar" else _cylinder_strip(24, 12)
+    R = RefHmat("3DR0-H", coor, conn, [E, nu], 32, 3.0, 1e-5, n_threads=4)
+    arr = R.arrays()
+    assert np.array_equal(arr.perm0, arr.perm1)
+    out = np.full(arr.fr_data.size, np.nan)
+    probe.fr_blocks(element_records(R, coor, conn), E / (2 * (1 + nu)), nu, len(arr.fr),
+                    np.ascontiguousarray(arr.fr, dtype=np.int64), np.ascontiguousarray(arr.perm0, dtype=np.int64), out)
+    err = np.max(np.abs(out - arr.fr_data)) / np.max(np.abs(arr.fr_data))
+    assert err < 1e-13, err
+
+
+def test_assembly_entry_rejects_bad_input_before_the_device():
+    """bw_r0_assemble_fr checks every index the kernel would use on the host;
+    these calls fail there, before any CUDA call."""
+    import ctypes as C
+
+    from bigwham_dev_b200 import _capi as A
+
+    L = A.lib()
+    rec = np.zeros((4, 17))
+    rec[:, 15:] = 0.5
+    fr = np.array([[0, 0, 2, 2], [2, 2, 4, 4]], dtype=np.int64)
+    perm = np.arange(4, dtype=np.int64)
+    out = C.c_void_p(8)  # never dereferenced: every call below fails its checks
+
+    def call(rec=rec, G=1.0, nu=0.25, fr=fr, perm=perm, n_points=4, out_len=72):
+        return L.bw_r0_assemble_fr(0, rec.shape[0], rec.ctypes.data, G, nu, fr.shape[0], fr.ctypes.data,
+                                   perm.ctypes.data, n_points, out, out_len, None)
+
+    assert call(perm=np.array([0, 1, 2, 4], dtype=np.int64)) == A.BW_ERR_ARG
+    assert "perm" in A.last_error(None)
+    assert call(fr=np.array([[0, 0, 2, 2], [2, 2, 5, 4]], dtype=np.int64)) == A.BW_ERR_ARG
+    assert "outside" in A.last_error(None)
+    assert call(out_len=71) == A.BW_ERR_ARG
+    assert call(G=0.0) == A.BW_ERR_ARG and call(nu=0.5) == A.BW_ERR_ARG
+
+
+def test_host_library_records_equal_the_oracles():
+    """BigWhamIOGpu.element_records (the host library's reference objects)
+    gives the same records as the oracle's build of the same mesh."""
+    if not os.path.exists(os.path.join(ROOT, "bigwham_dev_b200", "_lib", "libbigwham_host.so")):
+        pytest.skip("host adapter not built")
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+    from oracle import RefHmat
+
+    coor, conn = _cylinder_strip(9, 4)
+    io = BigWhamIOGpu(coor, conn, "3DR0-H", [1.0, 0.25], 2, useCuda=False)
+    mine = io.element_records()
+    io.close()
+    R = RefHmat("3DR0-H", coor, conn, [1.0, 0.25], 32, 3.0, 1e-5, n_threads=2)
+    assert mine.shape == (36, 17)
+    assert np.array_equal(mine, element_records(R, coor, conn))
