@@ -1,5 +1,6 @@
 // Host build of bigwham_dev_b200/csrc/bw_r0.h for tests/test_r0_kernel_cpu.py:
 // the same functions the device code uses, exported with C linkage.
+#include "bw_aca.h"
 #include "bw_r0.h"
 
 extern "C" {
@@ -43,6 +44,26 @@ void probe_r0_fr_blocks(const double *frames, double G, double nu, long long n_f
                                    3 * jj);
     off += 9 * mp * np_;
   }
+}
+
+// Block ACA of the low-rank block (rows [i0, i1), columns [j0, j1) in
+// permuted points) of a 3DR0-H H-matrix, with the entry function of the
+// device assembly.  A: (i1 - i0) 3 x cap 3, B: cap 3 x (j1 - j0) 3,
+// column-major; returns the rank in blocks (-1 when cap was too small).
+int probe_r0_aca(const double *frames, double G, double nu, const long long *perm, long long i0, long long j0,
+                 long long i1, long long j1, double eps, int cap, double *A, double *B, double *err) {
+  const int n0 = (int)(i1 - i0), n1 = (int)(j1 - j0);
+  double *work = new double[(size_t)(n0 + n1) * 9 + n0 + n1];
+  auto entry = [&](int i, int j, double K[3][3]) {
+    bw::r0::influence_h(frames + bw::r0::kFrameDoubles * perm[j0 + j], frames + bw::r0::kFrameDoubles * perm[j0 + j] + 3,
+                        frames[bw::r0::kFrameDoubles * perm[j0 + j] + 15], frames[bw::r0::kFrameDoubles * perm[j0 + j] + 16],
+                        frames + bw::r0::kFrameDoubles * perm[i0 + i], frames + bw::r0::kFrameDoubles * perm[i0 + i] + 3,
+                        frames + bw::r0::kFrameDoubles * perm[i0 + i] + 12, G, nu, K);
+  };
+  const bw::aca::Result r = bw::aca::block_aca_host(entry, n0, n1, eps, cap, A, B, work);
+  delete[] work;
+  *err = r.error;
+  return r.overflow ? -1 : r.rank_blocks;
 }
 
 }  // extern "C"
