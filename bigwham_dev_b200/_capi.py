@@ -61,6 +61,8 @@ _SIGS = {
     "bw_file_read": (C.c_int, [C.c_char_p, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "bw_create_from_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(_P)]),
     "bw_r0_assemble_fr": (C.c_int, [C.c_int, _I64, _P, C.c_double, C.c_double, _I64, _P, _P, _I64, _P, _I64, _P]),
+    "bw_r0_aca": (C.c_int, [C.c_int, _I64, _P, C.c_double, C.c_double, _I64, _P, _P, _I64, C.c_double, C.c_int,
+                            _P, _I64, _P, _I64, _P, _P, _P]),
     "bw_destroy": (C.c_int, [_P]),
     "bw_version": (C.c_char_p, []),
 }

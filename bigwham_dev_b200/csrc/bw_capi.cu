@@ -13,6 +13,7 @@
 #include "bigwham_b200.h"
 #include "bw_kernels.cuh"
 #include "bw_mm_kernels.cuh"
+#include "bw_aca_kernels.cuh"
 #include "bw_assemble_kernels.cuh"
 #include "bw_file.h"
 #include "bw_layout.h"
@@ -1496,6 +1497,75 @@ int bw_r0_assemble_fr(int device, int64_t n_elems, const double *records, double
       throw;
     }
     release();
+    return BW_OK;
+  });
+}
+
+int bw_r0_aca(int device, int64_t n_elems, const double *records, double G, double nu, int64_t n_lr,
+              const int64_t *lr, const int64_t *perm, int64_t n_points, double eps, int cap_blocks,
+              double *factors_a, int64_t a_len, double *factors_b, int64_t b_len, int32_t *rank_out,
+              double *err_out, void *stream) {
+  return device_guarded([&] {
+    if (!records || n_elems < 1 || n_lr < 0 || n_points < 1 || (n_lr && (!lr || !perm || !factors_a ||
+                                                                        !factors_b || !rank_out || !err_out)))
+      throw std::invalid_argument("bw_r0_aca: null or empty argument");
+    if (n_elems >= (int64_t(1) << 31) || n_points >= (int64_t(1) << 31) || n_lr >= (int64_t(1) << 31))
+      throw std::invalid_argument("bw_r0_aca: more than 2^31 elements or blocks");
+    if (!(G > 0.0) || !(nu > -1.0 && nu < 0.5) || !(eps > 0.0) || cap_blocks < 1)
+      throw std::invalid_argument("bw_r0_aca: bad G, nu, eps or capacity");
+    std::vector<int32_t> p32(n_points);
+    for (int64_t i = 0; i < n_points; i++) {
+      if (perm[i] < 0 || perm[i] >= n_elems) throw std::invalid_argument("bw_r0_aca: perm out of range");
+      p32[i] = (int32_t)perm[i];
+    }
+    std::vector<bw::AcaBlock> blocks(n_lr);
+    int64_t ao = 0, bo = 0, slot = 1;
+    for (int64_t k = 0; k < n_lr; k++) {
+      const int64_t i0 = lr[4 * k], j0 = lr[4 * k + 1], i1 = lr[4 * k + 2], j1 = lr[4 * k + 3];
+      if (!(0 <= i0 && i0 < i1 && i1 <= n_points && 0 <= j0 && j0 < j1 && j1 <= n_points))
+        throw std::invalid_argument("bw_r0_aca: block " + std::to_string(k) + " outside the matrix");
+      const int64_t n0 = i1 - i0, n1 = j1 - j0, cap = std::min<int64_t>(cap_blocks, std::min(n0, n1));
+      blocks[k] = {ao, bo, 0, (int)i0, (int)j0, (int)n0, (int)n1, (int)cap, 0};
+      ao += 9 * n0 * cap;
+      bo += 9 * n1 * cap;
+      slot = std::max<int64_t>(slot, 9 * n1 + n0 + n1 + 2);  // row band + used flags (ints)
+    }
+    if (ao > a_len || bo > b_len) throw std::invalid_argument("bw_r0_aca: factor storage smaller than the capacity");
+    if (!n_lr) return BW_OK;
+    BW_CUDA(cudaSetDevice(device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int grid = (int)std::min<int64_t>(n_lr, 148 * 4);
+    void *d_rec = nullptr, *d_perm = nullptr, *d_blk = nullptr, *d_scr = nullptr, *d_rank = nullptr, *d_err = nullptr;
+    auto release = [&] {
+      for (void *q : {d_rec, d_perm, d_blk, d_scr, d_rank, d_err}) cudaFree(q);
+    };
+    try {
+      const size_t rb = sizeof(double) * bw::r0::kFrameDoubles * (size_t)n_elems;
+      BW_CUDA(cudaMalloc(&d_rec, rb));
+      BW_CUDA(cudaMalloc(&d_perm, 4 * p32.size()));
+      BW_CUDA(cudaMalloc(&d_blk, sizeof(bw::AcaBlock) * blocks.size()));
+      BW_CUDA(cudaMalloc(&d_scr, sizeof(double) * (size_t)slot * grid));
+      BW_CUDA(cudaMalloc(&d_rank, 4 * (size_t)n_lr));
+      BW_CUDA(cudaMalloc(&d_err, 8 * (size_t)n_lr));
+      BW_CUDA(cudaMemcpyAsync(d_rec, records, rb, cudaMemcpyHostToDevice, st));
+      BW_CUDA(cudaMemcpyAsync(d_perm, p32.data(), 4 * p32.size(), cudaMemcpyHostToDevice, st));
+      BW_CUDA(cudaMemcpyAsync(d_blk, blocks.data(), sizeof(bw::AcaBlock) * blocks.size(), cudaMemcpyHostToDevice, st));
+      bw::r0_aca_kernel<<<grid, bw::kAcaThreads, 0, st>>>(
+          static_cast<const double *>(d_rec), static_cast<const int *>(d_perm),
+          static_cast<const bw::AcaBlock *>(d_blk), (int)n_lr, G, nu, eps, factors_a, factors_b,
+          static_cast<double *>(d_scr), slot, static_cast<int *>(d_rank), static_cast<double *>(d_err));
+      BW_CUDA(cudaGetLastError());
+      BW_CUDA(cudaMemcpyAsync(rank_out, d_rank, 4 * (size_t)n_lr, cudaMemcpyDeviceToHost, st));
+      BW_CUDA(cudaMemcpyAsync(err_out, d_err, 8 * (size_t)n_lr, cudaMemcpyDeviceToHost, st));
+      BW_CUDA(cudaStreamSynchronize(st));
+    } catch (...) {
+      cudaStreamSynchronize(st);
+      release();
+      throw;
+    }
+    release();
+    for (int64_t k = 0; k < n_lr; k++)
+      if (rank_out[k] > 0) rank_out[k] *= 3;  // scalar rank (LRB_pattern flag); -1: capacity too small
     return BW_OK;
   });
 }

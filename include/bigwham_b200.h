@@ -332,6 +332,22 @@ int bw_r0_assemble_fr(int device, int64_t n_elems, const double *records, double
                       const int64_t *fr, const int64_t *perm, int64_t n_points, double *out, int64_t out_len,
                       void *stream);
 
+/* Low-rank blocks of a 3DR0-H H-matrix compressed on the device by block ACA
+ * (3 x 3 pivots, the reference's adaptiveCrossApproximation<3>,
+ * src/hmat/compression/adaptiveCrossApproximation.h:24-226), one CTA per
+ * block.  records / perm / G / nu as for bw_r0_assemble_fr; lr: n_lr x 4
+ * admissible blocks in permuted points; eps: the ACA tolerance.  Block k gets
+ * cap_k = min(cap_blocks, rows, columns) rank blocks of storage: A_k (rows 3 x
+ * cap_k 3) at factors_a + sum_{l<k} 9 rows_l cap_l and B_k (cap_k 3 x
+ * columns 3) at factors_b + sum_{l<k} 9 columns_l cap_l, column-major, device
+ * memory (a_len / b_len doubles available).  rank_out (host): each block's
+ * scalar rank, -1 when cap_k was too small; err_out (host): the ACA error
+ * estimate.  Every index is checked on the host before the launch. */
+int bw_r0_aca(int device, int64_t n_elems, const double *records, double G, double nu, int64_t n_lr,
+              const int64_t *lr, const int64_t *perm, int64_t n_points, double eps, int cap_blocks,
+              double *factors_a, int64_t a_len, double *factors_b, int64_t b_len, int32_t *rank_out,
+              double *err_out, void *stream);
+
 /* Release everything. */
 int bw_destroy(bw_hmat *h);
 

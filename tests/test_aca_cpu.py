@@ -78,3 +78,27 @@ def test_block_aca_matches_the_reference_accuracy(lib):
     assert np.median(agree) < 1e-9
     assert max(mine_err) <= 1.5 * max(ref_err), (max(mine_err), max(ref_err))
     assert np.median(mine_err) <= 1.5 * np.median(ref_err), (np.median(mine_err), np.median(ref_err))
+
+
+def test_device_aca_entry_rejects_bad_input_before_the_device():
+    """bw_r0_aca checks every index and the factor capacity on the host; these
+    calls fail there, before any CUDA call."""
+    from bigwham_dev_b200 import _capi as A
+
+    L = A.lib()
+    rec = np.zeros((8, 17))
+    lr = np.array([[0, 4, 4, 8]], dtype=np.int64)
+    perm = np.arange(8, dtype=np.int64)
+    rank = np.zeros(1, dtype=np.int32)
+    err = np.zeros(1)
+    dev = C.c_void_p(8)  # never dereferenced: every call below fails its checks
+
+    def call(lr=lr, perm=perm, eps=1e-5, cap=4, a_len=144, b_len=144):
+        return L.bw_r0_aca(0, 8, rec.ctypes.data, 1.0, 0.25, lr.shape[0], lr.ctypes.data, perm.ctypes.data, 8, eps,
+                           cap, dev, a_len, dev, b_len, rank.ctypes.data, err.ctypes.data, None)
+
+    assert call(perm=np.array([0, 1, 2, 3, 4, 5, 6, 9], dtype=np.int64)) == A.BW_ERR_ARG
+    assert call(lr=np.array([[0, 4, 4, 9]], dtype=np.int64)) == A.BW_ERR_ARG
+    assert "outside" in A.last_error(None)
+    assert call(a_len=143) == A.BW_ERR_ARG and "capacity" in A.last_error(None)
+    assert call(eps=0.0) == A.BW_ERR_ARG and call(cap=0) == A.BW_ERR_ARG
