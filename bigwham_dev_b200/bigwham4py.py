@@ -33,6 +33,7 @@ _P, _I64 = C.c_void_p, C.c_int64
 _HSIGS = {
     "bwh_create": (C.c_int, [_P, _I64, _P, _I64, C.c_char_p, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_P)]),
     "bwh_build": (C.c_int, [_P, C.c_int, C.c_double, C.c_double]),
+    "bwh_build_pattern": (C.c_int, [_P, C.c_int, C.c_double]),
     "bwh_attach_gpu": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
     "bwh_set_precision": (C.c_int, [_P, C.c_int]),
     "bwh_set_tuning": (C.c_int, [_P, C.c_char_p, C.c_int64]),
@@ -116,6 +117,11 @@ class BigWhamIOGpu:
         _check(self._L.bwh_build(self._h, int(max_leaf_size), float(eta), float(eps_aca)))
         if self.use_cuda:
             self.attach_gpu(self._precisions, self._transpose)
+
+    def build_pattern(self, max_leaf_size: int, eta: float) -> None:
+        """Cluster tree and block pattern only (BigWhamIO::BuildPattern); see
+        devbuild.build_r0 for building the blocks on the device."""
+        _check(self._L.bwh_build_pattern(self._h, int(max_leaf_size), float(eta)))
 
     def attach_gpu(self, precisions=("fp64",), transpose: bool = False, release_host: bool = True,
                    matmat: bool = False, tuning: dict | None = None) -> HmatGpu:

@@ -71,6 +71,14 @@ int bwh_build(bwh_io *h, int leaf, double eta, double eps) {
   });
 }
 
+int bwh_build_pattern(bwh_io *h, int leaf, double eta) {
+  if (!h) return fail("null handle");
+  return guarded([&] {
+    h->io->BuildPattern(leaf, eta);
+    return 0;
+  });
+}
+
 int bwh_attach_gpu(bwh_io *h, int device, int storage, int release_host) {
   if (!h) return fail("null handle");
   return guarded([&] {

@@ -32,6 +32,10 @@ int bwh_create(const double *coor, int64_t n_coor, const int *conn, int64_t n_co
 
 /* BigWhamIO::BuildHierarchicalMatrix (bigwham_io.cc:635-704), host build. */
 int bwh_build(bwh_io *io, int max_leaf_size, double eta, double eps_aca);
+/* BigWhamIO::BuildPattern (src/io/bigwham_io.cc:487-511): cluster tree and
+ * block pattern only, no blocks; bwh_hpattern and bwh_permutation then
+ * describe the pattern, for a build of the blocks on the device. */
+int bwh_build_pattern(bwh_io *io, int max_leaf_size, double eta);
 
 /* Upload the built H-matrix to `device` in the precisions of `storage`
  * (BW_FP64 | BW_FP32 | BW_BF16 [| BW_STORE_TRANSPOSE]) and install it with
