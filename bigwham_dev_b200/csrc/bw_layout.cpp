@@ -2,6 +2,7 @@
 #include "bw_layout.h"
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -9,6 +10,7 @@
 #include <numeric>
 #include <queue>
 #include <stdexcept>
+#include <string>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -35,6 +37,20 @@ float from_bf16(uint16_t b) {
 }
 
 namespace {
+
+// Offsets, counts and row indices of the plan are 32-bit fields the kernels
+// read; a problem whose layout outgrows them is refused instead of wrapping.
+int32_t i32(int64_t v, const char *what) {
+  if (v < INT32_MIN || v > INT32_MAX)
+    throw std::length_error(std::string("layout field ") + what + " exceeds 32 bits (" + std::to_string(v) + ")");
+  return static_cast<int32_t>(v);
+}
+
+uint32_t u31(int64_t v, const char *what) {
+  if (v < 0 || v > 0x7fffffffLL)
+    throw std::length_error(std::string("layout field ") + what + " exceeds 31 bits (" + std::to_string(v) + ")");
+  return static_cast<uint32_t>(v);
+}
 
 // The blocks of the operator being laid out: H itself, or H^T built from the
 // same storage (FR: A^T; LR: (A B)^T = B^T A^T, i.e. A' = B^T and B' = A^T).
@@ -130,10 +146,10 @@ void build_operator(const Problem &p, bool tr, int grid, OperatorPlan &op) {
     int64_t br = 0;     // next row inside that block
     for (int64_t r0 = 0; r0 < R; r0 += cut) {
       Item it;
-      it.h = static_cast<int32_t>(std::min<int64_t>(cut, R - r0));
-      it.hpad = static_cast<int32_t>(align_up(it.h, kRowAlign));
+      it.h = i32(std::min<int64_t>(cut, R - r0), "item rows");
+      it.hpad = i32(align_up(it.h, kRowAlign), "item rows");
       it.ncols = n;
-      it.out_off = static_cast<int32_t>(op.t_off[kv.second[bi]] + br);
+      it.out_off = i32(op.t_off[kv.second[bi]] + br, "t offset");
       int64_t need = it.h;
       while (need > 0) {
         const int64_t k = kv.second[bi];
@@ -246,9 +262,9 @@ void build_operator(const Problem &p, bool tr, int grid, OperatorPlan &op) {
     const int64_t cut = align_up((H + parts - 1) / parts, kRowAlign);
     for (int64_t r0 = 0; r0 < H; r0 += cut) {
       Item it;
-      it.h = static_cast<int32_t>(std::min<int64_t>(cut, H - r0));
-      it.hpad = static_cast<int32_t>(align_up(it.h, kRowAlign));
-      it.out_off = static_cast<int32_t>(pb[q] + r0);
+      it.h = i32(std::min<int64_t>(cut, H - r0), "item rows");
+      it.hpad = i32(align_up(it.h, kRowAlign), "item rows");
+      it.out_off = i32(pb[q] + r0, "output row");
       for (int pass = 0; pass < 2; pass++) {
         for (const Cover &e : cov[q]) {
           if (e.kind != pass) continue;
@@ -347,16 +363,16 @@ void chunk_item(const OperatorPlan &op, const Item &it, int prec, int phase, int
     Chunk ch;
     std::memset(&ch, 0, sizeof ch);
     ch.data_off = it.off[prec] + (tiled ? (c0 / 8) * 8 * int64_t(it.hpad) : c0 * int64_t(it.hpad));
-    ch.ncols = static_cast<int32_t>(take);
+    ch.ncols = i32(take, "chunk columns");
     ch.hpad = it.hpad;
     ch.rows = it.h;
     ch.out_off = it.out_off;
     if (phase == 0) {
-      ch.g_off = it.segs.empty() ? 0 : static_cast<int32_t>(it.segs[0].src_off + c0);
+      ch.g_off = it.segs.empty() ? 0 : i32(it.segs[0].src_off + c0, "vector offset");
     } else {
       const int64_t g = (g_len + 3) / 4 * 4;  // 16-byte aligned slice in FP32, 32 in FP64
       if (g + take > INT32_MAX) throw std::runtime_error("gather array above 2^31 entries");
-      ch.g_off = static_cast<int32_t>(g);
+      ch.g_off = i32(g, "G2 offset");
       g_len = g + take;
       while (s_at < it.segs.size() && seg_start[s_at + 1] <= c0) s_at++;
       for (size_t s = s_at; s < it.segs.size() && seg_start[s] < c0 + take; s++) {
@@ -364,9 +380,9 @@ void chunk_item(const OperatorPlan &op, const Item &it, int prec, int phase, int
         if (b <= a) continue;
         const Segment &sg = it.segs[s];
         GatherSeg gs;
-        gs.dst = static_cast<int32_t>(g + (a - c0));
-        gs.src_off = static_cast<int32_t>(sg.src_off + (a - seg_start[s]));
-        gs.cols_src = static_cast<uint32_t>(b - a) | (sg.src ? 0x80000000u : 0u);
+        gs.dst = i32(g + (a - c0), "G2 offset");
+        gs.src_off = i32(sg.src_off + (a - seg_start[s]), "gather source");
+        gs.cols_src = u31(b - a, "gather run") | (sg.src ? 0x80000000u : 0u);
         gs.scale = seg_scale(op, sg, prec);
         gsegs.push_back(gs);
       }
@@ -415,7 +431,7 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
     for (int64_t q : order) {
       cp.chunks.insert(cp.chunks.end(), per_item[q].begin(), per_item[q].end());
       if (cp.chunks.size() > (size_t)INT32_MAX) fail("too many chunks");
-      cp.item_ptr.push_back(static_cast<int32_t>(cp.chunks.size()));
+      cp.item_ptr.push_back(i32((int64_t)cp.chunks.size(), "chunk count"));
     }
   }
 }
@@ -500,12 +516,12 @@ void mm_chunk_item(const MmItem &it, std::vector<MmChunk> &out) {
       if (b <= a) continue;
       if (nr == kMmMaxRuns) throw std::runtime_error("matmat chunk needs more than the run cap");
       const MmSeg &sg = it.segs[s];
-      ch.run[nr].src = static_cast<uint32_t>(sg.src_row + (a - seg_start[s])) | (sg.src ? 0x80000000u : 0u);
-      ch.run[nr].rows = static_cast<uint32_t>(b - a);
+      ch.run[nr].src = u31(sg.src_row + (a - seg_start[s]), "operand row") | (sg.src ? 0x80000000u : 0u);
+      ch.run[nr].rows = u31(b - a, "operand rows");
       nr++;
     }
     ch.data_off = it.off + (c0 / 8) * 8 * int64_t(it.hpad);
-    ch.kc = static_cast<int32_t>(end - c0);
+    ch.kc = i32(end - c0, "chunk columns");
     ch.hpad = it.hpad;
     ch.rows = it.h;
     ch.out_off = it.out_off;
@@ -565,9 +581,9 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
     const int64_t cut = align_up((R8 + nit - 1) / nit, 8);
     for (int64_t r0 = 0; r0 < R8; r0 += cut) {
       MmItem it;
-      it.h = static_cast<int32_t>(std::min<int64_t>(cut, R8 - r0));
+      it.h = i32(std::min<int64_t>(cut, R8 - r0), "item rows");
       it.hpad = it.h;
-      it.out_off = static_cast<int32_t>(st.t8_base + r0);
+      it.out_off = i32(st.t8_base + r0, "T8 offset");
       it.ncols = W;
       it.stack = (int64_t)s;
       it.srow0 = r0;
@@ -602,9 +618,9 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
     const int64_t cut = align_up((src.h + parts - 1) / parts, 8);
     for (int64_t r0 = 0; r0 < src.h; r0 += cut) {
       MmItem it;
-      it.h = static_cast<int32_t>(std::min<int64_t>(cut, src.h - r0));
-      it.hpad = static_cast<int32_t>(align_up(it.h, 8));
-      it.out_off = static_cast<int32_t>(src.out_off + r0);
+      it.h = i32(std::min<int64_t>(cut, src.h - r0), "item rows");
+      it.hpad = i32(align_up(it.h, 8), "item rows");
+      it.out_off = i32(src.out_off + r0, "output row");
       for (const Segment &sg : src.segs) {
         it.segs.push_back(window(sg, r0));
         it.ncols += it.segs.back().ncols;
@@ -640,7 +656,7 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
     for (int64_t q : order) {
       ph.chunks.insert(ph.chunks.end(), per_item[q].begin(), per_item[q].end());
       if (ph.chunks.size() > (size_t)INT32_MAX) fail("too many matmat chunks");
-      ph.item_ptr.push_back(static_cast<int32_t>(ph.chunks.size()));
+      ph.item_ptr.push_back(i32((int64_t)ph.chunks.size(), "chunk count"));
     }
   }
 }
