@@ -436,48 +436,90 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
   }
 }
 
-void fill_items(const Problem &p, bool tr, const OperatorPlan &op, int phase, int prec, int64_t i_begin,
-                int64_t i_end, int64_t base, void *dst) {
-  const PhasePlan &ph = op.ph[phase];
-  auto put = [&](int64_t e, double val, double inv) {
-    if (prec == 0)
-      static_cast<double *>(dst)[e] = val;
-    else if (prec == 1)
-      static_cast<float *>(dst)[e] = static_cast<float>(val);
+namespace {
+
+// One column run of an item: rows [r0, r0 + n) of item column c from
+// src[i * stride], converted to the precision's storage (FP32: rounded; BF16:
+// times inv, rounded to FP32 then BF16) at the item_index positions.
+template <int PREC>
+inline void put_run(void *dst, int64_t e0, int64_t hpad, int64_t r0, int64_t c, const double *src, int64_t stride,
+                    int64_t n, double inv) {
+  if constexpr (PREC == 0) {
+    double *d = static_cast<double *>(dst) + e0 + c * hpad + r0;
+    if (stride == 1)
+      std::memcpy(d, src, sizeof(double) * (size_t)n);
     else
-      static_cast<uint16_t *>(dst)[e] = to_bf16(static_cast<float>(val * inv));
-  };
+      for (int64_t i = 0; i < n; i++) d[i] = src[i * stride];
+  } else if constexpr (PREC == 1) {
+    float *d = static_cast<float *>(dst) + e0 + c * hpad + r0;
+    for (int64_t i = 0; i < n; i++) d[i] = static_cast<float>(src[i * stride]);
+  } else {
+    uint16_t *d = static_cast<uint16_t *>(dst) + e0 + (c >> 3) * (8 * hpad) + (c & 7) * 8;
+    for (int64_t i = 0; i < n; i++) {
+      const int64_t r = r0 + i;
+      d[(r >> 3) * 64 + (r & 7)] = to_bf16(static_cast<float>(src[i * stride] * inv));
+    }
+  }
+}
+
+// Column c of a view from row r0 on, as (pointer, stride).
+inline const double *view_column(const View &v, int64_t r0, int64_t c, int64_t &stride) {
+  stride = v.trans ? v.ld : 1;
+  return v.trans ? v.p + r0 * v.ld + c : v.p + r0 + c * v.ld;
+}
+
+template <int PREC>
+void fill_items_t(const Problem &p, bool tr, const OperatorPlan &op, int phase, int64_t i_begin, int64_t i_end,
+                  int64_t base, void *dst) {
+  const PhasePlan &ph = op.ph[phase];
 #pragma omp parallel for schedule(dynamic, 4)
   for (int64_t q = i_begin; q < i_end; q++) {
     const Item &it = ph.items[q];
-    const int64_t e0 = it.off[prec] - base;
+    const int64_t e0 = it.off[PREC] - base;
+    int64_t stride;
     if (phase == 0) {  // stacked B rows, one segment of columns
       int64_t row = 0;
       for (const RowPiece &pc : it.pieces) {
         const View B = eff_low(p, tr, pc.block).B;
-        const double inv = prec == 2 ? 1.0 / op.scale_b[pc.block] : 1.0;
-        for (int64_t c = 0; c < it.ncols; c++)
-          for (int64_t i = 0; i < pc.n; i++) put(e0 + item_index(prec, it.hpad, row + i, c), B.at(pc.r0 + i, c), inv);
+        const double inv = PREC == 2 ? 1.0 / op.scale_b[pc.block] : 1.0;
+        for (int64_t c = 0; c < it.ncols; c++) {
+          const double *src = view_column(B, pc.r0, c, stride);
+          put_run<PREC>(dst, e0, it.hpad, row, c, src, stride, pc.n, inv);
+        }
         row += pc.n;
       }
       continue;
     }
     int64_t col = 0;
-    for (const Segment &s : it.segs) {
+    for (const Segment &sg : it.segs) {
       View v;
       double inv = 1.0;
-      if (s.kind == 0) {
-        v = eff_full(p, tr, s.block).a;
-        if (prec == 2) inv = 1.0 / op.scale_fr[s.block];
+      if (sg.kind == 0) {
+        v = eff_full(p, tr, sg.block).a;
+        if (PREC == 2) inv = 1.0 / op.scale_fr[sg.block];
       } else {
-        v = eff_low(p, tr, s.block).A;
-        if (prec == 2) inv = 1.0 / op.scale_a[s.block];
+        v = eff_low(p, tr, sg.block).A;
+        if (PREC == 2) inv = 1.0 / op.scale_a[sg.block];
       }
-      for (int64_t c = 0; c < s.ncols; c++)
-        for (int64_t i = 0; i < it.h; i++) put(e0 + item_index(prec, it.hpad, i, col + c), v.at(s.row0 + i, c), inv);
-      col += s.ncols;
+      for (int64_t c = 0; c < sg.ncols; c++) {
+        const double *src = view_column(v, sg.row0, c, stride);
+        put_run<PREC>(dst, e0, it.hpad, 0, col + c, src, stride, it.h, inv);
+      }
+      col += sg.ncols;
     }
   }
+}
+
+}  // namespace
+
+void fill_items(const Problem &p, bool tr, const OperatorPlan &op, int phase, int prec, int64_t i_begin,
+                int64_t i_end, int64_t base, void *dst) {
+  if (prec == 0)
+    fill_items_t<0>(p, tr, op, phase, i_begin, i_end, base, dst);
+  else if (prec == 1)
+    fill_items_t<1>(p, tr, op, phase, i_begin, i_end, base, dst);
+  else
+    fill_items_t<2>(p, tr, op, phase, i_begin, i_end, base, dst);
 }
 
 // ---------------------------------------------------------------------------- matmat plan
