@@ -53,6 +53,15 @@ _HSIGS = {
     "bwh_export": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "bwh_write_to_file": (C.c_int, [_P, C.c_char_p]),
     "bwh_element_frames": (_I64, [_P, _P]),
+    "bwh_convert": (C.c_int, [_P, C.c_int, _P, _I64, _P]),
+    "bwh_element_normals": (_I64, [_P, _P]),
+    "bwh_rotation_matrix": (_I64, [_P, _P]),
+    "bwh_max_error_aca": (C.c_double, [_P]),
+    "bwh_full_blocks": (_I64, [_P, C.c_int, _P, _P, _P]),
+    "bwh_compute_fields": (_I64, [_P, C.c_int, _P, _I64, _P, _I64, _P, _I64]),
+    "bwh_storage_requirement": (_I64, [_P]),
+    "bwh_omp_threads": (C.c_int, [_P]),
+    "bwh_spatial_dimension": (C.c_int, [_P]),
     "bwh_gpu_handle": (_P, [_P]),
     "bwh_destroy": (C.c_int, [_P]),
     "bwh_last_error": (C.c_char_p, []),
@@ -108,15 +117,18 @@ class BigWhamIOGpu:
         self._transpose = False
 
     # ---------------------------------------------------------------- build
-    def set_gpu_storage(self, precisions=("fp64",), transpose: bool = False) -> None:
-        """Precisions (and H^T) to lay out on the device at the next build."""
+    def set_gpu_storage(self, precisions=("fp64",), transpose: bool = False, keep_host: bool = False) -> None:
+        """Precisions (and H^T) to lay out on the device at the next build;
+        keep_host: keep the host blocks after the upload (write_hmatrix needs
+        them)."""
         self._precisions = tuple(precisions)
         self._transpose = bool(transpose)
+        self._keep_host = bool(keep_host)
 
     def build_hierarchical_matrix(self, max_leaf_size: int, eta: float, eps_aca: float) -> None:
         _check(self._L.bwh_build(self._h, int(max_leaf_size), float(eta), float(eps_aca)))
         if self.use_cuda:
-            self.attach_gpu(self._precisions, self._transpose)
+            self.attach_gpu(self._precisions, self._transpose, release_host=not getattr(self, "_keep_host", False))
 
     def build_pattern(self, max_leaf_size: int, eta: float) -> None:
         """Cluster tree and block pattern only (BigWhamIO::BuildPattern); see
@@ -237,6 +249,94 @@ class BigWhamIOGpu:
         ab = np.stack([np.linalg.norm(v[:, 1] - v[:, 0], axis=1), np.linalg.norm(v[:, 3] - v[:, 0], axis=1)], 1) / 2
         return np.ascontiguousarray(np.hstack([fr, ab]))
 
+    # -- pass-throughs to the reference's BigWhamIO (py_bigwham.cc:141-260) --
+    def _vec(self, fn, *args):
+        n = int(fn(self._h, *args, None))
+        if n < 0:
+            _check(1)
+        out = np.empty(n)
+        fn(self._h, *args, out.ctypes.data)
+        return out
+
+    def get_spatial_dimension(self) -> int:
+        return int(self._L.bwh_spatial_dimension(self._h))
+
+    def convert_to_local(self, x_global):
+        x = np.ascontiguousarray(x_global, dtype=np.float64).ravel()
+        out = np.empty_like(x)
+        _check(self._L.bwh_convert(self._h, 0, x.ctypes.data, x.size, out.ctypes.data))
+        return out
+
+    def convert_to_global(self, x_local):
+        x = np.ascontiguousarray(x_local, dtype=np.float64).ravel()
+        out = np.empty_like(x)
+        _check(self._L.bwh_convert(self._h, 1, x.ctypes.data, x.size, out.ctypes.data))
+        return out
+
+    def get_element_normals(self):
+        return self._vec(self._L.bwh_element_normals)
+
+    def get_rotation_matrix(self):
+        return self._vec(self._L.bwh_rotation_matrix)
+
+    def get_max_error_ACA(self) -> float:
+        e = float(self._L.bwh_max_error_aca(self._h))
+        if e < 0:
+            _check(1)
+        return e
+
+    def get_full_blocks(self, original_order: bool = True):
+        """(values, rows, cols) of the full-rank blocks' entries (GetFullBlocks /
+        GetFullBlocksPerm)."""
+        n = int(self._L.bwh_full_blocks(self._h, int(original_order), None, None, None))
+        if n < 0:
+            _check(1)
+        val, row, col = np.empty(n), np.empty(n, np.int32), np.empty(n, np.int32)
+        self._L.bwh_full_blocks(self._h, int(original_order), val.ctypes.data, row.ctypes.data, col.ctypes.data)
+        return val, row, col
+
+    def _fields(self, kind, coor, x):
+        c = np.ascontiguousarray(coor, dtype=np.float64).ravel()
+        v = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        n = int(self._L.bwh_compute_fields(self._h, kind, c.ctypes.data, c.size, v.ctypes.data, v.size, None, 0))
+        if n < 0:
+            _check(1)
+        out = np.empty(n)
+        if self._L.bwh_compute_fields(self._h, kind, c.ctypes.data, c.size, v.ctypes.data, v.size, out.ctypes.data,
+                                      n) < 0:
+            _check(1)
+        return out
+
+    def compute_displacements(self, coor, x):
+        """ComputeDisplacements: the reference's host code (flat output)."""
+        return self._fields(0, coor, x)
+
+    def compute_stresses(self, coor, x):
+        """ComputeStresses: the reference's host code (flat output)."""
+        return self._fields(1, coor, x)
+
+    def get_storage_requirement(self) -> int:
+        return int(self._L.bwh_storage_requirement(self._h))
+
+    def get_gpu_storage_requirement(self) -> int:
+        """Device bytes held by the GPU H-matrix (0 before attach_gpu)."""
+        return int(self.gpu.info()["device_bytes"]) if self.gpu is not None else 0
+
+    def get_omp_threads(self) -> int:
+        return int(self._L.bwh_omp_threads(self._h))
+
+    def get_cuda_available(self) -> bool:
+        try:
+            import torch
+
+            return bool(torch.cuda.is_available()) and os.path.exists(A.LIB_PATH)
+        except Exception:
+            return False
+
+    def write_hmatrix(self, filename) -> None:
+        """Hmat::writeToFile's counterpart: a block file (see write_to_file)."""
+        self.write_to_file(filename)
+
     def write_to_file(self, path) -> None:
         """Save the built H-matrix as a block file (before attach_gpu): the
         reference's Hmat::writeToFile (src/hmat/hmatrix/hmat.cc:749-835) without
@@ -270,12 +370,15 @@ class BEMatrix(_LinOp):
     def __init__(self, kernel: str, coor, conn, properties, max_leaf_size: int = 32, eta: float = 3.0,
                  eps_aca: float = 1.0e-3, n_openMP_threads: int = 8, n_GPUs: int = 1, directly_build: bool = True,
                  verbose: bool = False, homogeneous_size_pattern: bool = False, fixed_rank=-1, useCuda=True,
-                 precisions=("fp64",), transpose: bool = False, device: int = 0):
+                 precisions=("fp64",), transpose: bool = False, device: int = 0, keep_host: bool = False):
         self.kernel_ = kernel
+        self.properties_ = properties
+        self.useCuda = True  # the matvec always runs on the GPU here
         self.max_leaf_size_, self.eta_, self.eps_aca_ = int(max_leaf_size), float(eta), float(eps_aca)
+        self.n_openMP_threads_ = n_openMP_threads
         self.H_ = BigWhamIOGpu(coor, conn, kernel, properties, n_openMP_threads, n_GPUs, verbose,
                                homogeneous_size_pattern, useCuda, fixed_rank, device)
-        self.H_.set_gpu_storage(precisions, transpose)
+        self.H_.set_gpu_storage(precisions, transpose, keep_host)
         self.built_ = False
         shape = (0, 0)
         if directly_build:
@@ -313,10 +416,134 @@ class BEMatrix(_LinOp):
         return self.H_.get_permutation()
 
     def getCollocationPoints(self):
-        return self.H_.get_collocation_points()
+        """(n_points, dim) collocation points of the mesh."""
+        n = self.getSpatialDimension()
+        return self.H_.get_collocation_points().reshape(-1, n)
+
+    def getMeshCollocationPoints(self):
+        return self.getCollocationPoints()
 
     def getSpatialDimension(self):
-        return 2 if self.kernel_.startswith("2D") else 3
+        return self.H_.get_spatial_dimension()
+
+    def get_omp_threads(self) -> int:
+        return self.H_.get_omp_threads()
+
+    def getStorageRequirement(self) -> int:
+        """Bytes of the H-matrix entries (entries x 8)."""
+        self._build()
+        return self.H_.get_storage_requirement()
+
+    def getGPUStorageRequirement(self) -> int:
+        """Device bytes of the laid-out H-matrix (all stored precisions)."""
+        self._build()
+        return self.H_.get_gpu_storage_requirement()
+
+    def convert_to_global(self, x_local):
+        return self.H_.convert_to_global(x_local)
+
+    def convert_to_local(self, x_global):
+        return self.H_.convert_to_local(x_global)
+
+    def get_element_normals(self):
+        return self.H_.get_element_normals()
+
+    def get_rotation_matrix(self):
+        return self.H_.get_rotation_matrix()
+
+    def get_diagonal(self):
+        return self.H_.get_diagonal()
+
+    def get_max_error_ACA(self) -> float:
+        return self.H_.get_max_error_ACA()
+
+    def isCudaAvailable(self) -> bool:
+        return self.H_.get_cuda_available()
+
+    def write_hmatrix(self, filename) -> None:
+        """The reference writes HDF5 (Hmat::writeToFile); this writes a block
+        file with the same content (HmatGpu.from_file / blockfile.read read it).
+        Needs keep_host=True (the host blocks are otherwise released once the
+        H-matrix is on the GPU)."""
+        self._build()
+        self.H_.write_hmatrix(filename)
+
+    def _getFullBlocks(self, original_order=True, keep_ratio: float = 1.0):
+        """Full-rank blocks as a scipy CSC matrix (bigwham4py.py:252-276)."""
+        from scipy.sparse import csc_matrix
+
+        if not (0 < keep_ratio <= 1):
+            raise ValueError("ratio must be a float between 0 and 1.")
+        self._build()
+        val, row, col = self.H_.get_full_blocks(original_order)
+        if keep_ratio < 1.0:
+            k = int(np.ceil(keep_ratio * val.size))
+            if k == 0:
+                return csc_matrix(self.shape)
+            thr = np.partition(np.abs(val), -k)[-k]
+            mask = np.abs(val) >= thr
+            val, row, col = val[mask], row[mask], col[mask]
+        return csc_matrix((val, (row, col)), shape=self.shape)
+
+    def _getPattern(self):
+        return self.H_.get_hpattern()
+
+    def H_ILU_prec(self, fill_factor=1, drop_tol=1e-3, keep_ratio=1.0):
+        """ILU of the full-rank blocks (scipy spilu, host), as the reference's
+        H_ILU_prec (bigwham4py.py:345-360); the full-rank blocks stay on the host
+        beside the GPU H-matrix, so this works with the GPU matvec."""
+        from scipy.sparse.linalg import LinearOperator, spilu
+
+        ilu = spilu(self._getFullBlocks(keep_ratio=keep_ratio), fill_factor=fill_factor, drop_tol=drop_tol)
+        return LinearOperator(self.shape, ilu.solve)
+
+    def compute_displacements(self, list_coor, local_solu):
+        """Displacements at points (the reference's host code); (n_points, dim)."""
+        self._build()
+        n = self.getSpatialDimension()
+        list_coor = np.asarray(list_coor, dtype=np.float64)
+        assert n == list_coor.shape[1], "Coordinates dimension of the given points is not matching the problem spatial dimension !"
+        return self.H_.compute_displacements(list_coor, local_solu).reshape(-1, n)
+
+    def compute_stresses(self, list_coor, local_solu):
+        """Stresses at points (the reference's host code); (n_points, 3 or 6)."""
+        self._build()
+        n = self.getSpatialDimension()
+        list_coor = np.asarray(list_coor, dtype=np.float64)
+        assert n == list_coor.shape[1], "Coordinates dimension of the given points is not matching the problem spatial dimension !"
+        return self.H_.compute_stresses(list_coor, local_solu).reshape(-1, 3 if n == 2 else 6)
+
+    def getMatvecTime(self, N_matvec=100):
+        """Seconds per matvec (host arrays, as the reference times it)."""
+        import time
+
+        x = np.ones(self.shape[0])
+        self._matvec(x)
+        t0 = time.time()
+        for _ in range(N_matvec):
+            self._matvec(x)
+        return (time.time() - t0) / N_matvec
+
+    def plotPattern(self, plot_index=False):
+        """The block pattern as a matplotlib figure (needs matplotlib)."""
+        import matplotlib.pyplot as plt
+        from matplotlib.collections import PatchCollection
+        from matplotlib.patches import Rectangle
+
+        pat = self._getPattern()
+        max_y = pat[:, 3].max()
+        fig, ax = plt.subplots()
+        patches = [Rectangle((r[1], max_y - r[0] - abs(r[0] - r[2])), abs(r[1] - r[3]), abs(r[0] - r[2])) for r in pat]
+        pc = PatchCollection(patches, edgecolors="black", alpha=0.4)
+        pc.set_array(pat[:, 4])
+        ax.add_collection(pc)
+        ax.set_ylim([pat[:, 0].min(), pat[:, 3].max()])
+        ax.set_xlim([pat[:, 1].min(), pat[:, 2].max()])
+        ax.set_aspect("equal")
+        return fig
+
+    def __getitem__(self, indices):
+        raise Exception("Bigwham matrix selection not implemented for CUDA support.")
 
     def H_diag(self):
         return self.H_.get_diagonal()

@@ -19,6 +19,7 @@ struct bwh_io {
   std::unique_ptr<BigWhamIO> io;
   std::shared_ptr<bigwham_b200::HmatGpu> gpu;
   std::vector<std::pair<std::string, int64_t>> tuning;  // for the next bwh_attach_gpu
+  std::shared_ptr<bigwham::Hmat<double>> cpu_kept;        // host blocks kept by bwh_attach_gpu(release_host = 0)
 };
 
 namespace {
@@ -87,7 +88,10 @@ int bwh_attach_gpu(bwh_io *h, int device, int storage, int release_host) {
     auto gpu = std::make_shared<bigwham_b200::HmatGpu>(cpu, device, storage, h->tuning);
     h->io->setHmat(gpu);
     h->gpu = gpu;
-    if (release_host) cpu->hmatMemFree();
+    if (release_host)
+      cpu->hmatMemFree();
+    else
+      h->cpu_kept = cpu;
     return 0;
   });
 }
@@ -250,12 +254,111 @@ int64_t bwh_element_frames(const bwh_io *h, double *out) {
 
 int bwh_write_to_file(const bwh_io *h, const char *path) {
   if (!h || !path) return fail("null argument");
-  if (h->gpu) return fail("bwh_write_to_file must run before bwh_attach_gpu (the host blocks are released there)");
+  if (h->gpu && !h->cpu_kept)
+    return fail("bwh_write_to_file: the host blocks were released by bwh_attach_gpu (attach with release_host = 0 "
+                "to keep them)");
   return guarded([&] {
-    bigwham_b200::write_block_file(*h->io->getHmat(), path);
+    bigwham_b200::write_block_file(h->gpu ? *h->cpu_kept : *h->io->getHmat(), path);
     return 0;
   });
 }
+
+int bwh_convert(const bwh_io *h, int to_global, const double *in, int64_t n, double *out) {
+  if (!h || !in || !out || n < 0) return fail("null argument");
+  return guarded([&] {
+    il::Array<double> v = to_global ? h->io->ConvertToGlobal(il::ArrayView<double>{in, n})
+                                    : h->io->ConvertToLocal(il::ArrayView<double>{in, n});
+    if (v.size() != n) return fail("bwh_convert: the mesh has a different number of values");
+    std::memcpy(out, v.data(), sizeof(double) * (size_t)n);
+    return 0;
+  });
+}
+
+namespace {
+int64_t vec_out(const std::vector<double> &v, double *out) {
+  if (out) std::memcpy(out, v.data(), sizeof(double) * v.size());
+  return (int64_t)v.size();
+}
+}  // namespace
+
+int64_t bwh_element_normals(const bwh_io *h, double *out) {
+  if (!h) return fail("null handle"), -1;
+  int64_t n = -1;
+  guarded([&] {
+    n = vec_out(h->io->GetElementNormals(), out);
+    return 0;
+  });
+  return n;
+}
+
+int64_t bwh_rotation_matrix(const bwh_io *h, double *out) {
+  if (!h) return fail("null handle"), -1;
+  int64_t n = -1;
+  guarded([&] {
+    n = vec_out(h->io->GetRotationMatrix(), out);
+    return 0;
+  });
+  return n;
+}
+
+double bwh_max_error_aca(const bwh_io *h) {
+  if (!h || !h->io->is_built()) return fail("bwh_max_error_aca before bwh_build"), -1.0;
+  double e = -1.0;
+  guarded([&] {
+    e = h->io->GetMaxErrorACA();
+    return 0;
+  });
+  return e;
+}
+
+int64_t bwh_full_blocks(const bwh_io *h, int original_order, double *val, int32_t *row, int32_t *col) {
+  if (!h || !h->io->is_built()) return fail("bwh_full_blocks before bwh_build"), -1;
+  int64_t n = -1;
+  guarded([&] {
+    std::vector<double> v;
+    std::vector<int> pos;
+    if (original_order)
+      h->io->GetFullBlocks(v, pos);
+    else
+      h->io->GetFullBlocksPerm(v, pos);
+    n = (int64_t)v.size();
+    if (val) std::memcpy(val, v.data(), sizeof(double) * v.size());
+    if (row && col)
+      for (int64_t i = 0; i < n; i++) {
+        row[i] = pos[2 * i];
+        col[i] = pos[2 * i + 1];
+      }
+    return 0;
+  });
+  return n;
+}
+
+int64_t bwh_compute_fields(const bwh_io *h, int kind, const double *coor_obs, int64_t n_coor, const double *sol,
+                           int64_t n_sol, double *out, int64_t out_len) {
+  if (!h || !coor_obs || !sol || n_coor < 0 || n_sol < 0) return fail("null argument"), -1;
+  int64_t n = -1;
+  guarded([&] {
+    const std::vector<double> c(coor_obs, coor_obs + n_coor);
+    il::Array<double> v = kind == 0 ? h->io->ComputeDisplacements(c, il::ArrayView<double>{sol, n_sol})
+                                    : h->io->ComputeStresses(c, il::ArrayView<double>{sol, n_sol});
+    n = v.size();
+    if (out) {
+      if (out_len < n) return fail("bwh_compute_fields: out is too short");
+      std::memcpy(out, v.data(), sizeof(double) * (size_t)n);
+    }
+    return 0;
+  });
+  return n;
+}
+
+int64_t bwh_storage_requirement(const bwh_io *h) {
+  if (!h || !h->io->is_built()) return fail("bwh_storage_requirement before bwh_build"), -1;
+  return (int64_t)h->io->getHmat()->nbOfEntries() * (int64_t)sizeof(double);
+}
+
+int bwh_omp_threads(const bwh_io *h) { return h ? h->io->GetOmpThreads() : -1; }
+
+int bwh_spatial_dimension(const bwh_io *h) { return h ? h->io->spatial_dimension() : -1; }
 
 struct bw_hmat *bwh_gpu_handle(bwh_io *h) { return (h && h->gpu) ? h->gpu->handle() : nullptr; }
 

@@ -91,10 +91,38 @@ int bwh_export(const bwh_io *io, int64_t *fr, int64_t *lr, double *fr_data, doub
 
 /* Save the built H-matrix as a block file (bw_file_write_blocks of
  * include/bigwham_b200.h: pattern with its HPattern spots, permutations, every
- * block and the ACA error estimates), before bwh_attach_gpu.  The content of
+ * block and the ACA error estimates), before bwh_attach_gpu or after one with
+ * release_host = 0.  The content of
  * the reference's Hmat::writeToFile (src/hmat/hmatrix/hmat.cc:749-835), which
  * needs HDF5.  Load it with bw_create_from_file / HmatGpu.from_file. */
 int bwh_write_to_file(const bwh_io *io, const char *path);
+
+/* Pass-throughs to the reference's BigWhamIO, as the pybind11 module
+ * exposes them (interfaces/python/py_bigwham.cc:141-260).  Array results:
+ * the function returns the element count and fills `out` when it is
+ * non-null (two calls: size, then data).  -1 on error (bwh_last_error). */
+/* ConvertToLocal (to_global = 0) / ConvertToGlobal (1): n values, out n values. */
+int bwh_convert(const bwh_io *io, int to_global, const double *in, int64_t n, double *out);
+/* GetElementNormals / GetRotationMatrix (flattened per element). */
+int64_t bwh_element_normals(const bwh_io *io, double *out);
+int64_t bwh_rotation_matrix(const bwh_io *io, double *out);
+/* GetMaxErrorACA (largest ACA error estimate over the low-rank blocks). */
+double bwh_max_error_aca(const bwh_io *io);
+/* GetFullBlocks (original_order != 0) / GetFullBlocksPerm: the full-rank
+ * blocks' entries with their row and column; returns the entry count. */
+int64_t bwh_full_blocks(const bwh_io *io, int original_order, double *val, int32_t *row, int32_t *col);
+/* ComputeDisplacements (kind 0) / ComputeStresses (kind 1) at the points
+ * coor_obs (n_coor values, spatial dimension per point) for the solution sol
+ * (n_sol values, local element frames, original ordering): out_len values
+ * (points x dof, or points x 3 / 6 stress components in 2D / 3D); returns the
+ * value count.  The reference's own host code. */
+int64_t bwh_compute_fields(const bwh_io *io, int kind, const double *coor_obs, int64_t n_coor, const double *sol,
+                           int64_t n_sol, double *out, int64_t out_len);
+/* GetStorageRequirement in bytes (entries x 8) and GetOmpThreads. */
+int64_t bwh_storage_requirement(const bwh_io *io);
+int bwh_omp_threads(const bwh_io *io);
+/* Spatial dimension of the mesh (2 or 3). */
+int bwh_spatial_dimension(const bwh_io *io);
 
 /* The device H-matrix after bwh_attach_gpu (owned by io), for the
  * extensions of include/bigwham_b200.h (precision choice, H^T, matmat). */
