@@ -28,10 +28,14 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 HOST_LIB_PATH = os.path.join(_HERE, "_lib", "libbigwham_host.so")
 
 kernels_id = ["2DS0-H", "2DS1-H", "S3DS0-H", "Axi3DS0-H", "3DT0-H", "3DT6-H", "3DR0-H", "3DR0-H-mode1"]
+# kernels of the rectangular (source mesh x receiver mesh) BigWhamIO, bigwham_io.cc:300-470
+kernels_rect_id = ["2DS0-2DS0-H", "2DS1-2DS1-H", "2DS0-2DP-T", "3DT0-3DT0-H", "3DR0-3DR0-H", "3DR0-3DR0-H-mode1"]
 
 _P, _I64 = C.c_void_p, C.c_int64
 _HSIGS = {
     "bwh_create": (C.c_int, [_P, _I64, _P, _I64, C.c_char_p, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_P)]),
+    "bwh_create_rect": (C.c_int, [_P, _I64, _P, _I64, _P, _I64, _P, _I64, C.c_char_p, _P, C.c_int, C.c_int, C.c_int,
+                                  C.c_int, C.POINTER(_P)]),
     "bwh_build": (C.c_int, [_P, C.c_int, C.c_double, C.c_double]),
     "bwh_build_pattern": (C.c_int, [_P, C.c_int, C.c_double]),
     "bwh_attach_gpu": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
@@ -115,6 +119,34 @@ class BigWhamIOGpu:
         self.gpu: HmatGpu | None = None
         self._precisions = ("fp64",)
         self._transpose = False
+
+    @classmethod
+    def rectangular(cls, coor_src, conn_src, coor_rec, conn_rec, kernel: str, properties, n_openMP_threads: int = 8,
+                    n_GPUs: int = 1, verbose: bool = False, homogeneous_size_pattern: bool = False,
+                    useCuda: bool = True, fixed_rank: int = -1, device: int = 0) -> "BigWhamIOGpu":
+        """The rectangular BigWhamIO (pybind11 BigWhamIORect): receiver rows,
+        source columns."""
+        if kernel not in kernels_rect_id:
+            raise ValueError(f"invalid kernel {kernel}; available: {', '.join(kernels_rect_id)}")
+        L = host_lib()
+        arrs = [np.ascontiguousarray(a, dtype=t).ravel() for a, t in
+                ((coor_src, np.float64), (conn_src, np.int32), (coor_rec, np.float64), (conn_rec, np.int32))]
+        props = np.ascontiguousarray(properties, dtype=np.float64).ravel()
+        h = C.c_void_p()
+        _check(L.bwh_create_rect(*[v for a in arrs for v in (a.ctypes.data, a.size)], kernel.encode(),
+                                 props.ctypes.data, props.size, int(n_openMP_threads), int(verbose), int(fixed_rank),
+                                 C.byref(h)))
+        self = cls.__new__(cls)
+        self._h, self._L = h, L
+        self._coor, self._conn = arrs[0], arrs[1]  # source mesh
+        self._keep = arrs
+        self.kernel = kernel
+        self.use_cuda = bool(useCuda)
+        self.device = int(device)
+        self.gpu = None
+        self._precisions = ("fp64",)
+        self._transpose = False
+        return self
 
     # ---------------------------------------------------------------- build
     def set_gpu_storage(self, precisions=("fp64",), transpose: bool = False, keep_host: bool = False) -> None:
@@ -554,3 +586,54 @@ class BEMatrix(_LinOp):
 
         inv = 1.0 / self.H_diag()
         return LinearOperator(self.shape, lambda v: inv * np.asarray(v).ravel(), dtype=float)
+
+
+class BEMatrixRectangular(_LinOp):
+    """scipy LinearOperator over the GPU H-matrix of a source mesh and a
+    receiver mesh (reference: bigwham4py.BEMatrixRectangular)."""
+
+    def __init__(self, kernel: str, coor_src, conn_src, coor_rec, conn_rec, properties, max_leaf_size: int = 100,
+                 eta: float = 3.0, eps_aca: float = 1.0e-3, n_openMP_threads: int = 8, n_GPUs: int = 1,
+                 directly_build: bool = True, verbose: bool = False, homogeneous_size_pattern: bool = False,
+                 useCuda=True, fixed_rank=-1, precisions=("fp64",), transpose: bool = False, device: int = 0):
+        self.kernel_ = kernel
+        self.properties_ = properties
+        self.max_leaf_size_, self.eta_, self.eps_aca_ = int(max_leaf_size), float(eta), float(eps_aca)
+        self.n_openMP_threads_ = n_openMP_threads
+        self.H_ = BigWhamIOGpu.rectangular(coor_src, conn_src, coor_rec, conn_rec, kernel, properties,
+                                           n_openMP_threads, n_GPUs, verbose, homogeneous_size_pattern, useCuda,
+                                           fixed_rank, device)
+        self.H_.set_gpu_storage(precisions, transpose)
+        self.built_ = False
+        shape = (0, 0)
+        if directly_build:
+            self._build()
+            shape = (self.H_.matrix_size(0), self.H_.matrix_size(1))
+        else:
+            self.H_.build_pattern(self.max_leaf_size_, self.eta_)
+        self.dtype_ = np.dtype(float)
+        super().__init__(self.dtype_, shape)
+
+    def _build(self):
+        if not self.built_:
+            self.H_.build_hierarchical_matrix(self.max_leaf_size_, self.eta_, self.eps_aca_)
+            self.built_ = True
+            self.matvec_size_ = self.H_.matrix_size(0)
+            super().__init__(np.dtype(float), (self.H_.matrix_size(0), self.H_.matrix_size(1)))
+
+    def _matvec(self, v):
+        return self.H_.matvec(np.asarray(v, dtype=np.float64).ravel())
+
+    def _rmatvec(self, v):
+        if self.H_.gpu is None or not self.H_.gpu.has_transpose:
+            raise RuntimeError("H^T not stored: build with transpose=True")
+        return self.H_.gpu.rmatvec(np.asarray(v, dtype=np.float64).ravel())
+
+    def getCompression(self) -> float:
+        return self.H_.get_compression_ratio()
+
+    def getPermutation(self):
+        return self.H_.get_permutation()
+
+    def getSpatialDimension(self):
+        return self.H_.get_spatial_dimension()

@@ -64,6 +64,26 @@ int bwh_create(const double *coor, int64_t n_coor, const int *conn, int64_t n_co
   });
 }
 
+int bwh_create_rect(const double *coor_src, int64_t n_coor_src, const int *conn_src, int64_t n_conn_src,
+                    const double *coor_rec, int64_t n_coor_rec, const int *conn_rec, int64_t n_conn_rec,
+                    const char *kernel, const double *properties, int n_properties, int n_openmp_threads,
+                    int verbose, int fixed_rank, bwh_io **out) {
+  if (!out || !coor_src || !conn_src || !coor_rec || !conn_rec || !kernel || !properties)
+    return fail("null argument");
+  *out = nullptr;
+  return guarded([&] {
+    openblas_set_num_threads(1);
+    std::vector<double> cs(coor_src, coor_src + n_coor_src), cr(coor_rec, coor_rec + n_coor_rec);
+    std::vector<int> es(conn_src, conn_src + n_conn_src), er(conn_rec, conn_rec + n_conn_rec);
+    std::vector<double> p(properties, properties + n_properties);
+    std::unique_ptr<bwh_io> h(new bwh_io);
+    h->io.reset(new BigWhamIO(cs, es, cr, er, std::string(kernel), p, n_openmp_threads, 0, verbose != 0, false,
+                              false, fixed_rank));
+    *out = h.release();
+    return 0;
+  });
+}
+
 int bwh_build(bwh_io *h, int leaf, double eta, double eps) {
   if (!h) return fail("null handle");
   return guarded([&] {

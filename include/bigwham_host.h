@@ -30,6 +30,14 @@ int bwh_create(const double *coor, int64_t n_coor, const int *conn, int64_t n_co
                const double *properties, int n_properties, int n_openmp_threads, int verbose, int fixed_rank,
                bwh_io **out);
 
+/* The rectangular BigWhamIO (src/io/bigwham_io.h:85-96; pybind11
+ * BigWhamIORect): a source mesh and a different receiver mesh, kernels such
+ * as "3DR0-3DR0-H"; the H-matrix has receiver rows and source columns. */
+int bwh_create_rect(const double *coor_src, int64_t n_coor_src, const int *conn_src, int64_t n_conn_src,
+                    const double *coor_rec, int64_t n_coor_rec, const int *conn_rec, int64_t n_conn_rec,
+                    const char *kernel, const double *properties, int n_properties, int n_openmp_threads,
+                    int verbose, int fixed_rank, bwh_io **out);
+
 /* BigWhamIO::BuildHierarchicalMatrix (bigwham_io.cc:635-704), host build. */
 int bwh_build(bwh_io *io, int max_leaf_size, double eta, double eps_aca);
 /* BigWhamIO::BuildPattern (src/io/bigwham_io.cc:487-511): cluster tree and

@@ -49,3 +49,37 @@ def test_dense_single_block_and_all_low_rank():
                               arr.perm1, device=-1, plan_only=True, precisions=("fp64",))
         x = np.random.default_rng(5).uniform(-1, 1, arr.n_cols)
         assert _rel(replay(h, x, "fp64"), oracle_matvec_perm(arr, x, 1)) < 1e-14
+
+
+def test_reference_built_rectangular_hmatrix():
+    """A real rectangular H-matrix (BigWhamIO's source x receiver constructor,
+    kernel 3DR0-3DR0-H: a 10 x 10 crack acting on a 7 x 9 grid of receivers on
+    a parallel plane): export, lay out, replay against the oracle, H and H^T."""
+    import os
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if not os.path.exists(os.path.join(root, "bigwham_dev_b200", "_lib", "libbigwham_host.so")):
+        pytest.skip("host adapter not built")
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+    from bigwham_dev_b200.meshes import square_crack_3d
+    from oracle import HmatArrays
+
+    cs, es = square_crack_3d(10)
+    cr, er = square_crack_3d(7, 9, half=1.3)
+    cr = cr + np.array([0.05, -0.1, 0.4])
+    io = BigWhamIOGpu.rectangular(cs, es, cr, er, "3DR0-3DR0-H", [1.0, 0.25], 2, useCuda=False)
+    io.build_hierarchical_matrix(16, 3.0, 1e-6)
+    ex = io.export_blocks()
+    assert (ex["n_rows"], ex["n_cols"]) == (3 * len(er), 3 * len(es))
+    assert sorted(ex["perm0"]) == list(range(len(er))) and sorted(ex["perm1"]) == list(range(len(es)))
+    assert np.array_equal(io.get_permutation(), ex["perm1"])
+    io.close()
+    arr = HmatArrays(ex["dof"], ex["n_rows"], ex["n_cols"], ex["fr"], ex["lr"], ex["fr_data"], ex["lr_data"],
+                     ex["perm0"], ex["perm1"])
+    h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
+                          arr.perm1, device=-1, plan_only=True, precisions=("fp64", "bf16"), transpose=True)
+    x = np.random.default_rng(4).uniform(-1, 1, arr.n_cols)
+    xr = np.random.default_rng(5).uniform(-1, 1, arr.n_rows)
+    assert _rel(replay(h, x, "fp64"), oracle_matvec_perm(arr, x, 1)) < 1e-14
+    assert _rel(replay(h, xr, "fp64", True), oracle_rmatvec_perm(arr, xr, 1)) < 1e-14
+    assert _rel(replay(h, x, "bf16"), oracle_matvec_perm(arr, x, 1)) < 1e-2
