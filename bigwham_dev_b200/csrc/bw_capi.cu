@@ -256,6 +256,17 @@ void host_copy(double *dst, const double *src, int64_t n) {
   }
 }
 
+// dst[0:bytes] = 0 with all host threads (staging pieces are 256 MB).
+void par_zero(void *dst, size_t bytes) {
+  const size_t kPart = size_t(4) << 20;
+  const int64_t parts = (int64_t)((bytes + kPart - 1) / kPart);
+#pragma omp parallel for schedule(static) if (parts > 1)
+  for (int64_t p = 0; p < parts; p++) {
+    const size_t a = (size_t)p * kPart, b = std::min(bytes, a + kPart);
+    std::memset(static_cast<unsigned char *>(dst) + a, 0, b - a);
+  }
+}
+
 // Bytes of the gathered-x region for a precision: the G values (+16 bytes,
 // vector runs are staged in 16-byte aligned windows) and, for BF16, a second
 // array of packed hi/lo words at the next 256-byte boundary.
@@ -309,7 +320,7 @@ void staged_upload(bw_hmat *h, void *dev, int64_t n_elems, int es, int64_t nit, 
         continue;
       }
       if (used[which]) BW_CUDA(cudaEventSynchronize(ev[which]));
-      std::memset(stage[which], 0, bytes);
+      par_zero(stage[which], bytes);
       fill(q, qe, e0, stage[which]);
       BW_CUDA(cudaMemcpyAsync(static_cast<unsigned char *>(dev) + (size_t)e0 * es, stage[which], bytes,
                               cudaMemcpyHostToDevice, h->stream));
