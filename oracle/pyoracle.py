@@ -95,6 +95,9 @@ def _ref():
         lib.ref_create.argtypes = [_f64p, C.c_int64, _i32p, C.c_int64, C.c_char_p, _f64p, C.c_int, C.c_int,
                                    C.c_int]
         lib.ref_create.restype = C.c_void_p
+        lib.ref_create_rect.argtypes = [_f64p, C.c_int64, _i32p, C.c_int64, _f64p, C.c_int64, _i32p, C.c_int64,
+                                        C.c_char_p, _f64p, C.c_int, C.c_int, C.c_int]
+        lib.ref_create_rect.restype = C.c_void_p
         lib.ref_build.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
         lib.ref_size.argtypes = [C.c_void_p, C.c_int]
         lib.ref_size.restype = C.c_int64
@@ -157,6 +160,27 @@ class RefHmat:
             raise RuntimeError(f"reference BuildHierarchicalMatrix failed ({rc})")
         self.shape = (lib.ref_size(self._h, 0), lib.ref_size(self._h, 1))
         self.dof = lib.ref_dof(self._h)
+
+    @classmethod
+    def rectangular(cls, kernel: str, coor_src, conn_src, coor_rec, conn_rec, properties, max_leaf_size=32,
+                    eta=3.0, eps_aca=1e-3, n_threads=8, verbose=False) -> "RefHmat":
+        """The reference's rectangular BigWhamIO (receiver rows, source columns)."""
+        lib = _ref()
+        self = cls.__new__(cls)
+        self.n_threads = lib.ref_set_threads(int(n_threads))
+        a = [np.ascontiguousarray(v, dtype=t).ravel() for v, t in
+             ((coor_src, np.float64), (conn_src, np.int32), (coor_rec, np.float64), (conn_rec, np.int32))]
+        props = np.ascontiguousarray(properties, dtype=np.float64).ravel()
+        self._h = lib.ref_create_rect(a[0], a[0].size, a[1], a[1].size, a[2], a[2].size, a[3], a[3].size,
+                                      kernel.encode(), props, props.size, int(n_threads), int(verbose))
+        if not self._h:
+            raise RuntimeError("reference rectangular BigWhamIO construction failed")
+        rc = lib.ref_build(self._h, int(max_leaf_size), float(eta), float(eps_aca))
+        if rc != 0:
+            raise RuntimeError(f"reference BuildHierarchicalMatrix failed ({rc})")
+        self.shape = (lib.ref_size(self._h, 0), lib.ref_size(self._h, 1))
+        self.dof = lib.ref_dof(self._h)
+        return self
 
     def __del__(self):
         if getattr(self, "_h", None) and _ref_lib is not None:

@@ -69,6 +69,23 @@ void *ref_create(const double *coor, int64_t n_coor, const int *conn, int64_t n_
   }
 }
 
+// Rectangular BigWhamIO (src/io/bigwham_io.h:85-96): source mesh x receiver
+// mesh, kernels such as "3DR0-3DR0-H"; CUDA off.
+void *ref_create_rect(const double *coor_src, int64_t n_coor_src, const int *conn_src, int64_t n_conn_src,
+                      const double *coor_rec, int64_t n_coor_rec, const int *conn_rec, int64_t n_conn_rec,
+                      const char *kernel, const double *props, int n_props, int n_threads, int verbose) {
+  try {
+    std::vector<double> cs(coor_src, coor_src + n_coor_src), cr(coor_rec, coor_rec + n_coor_rec);
+    std::vector<int> es(conn_src, conn_src + n_conn_src), er(conn_rec, conn_rec + n_conn_rec);
+    std::vector<double> p(props, props + n_props);
+    auto *h = new RefHandle;
+    h->io.reset(new BigWhamIO(cs, es, cr, er, std::string(kernel), p, n_threads, 0, verbose != 0, false, false, -1));
+    return h;
+  } catch (...) {
+    return nullptr;
+  }
+}
+
 int ref_build(void *h, int leaf, double eta, double eps) {
   try {
     H(h)->io->BuildHierarchicalMatrix(leaf, eta, eps);

@@ -3,7 +3,8 @@
 Run in a tree where the reference library has been compiled by
 ``make -C oracle ref`` (it needs the reference sources only at compile time):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py           # square cases (tests/golden/*.npz)
+    python tests/golden/make_golden.py --rect    # rectangular cases (tests/golden/rect/)
 
 For every case the reference's own code (BigWhamIO + BuildHierarchicalMatrix,
 src/io/bigwham_io.cc:635-704) builds the H-matrix; the fixture stores the flat
@@ -39,6 +40,17 @@ CASES = {
 }
 
 
+# rectangular cases (source mesh x receiver mesh), stored under rect/ so the
+# square-only fixture set (every *.npz here) is unchanged
+RECT_CASES = {
+    # name: (kernel, source mesh fn, receiver mesh fn, properties, leaf, eta, eps, seed)
+    "3dr0_rect": ("3DR0-3DR0-H", lambda: square_crack_3d(10),
+                  lambda: (square_crack_3d(7, 9, half=1.3)[0] + np.array([0.05, -0.1, 0.4]),
+                           square_crack_3d(7, 9, half=1.3)[1]),
+                  [1.0, 0.25], 16, 3.0, 1e-6, 6),
+}
+
+
 def dense_from(arr):
     D = np.zeros((arr.n_rows, arr.n_cols))
     for i0, j0, a in arr.fr_blocks():
@@ -71,5 +83,24 @@ def main():
               f"entries={arr.fr_data.size + arr.lr_data.size} size={os.path.getsize(out) / 1e3:.0f} kB")
 
 
+def main_rect():
+    os.makedirs(os.path.join(HERE, "rect"), exist_ok=True)
+    for name, (kernel, src, rec, props, leaf, eta, eps, seed) in RECT_CASES.items():
+        (cs, es), (cr, er) = src(), rec()
+        R = RefHmat.rectangular(kernel, cs, es, cr, er, props, leaf, eta, eps, n_threads=4)
+        arr = R.arrays()
+        x = np.random.default_rng(seed).uniform(-1.0, 1.0, R.shape[1])
+        Rd = RefHmat.rectangular(kernel, cs, es, cr, er, props, leaf, 0.0, eps, n_threads=4)
+        D = dense_from(Rd.arrays())
+        out = os.path.join(HERE, "rect", f"{name}.npz")
+        arr.save(out, kernel=kernel, properties=np.asarray(props), leaf=leaf, eta=eta, eps=eps, seed=seed, x=x,
+                 y_ref=R.matvec(x), y_perm_ref=R.matvec_perm(x), y_dense=Rd.matvec(x), y_dense_assembled=D @ x)
+        print(f"{name}: {R.shape[0]} x {R.shape[1]} n_fr={arr.fr.shape[0]} n_lr={arr.lr.shape[0]} "
+              f"size={os.path.getsize(out) / 1e3:.0f} kB")
+
+
 if __name__ == "__main__":
-    main()
+    if "--rect" in sys.argv:
+        main_rect()
+    else:
+        main()

@@ -83,3 +83,25 @@ def test_reference_built_rectangular_hmatrix():
     assert _rel(replay(h, x, "fp64"), oracle_matvec_perm(arr, x, 1)) < 1e-14
     assert _rel(replay(h, xr, "fp64", True), oracle_rmatvec_perm(arr, xr, 1)) < 1e-14
     assert _rel(replay(h, x, "bf16"), oracle_matvec_perm(arr, x, 1)) < 1e-2
+
+
+def test_rectangular_golden_against_the_reference_matvec():
+    """tests/golden/rect/3dr0_rect.npz (make_golden.py --rect): a 3DR0-3DR0-H
+    matrix built by the reference, with the reference's own MatVec and
+    MatVecPerm outputs.  The oracle restatement and our replayed plan must
+    match them to 1e-12; both are within the ACA tolerance of the dense
+    (eta = 0) product."""
+    import os
+
+    from oracle import HmatArrays, oracle_matvec
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rect", "3dr0_rect.npz")
+    arr, ex = HmatArrays.load(path)
+    assert arr.n_rows != arr.n_cols
+    x = ex["x"]
+    assert _rel(oracle_matvec(arr, x, 1), ex["y_ref"]) < 1e-12
+    h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
+                          arr.perm1, device=-1, plan_only=True, precisions=("fp64",))
+    # MatVecPerm takes x in the clustered ordering, as the replay does
+    assert _rel(replay(h, x, "fp64"), ex["y_perm_ref"]) < 1e-12
+    assert _rel(ex["y_ref"], ex["y_dense"]) < 1e-4
