@@ -522,6 +522,70 @@ void fill_items(const Problem &p, bool tr, const OperatorPlan &op, int phase, in
     fill_items_t<2>(p, tr, op, phase, i_begin, i_end, base, dst);
 }
 
+void build_pack_runs(const Problem &p, bool tr, const OperatorPlan &op, int phase, int prec, const double *fr_base,
+                     int64_t fr_len, const double *lr_base, int64_t lr_len, std::vector<PackRun> &out) {
+  const PhasePlan &ph = op.ph[phase];
+  out.clear();
+  auto locate = [&](const View &v, int64_t rows, int64_t cols, PackRun &r) {
+    // every element of the view the run reads must lie in its array
+    const int64_t span = v.trans ? (rows - 1) * v.ld + cols : (cols - 1) * v.ld + rows;
+    if (v.p >= fr_base && v.p + span <= fr_base + fr_len) {
+      r.array = 0;
+      r.src_off = v.p - fr_base;
+    } else if (v.p >= lr_base && v.p + span <= lr_base + lr_len) {
+      r.array = 1;
+      r.src_off = v.p - lr_base;
+    } else {
+      throw std::invalid_argument("build_pack_runs: a block view lies outside the flat block arrays");
+    }
+    r.ld = v.ld;
+    r.trans = v.trans ? 1 : 0;
+  };
+  for (const Item &it : ph.items) {
+    PackRun r;
+    std::memset(&r, 0, sizeof r);
+    r.item_off = it.off[prec];
+    r.hpad = it.hpad;
+    if (phase == 0) {
+      int64_t row = 0;
+      for (const RowPiece &pc : it.pieces) {
+        const EffLow e = eff_low(p, tr, pc.block);
+        locate(e.B, e.r, e.n, r);
+        r.inv = prec == 2 ? 1.0 / op.scale_b[pc.block] : 1.0;
+        r.dst_r0 = i32(row, "item row");
+        r.dst_c0 = 0;
+        r.src_r0 = i32(pc.r0, "factor row");
+        r.src_c0 = 0;
+        r.n = i32(pc.n, "rows");
+        r.ncols = i32(it.ncols, "columns");
+        out.push_back(r);
+        row += pc.n;
+      }
+      continue;
+    }
+    int64_t col = 0;
+    for (const Segment &sg : it.segs) {
+      if (sg.kind == 0) {
+        const EffFull e = eff_full(p, tr, sg.block);
+        locate(e.a, e.m, e.n, r);
+        r.inv = prec == 2 ? 1.0 / op.scale_fr[sg.block] : 1.0;
+      } else {
+        const EffLow e = eff_low(p, tr, sg.block);
+        locate(e.A, e.m, e.r, r);
+        r.inv = prec == 2 ? 1.0 / op.scale_a[sg.block] : 1.0;
+      }
+      r.dst_r0 = 0;
+      r.dst_c0 = i32(col, "item column");
+      r.src_r0 = i32(sg.row0, "block row");
+      r.src_c0 = 0;
+      r.n = it.h;
+      r.ncols = i32(sg.ncols, "columns");
+      out.push_back(r);
+      col += sg.ncols;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------- matmat plan
 
 namespace {

@@ -291,6 +291,28 @@ struct MmPlan {
 // and the operator's matvec plan (its row panels are reused).
 void build_mm_plan(const Problem &p, bool transposed, int grid, const OperatorPlan &op, MmPlan &mm);
 
+// The layout fill (fill_items) as column-block copies, for packing on the
+// device from flat block arrays: run k copies rows [src_r0, src_r0 + n) x
+// columns [src_c0, src_c0 + ncols) of a block view (array 0: the full-rank
+// data, 1: the low-rank data; element (i, j) at src_off + i + j ld, or
+// src_off + i ld + j when trans) into item rows [dst_r0, dst_r0 + n) x columns
+// [dst_c0, dst_c0 + ncols) of the item at element item_off, in the storage of
+// one precision (bw_pack.h).  inv: 1 / the block's BF16 scale (1 otherwise).
+struct PackRun {
+  int64_t item_off, src_off, ld;
+  double inv;
+  int32_t hpad, dst_r0, dst_c0, src_r0, src_c0, n, ncols;
+  int8_t trans, array;
+  int16_t pad;
+};
+
+// Runs of one phase and precision, in item order.  The blocks' views must
+// point into [fr_base, fr_base + fr_len) or [lr_base, lr_base + lr_len)
+// (std::invalid_argument otherwise).
+void build_pack_runs(const Problem &p, bool transposed, const OperatorPlan &op, int phase, int prec,
+                     const double *fr_base, int64_t fr_len, const double *lr_base, int64_t lr_len,
+                     std::vector<PackRun> &out);
+
 // Writes the BF16 data of items [i_begin, i_end) of one matmat phase into dst
 // (dst[0] is element `base` of the phase's array; dst must be zeroed).
 void fill_mm_items(const Problem &p, bool transposed, const MmPlan &mm, int phase, int64_t i_begin, int64_t i_end,
