@@ -90,3 +90,41 @@ def test_field_computations_are_linear():
     assert np.allclose(s2, 2 * s1, rtol=1e-13, atol=0)
     assert np.array_equal(io.compute_stresses(pts, 0 * sol), np.zeros(9))
     io.close()
+
+
+def test_bematrix_reference_methods_without_gpu():
+    """BEMatrix built with useCuda=False (host build, no GPU H-matrix): the
+    reference-named methods that do not apply the operator."""
+    from scipy.sparse.linalg import LinearOperator
+
+    from bigwham_dev_b200.bigwham4py import BEMatrix
+    from bigwham_dev_b200.meshes import straight_crack_2d
+
+    coor, conn = straight_crack_2d(64)
+    A = BEMatrix("2DS0-H", coor, conn, np.array([1.0, 0.25]), 16, 2.0, 1e-4, n_openMP_threads=2, useCuda=False)
+    n = 2 * len(conn)
+    assert A.shape == (n, n) and A.getSpatialDimension() == 2
+    # the reference clamps the request to the process's current OpenMP team
+    # size, which every earlier BigWhamIO constructor set globally
+    assert 1 <= A.get_omp_threads() <= 2
+    assert A.getCollocationPoints().shape == (len(conn), 2)
+    assert A.getStorageRequirement() > 0 and A.getGPUStorageRequirement() == 0
+    fb = A._getFullBlocks()
+    assert fb.shape == (n, n) and fb.nnz > 0
+    assert np.allclose(fb.diagonal(), A.H_diag())
+    half = A._getFullBlocks(keep_ratio=0.5)
+    assert 0 < half.nnz < fb.nnz
+    assert isinstance(A.H_ILU_prec(), LinearOperator)
+    # no dropping and room for all fill-in: the ILU is the LU of the full blocks
+    P = A.H_ILU_prec(fill_factor=100, drop_tol=0.0)
+    v = np.random.default_rng(3).uniform(-1, 1, n)
+    assert np.linalg.norm(fb @ (P @ v) - v) / np.linalg.norm(v) < 1e-10
+    assert A._getPattern().shape[1] == 6
+    x = np.random.default_rng(4).uniform(-1, 1, n)
+    assert np.allclose(A.convert_to_global(A.convert_to_local(x)), x)
+    pts = np.array([[0.0, 0.5], [3.0, -1.0]])
+    assert A.compute_stresses(pts, x).shape == (2, 3) and A.compute_displacements(pts, x).shape == (2, 2)
+    assert A.get_max_error_ACA() >= 0
+    assert A.get_element_normals().size == 2 * len(conn) and A.get_rotation_matrix().size == 4 * len(conn)
+    with pytest.raises(Exception, match="not implemented for CUDA"):
+        A[np.ix_([0, 1], [0, 1])]
