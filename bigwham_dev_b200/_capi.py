@@ -36,6 +36,7 @@ _SIGS = {
     "bw_test_withhold_chunk": (C.c_int, [_P, C.c_int]),
     "bw_add_full": (C.c_int, [_P, _I64, _I64, _I64, _I64, _P, _I64]),
     "bw_add_lowrank": (C.c_int, [_P, _I64, _I64, _I64, _I64, _I64, _P, _I64, _P, _I64]),
+    "bw_add_flat_device": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _I64]),
     "bw_finalize": (C.c_int, [_P, C.c_int]),
     "bw_matvec": (C.c_int, [_P, _P, _P, C.c_int, _P]),
     "bw_matvec_host": (C.c_int, [_P, _P, _P, C.c_int]),

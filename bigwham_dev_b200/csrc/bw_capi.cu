@@ -15,6 +15,7 @@
 #include "bw_mm_kernels.cuh"
 #include "bw_aca_kernels.cuh"
 #include "bw_assemble_kernels.cuh"
+#include "bw_devlayout_kernels.cuh"
 #include "bw_file.h"
 #include "bw_layout.h"
 
@@ -117,6 +118,11 @@ struct bw_hmat {
   long long spin_limit = 2000000000LL;  // 2 s bound on every in-kernel wait
   int withhold = -1;                    // bw_test_withhold_chunk: applies to the next streaming launch only
   std::shared_ptr<void> borrowed;       // mapped block file the registered blocks point into (until finalize)
+  // bw_add_flat_device: the blocks live in these device arrays (flat layout)
+  const double *dev_fr = nullptr, *dev_lr = nullptr;
+  int64_t dev_fr_len = 0, dev_lr_len = 0;
+  std::vector<double> dev_max_fr, dev_max_a, dev_max_b;  // per-block maxima (device pass)
+  std::vector<int> dev_bad_fr, dev_bad_lr;
   int take_withhold() {
     const int w = withhold;
     withhold = -1;
@@ -348,6 +354,95 @@ void staged_upload(bw_hmat *h, void *dev, int64_t n_elems, int es, int64_t nit, 
   cudaEventDestroy(ev[1]);
 }
 
+// Scratch device memory of one call, freed when it goes out of scope (also on
+// an exception).
+struct DevTemp {
+  void *p = nullptr;
+  explicit DevTemp(size_t bytes) {
+    const cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 1));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+      throw OomError("cudaMalloc(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    }
+  }
+  ~DevTemp() {
+    if (p) cudaFree(p);
+  }
+  DevTemp(const DevTemp &) = delete;
+  DevTemp &operator=(const DevTemp &) = delete;
+  template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Device-resident blocks (bw_add_flat_device): per-block maxima and
+// non-finite flags on the device, for scales_from_maxima.
+void device_maxima(bw_hmat *h) {
+  const bw::Problem &p = h->prob;
+  const int64_t nfr = (int64_t)p.fr.size(), nlr = (int64_t)p.lr.size();
+  std::vector<bw::MaxSpan> spans;
+  spans.reserve((size_t)(nfr + 2 * nlr));
+  for (const bw::FullBlock &b : p.fr) spans.push_back({b.a.p - h->dev_fr, b.m, b.n, 0, 0});
+  for (const bw::LowRankBlock &b : p.lr) spans.push_back({b.A.p - h->dev_lr, b.m, b.r, 1, 0});
+  for (const bw::LowRankBlock &b : p.lr) spans.push_back({b.B.p - h->dev_lr, b.r, b.n, 1, 0});
+  const int n = (int)spans.size();
+  std::vector<double> mx(std::max(1, n), 0.0);
+  std::vector<int> bad(std::max(1, n), 0);
+  if (n) {
+    DevTemp d_sp(sizeof(bw::MaxSpan) * spans.size()), d_mx(8 * (size_t)n), d_bad(4 * (size_t)n);
+    BW_CUDA(cudaMemcpy(d_sp.p, spans.data(), sizeof(bw::MaxSpan) * spans.size(), cudaMemcpyHostToDevice));
+    bw::block_maxabs_kernel<<<std::min(n, 148 * 8), bw::kDevLayoutThreads>>>(
+        d_sp.as<bw::MaxSpan>(), n, h->dev_fr, h->dev_lr, d_mx.as<double>(), d_bad.as<int>());
+    BW_CUDA(cudaGetLastError());
+    BW_CUDA(cudaMemcpy(mx.data(), d_mx.p, 8 * (size_t)n, cudaMemcpyDeviceToHost));
+    BW_CUDA(cudaMemcpy(bad.data(), d_bad.p, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+  }
+  h->dev_max_fr.assign(mx.begin(), mx.begin() + nfr);
+  h->dev_max_a.assign(mx.begin() + nfr, mx.begin() + nfr + nlr);
+  h->dev_max_b.assign(mx.begin() + nfr + nlr, mx.begin() + nfr + 2 * nlr);
+  h->dev_bad_fr.assign(bad.begin(), bad.begin() + nfr);
+  h->dev_bad_lr.assign((size_t)nlr, 0);
+  for (int64_t k = 0; k < nlr; k++) h->dev_bad_lr[k] = bad[nfr + k] | bad[nfr + nlr + k];
+}
+
+// Hmat::diagonal from device-resident full-rank blocks.
+void device_diagonal(bw_hmat *h) {
+  const int64_t n = std::max(h->n_rows, h->n_cols);
+  h->diag_perm.assign((size_t)n, 0.0);
+  std::vector<bw::DiagSpan> spans;
+  for (const bw::FullBlock &b : h->prob.fr) {
+    const int64_t lo = std::max(b.i0, b.j0), hi = std::min(b.i0 + b.m, b.j0 + b.n);
+    if (lo < hi) spans.push_back({b.a.p - h->dev_fr, b.a.ld, b.i0, b.j0, lo, hi});
+  }
+  if (spans.empty() || n == 0) return;
+  DevTemp d_sp(sizeof(bw::DiagSpan) * spans.size()), d_diag(8 * (size_t)n);
+  BW_CUDA(cudaMemset(d_diag.p, 0, 8 * (size_t)n));
+  BW_CUDA(cudaMemcpy(d_sp.p, spans.data(), sizeof(bw::DiagSpan) * spans.size(), cudaMemcpyHostToDevice));
+  bw::diag_kernel<<<(int)std::min<size_t>(spans.size(), 148 * 8), bw::kDevLayoutThreads>>>(
+      d_sp.as<bw::DiagSpan>(), (int)spans.size(), h->dev_fr, d_diag.as<double>());
+  BW_CUDA(cudaGetLastError());
+  BW_CUDA(cudaMemcpy(h->diag_perm.data(), d_diag.p, 8 * (size_t)n, cudaMemcpyDeviceToHost));
+}
+
+// The data of one phase packed on the device from device-resident blocks.
+void pack_phase_device(bw_hmat *h, int o, int prec, int phase, void *dst) {
+  std::vector<bw::PackRun> runs;
+  bw::build_pack_runs(h->prob, o == 1, h->op[o], phase, prec, h->dev_fr, h->dev_fr_len, h->dev_lr, h->dev_lr_len,
+                      runs);
+  const int64_t es = bw::esize_of(prec), n_elems = h->op[o].ph[phase].n_elems[prec];
+  BW_CUDA(cudaMemset(dst, 0, (size_t)(n_elems * es)));  // padding rows and tile slack
+  if (runs.empty()) return;
+  DevTemp d_runs(sizeof(bw::PackRun) * runs.size());
+  BW_CUDA(cudaMemcpy(d_runs.p, runs.data(), sizeof(bw::PackRun) * runs.size(), cudaMemcpyHostToDevice));
+  const long long nr = (long long)runs.size();
+  const int grid = (int)std::min<long long>(nr, 148LL * 8);
+  const bw::PackRun *r = d_runs.as<bw::PackRun>();
+  if (prec == 0) bw::pack_runs_kernel<0><<<grid, bw::kDevLayoutThreads>>>(r, nr, h->dev_fr, h->dev_lr, dst);
+  if (prec == 1) bw::pack_runs_kernel<1><<<grid, bw::kDevLayoutThreads>>>(r, nr, h->dev_fr, h->dev_lr, dst);
+  if (prec == 2) bw::pack_runs_kernel<2><<<grid, bw::kDevLayoutThreads>>>(r, nr, h->dev_fr, h->dev_lr, dst);
+  BW_CUDA(cudaGetLastError());
+  BW_CUDA(cudaDeviceSynchronize());
+}
+
 // Upload the data of one phase in pieces through two pinned staging buffers.
 void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   const bw::OperatorPlan &op = h->op[o];
@@ -380,6 +475,10 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   }
 
   const int64_t nit = (int64_t)ph.items.size();
+  if (h->dev_fr || h->dev_lr) {
+    pack_phase_device(h, o, prec, phase, dp.data);
+    return;
+  }
   staged_upload(
       h, dp.data, ph.n_elems[prec], es, nit,
       [&](int64_t q) { return q < nit ? ph.items[q].off[prec] : ph.n_elems[prec]; },
@@ -731,8 +830,8 @@ int bw_create_batch(int dof, int count, const int64_t *n_rows_k, const int64_t *
 
 int bw_add_full(bw_hmat *h, int64_t i0, int64_t j0, int64_t m, int64_t n, const double *a, int64_t lda) {
   if (!h) return BW_ERR_ARG;
-  if (h->finalized) {
-    h->err = "bw_add_full after bw_finalize";
+  if (h->finalized || h->dev_fr || h->dev_lr) {
+    h->err = "bw_add_full after bw_finalize or bw_add_flat_device";
     return BW_ERR_STATE;
   }
   return guarded(h, [&] {
@@ -741,11 +840,60 @@ int bw_add_full(bw_hmat *h, int64_t i0, int64_t j0, int64_t m, int64_t n, const 
   });
 }
 
+int bw_add_flat_device(bw_hmat *h, int64_t n_fr, const int64_t *fr, int64_t n_lr, const int64_t *lr,
+                       const double *fr_data, int64_t fr_len, const double *lr_data, int64_t lr_len) {
+  if (!h) return BW_ERR_ARG;
+  if (h->finalized || !h->prob.fr.empty() || !h->prob.lr.empty()) {
+    h->err = "bw_add_flat_device needs an empty handle (before any bw_add_* and bw_finalize)";
+    return BW_ERR_STATE;
+  }
+  return guarded(h, [&] {
+    if (h->device < 0) throw StateError("bw_add_flat_device needs a handle with a device");
+    if (n_fr < 0 || n_lr < 0 || fr_len < 0 || lr_len < 0 || (n_fr && (!fr || !fr_data)) ||
+        (n_lr && (!lr || !lr_data)))
+      throw std::invalid_argument("bw_add_flat_device: null or negative argument");
+    const int64_t d = h->dof, rp = h->n_rows / d, cp = h->n_cols / d;
+    auto extent = [&](int64_t a0, int64_t a1, int64_t lim, const char *what, int64_t k) {
+      if (!(0 <= a0 && a0 < a1 && a1 <= lim))
+        throw std::invalid_argument(std::string("bw_add_flat_device: ") + what + " block " + std::to_string(k) +
+                                    " lies outside the matrix");
+      return (a1 - a0) * d;
+    };
+    std::vector<bw::FullBlock> vf;
+    std::vector<bw::LowRankBlock> vl;
+    int64_t o = 0;
+    for (int64_t k = 0; k < n_fr; k++) {
+      const int64_t *c = fr + 4 * k;
+      const int64_t m = extent(c[0], c[2], rp, "FR", k), n = extent(c[1], c[3], cp, "FR", k);
+      if (m * n > fr_len - o) throw std::invalid_argument("bw_add_flat_device: fr_data shorter than the pattern");
+      vf.push_back({c[0] * d, c[1] * d, m, n, bw::View{fr_data + o, m, false}});
+      o += m * n;
+    }
+    o = 0;
+    for (int64_t k = 0; k < n_lr; k++) {
+      const int64_t *c = lr + 5 * k;
+      const int64_t m = extent(c[0], c[2], rp, "LR", k), n = extent(c[1], c[3], cp, "LR", k), r = c[4];
+      if (r < 0 || r > std::min(m, n)) throw std::invalid_argument("bw_add_flat_device: bad rank");
+      if (r * (m + n) > lr_len - o) throw std::invalid_argument("bw_add_flat_device: lr_data shorter than the pattern");
+      vl.push_back({c[0] * d, c[1] * d, m, n, r, bw::View{lr_data + o, std::max<int64_t>(1, m), false},
+                    bw::View{lr_data + o + m * r, std::max<int64_t>(1, r), false}});
+      o += r * (m + n);
+    }
+    h->prob.fr = std::move(vf);
+    h->prob.lr = std::move(vl);
+    h->dev_fr = fr_data;
+    h->dev_lr = lr_data;
+    h->dev_fr_len = fr_len;
+    h->dev_lr_len = lr_len;
+    return BW_OK;
+  });
+}
+
 int bw_add_lowrank(bw_hmat *h, int64_t i0, int64_t j0, int64_t m, int64_t n, int64_t r, const double *A,
                    int64_t lda, const double *B, int64_t ldb) {
   if (!h) return BW_ERR_ARG;
-  if (h->finalized) {
-    h->err = "bw_add_lowrank after bw_finalize";
+  if (h->finalized || h->dev_fr || h->dev_lr) {
+    h->err = "bw_add_lowrank after bw_finalize or bw_add_flat_device";
     return BW_ERR_STATE;
   }
   return guarded(h, [&] {
@@ -775,6 +923,10 @@ int bw_finalize(bw_hmat *h, int flags) {
     const bool want_t = (flags & BW_STORE_TRANSPOSE) != 0;
     const bool check = (flags & BW_NO_FINITE_CHECK) == 0;
     const bool want_mm = (flags & BW_STORE_MATMAT) != 0;
+    if ((h->dev_fr || h->dev_lr) && h->plan_only)
+      throw StateError("device-resident blocks (bw_add_flat_device) cannot make a plan-only handle");
+    if ((h->dev_fr || h->dev_lr) && want_mm)
+      throw UnsupportedError("the matmat layout is not built from device-resident blocks");
     // statistics
     h->entries = 0;
     h->sum_rank = 0;
@@ -787,12 +939,21 @@ int bw_finalize(bw_hmat *h, int flags) {
     }
     for (int o = 0; o < (want_t ? 2 : 1); o++) {
       bw::build_operator(h->prob, o == 1, h->grid, h->op[o]);
-      bw::compute_scales(h->prob, o == 1, check && o == 0, h->op[o]);
+      if (h->dev_fr || h->dev_lr) {
+        if (o == 0) device_maxima(h);
+        bw::scales_from_maxima(h->prob, o == 1, check && o == 0, h->dev_max_fr.data(), h->dev_max_a.data(),
+                               h->dev_max_b.data(), h->dev_bad_fr.data(), h->dev_bad_lr.data(), h->op[o]);
+      } else {
+        bw::compute_scales(h->prob, o == 1, check && o == 0, h->op[o]);
+      }
       for (int p = 0; p < 3; p++)
         if (mask & (1 << p)) bw::build_chunks(h->prob, o == 1, p, h->grid, h->op[o]);
       if (want_mm) bw::build_mm_plan(h->prob, o == 1, h->grid, h->op[o], h->mm[o]);
     }
-    compute_diagonal(h);
+    if (h->dev_fr || h->dev_lr)
+      device_diagonal(h);
+    else
+      compute_diagonal(h);
     if (!h->plan_only) {
       // size check before any allocation
       int64_t need = 0;

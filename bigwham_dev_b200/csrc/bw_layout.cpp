@@ -335,6 +335,34 @@ void compute_scales(const Problem &p, bool tr, bool check_finite, OperatorPlan &
   }
 }
 
+void scales_from_maxima(const Problem &p, bool tr, bool check_finite, const double *max_fr, const double *max_a,
+                        const double *max_b, const int *nonfinite_fr, const int *nonfinite_lr, OperatorPlan &op) {
+  const int64_t nfr = (int64_t)p.fr.size(), nlr = (int64_t)p.lr.size();
+  auto scale = [](double s) { return (s > 0 && std::isfinite(s)) ? static_cast<float>(s) : 1.0f; };
+  op.scale_fr.assign(nfr, 1.0f);
+  op.scale_a.assign(nlr, 1.0f);
+  op.scale_b.assign(nlr, 1.0f);
+  int64_t bad_fr = -1, bad_lr = -1;
+  for (int64_t k = 0; k < nfr; k++) {
+    op.scale_fr[k] = scale(max_fr[k]);
+    if (nonfinite_fr[k]) bad_fr = k;
+  }
+  for (int64_t k = 0; k < nlr; k++) {
+    if (p.lr[k].r == 0) continue;
+    // H^T's factors are B^T and A^T (eff_low): the scales swap
+    op.scale_a[k] = scale(tr ? max_b[k] : max_a[k]);
+    op.scale_b[k] = scale(tr ? max_a[k] : max_b[k]);
+    if (nonfinite_lr[k]) bad_lr = k;
+  }
+  if (check_finite && bad_fr >= 0) fail("non-finite entry in full block " + std::to_string(bad_fr));
+  if (check_finite && bad_lr >= 0) fail("non-finite entry in low-rank block " + std::to_string(bad_lr));
+  op.t_scale.assign((size_t)std::max<int64_t>(1, op.t_len), 1.0f);
+  for (int64_t k = 0; k < nlr; k++) {
+    const int64_t r = p.lr[k].r;
+    for (int64_t i = 0; i < r; i++) op.t_scale[op.t_off[k] + i] = op.scale_a[k] * op.scale_b[k];
+  }
+}
+
 namespace {
 
 float seg_scale(const OperatorPlan &op, const Segment &s, int prec) {

@@ -291,6 +291,16 @@ struct MmPlan {
 // and the operator's matvec plan (its row panels are reused).
 void build_mm_plan(const Problem &p, bool transposed, int grid, const OperatorPlan &op, MmPlan &mm);
 
+// compute_scales from per-block maxima instead of the data: max_fr[k] =
+// max |entry| of stored full-rank block k, max_a[k] / max_b[k] of low-rank
+// block k's A / B factors, and nonfinite_fr[k] / nonfinite_lr[k] = 1 when the
+// block (or either factor) holds an entry that is not <= 1e300 in magnitude.
+// The results equal compute_scales' bit for bit (a maximum does not depend on
+// the order it is taken in), for H and H^T.
+void scales_from_maxima(const Problem &p, bool transposed, bool check_finite, const double *max_fr,
+                        const double *max_a, const double *max_b, const int *nonfinite_fr, const int *nonfinite_lr,
+                        OperatorPlan &op);
+
 // The layout fill (fill_items) as column-block copies, for packing on the
 // device from flat block arrays: run k copies rows [src_r0, src_r0 + n) x
 // columns [src_c0, src_c0 + ncols) of a block view (array 0: the full-rank

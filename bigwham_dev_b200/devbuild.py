@@ -86,11 +86,12 @@ def _host(a):
 
 
 def build_r0(io, max_leaf_size: int, eta: float, eps_aca: float, E: float, nu: float, device: int = 0,
-             cap_blocks: int = 48, kernels=None) -> dict:
+             cap_blocks: int = 48, kernels=None, on_device: bool = False) -> dict:
     """Blocks of the 3DR0-H H-matrix of `io` (a BigWhamIOGpu of a rectangle
-    mesh) built on the device; returns the flat form (numpy arrays) with
-    "lr_error".  kernels: an object with the methods of DeviceKernels
-    (default: the CUDA entries on `device`)."""
+    mesh) built on the device; returns the flat form with "lr_error".  The
+    block data are numpy arrays, or (on_device) CUDA tensors for
+    HmatGpu.from_device_flat.  kernels: an object with the methods of
+    DeviceKernels (default: the CUDA entries on `device`)."""
     kernels = kernels or DeviceKernels(device)
     io.build_pattern(max_leaf_size, eta)
     pat = io.get_hpattern()
@@ -127,10 +128,13 @@ def build_r0(io, max_leaf_size: int, eta: float, eps_aca: float, E: float, nu: f
         cap *= 2
     lr_data = _cat([p for ab in parts for p in ab])
     d = 3
+    if on_device:
+        fr_out, lr_out = fr_data.contiguous(), lr_data.contiguous()
+    else:
+        fr_out, lr_out = np.ascontiguousarray(_host(fr_data)), np.ascontiguousarray(_host(lr_data))
     return {"dof": d, "n_rows": d * n_pts, "n_cols": d * n_pts, "fr": fr,
             "lr": np.column_stack([lr4, ranks]).astype(np.int64).reshape(-1, 5),
-            "fr_data": np.ascontiguousarray(_host(fr_data)), "lr_data": np.ascontiguousarray(_host(lr_data)),
-            "perm0": perm, "perm1": perm.copy(), "lr_error": errs}
+            "fr_data": fr_out, "lr_data": lr_out, "perm0": perm, "perm1": perm.copy(), "lr_error": errs}
 
 
 def ex_args(ex: dict) -> dict:
@@ -162,9 +166,14 @@ def main(argv=None) -> int:
     io = BigWhamIOGpu(coor, conn, "3DR0-H", [E, nu], useCuda=False)
     torch.cuda.synchronize()
     t0 = time.time()
-    ex = build_r0(io, 32, 3.0, a.eps, E, nu, cap_blocks=a.cap)
+    exd = build_r0(io, 32, 3.0, a.eps, E, nu, cap_blocks=a.cap, on_device=True)
     torch.cuda.synchronize()
     t_dev = time.time() - t0
+    t0 = time.time()
+    h0 = HmatGpu.from_device_flat(**ex_args(exd), precisions=("fp64",))
+    torch.cuda.synchronize()
+    t_dev_layout = time.time() - t0
+    ex = dict(exd, fr_data=exd["fr_data"].cpu().numpy(), lr_data=exd["lr_data"].cpu().numpy())
     io.close()
     io = BigWhamIOGpu(coor, conn, "3DR0-H", [E, nu], useCuda=False)
     t0 = time.time()
@@ -175,9 +184,11 @@ def main(argv=None) -> int:
     x = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, ex["n_cols"])).cuda()
     h1 = HmatGpu.from_flat(**ex_args(ex), precisions=("fp64",))
     h2 = HmatGpu.from_flat(**ex_args(ref), precisions=("fp64",))
-    y1, y2 = h1.matvec(x), h2.matvec(x)
+    y1, y2, y0 = h1.matvec(x), h2.matvec(x), h0.matvec(x)
     torch.cuda.synchronize()
     print(json.dumps({"mesh": a.mesh, "dof": ex["n_rows"], "device_build_s": round(t_dev, 3),
+                      "device_layout_s": round(t_dev_layout, 3),
+                      "device_layout_vs_host_layout_max_diff": float(torch.max(torch.abs(y0 - y1))),
                       "host_build_s": round(t_host, 3), "lr_entries": [int(ex["lr_data"].size), int(ref["lr_data"].size)],
                       "matvec_rel_diff": float(torch.linalg.vector_norm(y1 - y2) / torch.linalg.vector_norm(y2))}))
     return 0

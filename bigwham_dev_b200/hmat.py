@@ -161,6 +161,25 @@ class HmatGpu:
         return h.finalize(**kw)
 
     @classmethod
+    def from_device_flat(cls, dof, n_rows, n_cols, fr, lr, fr_data, lr_data, perm0, perm1, device=0,
+                         **kw) -> "HmatGpu":
+        """Handle from the flat form with the block data in device memory
+        (CUDA float64 tensors on `device`, e.g. from devbuild.build_r0(...,
+        on_device=True)), laid out on the device by finalize(**kw)
+        (bw_add_flat_device): the host never reads the blocks."""
+        fr = np.ascontiguousarray(fr, dtype=np.int64).reshape(-1, 4)
+        lr = np.ascontiguousarray(lr, dtype=np.int64).reshape(-1, 5)
+        for t in (fr_data, lr_data):
+            if not (getattr(t, "is_cuda", False) and str(t.dtype) == "torch.float64" and t.is_contiguous()):
+                raise TypeError("fr_data and lr_data must be contiguous CUDA float64 tensors")
+        self = cls(dof, n_rows, n_cols, perm0, perm1, device)
+        A.check(self._lib.bw_add_flat_device(self._h, fr.shape[0], fr.ctypes.data, lr.shape[0], lr.ctypes.data,
+                                             fr_data.data_ptr(), fr_data.numel(), lr_data.data_ptr(),
+                                             lr_data.numel()), self._h)
+        self._keep = [fr, lr, fr_data, lr_data]
+        return self.finalize(**kw)
+
+    @classmethod
     def from_file(cls, path, device: int = 0, verify: bool = True, **kw) -> "HmatGpu":
         """Handle from a block file (bw_create_from_file; written by
         ``blockfile.write`` or ``BigWhamIOGpu.write_to_file``): the blocks are

@@ -133,6 +133,17 @@ int bw_add_lowrank(bw_hmat *h, int64_t i0, int64_t j0, int64_t m, int64_t n, int
  * BW_BF16, optionally BW_STORE_TRANSPOSE, BW_NO_FINITE_CHECK, BW_PLAN_ONLY)
  * and upload it.  Synchronous.  After it returns the borrowed block pointers
  * are no longer used. */
+/* Register all blocks from the flat form (as bw_file_write takes it: fr
+ * n_fr x 4 and lr n_lr x 5 in points on the host, the blocks back to back in
+ * fr_data / lr_data) when the block data is in DEVICE memory of the handle's
+ * device, e.g. from bw_r0_assemble_fr / bw_r0_aca.  bw_finalize then computes
+ * the BF16 scales, the diagonal and the packed layout on the device (the host
+ * never reads the data; results equal the host path's bit for bit).  The
+ * arrays are borrowed until bw_finalize.  Only on an empty handle with a
+ * device; not with BW_PLAN_ONLY or BW_STORE_MATMAT. */
+int bw_add_flat_device(bw_hmat *h, int64_t n_fr, const int64_t *fr, int64_t n_lr, const int64_t *lr,
+                       const double *fr_data, int64_t fr_len, const double *lr_data, int64_t lr_len);
+
 int bw_finalize(bw_hmat *h, int flags);
 
 /* y = H x (or H^T x with BW_TRANSPOSE) on DEVICE pointers, stream-ordered on

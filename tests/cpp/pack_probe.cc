@@ -1,6 +1,8 @@
 // Run-based packing (bigwham_dev_b200/csrc/bw_pack.h, the device packer's
 // element copy) against the host fill (bw::fill_items) on a real plan built by
 // the layout library, byte for byte; used by tests/test_pack_cpu.py.
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -29,11 +31,36 @@ extern "C" int probe_pack_compare(int dof, long long n_rows, long long n_cols, l
                       bw::View{lr_data + o + m * r, r > 0 ? r : 1, false}});
       o += r * (m + n);
     }
+    // per stored block maxima, as a device reduction would compute them
+    std::vector<double> mfr(p.fr.size()), ma(p.lr.size()), mb(p.lr.size());
+    std::vector<int> bfr(p.fr.size(), 0), blr(p.lr.size(), 0);
+    auto mx = [](const bw::View &v, long long m, long long n, int &bad) {
+      double s = 0.0;
+      for (long long j = 0; j < n; j++)
+        for (long long i = 0; i < m; i++) {
+          const double a = std::fabs(v.at(i, j));
+          if (!(a <= 1.0e300)) bad = 1;
+          s = std::max(s, a);
+        }
+      return s;
+    };
+    for (size_t k = 0; k < p.fr.size(); k++) mfr[k] = mx(p.fr[k].a, p.fr[k].m, p.fr[k].n, bfr[k]);
+    for (size_t k = 0; k < p.lr.size(); k++) {
+      ma[k] = mx(p.lr[k].A, p.lr[k].m, p.lr[k].r, blr[k]);
+      mb[k] = mx(p.lr[k].B, p.lr[k].r, p.lr[k].n, blr[k]);
+    }
     int q = 0;
     for (int tr = 0; tr < 2; tr++) {
       bw::OperatorPlan op;
       bw::build_operator(p, tr == 1, 148, op);
       bw::compute_scales(p, tr == 1, true, op);
+      {
+        bw::OperatorPlan op2 = op;
+        bw::scales_from_maxima(p, tr == 1, true, mfr.data(), ma.data(), mb.data(), bfr.data(), blr.data(), op2);
+        if (op2.scale_fr != op.scale_fr || op2.scale_a != op.scale_a || op2.scale_b != op.scale_b ||
+            op2.t_scale != op.t_scale)
+          return 2;
+      }
       for (int prec = 0; prec < 3; prec++) bw::build_chunks(p, tr == 1, prec, 148, op);
       for (int phase = 0; phase < 2; phase++)
         for (int prec = 0; prec < 3; prec++, q++) {

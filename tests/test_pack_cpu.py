@@ -51,3 +51,14 @@ def test_pack_runs_equal_the_host_fill_on_a_rectangular_synthetic(probe):
     from synth import synthetic_hmat
 
     _compare(probe, synthetic_hmat(70, 45, 3, seed=5))
+
+
+def test_device_blocks_need_a_device_handle():
+    """bw_add_flat_device is refused on a host-only handle (before any device
+    call); the device path itself runs on a GPU."""
+    from bigwham_dev_b200 import HmatGpu
+    from bigwham_dev_b200 import _capi as A
+
+    h = HmatGpu(3, 12, 12, np.arange(4), np.arange(4), device=-1)
+    assert h._lib.bw_add_flat_device(h._h, 0, None, 0, None, None, 0, None, 0) == A.BW_ERR_STATE
+    assert "device" in A.last_error(h._h)
