@@ -1,6 +1,6 @@
 """GMRES and mixed-precision refinement on the GPU (-m gpu).
 
-Targets (north star): Jacobi-preconditioned GMRES(50) on the FP64 H-matrix to
+Targets: Jacobi-preconditioned GMRES(50) on the FP64 H-matrix to
 a relative residual of 1e-8; refinement with FP32 / BF16 inner solves reaches
 the same residual with <= 1e-6 relative error against the FP64 solution; the
 solution of the small golden systems matches a dense FP64 solve of the same
