@@ -291,3 +291,18 @@ def test_host_library_records_equal_the_oracles():
     R = RefHmat("3DR0-H", coor, conn, [1.0, 0.25], 32, 3.0, 1e-5, n_threads=2)
     assert mine.shape == (36, 17)
     assert np.array_equal(mine, element_records(R, coor, conn))
+
+
+def test_continuity_between_the_in_plane_and_off_plane_forms(probe):
+    """z = +-1e-13 (rounding of a frame rotation on a nearly planar mesh) goes
+    through the off-plane forms; it must agree with the z = 0 forms, and with
+    the reference at the same z, on points inside, outside and at the centre
+    of the element."""
+    stress, _ = probe
+    a, b, G, nu = 0.5, 0.35, 1.3, 0.27
+    for x, y in ((0.0, 0.0), (0.2, -0.1), (1.7, 0.3), (-2.5, -1.9), (0.3, 2.2)):
+        s0 = stress(x, y, 0.0, a, b, G, nu)
+        for z in (1e-13, -1e-13):
+            sz = stress(x, y, z, a, b, G, nu)
+            assert _err(sz, s0) < 1e-9, (x, y, z)
+            assert _err(sz, ref_r0_stress(x, y, z, a, b, G, nu)) < 1e-9, (x, y, z)
