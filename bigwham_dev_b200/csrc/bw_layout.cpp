@@ -759,6 +759,16 @@ void build_mm_plan(const Problem &p, bool tr, int grid, const OperatorPlan &op, 
         it.segs.push_back(window(sg, r0));
         it.ncols += it.segs.back().ncols;
       }
+      if (it.segs.empty()) {
+        // every block of the panel has rank 0: one window of zero block
+        // columns over T8's zeroed padding rows, so the rows are written (as 0)
+        MmSeg z{};
+        z.kind = 1;
+        z.block = -1;
+        z.src = 1;
+        z.src_row = mm.t8_len;
+        it.segs.push_back(z);
+      }
       // a multiple of 16 columns, at least kMmMinCols: more tile rows of the
       // last operand window (zero columns)
       const int64_t want = std::max<int64_t>(kMmMinCols, align_up(it.ncols, 16));
@@ -822,6 +832,10 @@ void fill_mm_items(const Problem &p, bool tr, const MmPlan &mm, int phase, int64
     }
     int64_t col = 0;
     for (const MmSeg &s : it.segs) {
+      if (s.width == 0) {  // a panel of rank-0 blocks only: zero columns
+        col += s.ncols;
+        continue;
+      }
       const View v = s.kind == 0 ? eff_full(p, tr, s.block).a : eff_low(p, tr, s.block).A;
       for (int64_t c = 0; c < s.width; c++)
         for (int64_t i = 0; i < it.h; i++)
