@@ -350,3 +350,28 @@ def test_header_layout_and_checksums_follow_the_format(tmp_path):
         assert hs == _section_hash_py(body), s
         end = off + nbytes
     assert end == len(raw)
+
+
+def test_rank_zero_blocks_round_trip_and_plan(tmp_path):
+    """Low-rank blocks of rank 0 (no factors) survive the file bitwise, and a
+    handle made from the file plans the same operator as the flat upload."""
+    from bigwham_dev_b200 import HmatGpu, blockfile
+    from planreplay import replay
+    from synth import synthetic_hmat
+
+    arr = synthetic_hmat(30, 22, 3, seed=31, lr_share=0.8, rank0_share=0.5)
+    assert (arr.lr[:, 4] == 0).any()
+    ex = {"dof": arr.dof, "n_rows": arr.n_rows, "n_cols": arr.n_cols, "fr": arr.fr, "lr": arr.lr,
+          "fr_data": arr.fr_data, "lr_data": arr.lr_data, "perm0": arr.perm0, "perm1": arr.perm1}
+    p = tmp_path / "r0.bwb"
+    blockfile.write(p, ex)
+    r = blockfile.read(p)
+    for k in FLAT:
+        assert np.array_equal(r[k], np.asarray(ex[k])), k
+    x = np.random.default_rng(2).uniform(-1, 1, arr.n_cols)
+    h1 = HmatGpu.from_file(p, device=-1, precisions=("fp64", "bf16"), plan_only=True)
+    h2 = HmatGpu(arr.dof, arr.n_rows, arr.n_cols, arr.perm0, arr.perm1, device=-1)
+    h2.add_flat(arr.fr, arr.lr, arr.fr_data, arr.lr_data)
+    h2.finalize(plan_only=True, precisions=("fp64", "bf16"))
+    for prec in ("fp64", "bf16"):
+        assert np.array_equal(replay(h1, x, prec), replay(h2, x, prec))

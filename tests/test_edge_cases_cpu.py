@@ -172,3 +172,57 @@ def test_rectangular_thin_matrices(shape):
     check_mm(h, DD, X)
     G = rng.uniform(-1, 1, (m, 3))
     check_mm(h, DD, G, transposed=True)
+
+
+def test_rank_zero_leaves_of_a_synthetic_partition():
+    """Irregular rectangular partitions where every leaf is low rank and half
+    of them have rank 0 (so whole row and column panels do), against the
+    restatement, H and H^T, every precision."""
+    from oracle import oracle_matvec_perm, oracle_rmatvec_perm
+    from synth import synthetic_hmat
+
+    for seed, (nr, nc) in enumerate([(40, 25), (25, 40), (33, 33)]):
+        arr = synthetic_hmat(nr, nc, 3, seed=20 + seed, lr_share=1.0, rank0_share=0.5)
+        assert (arr.lr[:, 4] == 0).any() and (arr.lr[:, 4] > 0).any()
+        h = HmatGpu(arr.dof, arr.n_rows, arr.n_cols, arr.perm0, arr.perm1, device=-1)
+        h.add_flat(arr.fr, arr.lr, arr.fr_data, arr.lr_data)
+        h.finalize(plan_only=True, precisions=("fp64", "fp32", "bf16"), transpose=True, matmat=True)
+        rng = np.random.default_rng(seed)
+        x = rng.uniform(-1, 1, arr.n_cols)
+        g = rng.uniform(-1, 1, arr.n_rows)
+        want, want_t = oracle_matvec_perm(arr, x, 1), oracle_rmatvec_perm(arr, g, 1)
+        assert np.abs(replay(h, x) - want).max() <= 1e-13 * max(1.0, np.abs(want).max())
+        assert np.abs(replay(h, g, transposed=True) - want_t).max() <= 1e-13 * max(1.0, np.abs(want_t).max())
+        for prec in ("fp32", "bf16"):
+            assert np.all(np.isfinite(replay(h, x, prec))) and np.all(np.isfinite(replay(h, g, prec, transposed=True)))
+        X = rng.uniform(-1, 1, (arr.n_cols, 4))
+        Y = mm_replay(h, X)
+        W = np.stack([oracle_matvec_perm(arr, X[:, c], 1) for c in range(4)], axis=1)
+        assert np.abs(Y - W).max() <= 2e-2 * max(1.0, np.abs(W).max())
+
+
+def test_batch_with_rank_zero_leaves_and_a_one_point_member():
+    """A batch of irregular members (rank-0 leaves among them) and a member of
+    one collocation point: each member's slice is its own product."""
+    from types import SimpleNamespace
+
+    from oracle import oracle_matvec_perm, oracle_rmatvec_perm
+    from synth import synthetic_hmat
+
+    rng = np.random.default_rng(9)
+    one = SimpleNamespace(dof=3, n_rows=3, n_cols=3, fr=np.array([[0, 0, 1, 1]]), lr=np.zeros((0, 5), np.int64),
+                          fr_data=rng.standard_normal(9), lr_data=np.zeros(0), perm0=np.zeros(1, np.int64),
+                          perm1=np.zeros(1, np.int64))
+    ms = [synthetic_hmat(20, 20, 3, seed=40, lr_share=0.8, rank0_share=0.5), one,
+          synthetic_hmat(17, 26, 3, seed=41, lr_share=1.0, rank0_share=0.5)]
+    h = HmatGpu.batch(ms, device=-1, plan_only=True, precisions=("fp64", "bf16"), transpose=True)
+    x = rng.uniform(-1, 1, h.n_cols)
+    g = rng.uniform(-1, 1, h.n_rows)
+    y, yt = replay(h, x), replay(h, g, transposed=True)
+    assert np.all(np.isfinite(replay(h, x, "bf16")))
+    for k, m in enumerate(ms):
+        r0, r1 = h.row_offsets[k], h.row_offsets[k + 1]
+        c0, c1 = h.col_offsets[k], h.col_offsets[k + 1]
+        w, wt = oracle_matvec_perm(m, x[c0:c1], 1), oracle_rmatvec_perm(m, g[r0:r1], 1)
+        assert np.abs(y[r0:r1] - w).max() <= 1e-13 * max(1.0, np.abs(w).max()), k
+        assert np.abs(yt[c0:c1] - wt).max() <= 1e-13 * max(1.0, np.abs(wt).max()), k

@@ -62,3 +62,12 @@ def test_device_blocks_need_a_device_handle():
     h = HmatGpu(3, 12, 12, np.arange(4), np.arange(4), device=-1)
     assert h._lib.bw_add_flat_device(h._h, 0, None, 0, None, None, 0, None, 0) == A.BW_ERR_STATE
     assert "device" in A.last_error(h._h)
+
+
+def test_pack_runs_with_rank_zero_leaves(probe):
+    """Rank-0 low-rank leaves (no factors) between ordinary ones."""
+    from synth import synthetic_hmat
+
+    arr = synthetic_hmat(40, 25, 3, seed=21, lr_share=0.7, rank0_share=0.5)
+    assert (arr.lr[:, 4] == 0).any()
+    _compare(probe, arr)
