@@ -248,7 +248,8 @@ class BigWhamIOGpu:
         return int(self._L.bwh_n_blocks(self._h, 0)), int(self._L.bwh_n_blocks(self._h, 1))
 
     def export_blocks(self, alloc=np.empty) -> dict:
-        """Flat copy of the built H-matrix (before attach_gpu): pattern,
+        """Flat copy of the built H-matrix (before attach_gpu, or after it with
+        the host blocks kept, set_gpu_storage(keep_host=True)): pattern,
         permutations and block data, as HmatGpu.add_flat takes them.  `alloc`
         (shape, dtype) -> array lets the caller place the arrays (e.g. in
         shared memory)."""
@@ -575,7 +576,19 @@ class BEMatrix(_LinOp):
         return fig
 
     def __getitem__(self, indices):
-        raise Exception("Bigwham matrix selection not implemented for CUDA support.")
+        """Sub-matrix selection ``A[np.ix_(rows, cols)]`` (reference:
+        bigwham4py.py:462-484 over BigWhamIO::hmatSelection, which raises with
+        CUDA): a LinearOperator over H[rows, cols] whose matvec runs on the GPU
+        (selection.HmatSelection, the selected sub-blocks as a handle of their
+        own).  rows / cols: element indices, original ordering, any shape (both
+        are flattened; the reference's binding reads only the first dimension,
+        py_bigwham.cc:262-268, so np.ix_'s 1 x m column array gives it one
+        column).  Needs the host blocks: build with keep_host=True."""
+        if not isinstance(indices, tuple) or len(indices) != 2:
+            raise IndexError("Subsetting requires indices of the form (np.ix_(row_indices, col_indices))")
+        self._build()
+        rows, cols = (np.asarray(i).ravel() for i in indices)
+        return BEMatrixSelection(self, rows, cols)
 
     def H_diag(self):
         return self.H_.get_diagonal()
@@ -586,6 +599,58 @@ class BEMatrix(_LinOp):
 
         inv = 1.0 / self.H_diag()
         return LinearOperator(self.shape, lambda v: inv * np.asarray(v).ravel(), dtype=float)
+
+
+class BEMatrixSelection(_LinOp):
+    """H[rows, cols] of a BEMatrix on the GPU (BEMatrix.__getitem__)."""
+
+    def __init__(self, parent: "BEMatrix", rows, cols):
+        from .selection import HmatSelection
+
+        io = parent.H_
+        ex = io.export_blocks()
+        precisions = tuple(io._precisions)
+        self.parent = parent
+        self.rows, self.cols = rows, cols
+        if io.use_cuda:
+            self.S_ = HmatSelection(ex, rows, cols, device=io.device, precisions=precisions)
+        else:  # a host build: the selection's plan only (no GPU H-matrix to apply)
+            self.S_ = HmatSelection(ex, rows, cols, device=-1, precisions=precisions, plan_only=True)
+        self._ex = ex
+        super().__init__(np.dtype(float), self.S_.shape)
+
+    def _matvec(self, v):
+        return self.S_.matvec(np.asarray(v, dtype=np.float64).ravel())
+
+    def _matvec_torch(self, x, y):
+        """y = H[rows, cols] x on CUDA float64 torch tensors."""
+        self.S_.matvec(x, out=y)
+
+    def _getFullBlocks(self, keep_ratio: float = 1.0):
+        """The selection's full-rank entries as a scipy CSC matrix (the
+        reference's GetFullBlocks on the selection, hmat_selection.cc:265-375)."""
+        from scipy.sparse import csc_matrix
+
+        if not (0 < keep_ratio <= 1):
+            raise ValueError("ratio must be a float between 0 and 1.")
+        val, pos = self.S_.full_blocks()
+        if keep_ratio < 1.0:
+            k = int(np.ceil(keep_ratio * val.size))
+            if k == 0:
+                return csc_matrix(self.shape)
+            thr = np.partition(np.abs(val), -k)[-k]
+            keep = np.abs(val) >= thr
+            val, pos = val[keep], pos[keep]
+        return csc_matrix((val, (pos[:, 0], pos[:, 1])), shape=self.shape)
+
+    def H_ILU_prec(self, fill_factor=1, drop_tol=1e-3, keep_ratio=1.0):
+        from scipy.sparse.linalg import LinearOperator, spilu
+
+        ilu = spilu(self._getFullBlocks(keep_ratio=keep_ratio), fill_factor=fill_factor, drop_tol=drop_tol)
+        return LinearOperator(self.shape, ilu.solve)
+
+    def close(self) -> None:
+        self.S_.close()
 
 
 class BEMatrixRectangular(_LinOp):

@@ -223,9 +223,10 @@ int64_t bwh_entries(const bwh_io *h, int kind) {
 int bwh_export(const bwh_io *h, int64_t *fr, int64_t *lr, double *fr_data, double *lr_data, int64_t *perm0,
                int64_t *perm1) {
   if (!h) return fail("null handle");
-  if (h->gpu) return fail("bwh_export must run before bwh_attach_gpu (the host blocks are released there)");
+  if (h->gpu && !h->cpu_kept)
+    return fail("bwh_export needs the host blocks: call it before bwh_attach_gpu, or attach with release_host = 0");
   return guarded([&] {
-    auto hm = h->io->getHmat();
+    auto hm = h->gpu ? h->cpu_kept : h->io->getHmat();
     auto p = hm->pattern();
     auto hr = hm->get_hr();
     for (il::int_t k = 0; k < p.n_FRB; k++)

@@ -90,7 +90,8 @@ int64_t bwh_n_blocks(const bwh_io *io, int kind);
 
 /* Stored entries of the FR blocks (kind 0) or of the LR factors A and B (kind 1). */
 int64_t bwh_entries(const bwh_io *io, int kind);
-/* Copy the built H-matrix out, before bwh_attach_gpu: fr (n_FR x 4: i0, j0,
+/* Copy the built H-matrix out (before bwh_attach_gpu, or after it when the
+ * host blocks were kept, release_host = 0): fr (n_FR x 4: i0, j0,
  * iend, jend in points), lr (n_LR x 5: ..., r), the FR blocks back to back and
  * per LR block A then B (column-major), and both permutations.  This is the
  * flat form bw_add_* accept and the form of the benchmark's block cache. */

@@ -113,6 +113,10 @@ def _ref():
         lib.ref_matvec.argtypes = [C.c_void_p, _f64p, _f64p]
         lib.ref_matvec_perm.argtypes = [C.c_void_p, _f64p, _f64p]
         lib.ref_diagonal.argtypes = [C.c_void_p, _f64p]
+        lib.ref_selection_matvec.argtypes = [C.c_void_p, _i32p, C.c_int64, _i32p, C.c_int64, _f64p, _f64p]
+        lib.ref_selection_full_blocks.argtypes = [C.c_void_p, _i32p, C.c_int64, _i32p, C.c_int64, C.c_void_p,
+                                                  C.c_void_p, C.c_int64]
+        lib.ref_selection_full_blocks.restype = C.c_int64
         lib.ref_collocation_points.argtypes = [C.c_void_p, C.c_void_p]
         lib.ref_dense_rows.argtypes = [C.c_void_p, C.c_char_p, _f64p, _i64p, C.c_int64, _f64p]
         lib.ref_collocation_points.restype = C.c_int64
@@ -198,6 +202,27 @@ class RefHmat:
         y = np.empty(self.shape[0])
         _ref().ref_matvec_perm(self._h, x, y)
         return y
+
+    def selection_matvec(self, rows, cols, x):
+        """The reference's BigWhamIO::hmatSelection(rows, cols).MatVec(x)."""
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        c = np.ascontiguousarray(cols, dtype=np.int32)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(r.size * self.dof)
+        if _ref().ref_selection_matvec(self._h, r, r.size, c, c.size, x, y) != 0:
+            raise IndexError("the reference rejected the selection")
+        return y
+
+    def selection_full_blocks(self, rows, cols):
+        """(val, pos) of the selection's GetFullBlocks: val[i] = H_sel(pos[i, 0], pos[i, 1])."""
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        c = np.ascontiguousarray(cols, dtype=np.int32)
+        n = _ref().ref_selection_full_blocks(self._h, r, r.size, c, c.size, None, None, 0)
+        if n < 0:
+            raise IndexError("the reference rejected the selection")
+        val, pos = np.empty(n), np.empty(2 * n, dtype=np.int32)
+        _ref().ref_selection_full_blocks(self._h, r, r.size, c, c.size, val.ctypes.data, pos.ctypes.data, n)
+        return val, pos.reshape(n, 2)
 
     def diagonal(self):
         d = np.empty(max(self.shape))

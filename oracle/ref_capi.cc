@@ -164,6 +164,52 @@ int ref_matvec_perm(void *h, const double *x, double *y) {
   return 0;
 }
 
+// Sub-matrix selection: BigWhamIO::hmatSelection (bigwham_io.cc:1365-1375)
+// wraps the built Hmat in an HmatSelection (hmat_selection.cc); element
+// indices rows / cols in the original ordering.  y = the selection's MatVec
+// (matvecOriginal, hmat_selection.cc:230-258), length n_rows * dof.
+// Returns 1 when the reference rejects the indices (validateIndices throws).
+int ref_selection_matvec(void *h, const int *rows, int64_t n_rows, const int *cols, int64_t n_cols,
+                         const double *x, double *y) {
+  try {
+    il::Array<int> r(n_rows), c(n_cols);
+    for (int64_t i = 0; i < n_rows; i++) r[i] = rows[i];
+    for (int64_t i = 0; i < n_cols; i++) c[i] = cols[i];
+    BigWhamIO sel = H(h)->io->hmatSelection(r, c);
+    il::ArrayView<double> xv{x, sel.getHmat()->size(1)};
+    il::Array<double> out = sel.MatVec(xv);
+    std::memcpy(y, out.data(), sizeof(double) * out.size());
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+// The selection's full-block entries through BigWhamIO::GetFullBlocks
+// (HmatSelection::fullBlocksOriginal, hmat_selection.cc:265-375):
+// val[i] = H_sel(pos[2i], pos[2i + 1]).  Returns the entry count (or -1);
+// val / pos are written when cap covers it.
+int64_t ref_selection_full_blocks(void *h, const int *rows, int64_t n_rows, const int *cols, int64_t n_cols,
+                                  double *val, int *pos, int64_t cap) {
+  try {
+    il::Array<int> r(n_rows), c(n_cols);
+    for (int64_t i = 0; i < n_rows; i++) r[i] = rows[i];
+    for (int64_t i = 0; i < n_cols; i++) c[i] = cols[i];
+    BigWhamIO sel = H(h)->io->hmatSelection(r, c);
+    std::vector<double> v;
+    std::vector<int> p;
+    sel.GetFullBlocks(v, p);
+    const int64_t n = (int64_t)v.size();
+    if (val && pos && cap >= n) {
+      std::memcpy(val, v.data(), sizeof(double) * n);
+      std::memcpy(pos, p.data(), sizeof(int) * 2 * n);
+    }
+    return n;
+  } catch (...) {
+    return -1;
+  }
+}
+
 // BigWhamIO::GetDiagonal, original ordering (bigwham_io.cc:909-916).
 int ref_diagonal(void *h, double *d) {
   std::vector<double> v;

@@ -94,7 +94,8 @@ def test_field_computations_are_linear():
 
 def test_bematrix_reference_methods_without_gpu():
     """BEMatrix built with useCuda=False (host build, no GPU H-matrix): the
-    reference-named methods that do not apply the operator."""
+    reference-named methods that do not apply the operator, and the selection's
+    full-block entries."""
     from scipy.sparse.linalg import LinearOperator
 
     from bigwham_dev_b200.bigwham4py import BEMatrix
@@ -126,5 +127,13 @@ def test_bematrix_reference_methods_without_gpu():
     assert A.compute_stresses(pts, x).shape == (2, 3) and A.compute_displacements(pts, x).shape == (2, 2)
     assert A.get_max_error_ACA() >= 0
     assert A.get_element_normals().size == 2 * len(conn) and A.get_rotation_matrix().size == 4 * len(conn)
-    with pytest.raises(Exception, match="not implemented for CUDA"):
-        A[np.ix_([0, 1], [0, 1])]
+    # selection (the reference raises here with CUDA): the selected full-rank
+    # entries are the full matrix's, at the selected rows and columns
+    rows, cols = np.array([0, 1, 5, 40]), np.array([3, 1, 60])
+    S = A[np.ix_(rows, cols)]
+    assert S.shape == (2 * rows.size, 2 * cols.size)
+    rd = (2 * rows[:, None] + np.arange(2)).ravel()
+    cd = (2 * cols[:, None] + np.arange(2)).ravel()
+    assert np.array_equal(S._getFullBlocks().toarray(), fb.toarray()[np.ix_(rd, cd)])
+    with pytest.raises(IndexError):
+        A[np.ix_([0, len(conn)], [0])]
