@@ -359,6 +359,19 @@ int bw_r0_aca(int device, int64_t n_elems, const double *records, double G, doub
               double *factors_a, int64_t a_len, double *factors_b, int64_t b_len, int32_t *rank_out,
               double *err_out, void *stream);
 
+/* Stresses and displacements at observation points from a solution on a
+ * 2DS0 mesh (straight segments, constant displacement discontinuity, plane
+ * strain): the device counterpart of BigWhamIO::ComputeStresses /
+ * ComputeDisplacements (src/io/bigwham_io.cc:1166-1324) for kernel 2DS0-H.
+ * All arrays are device memory.  records: n_elems x 5 (centre x, y, half
+ * length, unit tangent x, y, the tangent running from the first vertex to the
+ * second); dd: n_elems x 2 local DDs (shear, normal), mesh order; pts:
+ * n_pts x 2; stress (n_pts x 3: s11, s22, s12) and / or disp (n_pts x 2,
+ * global frame) may be null, not both.  Each point sums the elements in mesh
+ * order.  Stream-ordered; returns after the launch. */
+int bw_s0_fields(int device, int64_t n_elems, const double *records, const double *dd, double G, double nu,
+                 int64_t n_pts, const double *pts, double *stress, double *disp, void *stream);
+
 /* Release everything. */
 int bw_destroy(bw_hmat *h);
 

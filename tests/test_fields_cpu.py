@@ -1,0 +1,196 @@
+"""2DS0 observation-point fields (bw_s0.h, the code s0_fields_kernel runs) on
+CPU through a host build of the same functions (tests/cpp/s0_probe.cc):
+* stresses at points from a DD solution on a bent, unevenly meshed crack vs
+  the reference's own BigWhamIO::ComputeStresses (host library; the cases stay
+  below its OpenMP threshold, sqrt(N_src N_obs) <= 400, where its shared
+  accumulation would race): 1e-12 of the largest stress;
+* displacements vs the reference's ComputeDisplacements for normal DDs, and
+  for the components its shear kernel gets right;
+* the displacement field's finite-difference strains give the stresses
+  (Hooke's law, plane strain) to 1e-7, also for the component where the
+  reference's shear kernel returns u1 in place of u2;
+* element records from the mesh equal the reference's element frames;
+* on an element's line, the limit from below, as the reference takes it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HOST_LIB = os.path.join(ROOT, "bigwham_dev_b200", "_lib", "libbigwham_host.so")
+needs_host = pytest.mark.skipif(not os.path.exists(HOST_LIB), reason="host adapter not built")
+E, NU = 1.0, 0.25
+G = E / (2 * (1 + NU))
+
+
+@pytest.fixture(scope="module")
+def probe():
+    out = os.path.join(ROOT, "_build", "libs0_probe.so")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-shared", "-fPIC", "-I", os.path.join(ROOT, "bigwham_dev_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "cpp", "s0_probe.cc"), "-o", out], check=True)
+    L = C.CDLL(out)
+    p = np.ctypeslib.ndpointer(np.float64, flags="C")
+    L.probe_s0_fields.argtypes = [C.c_int64, p, p, C.c_double, C.c_double, C.c_int64, p, p, p]
+    L.probe_s0_local.argtypes = [C.c_double] * 5 + [p, p]
+    return L
+
+
+def host_fields(L, coor, conn, dd, pts):
+    from bigwham_dev_b200.fields import s0_records
+
+    rec = s0_records(coor, conn)
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    s, u = np.empty((len(pts), 3)), np.empty((len(pts), 2))
+    L.probe_s0_fields(rec.shape[0], rec, np.ascontiguousarray(dd, dtype=np.float64), G, NU, len(pts), pts, s, u)
+    return s, u
+
+
+def bent_crack(n=60, seed=0):
+    """A crack along a curve, with uneven element lengths."""
+    rng = np.random.default_rng(seed)
+    s = np.sort(np.concatenate([[0.0, 1.0], rng.uniform(0, 1, n - 1)]))
+    x = -1.0 + 2.0 * s
+    coor = np.column_stack([x, 0.3 * np.sin(2.5 * x)])
+    conn = np.column_stack([np.arange(n), np.arange(1, n + 1)])
+    return coor, conn
+
+
+def off_mesh_points(rng, n):
+    return np.column_stack([rng.uniform(-2, 2, n), rng.uniform(-1.5, 1.5, n)])
+
+
+@pytest.fixture(scope="module")
+def ref_io():
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+
+    coor, conn = bent_crack()
+    io = BigWhamIOGpu(coor, conn, "2DS0-H", [E, NU], 4, useCuda=False)
+    io.build_hierarchical_matrix(16, 2.0, 1e-4)
+    yield io, coor, conn
+    io.close()
+
+
+@needs_host
+def test_records_are_the_reference_frames(ref_io):
+    from bigwham_dev_b200.fields import s0_records
+
+    io, coor, conn = ref_io
+    rec = s0_records(coor, conn)
+    rot = io.get_rotation_matrix().reshape(-1, 2, 2)  # rows: tangent, normal
+    assert np.allclose(rec[:, 3:5], rot[:, 0, :], atol=1e-15, rtol=0)
+    assert np.allclose(np.column_stack([-rec[:, 4], rec[:, 3]]), rot[:, 1, :], atol=1e-15, rtol=0)
+    assert np.allclose(rec[:, :2], io.get_collocation_points().reshape(-1, 2), atol=1e-15, rtol=0)
+
+
+@needs_host
+def test_stresses_equal_the_reference(probe, ref_io):
+    io, coor, conn = ref_io
+    rng = np.random.default_rng(1)
+    pts = off_mesh_points(rng, 200)
+    dd = rng.uniform(-1, 1, 2 * len(conn))
+    s, _ = host_fields(probe, coor, conn, dd, pts)
+    want = io.compute_stresses(pts, dd).reshape(-1, 3)
+    assert np.abs(s - want).max() <= 1e-12 * np.abs(want).max()
+
+
+@needs_host
+def test_displacements_against_the_reference(probe, ref_io):
+    io, coor, conn = ref_io
+    rng = np.random.default_rng(2)
+    pts = off_mesh_points(rng, 150)
+    n = len(conn)
+    dd = np.zeros(2 * n)
+    dd[1::2] = rng.uniform(-1, 1, n)  # normal DDs: every component agrees
+    _, u = host_fields(probe, coor, conn, dd, pts)
+    want = io.compute_displacements(pts, dd).reshape(-1, 2)
+    assert np.abs(u - want).max() <= 1e-12 * np.abs(want).max()
+    # shear DD on one element along x: the reference's u1 agrees, its u2 is u1
+    c1 = np.array([[-1.0, 0.0], [1.0, 0.0]])
+    e1 = np.array([[0, 1]])
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+
+    one = BigWhamIOGpu(c1, e1, "2DS0-H", [E, NU], 4, useCuda=False)
+    one.build_hierarchical_matrix(16, 2.0, 1e-4)
+    _, u1 = host_fields(probe, c1, e1, np.array([1.0, 0.0]), pts)
+    w1 = one.compute_displacements(pts, np.array([1.0, 0.0])).reshape(-1, 2)
+    one.close()
+    assert np.abs(u1[:, 0] - w1[:, 0]).max() <= 1e-12 * np.abs(w1).max()
+    assert np.array_equal(w1[:, 0], w1[:, 1])
+    assert np.abs(u1[:, 1] - w1[:, 1]).max() > 1e-2
+
+
+def test_displacement_strains_give_the_stresses(probe):
+    """sigma = 2 G eps + lambda tr(eps) I from central differences of u."""
+    coor, conn = bent_crack(30, seed=3)
+    rng = np.random.default_rng(4)
+    dd = rng.uniform(-1, 1, 2 * len(conn))
+    pts = off_mesh_points(rng, 80)
+    # central differences need the field smooth over the stencil: points at
+    # least 0.1 from every element's centre line
+    from bigwham_dev_b200.fields import s0_records
+
+    rec = s0_records(coor, conn)
+    d = pts[:, None, :] - rec[None, :, :2]
+    along = np.einsum("pek,ek->pe", d, rec[:, 3:5])
+    across = np.abs(d[..., 0] * -rec[:, 4] + d[..., 1] * rec[:, 3])
+    near = ((np.abs(along) <= rec[:, 2] + 0.1) & (across < 0.1)).any(axis=1)
+    pts = pts[~near]
+    assert len(pts) > 40
+    lam = 2 * G * NU / (1 - 2 * NU)
+    h = 1e-5
+    s, _ = host_fields(probe, coor, conn, dd, pts)
+    _, ux_p = host_fields(probe, coor, conn, dd, pts + [h, 0])
+    _, ux_m = host_fields(probe, coor, conn, dd, pts - [h, 0])
+    _, uy_p = host_fields(probe, coor, conn, dd, pts + [0, h])
+    _, uy_m = host_fields(probe, coor, conn, dd, pts - [0, h])
+    du_dx, du_dy = (ux_p - ux_m) / (2 * h), (uy_p - uy_m) / (2 * h)
+    exx, eyy, exy = du_dx[:, 0], du_dy[:, 1], 0.5 * (du_dy[:, 0] + du_dx[:, 1])
+    s_fd = np.column_stack([2 * G * exx + lam * (exx + eyy), 2 * G * eyy + lam * (exx + eyy), 2 * G * exy])
+    assert np.abs(s_fd - s).max() <= 1e-7 * np.abs(s).max()
+
+
+def test_fields_decay_and_are_linear_in_dd(probe):
+    coor, conn = bent_crack(20, seed=5)
+    rng = np.random.default_rng(6)
+    dd = rng.uniform(-1, 1, 2 * len(conn))
+    pts = off_mesh_points(rng, 10)
+    s1, u1 = host_fields(probe, coor, conn, dd, pts)
+    s2, u2 = host_fields(probe, coor, conn, 2.5 * dd, pts)
+    assert np.allclose(s2, 2.5 * s1, rtol=1e-14, atol=0) and np.allclose(u2, 2.5 * u1, rtol=1e-14, atol=0)
+    far = np.array([[1e4, 3e3]])
+    sf, uf = host_fields(probe, coor, conn, dd, far)
+    assert np.abs(sf).max() < 1e-6 and np.abs(uf).max() < 1e-3
+
+
+@needs_host
+def test_on_the_element_line_the_limit_from_below(probe):
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+
+    c1 = np.array([[-1.0, 0.0], [1.0, 0.0]])
+    e1 = np.array([[0, 1]])
+    one = BigWhamIOGpu(c1, e1, "2DS0-H", [E, NU], 4, useCuda=False)
+    one.build_hierarchical_matrix(16, 2.0, 1e-4)
+    pl = np.array([[0.3, 0.0], [-0.7, 0.0], [1.5, 0.0], [-2.0, 0.0]])
+    s, u = host_fields(probe, c1, e1, np.array([0.0, 1.0]), pl)
+    ws = one.compute_stresses(pl, np.array([0.0, 1.0])).reshape(-1, 3)
+    wu = one.compute_displacements(pl, np.array([0.0, 1.0])).reshape(-1, 2)
+    one.close()
+    assert np.abs(s - ws).max() <= 1e-13 * np.abs(ws).max()
+    assert np.abs(u - wu).max() <= 1e-13 * np.abs(wu).max()
+    assert u[0, 1] == pytest.approx(0.5) and u[1, 1] == pytest.approx(0.5)  # half the opening, below
+
+
+def test_device_entry_checks_arguments_without_a_gpu():
+    """bw_s0_fields rejects bad arguments before any device call."""
+    from bigwham_dev_b200 import _capi as A
+
+    L = A.lib()
+    assert L.bw_s0_fields(0, 0, 1, 1, G, NU, 1, 1, 1, 0, 0) == A.BW_ERR_ARG  # no elements
+    assert L.bw_s0_fields(0, 2, 1, 1, G, NU, 1, 1, 0, 0, 0) == A.BW_ERR_ARG  # no output
+    assert L.bw_s0_fields(0, 2, 1, 1, -1.0, NU, 1, 1, 1, 0, 0) == A.BW_ERR_ARG  # bad G
+    assert L.bw_s0_fields(0, 2, 1, 1, G, 0.5, 1, 1, 1, 0, 0) == A.BW_ERR_ARG  # bad nu
+    assert L.bw_s0_fields(0, 2, 1, 1, G, NU, 0, 0, 0, 0, 0) == A.BW_OK  # no points: nothing to do
