@@ -65,6 +65,7 @@ _SIGS = {
     "bw_r0_aca": (C.c_int, [C.c_int, _I64, _P, C.c_double, C.c_double, _I64, _P, _P, _I64, C.c_double, C.c_int,
                             _P, _I64, _P, _I64, _P, _P, _P]),
     "bw_s0_fields": (C.c_int, [C.c_int, _I64, _P, _P, C.c_double, C.c_double, _I64, _P, _P, _P, _P]),
+    "bw_r0_fields": (C.c_int, [C.c_int, _I64, _P, _P, C.c_double, C.c_double, _I64, _P, _P, _P, _P]),
     "bw_destroy": (C.c_int, [_P]),
     "bw_version": (C.c_char_p, []),
 }

@@ -1433,6 +1433,27 @@ void par_copy(void *dst, const void *src, int64_t bytes) {
     std::memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, (size_t)std::min(step, bytes - o));
 }
 
+// Shared checks and launch of the observation-field kernels.
+template <typename Launch>
+int fields_entry(const char *name, int device, int64_t n_elems, const double *records, const double *dd, double G,
+                 double nu, int64_t n_pts, const double *pts, const double *stress, const double *disp, int threads,
+                 Launch &&launch) {
+  return device_guarded([&] {
+    if (!records || !dd || n_elems < 1 || n_pts < 0 || (n_pts > 0 && (!pts || (!stress && !disp))))
+      throw std::invalid_argument(std::string(name) + ": null or empty argument");
+    if (n_elems >= (int64_t(1) << 31)) throw std::invalid_argument(std::string(name) + ": more than 2^31 elements");
+    if (!(G > 0.0) || !(nu > -1.0 && nu < 0.5)) throw std::invalid_argument(std::string(name) + ": bad G or nu");
+    if (n_pts == 0) return BW_OK;
+    BW_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    BW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int64_t need = (n_pts + threads - 1) / threads;
+    launch(static_cast<int>(std::min<int64_t>(need, int64_t(std::max(1, sms)) * 4)));
+    BW_CUDA(cudaGetLastError());
+    return BW_OK;
+  });
+}
+
 }  // namespace
 
 extern "C" {
@@ -1611,22 +1632,22 @@ int bw_create_from_file(const char *path, int device, int verify, bw_hmat **out)
 
 int bw_s0_fields(int device, int64_t n_elems, const double *records, const double *dd, double G, double nu,
                  int64_t n_pts, const double *pts, double *stress, double *disp, void *stream) {
-  return device_guarded([&] {
-    if (!records || !dd || n_elems < 1 || n_pts < 0 || (n_pts > 0 && (!pts || (!stress && !disp))))
-      throw std::invalid_argument("bw_s0_fields: null or empty argument");
-    if (n_elems >= (int64_t(1) << 31)) throw std::invalid_argument("bw_s0_fields: more than 2^31 elements");
-    if (!(G > 0.0) || !(nu > -1.0 && nu < 0.5)) throw std::invalid_argument("bw_s0_fields: bad G or nu");
-    if (n_pts == 0) return BW_OK;
-    BW_CUDA(cudaSetDevice(device));
-    int sms = 0;
-    BW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    const int64_t need = (n_pts + bw::kS0Threads - 1) / bw::kS0Threads;
-    const int grid = static_cast<int>(std::min<int64_t>(need, int64_t(std::max(1, sms)) * 4));
-    bw::s0_fields_kernel<<<grid, bw::kS0Threads, 0, static_cast<cudaStream_t>(stream)>>>(
-        records, dd, static_cast<int>(n_elems), pts, static_cast<long long>(n_pts), G, nu, stress, disp);
-    BW_CUDA(cudaGetLastError());
-    return BW_OK;
-  });
+  return fields_entry("bw_s0_fields", device, n_elems, records, dd, G, nu, n_pts, pts, stress, disp, bw::kS0Threads,
+                      [&](int grid) {
+                        bw::s0_fields_kernel<<<grid, bw::kS0Threads, 0, static_cast<cudaStream_t>(stream)>>>(
+                            records, dd, static_cast<int>(n_elems), pts, static_cast<long long>(n_pts), G, nu,
+                            stress, disp);
+                      });
+}
+
+int bw_r0_fields(int device, int64_t n_elems, const double *records, const double *dd, double G, double nu,
+                 int64_t n_pts, const double *pts, double *stress, double *disp, void *stream) {
+  return fields_entry("bw_r0_fields", device, n_elems, records, dd, G, nu, n_pts, pts, stress, disp,
+                      bw::kR0FieldThreads, [&](int grid) {
+                        bw::r0_fields_kernel<<<grid, bw::kR0FieldThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+                            records, dd, static_cast<int>(n_elems), pts, static_cast<long long>(n_pts), G, nu,
+                            stress, disp);
+                      });
 }
 
 int bw_r0_assemble_fr(int device, int64_t n_elems, const double *records, double G, double nu, int64_t n_fr,

@@ -169,9 +169,9 @@ BW_HD Derivs derivs(double x, double y, double z, double a, double b) {
 }
 
 // Stresses in the element's local frame: s[dd][c], dd = DD x, y, z and
-// c = xx, yy, zz, xy, xz, yz (the reference's StressesKernelR0 layout).
-BW_HD void stress(double x, double y, double z, double a, double b, double G, double nu, double s[3][6]) {
-  const Derivs D = derivs(x, y, z, a, b);
+// c = xx, yy, zz, xy, xz, yz (the reference's StressesKernelR0 layout), from
+// the derivatives at (x, y, z); stress() evaluates them first.
+BW_HD void stress_from(const Derivs &D, double z, double G, double nu, double s[3][6]) {
   const double C = G / (4.0 * kPi * (1.0 - nu));
   s[0][0] = C * (2.0 * D.xz - z * D.xxx);
   s[0][1] = C * (2.0 * nu * D.xz - z * D.xyy);
@@ -193,10 +193,14 @@ BW_HD void stress(double x, double y, double z, double a, double b, double G, do
   s[2][5] = -C * z * D.yzz;
 }
 
+BW_HD void stress(double x, double y, double z, double a, double b, double G, double nu, double s[3][6]) {
+  stress_from(derivs(x, y, z, a, b), z, G, nu, s);
+}
+
 // Displacements in the element's local frame: u[i][j] = component i due to
-// unit DD j (the reference's DisplacementKernelR0 layout).
-BW_HD void displacement(double x, double y, double z, double a, double b, double nu, double u[3][3]) {
-  const Derivs D = derivs(x, y, z, a, b);
+// unit DD j (the reference's DisplacementKernelR0 layout), from the
+// derivatives; displacement() evaluates them first.
+BW_HD void displacement_from(const Derivs &D, double z, double nu, double u[3][3]) {
   const double c = 1.0 / (8.0 * kPi * (1.0 - nu)), k1 = 2.0 * (1.0 - nu), k2 = 1.0 - 2.0 * nu;
   u[0][0] = c * (k1 * D.z - z * D.xx);
   u[1][0] = -c * z * D.xy;
@@ -207,6 +211,10 @@ BW_HD void displacement(double x, double y, double z, double a, double b, double
   u[0][2] = -c * (k2 * D.x + z * D.xz);
   u[1][2] = -c * (k2 * D.y + z * D.yz);
   u[2][2] = c * (k1 * D.z - z * D.zz);
+}
+
+BW_HD void displacement(double x, double y, double z, double a, double b, double nu, double u[3][3]) {
+  displacement_from(derivs(x, y, z, a, b), z, nu, u);
 }
 
 // Hypersingular (H) kernel entry between two rectangles: tractions at the

@@ -372,6 +372,19 @@ int bw_r0_aca(int device, int64_t n_elems, const double *records, double G, doub
 int bw_s0_fields(int device, int64_t n_elems, const double *records, const double *dd, double G, double nu,
                  int64_t n_pts, const double *pts, double *stress, double *disp, void *stream);
 
+/* Stresses and displacements at observation points from a solution on a
+ * 3DR0 mesh (rectangles, constant displacement discontinuity), global frame.
+ * The reference's BigWhamIO returns zeros for this kernel family (its 3DR0
+ * observation kernels are stubs); these are the sums of its element kernels
+ * StressesKernelR0 / DisplacementKernelR0 in the layout of its 3D
+ * observation kernels.  All arrays are device memory.  records: n_elems x 17
+ * as for bw_r0_assemble_fr; dd: n_elems x 3 local DDs, mesh order; pts:
+ * n_pts x 3; stress (n_pts x 6: s11, s22, s33, s12, s13, s23) and / or disp
+ * (n_pts x 3) may be null, not both.  Each point sums the elements in mesh
+ * order.  Stream-ordered; returns after the launch. */
+int bw_r0_fields(int device, int64_t n_elems, const double *records, const double *dd, double G, double nu,
+                 int64_t n_pts, const double *pts, double *stress, double *disp, void *stream);
+
 /* Release everything. */
 int bw_destroy(bw_hmat *h);
 

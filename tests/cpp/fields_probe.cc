@@ -1,0 +1,40 @@
+// Host builds of the observation-field code the device kernels run per
+// (point, element) pair, in the kernels' order (per point, elements in mesh
+// order): 2DS0 (bigwham_dev_b200/csrc/bw_s0.h, s0_fields_kernel) and 3DR0
+// (bw_r0_fields.h, r0_fields_kernel).  Test helper: compiled by
+// tests/test_fields_cpu.py with g++.
+#include "bw_r0_fields.h"
+#include "bw_s0.h"
+
+#include <cstdint>
+
+extern "C" int probe_s0_fields(int64_t n_elems, const double *rec, const double *dd, double G, double nu,
+                               int64_t n_pts, const double *pts, double *stress, double *disp) {
+  for (int64_t p = 0; p < n_pts; p++) {
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int64_t e = 0; e < n_elems; e++)
+      bw::s0::add_point_fields(rec + bw::s0::kRecordDoubles * e, dd[2 * e], dd[2 * e + 1], pts[2 * p],
+                               pts[2 * p + 1], G, nu, acc);
+    for (int k = 0; k < 3; k++) stress[3 * p + k] = acc[k];
+    for (int k = 0; k < 2; k++) disp[2 * p + k] = acc[3 + k];
+  }
+  return 0;
+}
+
+// records: n_elems x 17 (the assembly records); the element values are packed
+// as r0_fields_kernel stages them.
+extern "C" int probe_r0_fields(int64_t n_elems, const double *rec, const double *dd, double G, double nu,
+                               int64_t n_pts, const double *pts, double *stress, double *disp) {
+  for (int64_t p = 0; p < n_pts; p++) {
+    double acc[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int64_t e = 0; e < n_elems; e++) {
+      double el[bw::r0::kFieldDoubles];
+      for (int k = 0; k < 14; k++) el[k] = rec[bw::r0::kFrameDoubles * e + (k < 12 ? k : k + 3)];
+      for (int k = 0; k < 3; k++) el[14 + k] = dd[3 * e + k];
+      bw::r0::add_point_fields(el, pts + 3 * p, G, nu, acc);
+    }
+    for (int k = 0; k < 6; k++) stress[6 * p + k] = acc[k];
+    for (int k = 0; k < 3; k++) disp[3 * p + k] = acc[6 + k];
+  }
+  return 0;
+}

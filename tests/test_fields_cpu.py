@@ -1,5 +1,7 @@
-"""2DS0 observation-point fields (bw_s0.h, the code s0_fields_kernel runs) on
-CPU through a host build of the same functions (tests/cpp/s0_probe.cc):
+"""Observation-point fields on CPU through host builds of the code the device
+kernels run (tests/cpp/fields_probe.cc).
+
+2DS0 (bw_s0.h, s0_fields_kernel):
 * stresses at points from a DD solution on a bent, unevenly meshed crack vs
   the reference's own BigWhamIO::ComputeStresses (host library; the cases stay
   below its OpenMP threshold, sqrt(N_src N_obs) <= 400, where its shared
@@ -11,6 +13,12 @@ CPU through a host build of the same functions (tests/cpp/s0_probe.cc):
   reference's shear kernel returns u1 in place of u2;
 * element records from the mesh equal the reference's element frames;
 * on an element's line, the limit from below, as the reference takes it.
+
+3DR0 (bw_r0_fields.h, r0_fields_kernel; the reference's BigWhamIO returns
+zeros for this family): on a crack rotated about a skew axis, the sums of
+the reference's own StressesKernelR0 / DisplacementKernelR0 contracted and
+rotated to global, 1e-12; the displacement's finite-difference strains give
+the stresses (3D Hooke's law) to 1e-7.
 """
 import ctypes as C
 import os
@@ -28,14 +36,14 @@ G = E / (2 * (1 + NU))
 
 @pytest.fixture(scope="module")
 def probe():
-    out = os.path.join(ROOT, "_build", "libs0_probe.so")
+    out = os.path.join(ROOT, "_build", "libfields_probe.so")
     os.makedirs(os.path.dirname(out), exist_ok=True)
     subprocess.run(["g++", "-std=c++17", "-O2", "-shared", "-fPIC", "-I", os.path.join(ROOT, "bigwham_dev_b200", "csrc"),
-                    os.path.join(ROOT, "tests", "cpp", "s0_probe.cc"), "-o", out], check=True)
+                    os.path.join(ROOT, "tests", "cpp", "fields_probe.cc"), "-o", out], check=True)
     L = C.CDLL(out)
     p = np.ctypeslib.ndpointer(np.float64, flags="C")
     L.probe_s0_fields.argtypes = [C.c_int64, p, p, C.c_double, C.c_double, C.c_int64, p, p, p]
-    L.probe_s0_local.argtypes = [C.c_double] * 5 + [p, p]
+    L.probe_r0_fields.argtypes = [C.c_int64, p, p, C.c_double, C.c_double, C.c_int64, p, p, p]
     return L
 
 
@@ -194,3 +202,104 @@ def test_device_entry_checks_arguments_without_a_gpu():
     assert L.bw_s0_fields(0, 2, 1, 1, -1.0, NU, 1, 1, 1, 0, 0) == A.BW_ERR_ARG  # bad G
     assert L.bw_s0_fields(0, 2, 1, 1, G, 0.5, 1, 1, 1, 0, 0) == A.BW_ERR_ARG  # bad nu
     assert L.bw_s0_fields(0, 2, 1, 1, G, NU, 0, 0, 0, 0, 0) == A.BW_OK  # no points: nothing to do
+
+
+# ---------------------------------------------------------------------------- 3DR0
+def r0_fields_host(L, rec, dd, pts):
+    pts = np.ascontiguousarray(pts, dtype=np.float64)
+    s, u = np.empty((len(pts), 6)), np.empty((len(pts), 3))
+    L.probe_r0_fields(rec.shape[0], np.ascontiguousarray(rec), np.ascontiguousarray(dd, dtype=np.float64), G, NU,
+                      len(pts), pts, s, u)
+    return s, u
+
+
+@pytest.fixture(scope="module")
+def tilted_r0():
+    """A 6 x 6 square crack rotated about a skew axis and shifted: every
+    element frame is a general rotation."""
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+    from bigwham_dev_b200.meshes import square_crack_3d
+
+    coor, conn = square_crack_3d(6)
+    coor = np.asarray(coor, dtype=np.float64).reshape(-1, 3)
+    ax = np.array([1.0, 2.0, 0.5]) / np.linalg.norm([1.0, 2.0, 0.5])
+    th = 0.7
+    K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    Rm = np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
+    coor = coor @ Rm.T + np.array([0.3, -0.2, 0.1])
+    io = BigWhamIOGpu(coor, conn, "3DR0-H", [E, NU], 4, useCuda=False)
+    rec = io.element_records()
+    io.close()
+    return rec
+
+
+def r0_reference_fields(rec, dd, pts):
+    """Sum over elements of the reference's StressesKernelR0 /
+    DisplacementKernelR0, contracted with the local DD and rotated to global."""
+    from oracle.pyoracle import ref_r0_displacement, ref_r0_stress
+
+    S, U = np.zeros((len(pts), 6)), np.zeros((len(pts), 3))
+    for p, x in enumerate(pts):
+        for e in range(rec.shape[0]):
+            cp, R, a, b = rec[e, :3], rec[e, 3:12].reshape(3, 3), rec[e, 15], rec[e, 16]
+            l = R @ (x - cp)
+            s = ref_r0_stress(l[0], l[1], l[2], a, b, G, NU)  # [dd][xx yy zz xy xz yz]
+            c = dd[3 * e:3 * e + 3] @ s
+            Sl = np.array([[c[0], c[3], c[4]], [c[3], c[1], c[5]], [c[4], c[5], c[2]]])
+            Sg = R.T @ Sl @ R
+            S[p] += [Sg[0, 0], Sg[1, 1], Sg[2, 2], Sg[0, 1], Sg[0, 2], Sg[1, 2]]
+            U[p] += R.T @ (ref_r0_displacement(l[0], l[1], l[2], a, b, NU) @ dd[3 * e:3 * e + 3])
+    return S, U
+
+
+@needs_host
+def test_r0_fields_equal_the_reference_element_kernels(probe, tilted_r0):
+    from oracle import ref_available
+
+    if not ref_available():
+        pytest.skip("oracle/_ref not built")
+    rec = tilted_r0
+    rng = np.random.default_rng(11)
+    dd = rng.uniform(-1, 1, 3 * rec.shape[0])
+    pts = rng.uniform(-1.5, 1.5, (25, 3))
+    s, u = r0_fields_host(probe, rec, dd, pts)
+    ws, wu = r0_reference_fields(rec, dd, pts)
+    # (measured: 5e-14 and 2e-14; the reference's own cancellation error near
+    # an element's plane, up to 9e-10, does not arise at these distances)
+    assert np.abs(s - ws).max() <= 1e-12 * np.abs(ws).max()
+    assert np.abs(u - wu).max() <= 1e-12 * np.abs(wu).max()
+
+
+@needs_host
+def test_r0_displacement_strains_give_the_stresses(probe, tilted_r0):
+    rec = tilted_r0
+    rng = np.random.default_rng(12)
+    dd = rng.uniform(-1, 1, 3 * rec.shape[0])
+    pts = rng.uniform(-1.5, 1.5, (60, 3))
+    # keep the stencil off the crack: points 0.15 or more from its plane
+    nrm = rec[0, 12:15]
+    pts = pts[np.abs((pts - rec[0, :3]) @ nrm) > 0.15][:30]
+    lam = 2 * G * NU / (1 - 2 * NU)
+    h = 1e-5
+    s, _ = r0_fields_host(probe, rec, dd, pts)
+    grad = np.zeros((len(pts), 3, 3))  # grad[p, i, j] = du_i / dx_j
+    for j in range(3):
+        e = np.zeros(3)
+        e[j] = h
+        _, up = r0_fields_host(probe, rec, dd, pts + e)
+        _, um = r0_fields_host(probe, rec, dd, pts - e)
+        grad[:, :, j] = (up - um) / (2 * h)
+    eps = 0.5 * (grad + grad.transpose(0, 2, 1))
+    tr = np.trace(eps, axis1=1, axis2=2)
+    sig = 2 * G * eps + lam * tr[:, None, None] * np.eye(3)
+    s_fd = np.column_stack([sig[:, 0, 0], sig[:, 1, 1], sig[:, 2, 2], sig[:, 0, 1], sig[:, 0, 2], sig[:, 1, 2]])
+    assert np.abs(s_fd - s).max() <= 1e-7 * np.abs(s).max()
+
+
+def test_r0_device_entry_checks_arguments_without_a_gpu():
+    from bigwham_dev_b200 import _capi as A
+
+    L = A.lib()
+    assert L.bw_r0_fields(0, 0, 1, 1, G, NU, 1, 1, 1, 0, 0) == A.BW_ERR_ARG
+    assert L.bw_r0_fields(0, 2, 1, 1, G, NU, 1, 1, 0, 0, 0) == A.BW_ERR_ARG
+    assert L.bw_r0_fields(0, 2, 1, 1, G, NU, 0, 0, 0, 0, 0) == A.BW_OK
