@@ -100,3 +100,30 @@ def test_out_of_range_indices_are_rejected_like_the_reference(built):
             HmatSelection(ex, rows, cols, device=-1, plan_only=True)
         with pytest.raises(IndexError):
             ref.selection_matvec(rows, cols, np.zeros(len(cols) * ex["dof"]))
+
+
+def test_selection_of_a_rectangular_base():
+    """A reference-built rectangular H-matrix (3DR0-3DR0-H, 63 receiver and
+    100 source elements: permutation_0_ and permutation_1_ differ in length):
+    rows go through permutation_0_, columns through permutation_1_; the
+    selection's product equals the H-matrix operator's own, restricted."""
+    import os
+
+    from oracle import HmatArrays, oracle_matvec
+
+    arr, _ = HmatArrays.load(os.path.join(os.path.dirname(__file__), "golden", "rect", "3dr0_rect.npz"))
+    ex = {"dof": arr.dof, "n_rows": arr.n_rows, "n_cols": arr.n_cols, "fr": arr.fr, "lr": arr.lr,
+          "fr_data": arr.fr_data, "lr_data": arr.lr_data, "perm0": arr.perm0, "perm1": arr.perm1}
+    d = arr.dof
+    D = np.column_stack([oracle_matvec(arr, np.eye(arr.n_cols)[:, j], 1) for j in range(arr.n_cols)])
+    rng = np.random.default_rng(6)
+    for rows, cols in ((rng.choice(63, 20, replace=False), rng.choice(100, 37, replace=False)),
+                       (np.arange(63), np.arange(100)), (np.array([62, 0, 62]), np.array([99, 5, 5]))):
+        sel = HmatSelection(ex, rows, cols, device=-1, plan_only=True)
+        x = rng.uniform(-1, 1, d * cols.size)
+        xf = np.zeros(arr.n_cols)
+        for i, c in enumerate(cols):  # in list order: the last of a repeated column counts
+            xf[d * c:d * c + d] = x[d * i:d * i + d]
+        want = (D @ xf)[(d * rows[:, None] + np.arange(d)).ravel()]
+        got = sel_matvec(sel, x)
+        assert np.abs(got - want).max() <= 1e-13 * max(1.0, np.abs(want).max())
