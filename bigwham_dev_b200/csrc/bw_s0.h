@@ -101,5 +101,22 @@ BW_S0_HD void add_point_fields(const double *rec, double dd_s, double dd_n, doub
   acc[4] += ux * ty + uy * ny;
 }
 
+// Hypersingular (H) entry between two elements: tractions at the receiver's
+// centre, in the receiver's frame (shear along its tangent, normal along its
+// normal), due to unit local DDs of the source; K[j][k] = traction j due to
+// DD k.  The reference's BieElastostatic<Segment<0>, Segment<0>, H>
+// (bie_elastostatic_segment_0_influence.h:176-232) stores the same 2 x 2
+// block column-major.
+BW_S0_HD void h_entry(const double *src, const double *rcv, double G, double nu, double K[2][2]) {
+  const double tx = rcv[3], ty = rcv[4], nx = -ty, ny = tx;
+  for (int k = 0; k < 2; k++) {
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    add_point_fields(src, k == 0 ? 1.0 : 0.0, k == 1 ? 1.0 : 0.0, rcv[0], rcv[1], G, nu, acc);
+    const double t1 = acc[0] * nx + acc[2] * ny, t2 = acc[2] * nx + acc[1] * ny;  // sigma n
+    K[0][k] = t1 * tx + t2 * ty;
+    K[1][k] = t1 * nx + t2 * ny;
+  }
+}
+
 }  // namespace s0
 }  // namespace bw

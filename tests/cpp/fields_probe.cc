@@ -38,3 +38,17 @@ extern "C" int probe_r0_fields(int64_t n_elems, const double *rec, const double 
   }
   return 0;
 }
+
+// Dense 2DS0 H matrix (original element order, 2 x 2 per pair) from
+// bw::s0::h_entry: H[(2 i + j), (2 e + k)] = traction j at element i due to
+// DD k of element e; out is (2 n) x (2 n) row-major.
+extern "C" int probe_s0_dense_h(int64_t n, const double *rec, double G, double nu, double *out) {
+  for (int64_t i = 0; i < n; i++)
+    for (int64_t e = 0; e < n; e++) {
+      double K[2][2];
+      bw::s0::h_entry(rec + 5 * e, rec + 5 * i, G, nu, K);
+      for (int j = 0; j < 2; j++)
+        for (int k = 0; k < 2; k++) out[(2 * i + j) * 2 * n + 2 * e + k] = K[j][k];
+    }
+  return 0;
+}

@@ -44,6 +44,7 @@ def probe():
     p = np.ctypeslib.ndpointer(np.float64, flags="C")
     L.probe_s0_fields.argtypes = [C.c_int64, p, p, C.c_double, C.c_double, C.c_int64, p, p, p]
     L.probe_r0_fields.argtypes = [C.c_int64, p, p, C.c_double, C.c_double, C.c_int64, p, p, p]
+    L.probe_s0_dense_h.argtypes = [C.c_int64, p, C.c_double, C.c_double, p]
     return L
 
 
@@ -303,3 +304,21 @@ def test_r0_device_entry_checks_arguments_without_a_gpu():
     assert L.bw_r0_fields(0, 0, 1, 1, G, NU, 1, 1, 1, 0, 0) == A.BW_ERR_ARG
     assert L.bw_r0_fields(0, 2, 1, 1, G, NU, 1, 1, 0, 0, 0) == A.BW_ERR_ARG
     assert L.bw_r0_fields(0, 2, 1, 1, G, NU, 0, 0, 0, 0, 0) == A.BW_OK
+
+
+def test_s0_h_entries_equal_the_reference_operator(probe):
+    """The element in its hypersingular use: H entries between all element
+    pairs of a bent, unevenly meshed crack (self-effects included) against
+    the reference's dense operator (an eta = 0 build: every block full rank)."""
+    from bigwham_dev_b200.fields import s0_records
+    from oracle import RefHmat, ref_available
+
+    if not ref_available():
+        pytest.skip("oracle/_ref not built")
+    coor, conn = bent_crack(40, seed=8)
+    n = len(conn)
+    ref = RefHmat("2DS0-H", coor, conn, [E, NU], 8, 0.0, 1e-5, n_threads=2)
+    D = np.column_stack([ref.matvec(np.eye(2 * n)[:, j]) for j in range(2 * n)])
+    H = np.empty((2 * n, 2 * n))
+    probe.probe_s0_dense_h(n, s0_records(coor, conn), G, NU, H)
+    assert np.abs(H - D).max() <= 1e-13 * np.abs(D).max()
