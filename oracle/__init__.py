@@ -17,6 +17,7 @@ Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 """
 from .pyoracle import (  # noqa: F401
     HmatArrays,
+    RefGaussian,
     RefHmat,
     oracle_available,
     oracle_diagonal,

@@ -113,6 +113,13 @@ def _ref():
         lib.ref_matvec.argtypes = [C.c_void_p, _f64p, _f64p]
         lib.ref_matvec_perm.argtypes = [C.c_void_p, _f64p, _f64p]
         lib.ref_diagonal.argtypes = [C.c_void_p, _f64p]
+        lib.ref_gaussian_create.argtypes = [C.c_int64, C.c_double, C.c_int, C.c_double, C.c_double, C.c_int]
+        lib.ref_gaussian_create.restype = C.c_void_p
+        lib.ref_gaussian_sizes.argtypes = [C.c_void_p, _i64p]
+        lib.ref_gaussian_export.argtypes = [C.c_void_p, _i64p, _i64p, _f64p, _f64p, _i64p]
+        lib.ref_gaussian_matvec_perm.argtypes = [C.c_void_p, _f64p, _f64p]
+        lib.ref_gaussian_diagonal.argtypes = [C.c_void_p, _f64p]
+        lib.ref_gaussian_destroy.argtypes = [C.c_void_p]
         lib.ref_selection_matvec.argtypes = [C.c_void_p, _i32p, C.c_int64, _i32p, C.c_int64, _f64p, _f64p]
         lib.ref_selection_full_blocks.argtypes = [C.c_void_p, _i32p, C.c_int64, _i32p, C.c_int64, C.c_void_p,
                                                   C.c_void_p, C.c_int64]
@@ -143,6 +150,45 @@ def ref_r0_displacement(x, y, z, a, b, nu):
     if _ref().ref_r0_displacement(x, y, z, a, b, nu, out) != 0:
         raise RuntimeError("ref_r0_displacement failed")
     return out.reshape(3, 3)
+
+
+class RefGaussian:
+    """The reference's Gaussian-matrix H-matrix (its own cluster tree,
+    pattern, GaussianMatrix generator and Hmat build, as
+    src/hmat/hmatrix/_test/Hmat_test_gaussian_mat.cpp makes it): n points on
+    a line, dof 1."""
+
+    def __init__(self, n: int, alpha: float, leaf: int = 32, eta: float = 3.0, eps: float = 1e-3, n_threads: int = 4):
+        lib = _ref()
+        self._h = lib.ref_gaussian_create(int(n), float(alpha), int(leaf), float(eta), float(eps), int(n_threads))
+        if not self._h:
+            raise RuntimeError("reference Gaussian H-matrix construction failed")
+        self.n = int(n)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _ref_lib is not None:
+            _ref_lib.ref_gaussian_destroy(self._h)
+            self._h = None
+
+    def arrays(self) -> "HmatArrays":
+        sz = np.zeros(4, np.int64)
+        _ref().ref_gaussian_sizes(self._h, sz)
+        fr, lr = np.zeros((sz[0], 4), np.int64), np.zeros((sz[1], 5), np.int64)
+        fd, ld = np.zeros(max(1, sz[2])), np.zeros(max(1, sz[3]))
+        perm = np.zeros(self.n, np.int64)
+        _ref().ref_gaussian_export(self._h, fr, lr, fd, ld, perm)
+        return HmatArrays(1, self.n, self.n, fr, lr, fd[:sz[2]], ld[:sz[3]], perm, perm.copy())
+
+    def matvec_perm(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.n)
+        _ref().ref_gaussian_matvec_perm(self._h, x, y)
+        return y
+
+    def diagonal(self):
+        d = np.empty(self.n)
+        _ref().ref_gaussian_diagonal(self._h, d)
+        return d
 
 
 class RefHmat:

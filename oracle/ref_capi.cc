@@ -26,6 +26,11 @@
 #include "elements/rectangle.h"
 #include "elements/segment.h"
 #include "elements/triangle.h"
+#include "hmat/arrayFunctor/GaussianMatrix.h"
+#include "hmat/cluster/cluster.h"
+#include "hmat/hierarchical_representation.h"
+#include "hmat/hmatrix/h_pattern.h"
+#include "hmat/hmatrix/hmat.h"
 #include "io/bigwham_io.h"
 
 #ifdef BIGWHAM_OPENMP
@@ -37,6 +42,15 @@ struct RefHandle {
   std::unique_ptr<BigWhamIO> io;
 };
 RefHandle *H(void *h) { return static_cast<RefHandle *>(h); }
+
+// The reference's Gaussian-matrix H-matrix (no mesh, no BigWhamIO): cluster
+// tree, pattern and Hmat built by its own code over its GaussianMatrix
+// generator (dof 1).
+struct RefGauss {
+  std::shared_ptr<bigwham::HRepresentation> hr;
+  std::unique_ptr<bigwham::Hmat<double>> h;
+};
+RefGauss *GS(void *h) { return static_cast<RefGauss *>(h); }
 }  // namespace
 
 extern "C" {
@@ -209,6 +223,85 @@ int64_t ref_selection_full_blocks(void *h, const int *rows, int64_t n_rows, cons
     return -1;
   }
 }
+
+// Gaussian-matrix H-build as the reference's own test makes it
+// (src/hmat/hmatrix/_test/Hmat_test_gaussian_mat.cpp:44-71): n points on a
+// line at x = i, cluster(leaf), hmatrixTreeIxI(eta), createPattern,
+// GaussianMatrix(n, alpha), Hmat(M, eps, threads).  permutation_1_ is left
+// unset there; it is set here to permutation_0_ (a square, self-interaction
+// matrix) so that the original-order products exist.
+void *ref_gaussian_create(int64_t n, double alpha, int leaf, double eta, double eps, int n_threads) {
+  try {
+    il::Array2D<double> points{n, 1, 0.0};
+    for (il::int_t i = 0; i < n; i++) points(i, 0) = 1.0 * i;
+    bigwham::Cluster cl = bigwham::cluster(leaf, il::io, points);
+    const il::Tree<bigwham::SubHMatrix, 4> tree = bigwham::hmatrixTreeIxI(points, cl.partition, eta);
+    auto *g = new RefGauss;
+    g->hr = std::make_shared<bigwham::HRepresentation>();
+    g->hr->pattern_ = bigwham::createPattern(tree);
+    g->hr->permutation_0_ = cl.permutation;
+    g->hr->permutation_1_ = cl.permutation;
+    bigwham::GaussianMatrix<double> M{n, alpha, g->hr};
+    g->h.reset(new bigwham::Hmat<double>(M, eps, n_threads, false));
+    return g;
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+// sizes[4] = (FR blocks, LR blocks, FR entries, LR entries A then B).
+int ref_gaussian_sizes(void *h, int64_t *sizes) {
+  auto p = GS(h)->h->pattern();
+  sizes[0] = p.n_FRB;
+  sizes[1] = p.n_LRB;
+  sizes[2] = sizes[3] = 0;
+  for (const auto &b : GS(h)->h->get_full_rank_blocks()) sizes[2] += b->size(0) * b->size(1);
+  for (const auto &b : GS(h)->h->get_low_rank_blocks()) sizes[3] += b->A.size(0) * b->A.size(1) + b->B.size(0) * b->B.size(1);
+  return 0;
+}
+
+// The flat form: fr n_FR x 4, lr n_LR x 5 (rank in scalar columns), blocks
+// column-major back to back (LR: A then B), the permutation.
+int ref_gaussian_export(void *h, int64_t *fr, int64_t *lr, double *fr_data, double *lr_data, int64_t *perm) {
+  auto *g = GS(h);
+  auto p = g->h->pattern();
+  for (il::int_t k = 0; k < p.n_FRB; k++)
+    for (int r = 0; r < 4; r++) fr[4 * k + r] = p.FRB_pattern(r + 1, k);
+  for (il::int_t k = 0; k < p.n_LRB; k++)
+    for (int r = 0; r < 5; r++) lr[5 * k + r] = p.LRB_pattern(r + 1, k);
+  int64_t o = 0;
+  for (const auto &b : g->h->get_full_rank_blocks()) {
+    copy_colmajor(*b, fr_data + o);
+    o += b->size(0) * b->size(1);
+  }
+  o = 0;
+  for (const auto &b : g->h->get_low_rank_blocks()) {
+    copy_colmajor(b->A, lr_data + o);
+    o += b->A.size(0) * b->A.size(1);
+    copy_colmajor(b->B, lr_data + o);
+    o += b->B.size(0) * b->B.size(1);
+  }
+  for (il::int_t i = 0; i < g->hr->permutation_0_.size(); i++) perm[i] = g->hr->permutation_0_[i];
+  return 0;
+}
+
+// Hmat::matvec (permuted ordering, hmat.cc:472-537) and Hmat::diagonal
+// (permuted ordering, hmat.cc:240-255).
+int ref_gaussian_matvec_perm(void *h, const double *x, double *y) {
+  const int64_t n = GS(h)->h->size(1);
+  il::ArrayView<double> xv{x, n};
+  il::Array<double> out = GS(h)->h->matvec(xv);
+  std::memcpy(y, out.data(), sizeof(double) * out.size());
+  return 0;
+}
+
+int ref_gaussian_diagonal(void *h, double *d) {
+  std::vector<double> v = GS(h)->h->diagonal();
+  std::memcpy(d, v.data(), sizeof(double) * v.size());
+  return 0;
+}
+
+void ref_gaussian_destroy(void *h) { delete GS(h); }
 
 // BigWhamIO::GetDiagonal, original ordering (bigwham_io.cc:909-916).
 int ref_diagonal(void *h, double *d) {
