@@ -226,3 +226,32 @@ def test_batch_with_rank_zero_leaves_and_a_one_point_member():
         w, wt = oracle_matvec_perm(m, x[c0:c1], 1), oracle_rmatvec_perm(m, g[r0:r1], 1)
         assert np.abs(y[r0:r1] - w).max() <= 1e-13 * max(1.0, np.abs(w).max()), k
         assert np.abs(yt[c0:c1] - wt).max() <= 1e-13 * max(1.0, np.abs(wt).max()), k
+
+
+def test_two_element_meshes_built_by_the_reference():
+    """The reference's two-element 3D meshes (the square [0,1]^2 as two
+    triangles, src/io/_test/bigwham_io_gen_test_3d.cc:22-48; and as two
+    rectangles): 6 x 6 H-matrices through the plan, against its own MatVec
+    (original ordering, both permutations applied)."""
+    from oracle import RefHmat, ref_available
+
+    if not ref_available():
+        pytest.skip("oracle/_ref not built")
+    tri = (np.array([0, 0, 0, 1, 0, 0, 0, 1, 0, 1, 1, 0], float), np.array([0, 1, 2, 1, 2, 3]), "3DT0-H")
+    rect = (np.array([0, 0, 0, 0.5, 0, 0, 1, 0, 0, 0, 1, 0, 0.5, 1, 0, 1, 1, 0], float),
+            np.array([0, 1, 4, 3, 1, 2, 5, 4]), "3DR0-H")
+    for coor, conn, kernel in (tri, rect):
+        ref = RefHmat(kernel, coor.reshape(-1, 3), conn.reshape(2, -1), [1.0, 0.0 if kernel == "3DT0-H" else 0.25],
+                      32, 0.0, 1e-3, n_threads=2)
+        arr = ref.arrays()
+        assert (arr.n_rows, arr.n_cols) == (6, 6)
+        h = HmatGpu(3, 6, 6, arr.perm0, arr.perm1, device=-1)
+        h.add_flat(arr.fr, arr.lr, arr.fr_data, arr.lr_data)
+        h.finalize(plan_only=True, precisions=("fp64",), transpose=True)
+        x = np.random.default_rng(3).uniform(-1, 1, 6)
+        d = 3
+        xp = x[(d * np.asarray(arr.perm1)[:, None] + np.arange(d)).ravel()]
+        y = np.empty(6)
+        y[(d * np.asarray(arr.perm0)[:, None] + np.arange(d)).ravel()] = replay(h, xp)
+        want = ref.matvec(x)
+        assert np.abs(y - want).max() <= 1e-14 * np.abs(want).max(), kernel
