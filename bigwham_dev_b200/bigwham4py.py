@@ -397,6 +397,21 @@ except Exception:  # pragma: no cover - scipy is part of the image
     _LinOp = object
 
 
+def _csc_entries(val, row, col, shape, keep_ratio: float):
+    """CSC matrix of the entries; keep_ratio < 1 keeps the largest |entries|
+    (that share of them, ties kept), as the reference's _getFullBlocks."""
+    from scipy.sparse import csc_matrix
+
+    if keep_ratio < 1.0:
+        k = int(np.ceil(keep_ratio * val.size))
+        if k == 0:
+            return csc_matrix(shape)
+        thr = np.partition(np.abs(val), -k)[-k]
+        keep = np.abs(val) >= thr
+        val, row, col = val[keep], row[keep], col[keep]
+    return csc_matrix((val, (row, col)), shape=shape)
+
+
 class BEMatrix(_LinOp):
     """scipy LinearOperator over the GPU H-matrix (reference: bigwham4py.BEMatrix)."""
 
@@ -503,20 +518,11 @@ class BEMatrix(_LinOp):
 
     def _getFullBlocks(self, original_order=True, keep_ratio: float = 1.0):
         """Full-rank blocks as a scipy CSC matrix (bigwham4py.py:252-276)."""
-        from scipy.sparse import csc_matrix
-
         if not (0 < keep_ratio <= 1):
             raise ValueError("ratio must be a float between 0 and 1.")
         self._build()
         val, row, col = self.H_.get_full_blocks(original_order)
-        if keep_ratio < 1.0:
-            k = int(np.ceil(keep_ratio * val.size))
-            if k == 0:
-                return csc_matrix(self.shape)
-            thr = np.partition(np.abs(val), -k)[-k]
-            mask = np.abs(val) >= thr
-            val, row, col = val[mask], row[mask], col[mask]
-        return csc_matrix((val, (row, col)), shape=self.shape)
+        return _csc_entries(val, row, col, self.shape, keep_ratio)
 
     def _getPattern(self):
         return self.H_.get_hpattern()
@@ -629,19 +635,10 @@ class BEMatrixSelection(_LinOp):
     def _getFullBlocks(self, keep_ratio: float = 1.0):
         """The selection's full-rank entries as a scipy CSC matrix (the
         reference's GetFullBlocks on the selection, hmat_selection.cc:265-375)."""
-        from scipy.sparse import csc_matrix
-
         if not (0 < keep_ratio <= 1):
             raise ValueError("ratio must be a float between 0 and 1.")
         val, pos = self.S_.full_blocks()
-        if keep_ratio < 1.0:
-            k = int(np.ceil(keep_ratio * val.size))
-            if k == 0:
-                return csc_matrix(self.shape)
-            thr = np.partition(np.abs(val), -k)[-k]
-            keep = np.abs(val) >= thr
-            val, pos = val[keep], pos[keep]
-        return csc_matrix((val, (pos[:, 0], pos[:, 1])), shape=self.shape)
+        return _csc_entries(val, pos[:, 0], pos[:, 1], self.shape, keep_ratio)
 
     def H_ILU_prec(self, fill_factor=1, drop_tol=1e-3, keep_ratio=1.0):
         from scipy.sparse.linalg import LinearOperator, spilu
