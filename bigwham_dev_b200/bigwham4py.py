@@ -536,20 +536,45 @@ class BEMatrix(_LinOp):
         ilu = spilu(self._getFullBlocks(keep_ratio=keep_ratio), fill_factor=fill_factor, drop_tol=drop_tol)
         return LinearOperator(self.shape, ilu.solve)
 
-    def compute_displacements(self, list_coor, local_solu):
-        """Displacements at points (the reference's host code); (n_points, dim)."""
+    def _device_fields(self):
+        """The GPU evaluator of observation fields for this mesh (fields.py;
+        kernels 2DS0-H and 3DR0-H), made once."""
+        if getattr(self, "_dev_fields", None) is None:
+            from .fields import R0Fields, S0Fields
+
+            E, nu = float(self.properties_[0]), float(self.properties_[1])
+            if self.kernel_ == "2DS0-H":
+                self._dev_fields = S0Fields(self.H_._coor.reshape(-1, 2), self.H_._conn.reshape(-1, 2), E, nu,
+                                            self.H_.device)
+            elif self.kernel_ == "3DR0-H":
+                self._dev_fields = R0Fields(self.H_.element_records(), E, nu, self.H_.device)
+            else:
+                raise NotImplementedError(f"device fields for {self.kernel_}: 2DS0-H and 3DR0-H only")
+        return self._dev_fields
+
+    def compute_displacements(self, list_coor, local_solu, device: bool = False):
+        """Displacements at points; (n_points, dim).  device=False: the
+        reference's host code; device=True: the GPU kernels of fields.py
+        (2DS0-H, 3DR0-H; for 3DR0-H the reference returns zeros)."""
         self._build()
         n = self.getSpatialDimension()
         list_coor = np.asarray(list_coor, dtype=np.float64)
         assert n == list_coor.shape[1], "Coordinates dimension of the given points is not matching the problem spatial dimension !"
+        if device:
+            return self._device_fields().fields(list_coor, np.asarray(local_solu, dtype=np.float64),
+                                                want_stress=False)[1]
         return self.H_.compute_displacements(list_coor, local_solu).reshape(-1, n)
 
-    def compute_stresses(self, list_coor, local_solu):
-        """Stresses at points (the reference's host code); (n_points, 3 or 6)."""
+    def compute_stresses(self, list_coor, local_solu, device: bool = False):
+        """Stresses at points; (n_points, 3 or 6).  device as for
+        compute_displacements."""
         self._build()
         n = self.getSpatialDimension()
         list_coor = np.asarray(list_coor, dtype=np.float64)
         assert n == list_coor.shape[1], "Coordinates dimension of the given points is not matching the problem spatial dimension !"
+        if device:
+            return self._device_fields().fields(list_coor, np.asarray(local_solu, dtype=np.float64),
+                                                want_disp=False)[0]
         return self.H_.compute_stresses(list_coor, local_solu).reshape(-1, 3 if n == 2 else 6)
 
     def getMatvecTime(self, N_matvec=100):
