@@ -127,3 +127,17 @@ def test_selection_of_a_rectangular_base():
         want = (D @ xf)[(d * rows[:, None] + np.arange(d)).ravel()]
         got = sel_matvec(sel, x)
         assert np.abs(got - want).max() <= 1e-13 * max(1.0, np.abs(want).max())
+
+
+def test_empty_selections_match_the_reference(built):
+    """No columns: the selected rows are zero (the reference's x_full is all
+    zero); no rows: an empty product."""
+    ref, ex, n = built
+    d = ex["dof"]
+    for rows, cols in (([1, 2, 7], []), ([], [3, 4]), ([], [])):
+        rows, cols = np.array(rows, np.int64), np.array(cols, np.int64)
+        sel = HmatSelection(ex, rows, cols, device=-1, plan_only=True)
+        assert sel.shape == (d * rows.size, d * cols.size)
+        x = np.ones(d * cols.size)
+        got, want = sel_matvec(sel, x), ref.selection_matvec(rows, cols, x)
+        assert got.shape == want.shape and np.array_equal(got, want)
