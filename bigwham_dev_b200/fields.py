@@ -62,11 +62,11 @@ class _Fields:
 
     def fields(self, points, dd, want_stress: bool = True, want_disp: bool = True):
         torch = self.torch
-        host = isinstance(points, np.ndarray)
+        host = not torch.is_tensor(points)  # numpy arrays, lists: numpy results
         dev = f"cuda:{self.device}"
         p = torch.as_tensor(np.ascontiguousarray(points, dtype=np.float64) if host else points,
                             dtype=torch.float64, device=dev).reshape(-1, self.dim).contiguous()
-        d = torch.as_tensor(np.ascontiguousarray(dd, dtype=np.float64) if isinstance(dd, np.ndarray) else dd,
+        d = torch.as_tensor(dd if torch.is_tensor(dd) else np.ascontiguousarray(dd, dtype=np.float64),
                             dtype=torch.float64, device=dev).reshape(-1).contiguous()
         if d.numel() != self.dof * self.n_elems:
             raise ValueError(f"dd has {d.numel()} values, the mesh {self.dof * self.n_elems} DDs")
