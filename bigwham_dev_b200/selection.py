@@ -207,8 +207,8 @@ class HmatSelection:
 
     def matvec(self, x, precision=None, out=None):
         precision = precision or self.precisions[0]
-        if isinstance(x, np.ndarray):
-            x = np.asarray(x, dtype=np.float64)
+        if not hasattr(x, "data_ptr"):  # numpy arrays, lists: the host path
+            x = np.asarray(x, dtype=np.float64).ravel()
             if x.size != self.shape[1]:
                 raise ValueError(f"x has {x.size} entries, the selection {self.shape[1]} columns")
             y_u = self.h.matvec(np.ascontiguousarray(x[self.x_take]), precision)
