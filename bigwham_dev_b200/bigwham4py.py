@@ -633,7 +633,10 @@ class BEMatrix(_LinOp):
 
 
 class BEMatrixSelection(_LinOp):
-    """H[rows, cols] of a BEMatrix on the GPU (BEMatrix.__getitem__)."""
+    """H[rows, cols] of a BEMatrix on the GPU (BEMatrix.__getitem__).  Made
+    from a host copy of the base's blocks (export_blocks: as large as the
+    H-matrix); once the selection's own handle is laid out only the
+    full-rank part is kept (for _getFullBlocks)."""
 
     def __init__(self, parent: "BEMatrix", rows, cols):
         from .selection import HmatSelection
@@ -647,7 +650,6 @@ class BEMatrixSelection(_LinOp):
             self.S_ = HmatSelection(ex, rows, cols, device=io.device, precisions=precisions)
         else:  # a host build: the selection's plan only (no GPU H-matrix to apply)
             self.S_ = HmatSelection(ex, rows, cols, device=-1, precisions=precisions, plan_only=True)
-        self._ex = ex
         super().__init__(np.dtype(float), self.S_.shape)
 
     def _matvec(self, v):

@@ -178,7 +178,8 @@ class HmatSelection:
         from .hmat import HmatGpu
 
         s = select_blocks(ex, rows, cols)
-        self._base = ex
+        # full_blocks reads the base's full-rank blocks only: keep those
+        self._base = {k: ex[k] for k in ("dof", "fr", "fr_data", "perm0", "perm1")}
         self._sel = s["_sel"]
         self.dof = d = s["dof"]
         self._R, self._C = s["_rows"], s["_cols"]
