@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_SOURCES = ["csrc/bw_capi.cu", "csrc/bw_layout.cpp", "csrc/bw_file.cpp"]
-CUDA_DEPS = CUDA_SOURCES + ["csrc/bw_kernels.cuh", "csrc/bw_mm_kernels.cuh", "csrc/bw_layout.h", "csrc/bw_file.h", "csrc/bw_r0.h", "csrc/bw_assemble_kernels.cuh", "csrc/bw_aca.h", "csrc/bw_aca_kernels.cuh", "csrc/bw_pack.h", "csrc/bw_devlayout_kernels.cuh", "../include/bigwham_b200.h"]
+CUDA_DEPS = CUDA_SOURCES + ["csrc/bw_kernels.cuh", "csrc/bw_mm_kernels.cuh", "csrc/bw_layout.h", "csrc/bw_file.h", "csrc/bw_r0.h", "csrc/bw_assemble_kernels.cuh", "csrc/bw_aca.h", "csrc/bw_aca_kernels.cuh", "csrc/bw_pack.h", "csrc/bw_devlayout_kernels.cuh", "csrc/bw_s0.h", "csrc/bw_r0_fields.h", "csrc/bw_fields_kernels.cuh", "../include/bigwham_b200.h"]
 
 
 def _newer(target: str, deps) -> bool:

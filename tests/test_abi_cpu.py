@@ -62,3 +62,16 @@ def test_host_bindings_match_the_header():
     assert set(sigs) == set(names), sorted(set(sigs) ^ set(names))
     for n, (_, args) in sigs.items():
         assert len(args) == names[n], f"{n}: {len(args)} ctypes arguments, header declares {names[n]}"
+
+
+def test_every_backend_header_is_a_build_dependency():
+    """build_cuda rebuilds when any header under csrc/ changes: each one is
+    listed among its dependencies."""
+    import glob
+
+    from bigwham_dev_b200 import build as B
+
+    here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "bigwham_dev_b200")
+    headers = {os.path.relpath(p, here) for p in glob.glob(os.path.join(here, "csrc", "*.h")) +
+               glob.glob(os.path.join(here, "csrc", "*.cuh"))}
+    assert headers <= set(B.CUDA_DEPS), sorted(headers - set(B.CUDA_DEPS))
