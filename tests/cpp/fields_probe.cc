@@ -3,6 +3,7 @@
 // order): 2DS0 (bigwham_dev_b200/csrc/bw_s0.h, s0_fields_kernel) and 3DR0
 // (bw_r0_fields.h, r0_fields_kernel).  Test helper: compiled by
 // tests/test_fields_cpu.py with g++.
+#include "bw_aca.h"
 #include "bw_r0_fields.h"
 #include "bw_s0.h"
 
@@ -51,4 +52,22 @@ extern "C" int probe_s0_dense_h(int64_t n, const double *rec, double G, double n
         for (int k = 0; k < 2; k++) out[(2 * i + j) * 2 * n + 2 * e + k] = K[j][k];
     }
   return 0;
+}
+
+// Block ACA with 2 x 2 pivots (bw::aca::block_aca_host<2>) of the 2DS0 block
+// [i0, i1) x [j0, j1) (permuted points; perm: permuted point -> element) with
+// the entries of bw::s0::h_entry.  A: (i1 - i0) 2 x cap 2, B: cap 2 x
+// (j1 - j0) 2, column-major; returns the rank in blocks (-1 when cap was too
+// small).
+extern "C" int probe_s0_aca(const double *rec, double G, double nu, const int64_t *perm, int64_t i0, int64_t j0,
+                            int64_t i1, int64_t j1, double eps, int cap, double *A, double *B, double *err) {
+  const int n0 = (int)(i1 - i0), n1 = (int)(j1 - j0);
+  double *work = new double[(size_t)(n0 + n1) * 4 + n0 + n1];
+  auto entry = [&](int i, int j, double K[2][2]) {
+    bw::s0::h_entry(rec + 5 * perm[j0 + j], rec + 5 * perm[i0 + i], G, nu, K);
+  };
+  const bw::aca::Result r = bw::aca::block_aca_host<2>(entry, n0, n1, eps, cap, A, B, work);
+  delete[] work;
+  *err = r.error;
+  return r.overflow ? -1 : r.rank_blocks;
 }
