@@ -6,8 +6,10 @@ z = 0 (196,608 DoF), E = 1, nu = 0.25, leaf 32, eta 3, ACA eps 1e-5; the
 reference's own host code builds the H-matrix (mesh, kernel, cluster tree,
 ACA: libbigwham_host.so), the blocks are uploaded once in FP64, FP32 and BF16
 (per-block FP32 scale), and one step is one H x over the whole matrix with
-x ~ U(-1,1) (seed 1) resident in HBM.  The headline value is the BF16-storage
-(FP32 accumulation) rate; the FP64 and FP32 rates ride along.
+x ~ U(-1,1) (seed 1) resident in HBM.  The headline value is the FP32-storage
+(FP32 accumulation) rate: the storage whose matvec stays within 1e-6 of the
+FP64 GPU matvec.  The FP64 and BF16 rates ride along; BF16 reaches 1e-6 only
+through FP64-refined GMRES (the north-star solve checks in the same line).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -21,9 +23,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -31,7 +31,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "H-matvec/s, 3DR0-H 196,608 DoF (BF16 blocks + FP32 accumulate; FP64 and FP32 alongside)"
+METRIC = ("H-matvec/s & %HBM roofline, 3DR0-H 196,608 DoF, mixed (FP32 blocks, FP32 accumulation) vs FP64 GPU "
+          "at <=1e-6 rel err; FP64 and BF16 alongside")
+HEAD = "fp32"  # headline storage precision
 UNIT = "matvec/s"
 PROPS = [1.0, 0.25]
 LEAF, ETA, EPS = 32, 3.0, 1e-5
@@ -66,43 +68,83 @@ def read_traffic(kernel_key):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event reasons of the GPU polled through NVML by a
+    thread every 2 ms; window()/end() bracket the timed loops, and the report
+    covers the samples inside them."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __init__(self, device_index):
-        self.dev = device_index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
+    def __init__(self, device_index, period_s=0.002):
+        self.dev, self.period = int(device_index), period_s
+        self.samples, self.windows = [], []
+        self.nv, self.h, self.thread, self.err = None, None, None, None
+        self._stop = False
+
+    def _handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:  # the CUDA device's NVML handle, whatever CUDA_VISIBLE_DEVICES says
+            pr = torch.cuda.get_device_properties(self.dev)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
+        import threading
+
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
-                                      stderr=subprocess.DEVNULL)
-        except Exception:
-            self.p = None
+            self.nv, self.h = self._handle()
+        except Exception as e:  # no NVML: the report says so
+            self.err = f"NVML unavailable: {e}"
+            return
+
+        def run():
+            nv = self.nv
+            while not self._stop:
+                try:
+                    self.samples.append((time.perf_counter(), nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM),
+                                         nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)))
+                except Exception as e:
+                    self.err = str(e)
+                    return
+                time.sleep(self.period)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+
+    def window(self):
+        self.windows.append([time.perf_counter(), None])
+
+    def end(self):
+        if self.windows and self.windows[-1][1] is None:
+            self.windows[-1][1] = time.perf_counter()
 
     def stop(self):
-        if self.p is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
-        self.p.terminate()
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "not sampled"], "samples": 0}
+        self._stop = True
+        self.thread.join(timeout=5)
+        inside = [s for s in self.samples if any(w0 <= s[0] <= (w1 or s[0]) for w0, w1 in self.windows)]
+        use = inside or self.samples
+        sm = [float(s[1]) for s in use]
+        mask = 0
+        for s in use:
+            mask |= int(s[2])
+        reasons = sorted(n for n, attr in self.REASONS if mask & int(getattr(self.nv, attr, 0)))
         try:
-            self.p.wait(timeout=5)
+            mx = float(self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM))
         except Exception:
-            self.p.kill()
-        self.f.flush()
-        self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
-        os.unlink(self.f.name)
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+            mx = max(sm) if sm else None
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(use), "source": "NVML, every 2 ms, inside the timed loops"
+                if inside else "NVML, every 2 ms (no sample inside the timed loops)"}
 
 
 def dist_setup(n_gpus, backend="nccl"):
@@ -275,11 +317,13 @@ def _events_ms(fn, steps):
 
 def time_matmat(a, h, dev, peak, ms_bf16_matvec):
     """H X for 64 right-hand sides on the tensor cores (BF16 matmat layout):
-    3 launches per product (X gather, phase 1, phase 2)."""
+    3 launches per product (X gather, phase 1, phase 2).  Returns the report
+    and (X, Y[:, [0, 63]]) on the host for the oracle check."""
     import torch
 
     k = 64
-    X = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, (h.n_cols, k))).to(dev).t().contiguous().t()
+    X_host = np.random.default_rng(5).uniform(-1, 1, (h.n_cols, k))
+    X = torch.from_numpy(X_host).to(dev).t().contiguous().t()
     Y = torch.empty(k, h.n_rows, dtype=torch.float64, device=dev).t()
     for _ in range(a.warmup):
         h.matmat(X, "bf16", out=Y)
@@ -294,12 +338,15 @@ def time_matmat(a, h, dev, peak, ms_bf16_matvec):
     for phase in (1, 2):
         c = h.mm_plan_export(phase)["chunks"].astype(np.int64)
         block += int((c[:, 2] * c[:, 3] * 2).sum())
-    return {"workload": f"3DR0-H {a.mesh}x{a.mesh}, 64 right-hand sides ~U(-1,1) seed 5, BF16 blocks and X, "
-                        "FP32 accumulate (tcgen05, TMEM accumulators)",
-            "steps": steps, "ms_per_matmat": ms, "rhs_per_s": k / (ms * 1e-3),
-            "per_rhs_speedup_vs_bf16_matvec": ms_bf16_matvec * k / ms, "block_bytes": block,
-            "block_gbs": block / (ms * 1e-3) / 1e9, "roofline_frac_of_measured_hbm": block / (ms * 1e-3) / 1e9 / peak,
-            f"rel_err_vs_{ref}_gpu_columns_0_63": errs, "launches_per_matmat": 3}
+    cols = Y[:, [0, k - 1]].cpu().numpy()
+    return ({"workload": f"3DR0-H {a.mesh}x{a.mesh}, 64 right-hand sides ~U(-1,1) seed 5, BF16 blocks and X, "
+                         "FP32 accumulate (tcgen05, TMEM accumulators)",
+             "steps": steps, "ms_per_matmat": ms, "rhs_per_s": k / (ms * 1e-3),
+             "per_rhs_speedup_vs_bf16_matvec": ms_bf16_matvec * k / ms, "block_bytes": block,
+             "block_gbs": block / (ms * 1e-3) / 1e9,
+             "roofline_frac_of_measured_hbm": block / (ms * 1e-3) / 1e9 / peak,
+             f"rel_err_vs_{ref}_gpu_columns_0_63": errs, "launches_per_matmat": 3},
+            (X_host, cols))
 
 
 def time_batch(a, dev):
@@ -365,14 +412,15 @@ def time_batch(a, dev):
 
 def cpu_baseline(a, x_host, y_fp64):
     """The reference's own OpenMP CPU matvec (oracle/_ref) on the same
-    H-matrix definition and x, on this host's cores; bounded sample."""
+    H-matrix definition and x, on this host's cores; bounded sample.  Returns
+    (report, FP64 parity, the reference object for the checks that follow)."""
     try:
         from oracle import RefHmat, ref_available
     except Exception as e:
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}, None
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}, None, None
     if not ref_available():
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                "sample": "unavailable: oracle/_ref not built"}, None
+        return ({"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                 "sample": "unavailable: oracle/_ref not built"}, None, None)
     from bigwham_dev_b200.meshes import square_crack_3d
 
     threads = os.cpu_count() or 1
@@ -390,11 +438,79 @@ def cpu_baseline(a, x_host, y_fp64):
         R.matvec(x_host)
     dt = time.perf_counter() - t0
     parity = float(np.linalg.norm(y_fp64 - y_ref) / np.linalg.norm(y_ref)) if y_fp64 is not None else None
-    del R
     return ({"value": k / dt, "unit": UNIT, "cores": threads, "kind": "reference",
              "sample": f"{k} full BigWhamIO::MatVec calls on the same {3 * a.mesh * a.mesh:,}-DoF H-matrix "
                        f"(reference build {build_s:.1f} s, untimed), {threads} OpenMP threads, 1 BLAS thread"},
-            parity)
+            parity, R)
+
+
+def northstar_checks(a, h, R, x_host, mm_cols):
+    """Accuracy of the target configuration against the FP64 dense oracle of
+    the same kernel on a sampled row subset (683 collocation points = 2,049
+    rows, numpy default_rng(7); the reference's own influence() per entry),
+    outside every timed region:
+    * every storage precision's matvec on those rows;
+    * FP64 Jacobi GMRES(50) to 1e-8 and FP64-refined GMRES with FP32 / BF16
+      inner solves to 1e-8 for a uniform unit normal traction: iterations,
+      residuals, the solution's residual on the dense rows, its difference
+      from the FP64 solution, wall time;
+    * the 64-right-hand-side matmat's columns 0 and 63 against the
+      reference's own FP64 matvec of the same columns."""
+    import torch
+
+    from bigwham_dev_b200.solve import Gmres, refine
+
+    out = {"workload": "uniform unit normal traction; dense rows: 683 collocation points (2,049 rows) x all columns"}
+    npts = h.n_rows // 3
+    sample = np.sort(np.random.default_rng(7).choice(npts, size=min(683, npts), replace=False))
+    t0 = time.time()
+    D = R.dense_rows("3DR0-H", PROPS, sample)
+    out["dense_rows_s"] = round(time.time() - t0, 2)
+    rows = (3 * sample[:, None] + np.arange(3)[None, :]).ravel()
+
+    def rel(u, v):
+        return float(np.linalg.norm(u - v) / np.linalg.norm(v))
+
+    yd = D @ x_host
+    out["matvec_rel_err_vs_dense_rows"] = {p: rel(h.matvec(x_host, p)[rows], yd) for p in a.precisions}
+    if "fp64" not in a.precisions:
+        return out
+    dev = torch.device("cuda", torch.cuda.current_device())
+    b_np = np.zeros(h.n_rows)
+    b_np[2::3] = 1.0
+    b = torch.from_numpy(b_np).to(dev)
+    minv = torch.from_numpy(1.0 / h.diagonal()).to(dev)
+    ops = {p: (lambda x, y, p=p: h.matvec(x, p, out=y)) for p in a.precisions}
+    r = torch.empty_like(b)
+
+    def true_res(x):
+        ops["fp64"](x, r)
+        return float(torch.linalg.vector_norm(b - r) / torch.linalg.vector_norm(b))
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x64, info = Gmres(ops["fp64"], h.n_rows, restart=50, minv=minv).solve(b, tol=1e-8, maxiter=5000)
+    torch.cuda.synchronize()
+    X64 = x64.cpu().numpy()
+    out["fp64_gmres"] = {"converged": info.converged, "arnoldi_steps": info.iterations,
+                         "s": round(time.perf_counter() - t0, 3), "rel_residual": true_res(x64),
+                         "dense_row_residual": rel(D @ X64, b_np[rows])}
+    out["refined"] = {}
+    for p in (q for q in ("fp32", "bf16") if q in a.precisions):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xr, inf = refine(ops["fp64"], ops[p], b, h.n_rows, minv=minv, tol=1e-8, inner_tol=1e-3, restart=50)
+        torch.cuda.synchronize()
+        Xr = xr.cpu().numpy()
+        out["refined"][p] = {"converged": inf.converged, "outer_steps": inf.outer, "inner_arnoldi_steps": inf.iterations,
+                             "s": round(time.perf_counter() - t0, 3), "rel_residual": true_res(xr),
+                             "rel_err_vs_fp64_solution": rel(Xr, X64),
+                             "dense_row_residual": rel(D @ Xr, b_np[rows])}
+    if mm_cols is not None:
+        X, cols = mm_cols
+        out["matmat_columns_vs_reference_matvec"] = [rel(cols[:, q], R.matvec(np.ascontiguousarray(X[:, j])))
+                                                     for q, j in enumerate((0, X.shape[1] - 1))]
+    return out
 
 
 def run_ours(a):
@@ -416,7 +532,7 @@ def run_ours(a):
     res = {}
     clocks.start()
     # the headline precision first, then the others
-    for p in sorted(a.precisions, key=lambda q: q != "bf16"):
+    for p in sorted(a.precisions, key=lambda q: q != HEAD):
         y = ys[p]
         for _ in range(a.warmup):
             h.matvec(x, p, out=y)
@@ -425,11 +541,13 @@ def run_ours(a):
         torch.cuda.synchronize()
         h.set_timing(True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks.window()
         e0.record(stream)
         for _ in range(a.steps):
             h.matvec(x, p, out=y)
         e1.record(stream)
         torch.cuda.synchronize()
+        clocks.end()
         ms_total = e0.elapsed_time(e1)
         launch_ms, nrec = h.timing_read()
         h.set_timing(False)
@@ -442,69 +560,79 @@ def run_ours(a):
                   "launch_ms_per_step": [v / max(1, nrec) for v in launch_ms],
                   "stream_kernel_gbs": (b1 + b2) / (t_stream * 1e-3) / 1e9,
                   "matvec_gbs": h.algorithmic_bytes(p) / (ms_total / a.steps * 1e-3) / 1e9}
-    # end-to-end through the reference-facing call with host buffers, headline precision
+    # end to end through the reference-facing call with host buffers, every precision
     e2e_steps = max(1, min(a.steps, 200))
-    if io is not None:
-        io.set_precision("bf16")
+    y_e2e = {}
+    for p in sorted(a.precisions, key=lambda q: q != HEAD):
+        if io is not None:
+            io.set_precision(p)
+            call = lambda: io.matvec(x_host)  # noqa: E731  BigWhamIO::MatVec -> HmatGpu -> bw_matvec_host
+            path = "BigWhamIO::MatVec(host arrays) -> HmatGpu::matvecOriginal -> bw_matvec_host"
+        else:
+            call = lambda p=p: h.matvec(x_host, p)  # noqa: E731  bw_matvec_host
+            path = "bw_matvec_host (host arrays)"
         for _ in range(min(3, a.warmup)):
-            io.matvec(x_host)
+            call()
         torch.cuda.synchronize()
+        barrier(world)
+        clocks.window()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            y_e2e = io.matvec(x_host)  # BigWhamIO::MatVec -> HmatGpu -> bw_matvec_host
+            y_e2e[p] = call()
         dt = time.perf_counter() - t0
-        e2e_path = "BigWhamIO::MatVec(host arrays) -> HmatGpu::matvecOriginal -> bw_matvec_host"
-    else:
-        for _ in range(min(3, a.warmup)):
-            h.matvec(x_host, "bf16")
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            y_e2e = h.matvec(x_host, "bf16")  # bw_matvec_host
-        dt = time.perf_counter() - t0
-        e2e_path = "bw_matvec_host (host arrays)"
-    dt = max_over_ranks(dt, world)
+        clocks.end()
+        dt = max_over_ranks(dt, world)
+        res[p]["e2e"] = {"value": world * e2e_steps / dt, "unit": UNIT, "ms_per_call": 1e3 * dt / e2e_steps,
+                         "h2d_bytes_per_step": 8 * n_in, "d2h_bytes_per_step": 8 * n_out, "path": path,
+                         "timer": "host wall clock, synchronous calls"}
     clk = clocks.stop()
-    yref = ys["fp64" if "fp64" in ys else "bf16"].cpu().numpy()
+    yref = ys["fp64" if "fp64" in ys else HEAD].cpu().numpy()
     y64 = yref if "fp64" in ys else None
     errs = {p: float(np.linalg.norm(ys[p].cpu().numpy() - yref) / np.linalg.norm(yref)) for p in ys if p != "fp64"}
-    errs["e2e_bf16_vs_device_bf16"] = float(np.linalg.norm(y_e2e - ys["bf16"].cpu().numpy()) / np.linalg.norm(yref))
-    extra = {}
+    for p in y_e2e:
+        errs[f"e2e_{p}_vs_device_{p}"] = float(np.linalg.norm(y_e2e[p] - ys[p].cpu().numpy()) / np.linalg.norm(yref))
+    extra, mm_cols = {}, None
     if world == 1 and a.matmat:
-        extra["matmat_64rhs"] = time_matmat(a, h, dev, peak, res["bf16"]["ms_per_step"])
+        extra["matmat_64rhs"], mm_cols = time_matmat(a, h, dev, peak, res["bf16"]["ms_per_step"])
     if world == 1 and not a.no_batch:
         extra["batched_2ds0_48"] = time_batch(a, dev)
     if rank != 0:
         return 0
     cpu, parity = (None, None)
     if world == 1 and not a.no_cpu_baseline:
-        if io is not None:
-            io.close()
-        cpu, parity = cpu_baseline(a, x_host, y64)
-    head = res["bf16"]
+        cpu, parity, R = cpu_baseline(a, x_host, y64)
+        if R is not None and not a.no_checks:
+            extra["northstar_checks"] = northstar_checks(a, h, R, x_host, mm_cols)
+        del R
+    if io is not None:
+        io.close()
+    head = res[HEAD]
     b1, b2 = head["phase_bytes"]
     t_stream = head["launch_ms_per_step"][1] + head["launch_ms_per_step"][3]
     achieved = (b1 + b2) / (t_stream * 1e-3) / 1e9
+    tkey = {"fp64": "stream_panels_fp64", "fp32": "stream_panels_fp32", "bf16": "stream_panels_bf16"}[HEAD]
+    kname = {"fp64": "double", "fp32": "float", "bf16": "Bf16"}[HEAD]
     out = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16", "data": "synthetic mesh (generated; no dataset), x ~ U(-1,1) seed 1",
-        "config": {**workload(a.mesh), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   **setup},
+        "vs_baseline": None, "dtype": {"fp64": "f64", "fp32": "f32", "bf16": "bf16"}[HEAD],
+        "data": "synthetic mesh (generated; no dataset), x ~ U(-1,1) seed 1",
+        "config": workload(a.mesh),
+        "setup": {"parallelism": f"replicas x{world}" if world > 1 else "single GPU", **setup},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6650 GB/s",
-                     "kernel": "stream_panels_kernel<Bf16> (phase 1 + phase 2 launches of one step)",
-                     "bytes_per_step": b1 + b2, "traffic": read_traffic("stream_panels_bf16")},
+                     "kernel": f"stream_panels_kernel<{kname}> (phase 1 + phase 2 launches of one step)",
+                     "bytes_per_step": b1 + b2, "traffic": read_traffic(tkey)},
         "cpu_baseline": cpu,
-        "e2e": {"value": world * e2e_steps / dt, "unit": UNIT, "h2d_bytes_per_step": 8 * n_in,
-                "d2h_bytes_per_step": 8 * n_out, "path": e2e_path, "timer": "host wall clock, synchronous calls"},
+        "e2e": {k: v for k, v in head["e2e"].items() if k != "ms_per_call"},
         "gpu_launches": 4 * a.steps,
         "launches_per_step": ["gather_x_kernel", "stream_panels_kernel (phase 1)", "gather_g2_kernel",
                               "stream_panels_kernel (phase 2)"],
         "clocks": clk,
         "precisions": {p: {k: v for k, v in res[p].items()} for p in res},
-        "speedup_vs_fp64": res["bf16"]["value"] / res["fp64"]["value"] if "fp64" in res else None,
         "speedup_fp32_vs_fp64": res["fp32"]["value"] / res["fp64"]["value"] if {"fp32", "fp64"} <= set(res) else None,
+        "speedup_bf16_vs_fp64": res["bf16"]["value"] / res["fp64"]["value"] if {"bf16", "fp64"} <= set(res) else None,
         "rel_err_vs_fp64_gpu": errs,
         "fp64_gpu_vs_reference_rel_err": parity,
         **extra,
@@ -526,21 +654,24 @@ def main(argv=None):
     ap.add_argument("--mesh", type=int, default=256, help="rectangles per side (256 -> 196,608 DoF)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precisions", default="fp64,fp32,bf16",
-                    help="storage precisions to upload and time (comma list; must include bf16, the headline)")
+                    help="storage precisions to upload and time (comma list; must include fp32, the headline, "
+                         "and bf16)")
     ap.add_argument("--no-matmat", dest="matmat", action="store_false",
                     help="skip the 64-right-hand-side tensor-core matmat line (N = 1 only)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 48 x 2DS0 batched line (N = 1 only)")
     ap.add_argument("--block-file", default=None,
                     help="block file of the H-matrix: read it when it exists (no host rebuild), else write it "
                          "after the build")
+    ap.add_argument("--no-checks", action="store_true",
+                    help="skip the accuracy checks against the dense rows (refined GMRES, N = 1 only)")
     ap.add_argument("--cpu-budget-s", type=float, default=10.0)
     ap.add_argument("--ref-budget-s", type=float, default=60.0)
     a = ap.parse_args(argv)
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")
     a.precisions = [p for p in a.precisions.split(",") if p]
-    if "bf16" not in a.precisions or not set(a.precisions) <= {"fp64", "fp32", "bf16"}:
-        ap.error("--precisions must be a subset of fp64,fp32,bf16 that includes bf16")
+    if not {HEAD, "bf16"} <= set(a.precisions) or not set(a.precisions) <= {"fp64", "fp32", "bf16"}:
+        ap.error("--precisions must be a subset of fp64,fp32,bf16 that includes fp32 and bf16")
     if a.impl == "reference":
         return run_reference(a)
     return run_ours(a)

@@ -397,6 +397,14 @@ except Exception:  # pragma: no cover - scipy is part of the image
     _LinOp = object
 
 
+def pattern_kind_index(pat):
+    """Index of every block of a pattern (rows as _getPattern returns them,
+    column 4 the kind: 0 full rank, 1 low rank) among the blocks of its kind,
+    in pattern order: the labels of plotPattern(plot_index=True)."""
+    low = np.asarray(pat)[:, 4] == 1
+    return np.where(low, np.cumsum(low) - 1, np.cumsum(~low) - 1).astype(np.int64)
+
+
 def _csc_entries(val, row, col, shape, keep_ratio: float):
     """CSC matrix of the entries; keep_ratio < 1 keeps the largest |entries|
     (that share of them, ties kept), as the reference's _getFullBlocks."""
@@ -589,7 +597,9 @@ class BEMatrix(_LinOp):
         return (time.time() - t0) / N_matvec
 
     def plotPattern(self, plot_index=False):
-        """The block pattern as a matplotlib figure (needs matplotlib)."""
+        """The block pattern as a matplotlib figure (needs matplotlib).
+        plot_index: write each block's index among the blocks of its kind
+        (full-rank or low-rank, in pattern order) at its centre."""
         import matplotlib.pyplot as plt
         from matplotlib.collections import PatchCollection
         from matplotlib.patches import Rectangle
@@ -598,6 +608,10 @@ class BEMatrix(_LinOp):
         max_y = pat[:, 3].max()
         fig, ax = plt.subplots()
         patches = [Rectangle((r[1], max_y - r[0] - abs(r[0] - r[2])), abs(r[1] - r[3]), abs(r[0] - r[2])) for r in pat]
+        if plot_index:
+            for r, k in zip(patches, pattern_kind_index(pat)):
+                ax.text(r.get_x() + r.get_width() / 2, r.get_y() + r.get_height() / 2, str(int(k)), ha="center",
+                        va="center", fontsize=8, fontweight="bold", color="black")
         pc = PatchCollection(patches, edgecolors="black", alpha=0.4)
         pc.set_array(pat[:, 4])
         ax.add_collection(pc)

@@ -49,13 +49,25 @@ def build_cuda(force: bool = False, verbose: bool = False) -> str:
     return out
 
 
+def reference_tree() -> str | None:
+    """The BigWham source tree the host adapter and the oracle compile from:
+    $BIGWHAM_REF when set, else a ``reference`` directory beside the
+    repository; None when neither holds the reference sources."""
+    cands = [os.environ["BIGWHAM_REF"]] if os.environ.get("BIGWHAM_REF") else []
+    cands.append(os.path.join(os.path.dirname(ROOT), "reference"))
+    for c in cands:
+        if os.path.isdir(os.path.join(c, "src", "hmat")):
+            return os.path.abspath(c)
+    return None
+
+
 def build_host(force: bool = False) -> str | None:
     """Builds the host adapter when the reference tree is present; returns the
     library path (None when the reference tree is absent and no prebuilt
     library exists)."""
     out = os.path.join(LIBDIR, "libbigwham_host.so")
-    ref = os.environ.get("BIGWHAM_REF", "/root/reference")
-    if not os.path.isdir(os.path.join(ref, "src", "hmat")):
+    ref = reference_tree()
+    if ref is None:
         return out if os.path.exists(out) else None
     args = ["make", "-C", os.path.join(HERE, "host"), f"REF={ref}", "-j", str(os.cpu_count() or 8)]
     if force:

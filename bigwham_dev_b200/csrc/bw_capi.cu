@@ -239,14 +239,23 @@ template <typename F> int guarded(bw_hmat *h, F &&f) {
   }
 }
 
+// Dynamic shared-memory opt-in of a kernel, set once per device.  The flags
+// are guarded by one mutex: first calls from several host threads (one per
+// device, or several handles on one device) do not race on them.
+std::mutex g_attr_mu;
+
+template <typename K> void smem_attr_once(bool (&done)[64], K kernel, int bytes) {
+  int dev = 0;
+  BW_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(g_attr_mu);
+  if (dev < 64 && done[dev]) return;
+  BW_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  if (dev < 64) done[dev] = true;
+}
+
 template <typename S> void set_smem_attr() {
   static bool done[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && done[dev]) return;
-  BW_CUDA(cudaFuncSetAttribute(bw::stream_panels_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               bw::SmemLayout<S>::kTotal));
-  if (dev < 64) done[dev] = true;
+  smem_attr_once(done, bw::stream_panels_kernel<S>, bw::SmemLayout<S>::kTotal);
 }
 
 int64_t align256(int64_t v) { return (v + 255) / 256 * 256; }
@@ -636,12 +645,7 @@ int64_t mm_xt_rows(const bw_hmat *h) { return (std::max(h->n_rows, h->n_cols) + 
 void launch_matmat_tc(bw_hmat *h, int o, const double *X, int64_t ldx, double *Y, int64_t ldy, int nrhs, bool permuted,
                       cudaStream_t st) {
   static bool attr_done[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 64 || !attr_done[dev]) {
-    BW_CUDA(cudaFuncSetAttribute(bw::mm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bw::kMmSmem));
-    if (dev < 64) attr_done[dev] = true;
-  }
+  smem_attr_once(attr_done, bw::mm_stream_kernel, bw::kMmSmem);
   const bw::MmPlan &mm = h->mm[o];
   const int32_t *perm_in = permuted ? nullptr : (o == 0 ? h->d_perm1 : h->d_perm0);
   const int32_t *perm_out = permuted ? nullptr : (o == 0 ? h->d_perm0 : h->d_perm1);
@@ -735,6 +739,14 @@ int bw_set_tuning(bw_hmat *h, const char *key, int64_t value) {
       t.mm_items_per_cta = (int)value;
     else
       t.items_per_cta[k.back() - '1'] = (int)value;
+    return BW_OK;
+  }
+  if (k == "unit_bytes") {
+    if (value < 0 || value > (int64_t(1) << 30)) {
+      h->err = "unit_bytes must be in [0, 2^30]";
+      return BW_ERR_ARG;
+    }
+    t.unit_bytes = (int)value;
     return BW_OK;
   }
   if (k == "chunk_bytes") {

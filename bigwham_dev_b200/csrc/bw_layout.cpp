@@ -454,12 +454,22 @@ void build_chunks(const Problem &p, bool tr, int prec, int grid, OperatorPlan &o
     std::vector<int64_t> order(n);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+    // Queue units: runs of consecutive items, closed once their cost
+    // reaches unit_bytes (a large item is a unit by itself).  The kernel
+    // walks a unit's chunks as one range; item boundaries stay in the chunk
+    // flags, so results do not depend on the grouping.
     cp.chunks.clear();
     cp.item_ptr.assign(1, 0);
-    for (int64_t q : order) {
+    int64_t unit_cost = 0;
+    for (size_t k = 0; k < order.size(); k++) {
+      const int64_t q = order[k];
       cp.chunks.insert(cp.chunks.end(), per_item[q].begin(), per_item[q].end());
       if (cp.chunks.size() > (size_t)INT32_MAX) fail("too many chunks");
-      cp.item_ptr.push_back(i32((int64_t)cp.chunks.size(), "chunk count"));
+      unit_cost += cost[q];
+      if (unit_cost >= p.tune.unit_bytes || k + 1 == order.size()) {
+        cp.item_ptr.push_back(i32((int64_t)cp.chunks.size(), "chunk count"));
+        unit_cost = 0;
+      }
     }
   }
 }

@@ -112,11 +112,12 @@ struct Item {
 };
 
 // Per precision: the chunks item by item, items in the order the CTAs take
-// them (decreasing cost), the items' chunk ranges, and (phase 2) the runs that
-// fill the gather array G2 of g_len values.
+// them (decreasing cost), the chunk ranges of the queue units (runs of
+// consecutive items, Tuning::unit_bytes), and (phase 2) the runs that fill
+// the gather array G2 of g_len values.
 struct ChunkPlan {
   std::vector<Chunk> chunks;
-  std::vector<int32_t> item_ptr;  // items + 1
+  std::vector<int32_t> item_ptr;  // queue units + 1 (chunk index of each unit's first chunk)
   std::vector<GatherSeg> gsegs;   // phase 2 only
   int64_t g_len = 0;
 };
@@ -139,12 +140,19 @@ struct OperatorPlan {
   int64_t n_stacks = 0;
 };
 
+// Queue units: consecutive items (in the queue's longest-first order) are
+// handed out together until the unit's cost reaches this many bytes, so a
+// CTA makes one queue round trip (atomic + chunk-range loads) per unit
+// rather than per item when items are small.  0: one item per unit.
+constexpr int kUnitBytes = 65536;
+
 // Plan parameters a tuner may change (bw_set_tuning); the defaults are the
 // compiled-in choices.
 struct Tuning {
   int items_per_cta[2] = {kItemsPerCta, kItemsPerCta};  // per phase: items per CTA share (granularity)
   int chunk_bytes = kStageBytes;                        // block data per chunk (<= kStageBytes)
   int mm_items_per_cta = kItemsPerCta;                  // matmat phase 1
+  int unit_bytes = kUnitBytes;                          // streaming queue: minimum cost of a unit
 };
 
 struct Problem {

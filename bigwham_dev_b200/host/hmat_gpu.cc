@@ -218,6 +218,14 @@ il::Array<double> HmatGpu::matvecOriginal(il::ArrayView<double> x) {
   return y;
 }
 
+void HmatGpu::matvecInto(const double *x, double *y) {
+  check(bw_matvec_host(h_, x, y, precision_ | BW_PERMUTED), "bw_matvec_host");
+}
+
+void HmatGpu::matvecOriginalInto(const double *x, double *y) {
+  check(bw_matvec_host(h_, x, y, precision_), "bw_matvec_host");
+}
+
 std::vector<double> HmatGpu::diagonal() {
   std::vector<double> d((size_t)std::max(size_[0], size_[1]));
   check(bw_diagonal(h_, d.data(), BW_PERMUTED), "bw_diagonal");

@@ -50,6 +50,9 @@ class HmatGpu : public bigwham::Hmat<double> {
   // Host arrays (BigWhamIO::MatVec(ArrayView), MatVecPerm, MatVecVoid).
   il::Array<double> matvec(il::ArrayView<double> x) override;
   il::Array<double> matvecOriginal(il::ArrayView<double> x) override;
+  // The same products into a caller's host array y of size(0) values.
+  void matvecInto(const double *x, double *y);
+  void matvecOriginalInto(const double *x, double *y);
 
   std::vector<double> diagonal() override;
   std::vector<double> diagonalOriginal() override;

@@ -130,14 +130,16 @@ int bwh_set_precision(bwh_io *h, int p) {
 }
 
 // The matvec entries require the GPU H-matrix: this library never applies the
-// reference's CPU matvec.
+// reference's CPU matvec.  BigWhamIO::MatVec / MatVecPerm return a new
+// il::Array (bigwham_io.cc:927-933, 965-971) that a binding then copies into
+// the caller's array; with the GPU H-matrix installed those two calls reduce
+// to HmatGpu's host-array product, which writes the caller's y directly (no
+// intermediate array, no second copy).
 int bwh_matvec(bwh_io *h, const double *x, double *y) {
   if (!h || !x || !y) return fail("null argument");
   if (!h->gpu) return fail("no GPU H-matrix attached (bwh_attach_gpu)");
   return guarded([&] {
-    const il::int_t n = h->io->MatrixSize(1);
-    il::Array<double> out = h->io->MatVec(il::ArrayView<double>{x, n});
-    std::memcpy(y, out.data(), sizeof(double) * out.size());
+    h->gpu->matvecOriginalInto(x, y);
     return 0;
   });
 }
@@ -146,9 +148,7 @@ int bwh_matvec_perm(bwh_io *h, const double *x, double *y) {
   if (!h || !x || !y) return fail("null argument");
   if (!h->gpu) return fail("no GPU H-matrix attached (bwh_attach_gpu)");
   return guarded([&] {
-    const il::int_t n = h->io->MatrixSize(1);
-    il::Array<double> out = h->io->MatVecPerm(il::ArrayView<double>{x, n});
-    std::memcpy(y, out.data(), sizeof(double) * out.size());
+    h->gpu->matvecInto(x, y);
     return 0;
   });
 }

@@ -15,6 +15,12 @@ Here the whole loop stays on the device:
   update use the FP64 H-matrix; the correction equation A d = r is solved by
   ``gmres`` with the FP32 or BF16 H-matrix (mixed precision), to a loose
   inner tolerance.
+* ``MultiGmres`` / ``refine_multi``: k systems at once, each with its own
+  Krylov space and stopping test, sharing one operator call per Arnoldi step:
+  the 64-right-hand-side tensor-core matmat (one H-matrix, k right-hand
+  sides), or one batched H-matrix (k independent H-matrices of uneven size,
+  vectors padded to a common length; ``BatchOperator``).  Each restart cycle
+  is one replayed CUDA graph, as in ``Gmres``.
 """
 from __future__ import annotations
 
@@ -178,3 +184,189 @@ def refine(op_hi, op_lo, b, n: int, minv=None, tol: float = 1e-8, inner_tol: flo
         info.cycles += inf.cycles
         x.add_(d)
     return x, info
+
+
+class MultiGmres:
+    """Restarted GMRES(m) for k systems op(X) = B at once.
+
+    Vectors are (k, n) CUDA float64 tensors, one system per row (row-major,
+    i.e. the column-major n x k layout of a matmat).  op(Z, W) writes the k
+    operator applications of Z's rows into W's rows, stream-ordered on the
+    current torch stream.  Every system keeps its own Arnoldi basis, FP64
+    Hessenberg matrix (classical Gram-Schmidt, two passes) and stopping test;
+    a system whose residual is zero contributes zero vectors.  minv: optional
+    right preconditioner, a (k, n) or (n,) tensor applied elementwise.
+    """
+
+    def __init__(self, op, k: int, n: int, restart: int = 50, minv=None, device="cuda", use_graph: bool = True):
+        import torch
+
+        self.torch = torch
+        self.op, self.k, self.n, self.m = op, int(k), int(n), int(restart)
+        self.minv = minv
+        dt = torch.float64
+        self.V = torch.zeros(self.m + 1, self.k, self.n, dtype=dt, device=device)
+        self.H = torch.zeros(self.k, self.m + 1, self.m, dtype=dt, device=device)
+        self.Z = torch.zeros(self.k, self.n, dtype=dt, device=device)
+        self.W = torch.zeros(self.k, self.n, dtype=dt, device=device)
+        self.use_graph = use_graph
+        self.graph = None
+
+    def _precondition(self, v, out):
+        if self.minv is None:
+            out.copy_(v)
+        else:
+            self.torch.mul(v, self.minv, out=out)
+
+    def _cycle(self):
+        torch = self.torch
+        V, H, Z, W = self.V, self.H, self.Z, self.W
+        for j in range(self.m):
+            self._precondition(V[j], Z)
+            self.op(Z, W)
+            Vj = V[:j + 1].transpose(0, 1)                  # (k, j+1, n)
+            h = torch.bmm(Vj, W.unsqueeze(2))               # (k, j+1, 1)
+            W.sub_(torch.bmm(Vj.transpose(1, 2), h).squeeze(2))
+            h2 = torch.bmm(Vj, W.unsqueeze(2))
+            W.sub_(torch.bmm(Vj.transpose(1, 2), h2).squeeze(2))
+            H[:, :j + 1, j] = (h + h2).squeeze(2)
+            nrm = torch.linalg.vector_norm(W, dim=1)        # (k,)
+            H[:, j + 1, j] = nrm
+            # a system with nothing left to reduce continues with zero vectors
+            safe = torch.where(nrm > 0, nrm, torch.ones_like(nrm))
+            torch.div(W, safe.unsqueeze(1), out=V[j + 1])
+
+    def _run_cycle(self):
+        torch = self.torch
+        if not self.use_graph:
+            self._cycle()
+            return
+        if self.graph is None:
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                self._cycle()
+            torch.cuda.current_stream().wait_stream(s)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._cycle()
+            self.graph = g
+        self.graph.replay()
+
+    def solve(self, B, tol: float = 1e-8, maxiter: int = 2000):
+        """Solve op(X) = B row by row to ||b_i - op(x_i)|| <= tol ||b_i||.
+        Returns (X, info) with info.converged true when every system met the
+        tolerance, and info.per_system the SolveInfo of each system."""
+        torch = self.torch
+        k = self.k
+        X = torch.zeros_like(B)
+        R = torch.empty_like(B)
+        bn = torch.linalg.vector_norm(B, dim=1).cpu().numpy()
+        infos = [SolveInfo() for _ in range(k)]
+        done = bn == 0.0
+        for i in np.nonzero(done)[0]:
+            infos[i].converged = True
+        total = SolveInfo()
+        while not done.all() and total.iterations < maxiter:
+            if total.iterations == 0:
+                R.copy_(B)
+            else:
+                self.op(X, R)
+                torch.sub(B, R, out=R)
+            beta = torch.linalg.vector_norm(R, dim=1).cpu().numpy()
+            for i in range(k):
+                if not done[i]:
+                    infos[i].residuals.append(beta[i] / bn[i])
+                    if beta[i] <= tol * bn[i]:
+                        done[i], infos[i].converged = True, True
+            if done.all():
+                break
+            scale = torch.from_numpy(np.where(done | (beta == 0.0), 0.0, 1.0 / np.where(beta == 0.0, 1.0, beta)))
+            torch.mul(R, scale.to(R.device).unsqueeze(1), out=self.V[0])
+            self._run_cycle()
+            total.cycles += 1
+            total.iterations += self.m
+            Hh = self.H.cpu().numpy()
+            Y = np.zeros((k, self.m))
+            for i in range(k):
+                if done[i]:
+                    continue
+                kk, y, res = _lstsq_prefix(Hh[i], float(beta[i]), tol * bn[i])
+                Y[i, :kk] = y
+                infos[i].iterations += self.m
+                infos[i].cycles += 1
+            upd = torch.einsum("jkn,kj->kn", self.V[:self.m], torch.from_numpy(Y).to(B.device))
+            self._precondition(upd, self.Z)
+            X.add_(self.Z)
+        total.converged = bool(done.all())
+        total.per_system = infos
+        return X, total
+
+
+class BatchOperator:
+    """The block-diagonal operator of a batched handle (HmatGpu.batch) on the
+    padded (count, L) layout of MultiGmres: member k's vector is row k,
+    entries beyond its length are zero and stay zero."""
+
+    def __init__(self, hb, precision: str = "fp64", device="cuda"):
+        import torch
+
+        self.hb, self.precision = hb, precision
+        ro, co = np.asarray(hb.row_offsets), np.asarray(hb.col_offsets)
+        if not np.array_equal(ro, co):
+            raise ValueError("BatchOperator needs square members")
+        self.count = len(ro) - 1
+        sizes = np.diff(ro)
+        self.L = int(sizes.max()) if self.count else 0
+        idx = np.concatenate([k * self.L + np.arange(sizes[k]) for k in range(self.count)]).astype(np.int64)
+        self.idx = torch.from_numpy(idx).to(device)
+        self.x = torch.zeros(int(ro[-1]), dtype=torch.float64, device=device)
+        self.y = torch.zeros(int(ro[-1]), dtype=torch.float64, device=device)
+
+    def pad(self, v):
+        """(count, L) padded form of a concatenated vector."""
+        import torch
+
+        out = torch.zeros(self.count, self.L, dtype=torch.float64, device=v.device)
+        out.view(-1).index_copy_(0, self.idx, v)
+        return out
+
+    def unpad(self, V):
+        return V.reshape(-1).index_select(0, self.idx)
+
+    def __call__(self, Z, W):
+        import torch
+
+        torch.index_select(Z.reshape(-1), 0, self.idx, out=self.x)
+        self.hb.matvec(self.x, self.precision, out=self.y)
+        W.view(-1).index_copy_(0, self.idx, self.y)
+
+
+def refine_multi(op_hi, op_lo, B, minv=None, tol: float = 1e-8, inner_tol: float = 1e-3, restart: int = 50,
+                 max_outer: int = 50, use_graph: bool = True):
+    """Mixed-precision iterative refinement of k systems (rows of B):
+    X += MultiGmres_lo(A D = B - A_hi X), until every row's relative residual
+    is <= tol.  op_hi, op_lo: (Z, W) operators on (k, n) tensors."""
+    import torch
+
+    k, n = B.shape
+    info = SolveInfo()
+    inner = MultiGmres(op_lo, k, n, restart, minv, device=B.device, use_graph=use_graph)
+    X = torch.zeros_like(B)
+    R = torch.empty_like(B)
+    bn = torch.linalg.vector_norm(B, dim=1)
+    bn = torch.where(bn > 0, bn, torch.ones_like(bn))
+    for it in range(max_outer):
+        op_hi(X, R)
+        torch.sub(B, R, out=R)
+        rel = float((torch.linalg.vector_norm(R, dim=1) / bn).max())
+        info.residuals.append(rel)
+        info.outer = it
+        if rel <= tol:
+            info.converged = True
+            break
+        D, inf = inner.solve(R, tol=inner_tol, maxiter=20 * restart)
+        info.iterations += inf.iterations
+        info.cycles += inf.cycles
+        X.add_(D)
+    return X, info

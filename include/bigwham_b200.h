@@ -109,7 +109,10 @@ int bw_test_withhold_chunk(bw_hmat *h, int index);
  *       (granularity of the work queue), 1..256, default 8;
  *   "chunk_bytes": block data per chunk, 4096..32768, multiple of 16,
  *       default 32768;
- *   "mm_items_per_cta": granularity of the matmat's phase 1, default 8.
+ *   "mm_items_per_cta": granularity of the matmat's phase 1, default 8;
+ *   "unit_bytes": the streaming queue hands out runs of consecutive items
+ *       until a run's cost reaches this many bytes (0: one item at a time),
+ *       0..2^30, default 65536.
  * Results do not depend on them (each item is reduced in a fixed order).
  * BW_ERR_ARG for an unknown key or a value out of range. */
 int bw_set_tuning(bw_hmat *h, const char *key, int64_t value);
@@ -160,7 +163,7 @@ int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream);
 /* Bytes of device memory reserved by bw_matvec_static_scratch (per device). */
 #define BW_STATIC_SCRATCH_BYTES (64u << 20)
 
-/* y = H x like bw_matvec, but without any device allocation, ever: for callers
+/* y = H x like bw_matvec, but the call allocates no device memory: for callers
  * that cannot let a library call cudaMalloc -- a process whose device memory
  * belongs to another allocator (a framework's caching pool, a solver that
  * reserved the card up front), or a latency-critical path where cudaMalloc /
@@ -173,8 +176,13 @@ int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream);
  * panel (the phase-2 gather array).  For the 3DR0-H square crack that is
  * 14 MB (FP64) or 7 MB (FP32, BF16) at 12,288 DoF and 40 MB or 20 MB at
  * 49,152 DoF; the 196,608-DoF matrix needs more and is rejected.
- * The first call on a device looks the array's address up (once per device);
- * make that first call before any stream capture.  Every call overwrites the
+ * The first call on a device looks the array's address up (once per device).
+ * With lazy module loading (the CUDA default) that first lookup can also load
+ * the library's device code, which reserves the array and may synchronize the
+ * device: make the first call on each device outside latency-critical code and
+ * before any stream capture.  The address is kept for the life of the process;
+ * after cudaDeviceReset on a device, do not call this entry point on it again.
+ * Every call overwrites the
  * scratch before reading it, so nothing in it needs to start at zero, and the
  * array keeps the last call's contents.  All calls on a device share the one
  * array: calls whose kernels overlap on the GPU (several streams or several

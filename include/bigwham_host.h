@@ -59,9 +59,11 @@ int bwh_set_precision(bwh_io *io, int precision);
  * unknown key or a bad value makes bwh_attach_gpu fail). */
 int bwh_set_tuning(bwh_io *io, const char *key, int64_t value);
 
-/* BigWhamIO::MatVec(il::ArrayView) -- host arrays, original ordering. */
+/* BigWhamIO::MatVec(il::ArrayView) -- host arrays, original ordering.  The
+ * product is written straight into y (n_rows values); the reference returns a
+ * new il::Array that its bindings copy into the caller's array. */
 int bwh_matvec(bwh_io *io, const double *x, double *y);
-/* BigWhamIO::MatVecPerm -- host arrays, permuted ordering. */
+/* BigWhamIO::MatVecPerm -- host arrays, permuted ordering, written into y. */
 int bwh_matvec_perm(bwh_io *io, const double *x, double *y);
 /* BigWhamIO::MatVec(double*, double*) -- device pointers (matvec_raw_ptr). */
 int bwh_matvec_raw_ptr(bwh_io *io, double *x, double *y);

@@ -26,6 +26,8 @@ import pytest
 
 from planreplay import replay
 
+from bigwham_dev_b200.build import reference_tree
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HOST_LIB = os.path.join(ROOT, "bigwham_dev_b200", "_lib", "libbigwham_host.so")
 needs_host = pytest.mark.skipif(not os.path.exists(HOST_LIB), reason="host adapter not built")
@@ -53,7 +55,7 @@ def crack(tmp_path_factory):
     return ex, str(path), nblk
 
 
-REF = os.environ.get("BIGWHAM_REF", "/root/reference")
+REF = reference_tree() or ""
 
 
 @needs_host

@@ -122,7 +122,14 @@ def test_bematrix_reference_methods_without_gpu():
     P = A.H_ILU_prec(fill_factor=100, drop_tol=0.0)
     v = np.random.default_rng(3).uniform(-1, 1, n)
     assert np.linalg.norm(fb @ (P @ v) - v) / np.linalg.norm(v) < 1e-10
-    assert A._getPattern().shape[1] == 6
+    pat = A._getPattern()
+    assert pat.shape[1] == 6
+    # plotPattern(plot_index=True) labels: each block's index among its kind, in pattern order
+    from bigwham_dev_b200.bigwham4py import pattern_kind_index
+
+    idx = pattern_kind_index(pat)
+    for kind in (0, 1):
+        assert np.array_equal(idx[pat[:, 4] == kind], np.arange(int((pat[:, 4] == kind).sum())))
     x = np.random.default_rng(4).uniform(-1, 1, n)
     assert np.allclose(A.convert_to_global(A.convert_to_local(x)), x)
     pts = np.array([[0.0, 0.5], [3.0, -1.0]])

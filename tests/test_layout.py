@@ -87,13 +87,50 @@ def test_items_longest_first():
             h.add_full(i * bs, j * bs, blocks[i, j])
     h.finalize(plan_only=True)
     p = h.plan_export("fp64", 2)
-    items = p["item_ptr"]
-    cost = [sum(decode(w)["ncols"] * decode(w)["hpad"] * 8 + 1024 for w in p["chunks"][items[b]:items[b + 1]])
-            for b in range(len(items) - 1)]
-    assert all(a >= b for a, b in zip(cost, cost[1:]))
+    # items (FIRST .. LAST chunk runs) come in non-increasing cost order
+    cost, cur = [], 0
+    for w in p["chunks"]:
+        d = decode(w)
+        cur += d["ncols"] * d["hpad"] * 8 + 1024
+        if d["flags"] & 2:
+            cost.append(cur)
+            cur = 0
+    assert len(cost) == nb and all(a >= b for a, b in zip(cost, cost[1:]))
+    # every item here costs more than the default unit (64 KB): one item per unit
+    assert len(p["item_ptr"]) == nb + 1
     D = np.block([[blocks[i, j] for j in range(nb)] for i in range(nb)])
     x = rng.standard_normal(n)
     assert rel(replay(h, x), D @ x) < 1e-14
+
+
+def test_queue_units_group_small_items():
+    """The queue hands out runs of whole items, each costing at least
+    unit_bytes (but the last); the plan's product does not change."""
+    dof, nb, bs = 1, 20, 24
+    n = nb * bs
+    rng = np.random.default_rng(1)
+    blocks = {(i, j): rng.standard_normal((bs, bs)) for i in range(nb) for j in range(nb)}
+    x = rng.standard_normal(n)
+    outs = []
+    for unit in (0, 65536, 300000):
+        h = HmatGpu(dof, n, n, np.arange(n), np.arange(n), device=-1).set_tuning(unit_bytes=unit)
+        for (i, j), b in blocks.items():
+            h.add_full(i * bs, j * bs, b)
+        h.finalize(plan_only=True)
+        p = h.plan_export("fp64", 2)
+        units = p["item_ptr"]
+        ucost = [sum(decode(w)["ncols"] * decode(w)["hpad"] * 8 + 1024 for w in p["chunks"][units[b]:units[b + 1]])
+                 for b in range(len(units) - 1)]
+        assert all(c >= unit for c in ucost[:-1])
+        assert decode(p["chunks"][units[0]])["flags"] & 1 and all(
+            decode(p["chunks"][u - 1])["flags"] & 2 for u in units[1:])
+        n_items = sum(1 for w in p["chunks"] if decode(w)["flags"] & 2)
+        if unit == 0:
+            assert len(units) - 1 == n_items
+        if unit == 300000:
+            assert len(units) - 1 < n_items / 2
+        outs.append(replay(h, x))
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
 
 
 def _simple(n=8):

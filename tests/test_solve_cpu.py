@@ -38,3 +38,79 @@ def test_zero_rhs():
     g = Gmres(lambda x, y: y.copy_(A @ x), 50, restart=5, device="cpu", use_graph=False)
     x, info = g.solve(torch.zeros(50, dtype=torch.float64))
     assert info.converged and float(x.abs().max()) == 0.0
+
+
+def _systems(k=5, n=120, seed=3):
+    rng = np.random.default_rng(seed)
+    As = [np.eye(n) * (3 + i) + rng.standard_normal((n, n)) / np.sqrt(n) for i in range(k)]
+    return torch.from_numpy(np.stack(As)), torch.from_numpy(rng.standard_normal((k, n)))
+
+
+def test_multi_gmres_solves_each_system_with_its_own_krylov_space():
+    from bigwham_dev_b200.solve import MultiGmres
+
+    A, B = _systems()
+    B[2] = 0.0  # a zero right-hand side: converged from the start, stays zero
+    op = lambda Z, W: W.copy_(torch.bmm(A, Z.unsqueeze(2)).squeeze(2))  # noqa: E731
+    minv = 1.0 / torch.diagonal(A, dim1=1, dim2=2)
+    X, info = MultiGmres(op, A.shape[0], A.shape[1], restart=8, minv=minv, device="cpu",
+                         use_graph=False).solve(B, tol=1e-11, maxiter=800)
+    assert info.converged and all(s.converged for s in info.per_system)
+    for i in range(A.shape[0]):
+        xt = torch.linalg.solve(A[i], B[i])
+        assert float(torch.linalg.vector_norm(X[i] - xt)) <= 1e-9 * max(1.0, float(torch.linalg.vector_norm(xt)))
+    assert float(X[2].abs().max()) == 0.0
+    # the same systems one at a time: the same Krylov spaces, the same answer
+    for i in (0, 4):
+        g = Gmres(lambda x, y, i=i: y.copy_(A[i] @ x), A.shape[1], restart=8, minv=minv[i], device="cpu",
+                  use_graph=False)
+        x1, _ = g.solve(B[i], tol=1e-11, maxiter=800)
+        assert float(torch.linalg.vector_norm(x1 - X[i])) <= 1e-9 * float(torch.linalg.vector_norm(x1))
+
+
+def test_refine_multi_recovers_high_precision():
+    from bigwham_dev_b200.solve import refine_multi
+
+    A, B = _systems(k=4, seed=5)
+    E = torch.from_numpy(np.random.default_rng(6).standard_normal(A.shape)) * 1e-3 / np.sqrt(A.shape[1])
+    op_hi = lambda Z, W: W.copy_(torch.bmm(A, Z.unsqueeze(2)).squeeze(2))  # noqa: E731
+    op_lo = lambda Z, W: W.copy_(torch.bmm(A + E, Z.unsqueeze(2)).squeeze(2))  # noqa: E731
+    X, info = refine_multi(op_hi, op_lo, B, tol=1e-12, inner_tol=1e-3, restart=15, use_graph=False)
+    assert info.converged and info.outer >= 2
+    for i in range(A.shape[0]):
+        xt = torch.linalg.solve(A[i], B[i])
+        assert float(torch.linalg.vector_norm(X[i] - xt) / torch.linalg.vector_norm(xt)) < 1e-10
+
+
+def test_batch_operator_pads_members_and_keeps_padding_zero():
+    """BatchOperator on a stand-in batched handle (block-diagonal dense
+    members of uneven size, concatenated vectors)."""
+    from types import SimpleNamespace
+
+    from bigwham_dev_b200.solve import BatchOperator, MultiGmres
+
+    rng = np.random.default_rng(7)
+    sizes = [7, 30, 1, 18]
+    mats = [np.eye(s) * 5 + rng.standard_normal((s, s)) / np.sqrt(s) for s in sizes]
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    D = np.zeros((off[-1], off[-1]))
+    for k, M in enumerate(mats):
+        D[off[k]:off[k + 1], off[k]:off[k + 1]] = M
+    Dt = torch.from_numpy(D)
+    hb = SimpleNamespace(row_offsets=off, col_offsets=off,
+                         matvec=lambda x, p, out: out.copy_(Dt @ x))
+    op = BatchOperator(hb, "fp64", device="cpu")
+    assert (op.count, op.L) == (4, 30)
+    b = torch.from_numpy(rng.standard_normal(off[-1]))
+    Bp = op.pad(b)
+    assert torch.equal(op.unpad(Bp), b)
+    W = torch.zeros_like(Bp)
+    op(Bp, W)
+    assert torch.allclose(op.unpad(W), Dt @ b)
+    mask = torch.ones_like(Bp, dtype=torch.bool)
+    mask.view(-1)[op.idx] = False
+    assert float(W[mask].abs().max()) == 0.0
+    X, info = MultiGmres(op, op.count, op.L, restart=10, device="cpu", use_graph=False).solve(Bp, tol=1e-12)
+    assert info.converged
+    assert float(torch.linalg.vector_norm(Dt @ op.unpad(X) - b) / torch.linalg.vector_norm(b)) < 1e-11
+    assert float(X[mask].abs().max()) == 0.0

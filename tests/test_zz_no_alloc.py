@@ -5,8 +5,11 @@ their path).  Its scratch lives in a fixed 64 MiB device array compiled into
 the library instead of memory allocated per handle.
 
 Checked through the C ABI against bw_matvec on the same handle, two calls in a
-row (the array keeps the previous call's contents), within the tolerances the
-other GPU tests use.  This file is collected last on purpose.
+row (the array keeps the previous call's contents): within the tolerances the
+other GPU tests use, and bit for bit (the same kernels take the same steps;
+only the scratch address differs), in all precisions, for H and H^T, original
+and permuted ordering.  After a first call, further calls leave the device's
+free memory unchanged.  This file is collected last on purpose.
 """
 import ctypes as C
 
@@ -37,8 +40,8 @@ def test_static_scratch_matches_bw_matvec(golden, transpose):
     nin, nout = (arr.n_rows, arr.n_cols) if transpose else (arr.n_cols, arr.n_rows)
     stream = torch.cuda.current_stream().cuda_stream
     rng = np.random.default_rng(21)
-    for prec in ("fp64", "fp32", "bf16"):
-        flags = A.PRECISIONS[prec] | (A.BW_TRANSPOSE if transpose else 0)
+    for prec, permuted in (("fp64", False), ("fp32", False), ("bf16", False), ("fp64", True), ("bf16", True)):
+        flags = A.PRECISIONS[prec] | (A.BW_TRANSPOSE if transpose else 0) | (A.BW_PERMUTED if permuted else 0)
         for call in range(2):
             x = torch.from_numpy(rng.uniform(-1, 1, nin)).cuda()
             y_ref = torch.empty(nout, dtype=torch.float64, device="cuda")
@@ -49,6 +52,29 @@ def test_static_scratch_matches_bw_matvec(golden, transpose):
             h.sync(stream)
             err = float(torch.linalg.norm(y - y_ref) / torch.linalg.norm(y_ref))
             assert err <= TOL[prec], (prec, call, err)
+            assert torch.equal(y, y_ref), (prec, permuted, call)
+
+
+def test_static_scratch_allocates_nothing(golden):
+    """Once the first call has run on the device, further calls do not change
+    the device's free memory."""
+    import torch
+
+    arr, ex = golden
+    h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
+                          arr.perm1, device=0, precisions=("fp64", "bf16"))
+    stream = torch.cuda.current_stream().cuda_stream
+    x = torch.from_numpy(ex["x"]).cuda()
+    y = torch.empty(arr.n_rows, dtype=torch.float64, device="cuda")
+    _static_matvec(h, x, y, A.BW_FP64, stream)
+    h.sync(stream)
+    free0, _ = torch.cuda.mem_get_info()
+    for prec in ("fp64", "bf16", "fp64"):
+        _static_matvec(h, x, y, A.PRECISIONS[prec], stream)
+    h.sync(stream)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    h.close()
 
 
 def test_static_scratch_rejects_oversize():
