@@ -349,21 +349,17 @@ def time_matmat(a, h, dev, peak, ms_bf16_matvec):
             (X_host, cols))
 
 
-def time_batch(a, dev):
-    """48 independent 2DS0-H straight cracks on [-1,1], segment counts
-    log-uniform in [256, 16,384] (seed 3), leaf 32, eta 3, eps 1e-5, built by
-    the reference's host code: one batched matvec (4 launches for all 48)
-    against 48 separate handles (4 launches each)."""
-    import torch
+def c4a_members(a):
+    """The 48 independent 2DS0-H straight cracks on [-1,1] of the batched
+    workload: segment counts log-uniform in [256, 16,384] (seed 3), leaf 32,
+    eta 3, eps 1e-5, each built by the reference's host code."""
     from types import SimpleNamespace
 
-    from bigwham_dev_b200 import HmatGpu
     from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
     from bigwham_dev_b200.meshes import straight_crack_2d
 
     rng = np.random.default_rng(3)
     sizes = np.round(np.exp(rng.uniform(np.log(256), np.log(16384), 48))).astype(int)
-    t0 = time.time()
     members = []
     for n in sizes:
         coor, conn = straight_crack_2d(int(n))
@@ -371,6 +367,54 @@ def time_batch(a, dev):
         io.build_hierarchical_matrix(LEAF, ETA, EPS)
         members.append(SimpleNamespace(**io.export_blocks()))
         io.close()
+    return sizes, members
+
+
+def run_batch_only(a):
+    """--batch-only: the batched matvec of the 48 x 2DS0-H workload alone (one
+    handle, the listed precisions), W warm-ups then K timed steps, with the
+    per-launch times; one JSON line.  A short, self-contained command for
+    profiling the batched kernels."""
+    import torch
+
+    from bigwham_dev_b200 import HmatGpu
+
+    torch.cuda.set_device(0)
+    sizes, members = c4a_members(a)
+    out = {"workload": f"48 x 2DS0-H straight cracks ({int(sizes.sum()):,} segments), one batched matvec per step"}
+    for p in a.precisions:
+        hb = HmatGpu.batch(members, device=0, precisions=(p,))
+        x = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, hb.n_cols)).cuda()
+        y = torch.empty(hb.n_rows, dtype=torch.float64, device="cuda")
+        for _ in range(a.warmup):
+            hb.matvec(x, p, out=y)
+        hb.sync()
+        hb.set_timing(True)
+        ms = _events_ms(lambda: hb.matvec(x, p, out=y), a.steps)
+        launch_ms, nrec = hb.timing_read()
+        hb.set_timing(False)
+        b1, b2 = hb.phase_bytes(p)
+        pe = [v / max(1, nrec) for v in launch_ms]
+        out[p] = {"ms_per_matvec": ms, "launch_ms": pe, "phase_bytes": [b1, b2],
+                  "phase_gbs": [b1 / (pe[1] * 1e-3) / 1e9, b2 / (pe[3] * 1e-3) / 1e9],
+                  "algorithmic_bytes": hb.algorithmic_bytes(p)}
+        hb.sync()
+        hb.close()
+    print(json.dumps(out))
+    return 0
+
+
+def time_batch(a, dev):
+    """48 independent 2DS0-H straight cracks on [-1,1], segment counts
+    log-uniform in [256, 16,384] (seed 3), leaf 32, eta 3, eps 1e-5, built by
+    the reference's host code: one batched matvec (4 launches for all 48)
+    against 48 separate handles (4 launches each)."""
+    import torch
+
+    from bigwham_dev_b200 import HmatGpu
+
+    t0 = time.time()
+    sizes, members = c4a_members(a)
     build_s = time.time() - t0
     precs = ("fp64", "bf16")
     hb = HmatGpu.batch(members, device=dev.index or 0, precisions=precs)
@@ -659,6 +703,8 @@ def main(argv=None):
     ap.add_argument("--no-matmat", dest="matmat", action="store_false",
                     help="skip the 64-right-hand-side tensor-core matmat line (N = 1 only)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 48 x 2DS0 batched line (N = 1 only)")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="time only the 48 x 2DS0 batched matvec in the listed precisions (one GPU)")
     ap.add_argument("--block-file", default=None,
                     help="block file of the H-matrix: read it when it exists (no host rebuild), else write it "
                          "after the build")
@@ -670,8 +716,12 @@ def main(argv=None):
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")
     a.precisions = [p for p in a.precisions.split(",") if p]
-    if not {HEAD, "bf16"} <= set(a.precisions) or not set(a.precisions) <= {"fp64", "fp32", "bf16"}:
-        ap.error("--precisions must be a subset of fp64,fp32,bf16 that includes fp32 and bf16")
+    if not set(a.precisions) <= {"fp64", "fp32", "bf16"}:
+        ap.error("--precisions must be a subset of fp64,fp32,bf16")
+    if a.batch_only:
+        return run_batch_only(a)
+    if not {HEAD, "bf16"} <= set(a.precisions):
+        ap.error("--precisions must include fp32 (the headline) and bf16")
     if a.impl == "reference":
         return run_reference(a)
     return run_ours(a)

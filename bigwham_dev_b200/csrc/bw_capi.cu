@@ -108,6 +108,7 @@ struct bw_hmat {
   void *d_xp = nullptr, *d_t = nullptr, *d_g2 = nullptr;
   double *d_xh = nullptr, *d_yh = nullptr;
   double *h_xpin = nullptr, *h_ypin = nullptr;  // pinned staging of bw_matvec_host
+  cudaEvent_t y_ready[4] = {nullptr, nullptr, nullptr, nullptr};  // bw_matvec_host: output pieces landed
   int *d_err = nullptr;
   int *h_err = nullptr;    // pinned
   cudaStream_t stream = nullptr;
@@ -197,6 +198,10 @@ struct bw_hmat {
     if (h_xpin) cudaFreeHost(h_xpin);
     if (h_ypin) cudaFreeHost(h_ypin);
     h_xpin = h_ypin = nullptr;
+    for (cudaEvent_t &e : y_ready) {
+      if (e) cudaEventDestroy(e);
+      e = nullptr;
+    }
     cudaFree(d_err);
     if (h_err) cudaFreeHost(h_err);
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
@@ -263,7 +268,7 @@ int64_t align256(int64_t v) { return (v + 255) / 256 * 256; }
 // dst[0:n] = src[0:n] with up to 8 host threads (a vector of 1.5 MB copies in
 // ~20 us instead of ~150 us on one thread).
 void host_copy(double *dst, const double *src, int64_t n) {
-  const int64_t kPart = 32768;  // doubles per piece
+  const int64_t kPart = 8192;  // doubles per thread's part (64 KB)
   const int64_t parts = (n + kPart - 1) / kPart;
 #pragma omp parallel for num_threads(8) schedule(static) if (parts > 1)
   for (int64_t p = 0; p < parts; p++) {
@@ -1011,6 +1016,7 @@ int bw_finalize(bw_hmat *h, int flags) {
       h->d_yh = static_cast<double *>(h->dmalloc((size_t)std::max<int64_t>(1, nmax) * 8));
       BW_CUDA(cudaMallocHost(&h->h_xpin, (size_t)std::max<int64_t>(1, nmax) * 8));
       BW_CUDA(cudaMallocHost(&h->h_ypin, (size_t)std::max<int64_t>(1, nmax) * 8));
+      for (cudaEvent_t &e : h->y_ready) BW_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       if (want_mm) {
         const size_t xb = (size_t)mm_xt_rows(h) * 2 * bw::kMmRhs, tb = (size_t)(t8_rows + bw::kMmPadRows) * 2 * bw::kMmRhs;
         h->d_xt = static_cast<uint16_t *>(h->dmalloc(xb));
@@ -1146,33 +1152,48 @@ int bw_sync(bw_hmat *h, void *stream) {
 
 int bw_matvec_host(bw_hmat *h, const double *x, double *y, int flags) {
   if (!h) return BW_ERR_ARG;
+  const bool tr = (flags & BW_TRANSPOSE) != 0;
+  int64_t nin = 0, nout = 0;
+  // Pieces of the vectors: the host copy of piece k overlaps the DMA of piece
+  // k - 1 on the way in, and the DMA of piece k + 1 on the way out.
+  constexpr int kPieces = 4;  // = the handle's y_ready events
+  auto piece = [](int64_t n, int k) { return (n * k) / kPieces; };
   int rc = guarded(h, [&] {
     if (!h->finalized || h->plan_only) throw StateError("no device state");
-    const bool tr = (flags & BW_TRANSPOSE) != 0;
-    const int64_t nin = tr ? h->n_rows : h->n_cols, nout = tr ? h->n_cols : h->n_rows;
+    nin = tr ? h->n_rows : h->n_cols;
+    nout = tr ? h->n_cols : h->n_rows;
     if ((nin && !x) || (nout && !y)) throw std::invalid_argument("null vector");
     BW_CUDA(cudaSetDevice(h->device));
     // through the handle's pinned vectors: a few host threads copy the
     // caller's (pageable) array, the DMA then runs at full link speed
-    host_copy(h->h_xpin, x, nin);
-    BW_CUDA(cudaMemcpyAsync(h->d_xh, h->h_xpin, (size_t)nin * 8, cudaMemcpyHostToDevice, h->stream));
+    for (int k = 0; k < kPieces; k++) {
+      const int64_t a = piece(nin, k), b = piece(nin, k + 1);
+      if (b <= a) continue;
+      host_copy(h->h_xpin + a, x + a, b - a);
+      BW_CUDA(cudaMemcpyAsync(h->d_xh + a, h->h_xpin + a, (size_t)(b - a) * 8, cudaMemcpyHostToDevice, h->stream));
+    }
     return BW_OK;
   });
   if (rc != BW_OK) return rc;
   rc = bw_matvec(h, h->d_xh, h->d_yh, flags, h->stream);
   if (rc != BW_OK) return rc;
   rc = guarded(h, [&] {
-    const bool tr = (flags & BW_TRANSPOSE) != 0;
-    const int64_t nout = tr ? h->n_cols : h->n_rows;
-    BW_CUDA(cudaMemcpyAsync(h->h_ypin, h->d_yh, (size_t)nout * 8, cudaMemcpyDeviceToHost, h->stream));
+    for (int k = 0; k < kPieces; k++) {
+      const int64_t a = piece(nout, k), b = piece(nout, k + 1);
+      if (b > a)
+        BW_CUDA(cudaMemcpyAsync(h->h_ypin + a, h->d_yh + a, (size_t)(b - a) * 8, cudaMemcpyDeviceToHost, h->stream));
+      BW_CUDA(cudaEventRecord(h->y_ready[k], h->stream));
+    }
+    for (int k = 0; k < kPieces; k++) {
+      const int64_t a = piece(nout, k), b = piece(nout, k + 1);
+      BW_CUDA(cudaEventSynchronize(h->y_ready[k]));
+      if (b > a) host_copy(y + a, h->h_ypin + a, b - a);
+    }
     return BW_OK;
   });
   if (rc != BW_OK) return rc;
-  rc = bw_sync(h, h->stream);
-  if (rc != BW_OK) return rc;
-  const int64_t nout = (flags & BW_TRANSPOSE) ? h->n_cols : h->n_rows;
-  host_copy(y, h->h_ypin, nout);
-  return BW_OK;
+  // the kernels' error word (y is unspecified when it is set)
+  return bw_sync(h, h->stream);
 }
 
 int bw_matmat(bw_hmat *h, const double *X, int64_t ldx, double *Y, int64_t ldy, int nrhs, int flags,

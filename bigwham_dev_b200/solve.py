@@ -38,6 +38,11 @@ class SolveInfo:
     residuals: list = field(default_factory=list)  # relative residual estimates per cycle / outer step
 
 
+# Relative size of an Arnoldi residual, against the operator output it was
+# taken from, below which the Krylov space counts as exhausted (breakdown).
+_BREAKDOWN = 1e-12
+
+
 def _lstsq_prefix(Hh: np.ndarray, beta: float, tol_abs: float):
     """Smallest k with ||beta e1 - H[:k+1,:k] y|| <= tol_abs (or k = m) and its y."""
     m = Hh.shape[1]
@@ -84,6 +89,7 @@ class Gmres:
         for j in range(self.m):
             self._precondition(V[j], z)
             self.op(z, w)
+            w0 = self.torch.linalg.vector_norm(w)
             Vj = V[:j + 1]
             h = Vj @ w
             w.sub_(Vj.t() @ h)
@@ -91,8 +97,12 @@ class Gmres:
             w.sub_(Vj.t() @ h2)
             H[:j + 1, j] = h + h2
             nrm = self.torch.linalg.vector_norm(w)
+            # breakdown (see MultiGmres._cycle): zero vectors from here on
+            live = nrm > _BREAKDOWN * w0
+            nrm = self.torch.where(live, nrm, self.torch.zeros_like(nrm))
             H[j + 1, j] = nrm
-            self.torch.div(w, nrm, out=V[j + 1])
+            self.torch.div(w, self.torch.where(live, nrm, self.torch.ones_like(nrm)), out=V[j + 1])
+            V[j + 1].mul_(live.to(V.dtype))
 
     def _precondition(self, v, out):
         if self.minv is None:
@@ -224,6 +234,7 @@ class MultiGmres:
         for j in range(self.m):
             self._precondition(V[j], Z)
             self.op(Z, W)
+            w0 = torch.linalg.vector_norm(W, dim=1)         # (k,)
             Vj = V[:j + 1].transpose(0, 1)                  # (k, j+1, n)
             h = torch.bmm(Vj, W.unsqueeze(2))               # (k, j+1, 1)
             W.sub_(torch.bmm(Vj.transpose(1, 2), h).squeeze(2))
@@ -231,10 +242,15 @@ class MultiGmres:
             W.sub_(torch.bmm(Vj.transpose(1, 2), h2).squeeze(2))
             H[:, :j + 1, j] = (h + h2).squeeze(2)
             nrm = torch.linalg.vector_norm(W, dim=1)        # (k,)
+            # Breakdown: the system's Krylov space is exhausted (what is left
+            # of W is rounding).  It continues with zero vectors and a zero
+            # subdiagonal, where its least-squares problem stops.
+            live = nrm > _BREAKDOWN * w0
+            nrm = torch.where(live, nrm, torch.zeros_like(nrm))
             H[:, j + 1, j] = nrm
-            # a system with nothing left to reduce continues with zero vectors
-            safe = torch.where(nrm > 0, nrm, torch.ones_like(nrm))
+            safe = torch.where(live, nrm, torch.ones_like(nrm))
             torch.div(W, safe.unsqueeze(1), out=V[j + 1])
+            V[j + 1].mul_(live.unsqueeze(1).to(V.dtype))
 
     def _run_cycle(self):
         torch = self.torch
@@ -305,8 +321,8 @@ class MultiGmres:
 
 class BatchOperator:
     """The block-diagonal operator of a batched handle (HmatGpu.batch) on the
-    padded (count, L) layout of MultiGmres: member k's vector is row k,
-    entries beyond its length are zero and stay zero."""
+    padded (count, L) layout of MultiGmres: member k's vector is row k, and
+    the entries beyond its length are ignored on input and zero on output."""
 
     def __init__(self, hb, precision: str = "fp64", device="cuda"):
         import torch
@@ -339,6 +355,7 @@ class BatchOperator:
 
         torch.index_select(Z.reshape(-1), 0, self.idx, out=self.x)
         self.hb.matvec(self.x, self.precision, out=self.y)
+        W.zero_()  # the padding of an output buffer may hold anything
         W.view(-1).index_copy_(0, self.idx, self.y)
 
 

@@ -112,7 +112,7 @@ int bw_test_withhold_chunk(bw_hmat *h, int index);
  *   "mm_items_per_cta": granularity of the matmat's phase 1, default 8;
  *   "unit_bytes": the streaming queue hands out runs of consecutive items
  *       until a run's cost reaches this many bytes (0: one item at a time),
- *       0..2^30, default 65536.
+ *       0..2^30, default 0.
  * Results do not depend on them (each item is reduced in a fixed order).
  * BW_ERR_ARG for an unknown key or a value out of range. */
 int bw_set_tuning(bw_hmat *h, const char *key, int64_t value);
@@ -190,7 +190,9 @@ int bw_matvec(bw_hmat *h, const double *x, double *y, int flags, void *stream);
 int bw_matvec_static_scratch(bw_hmat *h, const double *x, double *y, int flags, void *stream);
 
 /* Same product on HOST arrays: copies x to the device, runs bw_matvec on the
- * handle's stream, copies y back and synchronizes.
+ * handle's stream, copies y back and synchronizes.  The vectors move in four
+ * pieces through pinned buffers of the handle, so the host copies overlap
+ * the DMA; on BW_ERR_DEVICE the contents of y are unspecified.
  * Replaces: Hmat<double>::matvecOriginal(il::ArrayView<double>) / matvec(...)
  * (hmat.cc:572-635 / :472-537), reached from BigWhamIO::MatVec(il::ArrayView)
  * (bigwham_io.cc:927-933) and MatVecPerm (bigwham_io.cc:965-980). */

@@ -114,3 +114,34 @@ def test_batch_operator_pads_members_and_keeps_padding_zero():
     assert info.converged
     assert float(torch.linalg.vector_norm(Dt @ op.unpad(X) - b) / torch.linalg.vector_norm(b)) < 1e-11
     assert float(X[mask].abs().max()) == 0.0
+
+
+def test_refine_multi_over_a_batch_with_tiny_members():
+    """Members of 1 and 3 unknowns exhaust their Krylov spaces within a
+    50-step cycle (breakdown: they continue with zero vectors), and output
+    buffers whose padding holds garbage (torch.empty) are zeroed by the batch
+    operator: every member converges, repeatably."""
+    from types import SimpleNamespace
+
+    from bigwham_dev_b200.solve import BatchOperator, refine_multi
+
+    rng = np.random.default_rng(7)
+    sizes = [8, 30, 1, 18, 60, 100, 3]
+    mats = [np.eye(s) * 5 + rng.standard_normal((s, s)) / np.sqrt(s) for s in sizes]
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    D = np.zeros((off[-1], off[-1]))
+    for k, M in enumerate(mats):
+        D[off[k]:off[k + 1], off[k]:off[k + 1]] = M
+    Dt = torch.from_numpy(D)
+    E = torch.from_numpy(rng.standard_normal(D.shape) * 1e-3) * (Dt != 0)
+    hb = SimpleNamespace(row_offsets=off, col_offsets=off,
+                         matvec=lambda x, p, out: out.copy_((Dt if p == "fp64" else Dt + E) @ x))
+    op64, op_lo = BatchOperator(hb, "fp64", device="cpu"), BatchOperator(hb, "lo", device="cpu")
+    b = torch.ones(off[-1], dtype=torch.float64)
+    B = op64.pad(b)
+    minv = op64.pad(1.0 / torch.diagonal(Dt))
+    for _ in range(3):
+        X, info = refine_multi(op64, op_lo, B, minv=minv, tol=1e-10, inner_tol=1e-3, restart=50, use_graph=False)
+        assert info.converged and info.residuals[0] == 1.0, info.residuals[:4]
+        x = op64.unpad(X)
+        assert float(torch.linalg.vector_norm(Dt @ x - b) / torch.linalg.vector_norm(b)) <= 1e-10
