@@ -488,6 +488,44 @@ def cpu_baseline(a, x_host, y_fp64):
             parity, R)
 
 
+def device_build(a, h, x_host, host_build_s):
+    """The same H-matrix built on the device (devbuild.build_r0: the host
+    builds the cluster tree and pattern, bw_r0_assemble_fr the full-rank
+    blocks, bw_r0_aca the low-rank ones) and laid out on the device
+    (bw_add_flat_device), against the host build of the reference's code:
+    wall times and the FP64 matvecs' relative difference (ACA pivots differ
+    in the last bits, ranks may differ by a block)."""
+    import torch
+
+    from bigwham_dev_b200 import HmatGpu
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+    from bigwham_dev_b200.devbuild import build_r0, ex_args
+    from bigwham_dev_b200.meshes import square_crack_3d
+
+    coor, conn = square_crack_3d(a.mesh)
+    io = BigWhamIOGpu(coor, conn, "3DR0-H", PROPS, os.cpu_count() or 1, useCuda=False)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    ex = build_r0(io, LEAF, ETA, EPS, PROPS[0], PROPS[1], on_device=True)
+    torch.cuda.synchronize()
+    t_build = time.time() - t0
+    io.close()
+    t0 = time.time()
+    hd = HmatGpu.from_device_flat(**ex_args(ex), device=torch.cuda.current_device(), precisions=("fp64",))
+    torch.cuda.synchronize()
+    t_layout = time.time() - t0
+    entries = int(ex["fr_data"].numel() + ex["lr_data"].numel())
+    del ex
+    x = torch.from_numpy(x_host).cuda()
+    yd, yh = hd.matvec(x, "fp64"), h.matvec(x, "fp64")
+    diff = float(torch.linalg.vector_norm(yd - yh) / torch.linalg.vector_norm(yh))
+    hd.close()
+    return {"workload": f"3DR0-H {a.mesh}x{a.mesh}: blocks computed on the device from the reference's pattern",
+            "device_build_s": round(t_build, 3), "device_layout_s": round(t_layout, 3),
+            "host_build_s": host_build_s, "entries_device_vs_host": [entries, h.info()["entries"]],
+            "fp64_matvec_rel_diff_vs_host_build": diff}
+
+
 def northstar_checks(a, h, R, x_host, mm_cols):
     """Accuracy of the target configuration against the FP64 dense oracle of
     the same kernel on a sampled row subset (683 collocation points = 2,049
@@ -640,6 +678,8 @@ def run_ours(a):
         extra["matmat_64rhs"], mm_cols = time_matmat(a, h, dev, peak, res["bf16"]["ms_per_step"])
     if world == 1 and not a.no_batch:
         extra["batched_2ds0_48"] = time_batch(a, dev)
+    if world == 1 and not a.no_devbuild:
+        extra["device_build_3dr0"] = device_build(a, h, x_host, setup.get("host_build_s"))
     if rank != 0:
         return 0
     cpu, parity = (None, None)
@@ -703,6 +743,8 @@ def main(argv=None):
     ap.add_argument("--no-matmat", dest="matmat", action="store_false",
                     help="skip the 64-right-hand-side tensor-core matmat line (N = 1 only)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 48 x 2DS0 batched line (N = 1 only)")
+    ap.add_argument("--no-devbuild", action="store_true",
+                    help="skip the device build of the same H-matrix (N = 1 only)")
     ap.add_argument("--batch-only", action="store_true",
                     help="time only the 48 x 2DS0 batched matvec in the listed precisions (one GPU)")
     ap.add_argument("--block-file", default=None,

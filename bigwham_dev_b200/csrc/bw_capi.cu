@@ -104,7 +104,6 @@ struct bw_hmat {
   std::vector<uint16_t> mm_host[2][2];  // BW_PLAN_ONLY
   uint16_t *d_xt = nullptr, *d_t8 = nullptr;  // matmat operands (8x8 BF16 tiles, bw::kMmRhs columns)
   int32_t *d_perm0 = nullptr, *d_perm1 = nullptr;
-  float *d_tscale[2] = {nullptr, nullptr};  // BF16 per-t-entry scales, per operator
   void *d_xp = nullptr, *d_t = nullptr, *d_g2 = nullptr;
   double *d_xh = nullptr, *d_yh = nullptr;
   double *h_xpin = nullptr, *h_ypin = nullptr;  // pinned staging of bw_matvec_host
@@ -187,9 +186,6 @@ struct bw_hmat {
     d_xt = d_t8 = nullptr;
     cudaFree(d_perm0);
     cudaFree(d_perm1);
-    cudaFree(d_tscale[0]);
-    cudaFree(d_tscale[1]);
-    d_tscale[0] = d_tscale[1] = nullptr;
     cudaFree(d_xp);
     cudaFree(d_t);
     cudaFree(d_g2);
@@ -588,7 +584,6 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
       a.gsrc = phase == 0 ? (kPacked ? static_cast<const void *>(xpk) : static_cast<const void *>(xp))
                           : static_cast<const void *>(g2_buf);
       a.t_out = t;
-      a.t_scale = prec == 2 ? h->d_tscale[o] : nullptr;
       a.y_out = y;
       a.perm_out = perm_out;
       a.dof = h->dof;
@@ -1002,12 +997,6 @@ int bw_finalize(bw_hmat *h, int flags) {
       p32.assign(h->perm1.begin(), h->perm1.end());
       h->d_perm1 = static_cast<int32_t *>(h->dmalloc(std::max<size_t>(1, p32.size()) * 4));
       if (!p32.empty()) BW_CUDA(cudaMemcpy(h->d_perm1, p32.data(), p32.size() * 4, cudaMemcpyHostToDevice));
-      if (mask & BW_BF16)
-        for (int o = 0; o < (want_t ? 2 : 1); o++) {
-          const std::vector<float> &ts = h->op[o].t_scale;
-          h->d_tscale[o] = static_cast<float *>(h->dmalloc(std::max<size_t>(1, ts.size()) * 4));
-          BW_CUDA(cudaMemcpy(h->d_tscale[o], ts.data(), ts.size() * 4, cudaMemcpyHostToDevice));
-        }
       // +16 bytes: the kernels stage vector segments in 16-byte aligned windows
       h->d_xp = h->dmalloc((size_t)std::max({xp_region_bytes(0, nmax), xp_region_bytes(2, nmax), (int64_t)1}));
       h->d_t = h->dmalloc((size_t)std::max<int64_t>(1, h->sum_rank) * 8 + 16);

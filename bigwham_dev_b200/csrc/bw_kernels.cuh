@@ -51,8 +51,7 @@ struct StreamArgs {
   int n_items;
   int *queue;                 // [next item, CTAs done]: zero at launch, reset to zero by the last CTA
   const void *gsrc;           // vector values: gathered x (phase 1) or G2 (phase 2), compute type
-  void *t_out;                // phase-1 output (compute type)
-  const float *t_scale;       // phase 1: per-t-entry output scale (BF16), or null
+  void *t_out;                // phase-1 output (compute type; BF16: unscaled, G2 applies the block scales)
   double *y_out;              // phase-2 output
   const int32_t *perm_out;    // phase 2: point permutation of the output, or null
   int dof;
@@ -93,6 +92,23 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
           smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// L2 policy for data read exactly once per launch (the block data): evict
+// first, so that the streamed gigabytes do not push the small arrays every
+// chunk touches (vectors, permutations, descriptors, queue ranges) out of L2.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// bulk_g2s with an L2 cache policy.
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                              uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
       : "memory");
 }
 __device__ __forceinline__ void fence_barrier_init() {
@@ -365,6 +381,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
     // ------------------------------------------------------------------ producer
     const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
     const unsigned char *gvec = static_cast<const unsigned char *>(a.gsrc);
+    const uint64_t stream_policy = l2_evict_first_policy();
     bool ok = true;
     int issued = 0;  // chunks staged so far by this CTA (stage = issued % kStages)
     ItemQueue iq;
@@ -415,7 +432,8 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
                                             static_cast<unsigned long long>(g_off) * sizeof(G);
               const unsigned long long glo = gs & ~15ull, ghi = (gs + ncols * sizeof(G) + 15ull) & ~15ull;
               mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>((hi - lo) + (ghi - glo)));
-              bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
+              bulk_g2s_hint(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s],
+                            stream_policy);
               bulk_g2s(st + L::kDataBytes, reinterpret_cast<const void *>(glo), static_cast<uint32_t>(ghi - glo),
                        &full[s]);
             } else {
@@ -475,7 +493,6 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
   const int ct = threadIdx.x - 32;
   const int cw = warp - 1;
   uint32_t items = 0;
-  float pre_scale[2] = {1.f, 1.f};
   long long pre_dst[2] = {0, 0};
   // FMA path state
   constexpr int R = kTensor ? 1 : Store<S>::kRows;
@@ -514,20 +531,15 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
     const int hpad = d.hpad;
     const int rows = d.rows, out_off = d.out_off;
     if (flags & kFirst) {
-      // Per-row output data of the item (BF16 t scale, or the permuted y
-      // index), loaded now so the latency is hidden behind the item's chunks.
+      // Phase 2: the permuted y index of the item's rows, loaded now so the
+      // latency is hidden behind the item's chunks.
 #pragma unroll
       for (int q = 0; q < 2; q++) {
         const int r = ct + q * kConsumers;
-        pre_scale[q] = 1.f;
         pre_dst[q] = out_off + r;
-        if (r < rows) {
-          if (a.phase == 1) {
-            if (a.t_scale) pre_scale[q] = a.t_scale[out_off + r];
-          } else if (a.perm_out) {
-            const int row = out_off + r;
-            pre_dst[q] = static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof);
-          }
+        if (r < rows && a.phase == 2 && a.perm_out) {
+          const int row = out_off + r;
+          pre_dst[q] = static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof);
         }
       }
     }
@@ -683,7 +695,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
           G sum = 0;
           for (int q = 0; q < nred; q++) sum += rb[q * hpad + r];
           if (a.phase == 1)
-            static_cast<G *>(a.t_out)[out_off + r] = sum * static_cast<G>(pre_scale[q2]);
+            static_cast<G *>(a.t_out)[out_off + r] = sum;
           else
             a.y_out[pre_dst[q2]] = static_cast<double>(sum);
         }

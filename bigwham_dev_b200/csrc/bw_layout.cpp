@@ -365,10 +365,14 @@ void scales_from_maxima(const Problem &p, bool tr, bool check_finite, const doub
 
 namespace {
 
+// Scale of a G2 run (BF16 only): a full block's scale, or for the t values of
+// a low-rank block the product of its two factor scales (phase 1 writes t
+// unscaled; the gather applies the product, one FP32 rounding either way).
 float seg_scale(const OperatorPlan &op, const Segment &s, int prec) {
   if (prec != 2) return 1.0f;
   if (s.kind == 0) return op.scale_fr[s.block];
-  return 1.0f;  // LR A slices and B stacks: the scales are folded into t (t_scale)
+  if (s.kind == 1) return op.scale_a[s.block] * op.scale_b[s.block];
+  return 1.0f;
 }
 
 // Chunks of one item for one precision; phase-2 chunks also get their slice of

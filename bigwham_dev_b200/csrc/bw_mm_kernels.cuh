@@ -287,7 +287,10 @@ __global__ void __launch_bounds__(kMmThreads, 1) mm_stream_kernel(MmArgs a) {
                   dst += rows * (2u * kMmRhs);
                 }
               }
-              bulk_g2s(st + bbytes, gdata + static_cast<unsigned long long>(data_off) * 2ull, dbytes, &full[s]);
+              // block data: read once per launch, evict first (the operand
+              // rows, re-read by many chunks, keep the normal policy)
+              bulk_g2s_hint(st + bbytes, gdata + static_cast<unsigned long long>(data_off) * 2ull, dbytes, &full[s],
+                            l2_evict_first_policy());
             } else {
               set_error(a.err, kErrMmBadChunk);
               sd->kc = 0;  // the MMA issuers skip the chunk

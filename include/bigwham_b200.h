@@ -278,8 +278,9 @@ int bw_phase_bytes(const bw_hmat *h, int precision, int transposed, int64_t *pha
  * cols | src << 31, scale bits), for inspection and testing. */
 int bw_plan_gather(const bw_hmat *h, int precision, int transposed, int64_t *n, int32_t *runs);
 
-/* Per-t-entry output scales of phase 1 (BF16: scale(A) * scale(B) of the
- * entry's low-rank block; 1 elsewhere), for inspection and testing. */
+/* Per-t-entry scales of the BF16 layout (scale(A) * scale(B) of the entry's
+ * low-rank block; 1 elsewhere), for inspection and testing.  Phase 1 writes t
+ * unscaled; the phase-2 gather runs that read t carry these products. */
 int bw_plan_tscale(const bw_hmat *h, int transposed, int64_t *n, float *out);
 
 /* ---- Block files ----------------------------------------------------------

@@ -31,7 +31,7 @@ def chunk_matrix(data, d, tiled):
     return t.transpose(1, 3, 0, 2).reshape(hp, ng * 8)[:, :nc]
 
 
-def run_phase(plan, gsrc, out, tiled=False, t_scale=None):
+def run_phase(plan, gsrc, out, tiled=False):
     chunks, items, data = plan["chunks"], plan["item_ptr"], plan["data"]
     for b in range(len(items) - 1):
         acc = None
@@ -42,10 +42,7 @@ def run_phase(plan, gsrc, out, tiled=False, t_scale=None):
             if d["ncols"]:
                 acc += chunk_matrix(data, d, tiled) @ gsrc[d["g_off"]:d["g_off"] + d["ncols"]]
             if d["flags"] & K_LAST:
-                r = acc[:d["rows"]]
-                if t_scale is not None:
-                    r = r * t_scale[d["out_off"]:d["out_off"] + d["rows"]]
-                out[d["out_off"]:d["out_off"] + d["rows"]] = r
+                out[d["out_off"]:d["out_off"] + d["rows"]] = acc[:d["rows"]]
     return out
 
 
@@ -77,15 +74,8 @@ def replay(h, x_perm, precision="fp64", transposed=False):
     p1 = h.plan_export(precision, 1, transposed)
     p2 = h.plan_export(precision, 2, transposed)
     tiled = precision == "bf16"
-    ts = None
-    if tiled:
-        n = C.c_int64()
-        A.check(A.lib().bw_plan_tscale(h._h, int(transposed), C.byref(n), None), h._h)
-        buf = (C.c_float * n.value)()
-        A.check(A.lib().bw_plan_tscale(h._h, int(transposed), C.byref(n), buf), h._h)
-        ts = np.frombuffer(buf, dtype=np.float32).astype(np.float64)
     t = np.zeros(max(1, h.info()["sum_rank"]))
-    run_phase(p1, x_perm, t, tiled, ts)
+    run_phase(p1, x_perm, t, tiled)  # BF16: t unscaled; the G2 runs carry the block scales
     g2 = build_g2(gather_runs(h, precision, transposed), x_perm, t)
     y = np.full(h.n_cols if transposed else h.n_rows, np.nan)
     run_phase(p2, g2, y, tiled)
