@@ -1166,11 +1166,14 @@ int bw_matvec_host(bw_hmat *h, const double *x, double *y, int flags) {
   if (rc != BW_OK) return rc;
   rc = bw_matvec(h, h->d_xh, h->d_yh, flags, h->stream);
   if (rc != BW_OK) return rc;
-  rc = guarded(h, [&] {
+  return guarded(h, [&] {
     for (int k = 0; k < kPieces; k++) {
       const int64_t a = piece(nout, k), b = piece(nout, k + 1);
       if (b > a)
         BW_CUDA(cudaMemcpyAsync(h->h_ypin + a, h->d_yh + a, (size_t)(b - a) * 8, cudaMemcpyDeviceToHost, h->stream));
+      // the kernels' error word travels with the last piece: one wait covers both
+      if (k == kPieces - 1)
+        BW_CUDA(cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
       BW_CUDA(cudaEventRecord(h->y_ready[k], h->stream));
     }
     for (int k = 0; k < kPieces; k++) {
@@ -1178,11 +1181,17 @@ int bw_matvec_host(bw_hmat *h, const double *x, double *y, int flags) {
       BW_CUDA(cudaEventSynchronize(h->y_ready[k]));
       if (b > a) host_copy(y + a, h->h_ypin + a, b - a);
     }
+    if (*h->h_err != 0) {  // y is unspecified; clear the word as bw_sync does
+      const int code = *h->h_err;
+      BW_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+      BW_CUDA(cudaStreamSynchronize(h->stream));
+      char buf[64];
+      snprintf(buf, sizeof buf, "kernel error word 0x%x", code);
+      h->err = buf;
+      return BW_ERR_DEVICE;
+    }
     return BW_OK;
   });
-  if (rc != BW_OK) return rc;
-  // the kernels' error word (y is unspecified when it is set)
-  return bw_sync(h, h->stream);
 }
 
 int bw_matmat(bw_hmat *h, const double *X, int64_t ldx, double *Y, int64_t ldy, int nrhs, int flags,

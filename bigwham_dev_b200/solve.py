@@ -36,6 +36,7 @@ class SolveInfo:
     cycles: int = 0              # restart cycles
     outer: int = 0               # refinement steps (refine only)
     residuals: list = field(default_factory=list)  # relative residual estimates per cycle / outer step
+    diverged: bool = False       # refinement stopped: the residual grew (see refine)
 
 
 # Relative size of an Arnoldi residual, against the operator output it was
@@ -170,15 +171,26 @@ class Gmres:
         return x, info
 
 
+# Refinement contracts the residual by about cond(A) x (the low precision's
+# relative error) per step.  Where that product exceeds one (an ill-conditioned
+# system with BF16 blocks) the residual grows instead; a system whose residual
+# exceeds _DIVERGED x its best so far is stopped at its best iterate and
+# reported as diverged (SolveInfo.diverged) rather than iterated to overflow.
+_DIVERGED = 10.0
+
+
 def refine(op_hi, op_lo, b, n: int, minv=None, tol: float = 1e-8, inner_tol: float = 1e-3, restart: int = 50,
            max_outer: int = 50, use_graph: bool = True):
-    """Mixed-precision iterative refinement: x += GMRES_lo(A d = b - A_hi x)."""
+    """Mixed-precision iterative refinement: x += GMRES_lo(A d = b - A_hi x).
+    Stops at the best iterate, with info.diverged set, when the residual
+    grows (see _DIVERGED)."""
     import torch
 
     info = SolveInfo()
     inner = Gmres(op_lo, n, restart, minv, device=b.device, use_graph=use_graph)
     x = torch.zeros_like(b)
     r = torch.empty_like(b)
+    best, x_best = np.inf, x.clone()
     bnorm = float(torch.linalg.vector_norm(b))
     for it in range(max_outer):
         op_hi(x, r)
@@ -189,6 +201,13 @@ def refine(op_hi, op_lo, b, n: int, minv=None, tol: float = 1e-8, inner_tol: flo
         if rel <= tol:
             info.converged = True
             break
+        if not np.isfinite(rel) or rel > _DIVERGED * best:
+            info.diverged = True
+            x.copy_(x_best)
+            break
+        if rel < best:
+            best = rel
+            x_best.copy_(x)
         d, inf = inner.solve(r, tol=inner_tol, maxiter=20 * restart)
         info.iterations += inf.iterations
         info.cycles += inf.cycles
@@ -363,27 +382,49 @@ def refine_multi(op_hi, op_lo, B, minv=None, tol: float = 1e-8, inner_tol: float
                  max_outer: int = 50, use_graph: bool = True):
     """Mixed-precision iterative refinement of k systems (rows of B):
     X += MultiGmres_lo(A D = B - A_hi X), until every row's relative residual
-    is <= tol.  op_hi, op_lo: (Z, W) operators on (k, n) tensors."""
+    is <= tol.  op_hi, op_lo: (Z, W) operators on (k, n) tensors.  A row whose
+    residual grows (see _DIVERGED) is stopped at its best iterate;
+    info.per_system[i] tells converged / diverged, info.converged is true when
+    every row converged."""
     import torch
 
     k, n = B.shape
     info = SolveInfo()
+    per = [SolveInfo() for _ in range(k)]
     inner = MultiGmres(op_lo, k, n, restart, minv, device=B.device, use_graph=use_graph)
     X = torch.zeros_like(B)
     R = torch.empty_like(B)
+    X_best = torch.zeros_like(B)
+    best = np.full(k, np.inf)
+    active = np.ones(k, dtype=bool)
     bn = torch.linalg.vector_norm(B, dim=1)
     bn = torch.where(bn > 0, bn, torch.ones_like(bn))
     for it in range(max_outer):
         op_hi(X, R)
         torch.sub(B, R, out=R)
-        rel = float((torch.linalg.vector_norm(R, dim=1) / bn).max())
-        info.residuals.append(rel)
+        rel = (torch.linalg.vector_norm(R, dim=1) / bn).cpu().numpy()
         info.outer = it
-        if rel <= tol:
-            info.converged = True
+        for i in np.nonzero(active)[0]:
+            per[i].residuals.append(float(rel[i]))
+            per[i].outer = it
+            if rel[i] <= tol:
+                per[i].converged, active[i] = True, False
+            elif not np.isfinite(rel[i]) or rel[i] > _DIVERGED * best[i]:
+                per[i].diverged, active[i] = True, False
+                X[i].copy_(X_best[i])
+            elif rel[i] < best[i]:
+                best[i] = rel[i]
+                X_best[i].copy_(X[i])
+        info.residuals.append(float(max((per[i].residuals[-1] for i in range(k) if per[i].residuals), default=0.0)))
+        if not active.any():
             break
+        # finished rows get a zero right-hand side: the inner solve leaves them alone
+        R.mul_(torch.from_numpy(active.astype(np.float64)).to(R.device).unsqueeze(1))
         D, inf = inner.solve(R, tol=inner_tol, maxiter=20 * restart)
         info.iterations += inf.iterations
         info.cycles += inf.cycles
         X.add_(D)
+    info.converged = all(p.converged for p in per)
+    info.diverged = any(p.diverged for p in per)
+    info.per_system = per
     return X, info

@@ -145,3 +145,31 @@ def test_refine_multi_over_a_batch_with_tiny_members():
         assert info.converged and info.residuals[0] == 1.0, info.residuals[:4]
         x = op64.unpad(X)
         assert float(torch.linalg.vector_norm(Dt @ x - b) / torch.linalg.vector_norm(b)) <= 1e-10
+
+
+def test_refinement_stops_when_the_low_precision_operator_is_too_coarse():
+    """Refinement contracts by ~cond(A) x (low-precision error) per step; with
+    cond 1e5 and a 1e-3 perturbation the residual grows.  The solver stops at
+    its best iterate and reports the divergence (no overflow); in the batched
+    form only that system stops, the well-conditioned one converges."""
+    from bigwham_dev_b200.solve import refine, refine_multi
+
+    rng = np.random.default_rng(11)
+    n = 60
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A_bad = torch.from_numpy(Q @ np.diag(np.logspace(0, -5, n)) @ Q.T)
+    A_good = torch.from_numpy(np.eye(n) * 3 + rng.standard_normal((n, n)) / np.sqrt(n))
+    E = torch.from_numpy(rng.standard_normal((n, n))) * 1e-3 / np.sqrt(n)
+    b = torch.from_numpy(rng.standard_normal(n))
+    x, info = refine(lambda v, w: w.copy_(A_bad @ v), lambda v, w: w.copy_((A_bad + E) @ v), b, n, tol=1e-12,
+                     inner_tol=1e-6, restart=n, use_graph=False)
+    assert info.diverged and not info.converged and bool(torch.isfinite(x).all())
+    assert float(torch.linalg.vector_norm(b - A_bad @ x) / torch.linalg.vector_norm(b)) <= 1.0
+    A2, B = torch.stack([A_good, A_bad]), torch.stack([b, b])
+    E2 = torch.stack([E, E])
+    X, info = refine_multi(lambda Z, W: W.copy_(torch.bmm(A2, Z.unsqueeze(2)).squeeze(2)),
+                           lambda Z, W: W.copy_(torch.bmm(A2 + E2, Z.unsqueeze(2)).squeeze(2)), B, tol=1e-12,
+                           inner_tol=1e-6, restart=n, use_graph=False)
+    assert info.per_system[0].converged and info.per_system[1].diverged and not info.converged
+    assert bool(torch.isfinite(X).all())
+    assert float(torch.linalg.vector_norm(b - A_good @ X[0]) / torch.linalg.vector_norm(b)) <= 1e-12
