@@ -283,6 +283,11 @@ template <int N> struct IntC {
   static constexpr int value = N;
 };
 
+// Work per consumer in a one-chunk item: at least this many columns per
+// thread (FMA paths) or K-steps per warp (tensor path).
+constexpr int kMinCols = 8;
+constexpr int kMinKsteps = 4;
+
 // The producer warp's view of the work queue, pipelined so that no latency
 // lands on an item boundary:
 //  * `cur` is the item being staged, its chunk range [cb, ce) already loaded;
@@ -432,8 +437,13 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
                                             static_cast<unsigned long long>(g_off) * sizeof(G);
               const unsigned long long glo = gs & ~15ull, ghi = (gs + ncols * sizeof(G) + 15ull) & ~15ull;
               mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>((hi - lo) + (ghi - glo)));
-              bulk_g2s_hint(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s],
-                            stream_policy);
+              // evict-first helps the BF16 launches (measured A/B at 196,608 DoF:
+              // -2 to -4%) and slows the FP32 / FP64 row panels (+1 to +3%)
+              if constexpr (kTensor)
+                bulk_g2s_hint(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s],
+                              stream_policy);
+              else
+                bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
               bulk_g2s(st + L::kDataBytes, reinterpret_cast<const void *>(glo), static_cast<uint32_t>(ghi - glo),
                        &full[s]);
             } else {
@@ -547,6 +557,11 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
       if (flags & kFirst) {
         hv = hpad / R;
         Q = kConsumers / hv;
+        // A one-chunk item with few columns: fewer column groups, each of at
+        // least kMinCols columns; the other threads skip the item (fewer
+        // instructions per chunk, fewer partial sums to reduce).  The split
+        // depends only on the item, so results do not depend on the CTA.
+        if ((flags & kLast) && ncols > 0) Q = max(1, min(Q, ncols / kMinCols));
         rv = ct % hv;
         cq = ct / hv;
         active = cq < Q;
@@ -562,10 +577,14 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
       if (flags & kFirst) {
         nMt = (hpad + 15) >> 4;
         const int mgroups = (nMt + 7) >> 3;
-        kparts = kConsumerWarps / mgroups;
-        mg = cw / kparts;
-        kp = cw % kparts;
-        wact = mg < mgroups;
+        const int kfull = kConsumerWarps / mgroups;
+        mg = cw / kfull;
+        kp = cw % kfull;
+        // A one-chunk item with few K-steps: fewer warps per m-group, each
+        // with at least kMinKsteps K-steps; the other warps skip the item.
+        kparts = kfull;
+        if ((flags & kLast) && ncols > 0) kparts = max(1, min(kfull, (((ncols + 15) >> 4) + kMinKsteps - 1) / kMinKsteps));
+        wact = mg < mgroups && kp < kparts;
         rot = 0;
 #pragma unroll
         for (int j = 0; j < 8; j++)
