@@ -283,11 +283,6 @@ template <int N> struct IntC {
   static constexpr int value = N;
 };
 
-// Work per consumer in a one-chunk item: at least this many columns per
-// thread (FMA paths) or K-steps per warp (tensor path).
-constexpr int kMinCols = 8;
-constexpr int kMinKsteps = 4;
-
 // The producer warp's view of the work queue, pipelined so that no latency
 // lands on an item boundary:
 //  * `cur` is the item being staged, its chunk range [cb, ce) already loaded;
@@ -557,11 +552,6 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
       if (flags & kFirst) {
         hv = hpad / R;
         Q = kConsumers / hv;
-        // A one-chunk item with few columns: fewer column groups, each of at
-        // least kMinCols columns; the other threads skip the item (fewer
-        // instructions per chunk, fewer partial sums to reduce).  The split
-        // depends only on the item, so results do not depend on the CTA.
-        if ((flags & kLast) && ncols > 0) Q = max(1, min(Q, ncols / kMinCols));
         rv = ct % hv;
         cq = ct / hv;
         active = cq < Q;
@@ -577,14 +567,10 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
       if (flags & kFirst) {
         nMt = (hpad + 15) >> 4;
         const int mgroups = (nMt + 7) >> 3;
-        const int kfull = kConsumerWarps / mgroups;
-        mg = cw / kfull;
-        kp = cw % kfull;
-        // A one-chunk item with few K-steps: fewer warps per m-group, each
-        // with at least kMinKsteps K-steps; the other warps skip the item.
-        kparts = kfull;
-        if ((flags & kLast) && ncols > 0) kparts = max(1, min(kfull, (((ncols + 15) >> 4) + kMinKsteps - 1) / kMinKsteps));
-        wact = mg < mgroups && kp < kparts;
+        kparts = kConsumerWarps / mgroups;
+        mg = cw / kparts;
+        kp = cw % kparts;
+        wact = mg < mgroups;
         rot = 0;
 #pragma unroll
         for (int j = 0; j < 8; j++)
