@@ -69,6 +69,7 @@ struct DevPhase {
   int64_t n_items = 0;
   int64_t n_elems = 0;
   int64_t n_gsegs = 0;
+  bool narrow = false;             // every item has <= narrow_rows padded rows: warp-per-item kernel
 };
 
 // Device data of one matmat phase (bw::MmPlan).
@@ -464,6 +465,9 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   const bw::ChunkPlan &cp = ph.cp[prec];
   dp.n_chunks = (int64_t)cp.chunks.size();
   dp.n_gsegs = (int64_t)cp.gsegs.size();
+  int max_hpad = 0;
+  for (const bw::Item &it : ph.items) max_hpad = std::max(max_hpad, (int)it.hpad);
+  dp.narrow = h->prob.tune.narrow_rows > 0 && max_hpad <= h->prob.tune.narrow_rows;
   if (h->plan_only) {
     auto &buf = h->host_data[o][prec][phase];
     buf.assign((size_t)ph.n_elems[prec] * es, 0);
@@ -591,7 +595,10 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
       a.err = h->d_err;
       a.spin_limit = h->spin_limit;
       a.withhold = h->take_withhold();
-      bw::stream_panels_kernel<S><<<h->grid, bw::threads_of<S>(), bw::SmemLayout<S>::kTotal, st>>>(a);
+      if (dp.narrow)  // the test hook applies to the CTA-wide kernel only
+        bw::narrow_items_kernel<S><<<2 * h->grid, 32 * bw::kNarrowWarps, 0, st>>>(a);
+      else
+        bw::stream_panels_kernel<S><<<h->grid, bw::threads_of<S>(), bw::SmemLayout<S>::kTotal, st>>>(a);
       BW_CUDA(cudaGetLastError());
     }
     if (ev) BW_CUDA(cudaEventRecord(ev[phase == 0 ? 2 : 4], st));
@@ -739,6 +746,14 @@ int bw_set_tuning(bw_hmat *h, const char *key, int64_t value) {
       t.mm_items_per_cta = (int)value;
     else
       t.items_per_cta[k.back() - '1'] = (int)value;
+    return BW_OK;
+  }
+  if (k == "narrow_rows") {
+    if (value < 0 || value > bw::kNarrowRows) {
+      h->err = "narrow_rows must be in [0, " + std::to_string(bw::kNarrowRows) + "]";
+      return BW_ERR_ARG;
+    }
+    t.narrow_rows = (int)value;
     return BW_OK;
   }
   if (k == "unit_bytes") {

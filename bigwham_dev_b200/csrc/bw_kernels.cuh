@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "bw_layout.h"
 
@@ -706,6 +707,201 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
         }
       }
       items++;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------- narrow phases
+// Phases whose items all have at most kNarrowRows padded rows (the row panels
+// and B stacks of 2DS0-H matrices, 8 to 64 rows) run warp per item instead:
+// a warp takes an item from the queue, walks its chunks with ordinary 16-byte
+// loads straight from global memory (no staging), keeps every row of the
+// item in registers and writes the item's outputs itself.  The CTA-wide
+// kernel above spends a fixed ~1.3 us per chunk on such items (every consumer
+// warp takes part in every chunk's barrier round trip and in every item's
+// shared-memory reduction, measured with per-chunk clock stamps on the
+// 48 x 2DS0 batch); here nothing is shared between warps and 32 items are in
+// flight per SM.  The chunk descriptors, the data layout and the vector
+// sources are the ones the CTA-wide kernel reads, and an item's arithmetic
+// does not depend on the warp that takes it.
+constexpr int kNarrowRows = 64;
+constexpr int kNarrowWarps = 16;  // per CTA; two CTAs per SM
+
+// x value of a packed (hi, lo) BF16 word (pack_hilo): hi + lo, exact in FP32.
+__device__ __forceinline__ float unpack_hilo(uint32_t w) {
+  return __uint_as_float(w << 16) + __uint_as_float(w & 0xffff0000u);
+}
+
+// One chunk of a column-major FP64 / FP32 item.  Lanes hold R = 16 / es
+// adjacent rows of one column slot; lpc lanes cover the padded rows, 32 / lpc
+// column slots run side by side.
+template <typename S, int R>
+__device__ __forceinline__ void narrow_fma_chunk(const unsigned char *base, const typename Store<S>::G *g, int hpad,
+                                                 int ncols, int lpc, int lane, typename Store<S>::G (&acc)[R]) {
+  using G = typename Store<S>::G;
+  using V = typename std::conditional<sizeof(G) == 8, double2, float4>::type;
+  const int cpp = 32 / lpc, slot = lane / lpc, r0 = (lane % lpc) * R;
+  if (r0 >= hpad) return;
+  const G *d = reinterpret_cast<const G *>(base) + r0;
+  int c = slot;
+#pragma unroll 1
+  for (; c + 3 * cpp < ncols; c += 4 * cpp) {
+    V v[4];
+    G x[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      v[q] = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(c + q * cpp) * hpad));
+      x[q] = __ldg(g + c + q * cpp);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const G *e = reinterpret_cast<const G *>(&v[q]);
+#pragma unroll
+      for (int k = 0; k < R; k++) acc[k] = fma(e[k], x[q], acc[k]);
+    }
+  }
+  for (; c < ncols; c += cpp) {
+    const V v = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(c) * hpad));
+    const G x = __ldg(g + c);
+    const G *e = reinterpret_cast<const G *>(&v);
+#pragma unroll
+    for (int k = 0; k < R; k++) acc[k] = fma(e[k], x, acc[k]);
+  }
+}
+
+// One chunk of an 8x8-tiled BF16 item: lane (c8, slot) takes column c8 of
+// every column group and the row groups slot and slot + 4; a 16-byte load is
+// 8 rows of one column (one tile column).
+__device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
+                                                  int lane, float (&acc)[2][8]) {
+  const int c8 = lane & 7, slot = lane >> 3, nrg = hpad >> 3;
+  const int ncg = (ncols + 7) >> 3;
+#pragma unroll 2
+  for (int cg = 0; cg < ncg; cg++) {
+    const int c = 8 * cg + c8;
+    if (c >= ncols) continue;
+    const float x = unpack_hilo(__ldg(g + c));
+    const uint16_t *col = base + static_cast<long long>(cg) * 8 * hpad + c8 * 8;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const int rg = slot + 4 * j;
+      if (rg < nrg) {
+        const uint4 w = __ldg(reinterpret_cast<const uint4 *>(col + rg * 64));
+        const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          acc[j][2 * k] = fmaf(__uint_as_float(ww[k] << 16), x, acc[j][2 * k]);
+          acc[j][2 * k + 1] = fmaf(__uint_as_float(ww[k] & 0xffff0000u), x, acc[j][2 * k + 1]);
+        }
+      }
+    }
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(32 * kNarrowWarps, 2) narrow_items_kernel(StreamArgs a) {
+  using G = typename Store<S>::G;
+  constexpr int es = Store<S>::kEsize;
+  constexpr bool kTensor = Store<S>::kRows == 0;
+  constexpr int R = kTensor ? 1 : 16 / es;
+  const int lane = threadIdx.x & 31;
+  const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(&a.queue[0], 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= a.n_items) break;
+    const int cb = __ldg(a.item_ptr + it), ce = __ldg(a.item_ptr + it + 1);
+    G acc[R];
+    float tacc[2][8];
+    for (int i = cb; i < ce; i++) {
+      const uint4 *dp = reinterpret_cast<const uint4 *>(a.chunks + i);
+      const uint4 w0 = __ldg(dp), w1 = __ldg(dp + 1);
+      const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w0.y) << 32) | w0.x);
+      const int ncols = static_cast<int>(w0.z), hpad = static_cast<int>(w0.w);
+      const int rows = static_cast<int>(w1.x), out_off = static_cast<int>(w1.y);
+      const uint32_t flags = w1.z;
+      const int g_off = static_cast<int>(w1.w);
+      if (hpad <= 0 || hpad > kNarrowRows || ncols < 0 || ncols > kMaxCols) {
+        if (lane == 0) set_error(a.err, kErrBadChunk);
+        continue;
+      }
+      if (flags & kFirst) {
+#pragma unroll
+        for (int k = 0; k < R; k++) acc[k] = 0;
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+          for (int k = 0; k < 8; k++) tacc[j][k] = 0.f;
+      }
+      if constexpr (kTensor) {
+        narrow_bf16_chunk(reinterpret_cast<const uint16_t *>(gdata) + data_off,
+                          static_cast<const uint32_t *>(a.gsrc) + g_off, hpad, ncols, lane, tacc);
+      } else {
+        int lpc = 1;
+        while (lpc * R < hpad) lpc <<= 1;
+        narrow_fma_chunk<S, R>(gdata + data_off * es, static_cast<const G *>(a.gsrc) + g_off, hpad, ncols, lpc,
+                               lane, acc);
+      }
+      if (!(flags & kLast)) continue;
+      // the item's outputs: sums over the column slots, then one store per row
+      if constexpr (kTensor) {
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+          for (int k = 0; k < 8; k++)
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) tacc[j][k] += __shfl_xor_sync(0xffffffffu, tacc[j][k], o);
+        const int c8 = lane & 7, slot = lane >> 3;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          float v = tacc[j][0];
+#pragma unroll
+          for (int k = 1; k < 8; k++)
+            if (c8 == k) v = tacc[j][k];
+          const int r = (slot + 4 * j) * 8 + c8;
+          if (r < rows) {
+            if (a.phase == 1) {
+              static_cast<G *>(a.t_out)[out_off + r] = v;
+            } else {
+              const int row = out_off + r;
+              a.y_out[a.perm_out ? static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof) : row] =
+                  static_cast<double>(v);
+            }
+          }
+        }
+      } else {
+        int lpc = 1;
+        while (lpc * R < hpad) lpc <<= 1;
+        for (int o = lpc; o < 32; o <<= 1)
+#pragma unroll
+          for (int k = 0; k < R; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+        if (lane < lpc) {
+#pragma unroll
+          for (int k = 0; k < R; k++) {
+            const int r = lane * R + k;
+            if (r < rows) {
+              if (a.phase == 1) {
+                static_cast<G *>(a.t_out)[out_off + r] = acc[k];
+              } else {
+                const int row = out_off + r;
+                a.y_out[a.perm_out ? static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof) : row] =
+                    static_cast<double>(acc[k]);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  // This CTA takes no more items; the last CTA returns the queue to zero.
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&a.queue[1], 1) == static_cast<int>(gridDim.x) - 1) {
+      a.queue[0] = 0;
+      a.queue[1] = 0;
+      __threadfence();
     }
   }
 }

@@ -156,6 +156,7 @@ struct Tuning {
   int chunk_bytes = kStageBytes;                        // block data per chunk (<= kStageBytes)
   int mm_items_per_cta = kItemsPerCta;                  // matmat phase 1
   int unit_bytes = kUnitBytes;                          // streaming queue: minimum cost of a unit
+  int narrow_rows = 64;  // phases whose items have at most this many padded rows run warp per item (0: never)
 };
 
 struct Problem {

@@ -117,7 +117,7 @@ class HmatGpu:
 
     def set_tuning(self, **kw) -> "HmatGpu":
         """Plan parameters (bw_set_tuning), before finalize: items_per_cta_phase1,
-        items_per_cta_phase2, chunk_bytes, mm_items_per_cta, unit_bytes."""
+        items_per_cta_phase2, chunk_bytes, mm_items_per_cta, unit_bytes, narrow_rows."""
         for k, v in kw.items():
             A.check(self._lib.bw_set_tuning(self._h, k.encode(), int(v)), self._h)
         return self

@@ -112,7 +112,10 @@ int bw_test_withhold_chunk(bw_hmat *h, int index);
  *   "mm_items_per_cta": granularity of the matmat's phase 1, default 8;
  *   "unit_bytes": the streaming queue hands out runs of consecutive items
  *       until a run's cost reaches this many bytes (0: one item at a time),
- *       0..2^30, default 0.
+ *       0..2^30, default 0;
+ *   "narrow_rows": a phase whose items all have at most this many padded
+ *       rows runs warp per item (no staging, no cross-warp reduction),
+ *       0..64, default 64 (0: always the CTA-wide kernel).
  * Results do not depend on them (each item is reduced in a fixed order).
  * BW_ERR_ARG for an unknown key or a value out of range. */
 int bw_set_tuning(bw_hmat *h, const char *key, int64_t value);
