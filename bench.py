@@ -253,6 +253,8 @@ def build_hmatrix(a, world, rank, local):
 
     precs = tuple(a.precisions)
     tuning = load_best(a.mesh, "bf16")  # committed autotuner result for this mesh, if any
+    if a.tune:
+        tuning = {**(tuning or {}), **a.tune}
     info = {"tuning": tuning or "defaults"}
     coor, conn = square_crack_3d(a.mesh)
     if world == 1:
@@ -383,7 +385,7 @@ def run_batch_only(a):
     sizes, members = c4a_members(a)
     out = {"workload": f"48 x 2DS0-H straight cracks ({int(sizes.sum()):,} segments), one batched matvec per step"}
     for p in a.precisions:
-        hb = HmatGpu.batch(members, device=0, precisions=(p,))
+        hb = HmatGpu.batch(members, device=0, precisions=(p,), tuning=a.tune or None)
         x = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, hb.n_cols)).cuda()
         y = torch.empty(hb.n_rows, dtype=torch.float64, device="cuda")
         for _ in range(a.warmup):
@@ -417,9 +419,9 @@ def time_batch(a, dev):
     sizes, members = c4a_members(a)
     build_s = time.time() - t0
     precs = ("fp64", "bf16")
-    hb = HmatGpu.batch(members, device=dev.index or 0, precisions=precs)
+    hb = HmatGpu.batch(members, device=dev.index or 0, precisions=precs, tuning=a.tune or None)
     hs = [HmatGpu.from_flat(m.dof, m.n_rows, m.n_cols, m.fr, m.lr, m.fr_data, m.lr_data, m.perm0, m.perm1,
-                            device=dev.index or 0, precisions=precs) for m in members]
+                            device=dev.index or 0, precisions=precs, tuning=a.tune or None) for m in members]
     x = torch.from_numpy(np.random.default_rng(0).uniform(-1, 1, hb.n_cols)).to(dev)
     y = torch.empty(hb.n_rows, dtype=torch.float64, device=dev)
     xs = [x[int(hb.col_offsets[k]):int(hb.col_offsets[k + 1])].contiguous() for k in range(len(hs))]
@@ -743,6 +745,8 @@ def main(argv=None):
     ap.add_argument("--no-matmat", dest="matmat", action="store_false",
                     help="skip the 64-right-hand-side tensor-core matmat line (N = 1 only)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 48 x 2DS0 batched line (N = 1 only)")
+    ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
+                    help="plan parameter (bw_set_tuning) for every handle of the run, e.g. narrow_rows=0; repeatable")
     ap.add_argument("--no-devbuild", action="store_true",
                     help="skip the device build of the same H-matrix (N = 1 only)")
     ap.add_argument("--batch-only", action="store_true",
@@ -758,6 +762,10 @@ def main(argv=None):
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")
     a.precisions = [p for p in a.precisions.split(",") if p]
+    try:
+        a.tune = {k: int(v) for k, v in (t.split("=", 1) for t in a.tune)}
+    except ValueError:
+        ap.error("--tune takes KEY=INTEGER")
     if not set(a.precisions) <= {"fp64", "fp32", "bf16"}:
         ap.error("--precisions must be a subset of fp64,fp32,bf16")
     if a.batch_only:
