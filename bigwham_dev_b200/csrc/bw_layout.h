@@ -156,7 +156,8 @@ struct Tuning {
   int chunk_bytes = kStageBytes;                        // block data per chunk (<= kStageBytes)
   int mm_items_per_cta = kItemsPerCta;                  // matmat phase 1
   int unit_bytes = kUnitBytes;                          // streaming queue: minimum cost of a unit
-  int narrow_rows = 64;  // phases whose items have at most this many padded rows run warp per item (0: never)
+  int narrow_rows = 64;   // small items: at most this many padded rows (0: no warp-per-item launches) ...
+  int narrow_cols = 512;  // ... and this many columns; they run warp per item
 };
 
 struct Problem {

@@ -113,9 +113,12 @@ int bw_test_withhold_chunk(bw_hmat *h, int index);
  *   "unit_bytes": the streaming queue hands out runs of consecutive items
  *       until a run's cost reaches this many bytes (0: one item at a time),
  *       0..2^30, default 0;
- *   "narrow_rows": a phase whose items all have at most this many padded
- *       rows runs warp per item (no staging, no cross-warp reduction),
- *       0..64, default 64 (0: always the CTA-wide kernel).
+ *   "narrow_rows", "narrow_cols": the small items of a phase (at most
+ *       narrow_rows padded rows, 0..64, default 64, and narrow_cols columns,
+ *       default 512), those after the last larger item in the queue's
+ *       cost order, run warp per item (no staging, no cross-warp reduction)
+ *       in a second launch; narrow_rows 0 keeps every item in the CTA-wide
+ *       kernel.
  * Results do not depend on them (each item is reduced in a fixed order).
  * BW_ERR_ARG for an unknown key or a value out of range. */
 int bw_set_tuning(bw_hmat *h, const char *key, int64_t value);
@@ -263,6 +266,11 @@ int bw_mm_plan_export(const bw_hmat *h, int phase, int transposed, int64_t *n_ch
  * available on a handle finalized with BW_PLAN_ONLY. */
 int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_chunks,
                    int32_t *chunks, int64_t *n_elems, double *data, int64_t *n_item_ptr, int32_t *item_ptr);
+
+/* How one phase's items divide between the two streaming kernels: items
+ * [0, n_wide) of bw_plan_export's item order run in the CTA-wide kernel, the
+ * rest warp per item (see the "narrow_rows" tuning key). */
+int bw_plan_split(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_wide);
 
 /* Per-launch timing for benchmarks.  With timing enabled every bw_matvec
  * records CUDA events on its stream around its four launches (x gather,
