@@ -49,7 +49,7 @@ _SIGS = {
     "bw_last_error": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
     "bw_set_device_limit": (C.c_int, [_P, _I64]),
     "bw_plan_export": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
-    "bw_plan_split": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
+    "bw_plan_split": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "bw_set_timing": (C.c_int, [_P, C.c_int]),
     "bw_timing_read": (C.c_int, [_P, _P, _P]),
     "bw_phase_bytes": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),

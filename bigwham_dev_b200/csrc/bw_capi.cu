@@ -69,9 +69,9 @@ struct DevPhase {
   int64_t n_items = 0;
   int64_t n_elems = 0;
   int64_t n_gsegs = 0;
-  // Queue units [0, n_wide) run in the CTA-wide kernel, the rest (each of at
-  // most narrow_rows padded rows and narrow_cols columns) warp per item.
-  int64_t n_wide = 0;
+  // Queue units [0, split.wide) run in the CTA-wide kernel, the rest in the
+  // warp-per-item kernel, [split.wide, split.coop) CTA-cooperatively.
+  bw::NarrowSplit split;
 };
 
 // Device data of one matmat phase (bw::MmPlan).
@@ -457,27 +457,36 @@ void pack_phase_device(bw_hmat *h, int o, int prec, int phase, void *dst) {
   BW_CUDA(cudaDeviceSynchronize());
 }
 
-// Where a phase's queue units stop needing the CTA-wide kernel: the units are
-// in decreasing cost order, and every unit from the returned index on holds
-// only items of at most narrow_rows padded rows and narrow_cols columns
-// (small items, which run warp per item; the few large items of a 2DS0-H
-// phase 1, thousands of columns each, keep the CTA-wide kernel's pipeline).
-int64_t narrow_split(const bw::ChunkPlan &cp, const bw::Tuning &tune) {
-  const int64_t n_units = (int64_t)cp.item_ptr.size() - 1;
-  if (tune.narrow_rows <= 0 || n_units <= 0) return std::max<int64_t>(0, n_units);
-  int64_t split = 0;
+// How a phase's queue units (in decreasing cost order) divide between the
+// streaming kernels.  wide: one past the last unit with an item of more than
+// narrow_rows padded rows (those need the CTA-wide kernel's staging); coop:
+// one past the last unit with an item of more than narrow_cols columns (the
+// few long items of a phase, thousands of columns in a 2DS0-H phase 1, which
+// the warp-per-item kernel's CTAs take whole).  narrow_coop 0 sends the long
+// items to the CTA-wide kernel instead; narrow_rows 0 sends everything there.
+bw::NarrowSplit narrow_split(const bw::ChunkPlan &cp, const bw::Tuning &tune) {
+  const int64_t n_units = std::max<int64_t>(0, (int64_t)cp.item_ptr.size() - 1);
+  bw::NarrowSplit sp{n_units, n_units};
+  if (tune.narrow_rows <= 0) return sp;
+  int64_t last_tall = -1, last_long = -1;
   for (int64_t u = 0; u < n_units; u++) {
-    bool small = true;
     int64_t cols = 0;
     for (int32_t i = cp.item_ptr[u]; i < cp.item_ptr[u + 1]; i++) {
       const Chunk &c = cp.chunks[i];
       if (c.flags & bw::kFirst) cols = 0;
       cols += c.ncols;
-      if (c.hpad > tune.narrow_rows || cols > tune.narrow_cols) small = false;
+      if (c.hpad > tune.narrow_rows) last_tall = u;
+      if (cols > tune.narrow_cols) last_long = u;
     }
-    if (!small) split = u + 1;
   }
-  return split;
+  if (tune.narrow_coop) {
+    sp.wide = last_tall + 1;
+    sp.coop = std::max(sp.wide, last_long + 1);
+  } else {
+    sp.wide = std::max(last_tall, last_long) + 1;
+    sp.coop = sp.wide;
+  }
+  return sp;
 }
 
 // Upload the data of one phase in pieces through two pinned staging buffers.
@@ -490,7 +499,7 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   const bw::ChunkPlan &cp = ph.cp[prec];
   dp.n_chunks = (int64_t)cp.chunks.size();
   dp.n_gsegs = (int64_t)cp.gsegs.size();
-  dp.n_wide = narrow_split(cp, h->prob.tune);
+  dp.split = narrow_split(cp, h->prob.tune);
   if (h->plan_only) {
     auto &buf = h->host_data[o][prec][phase];
     buf.assign((size_t)ph.n_elems[prec] * es, 0);
@@ -501,8 +510,8 @@ void upload_phase(bw_hmat *h, int o, int prec, int phase) {
   dp.chunks = static_cast<Chunk *>(h->dmalloc(std::max<size_t>(1, cp.chunks.size()) * sizeof(Chunk)));
   dp.n_items = (int64_t)cp.item_ptr.size() - 1;
   dp.items = static_cast<int32_t *>(h->dmalloc(cp.item_ptr.size() * sizeof(int32_t)));
-  dp.queue = static_cast<int *>(h->dmalloc(4 * sizeof(int)));  // CTA-wide kernel, warp-per-item kernel
-  BW_CUDA(cudaMemset(dp.queue, 0, 4 * sizeof(int)));
+  dp.queue = static_cast<int *>(h->dmalloc(8 * sizeof(int)));  // CTA-wide kernel [0, 2), the other [2, 5)
+  BW_CUDA(cudaMemset(dp.queue, 0, 8 * sizeof(int)));
   if (!cp.chunks.empty())
     BW_CUDA(cudaMemcpy(dp.chunks, cp.chunks.data(), cp.chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
   BW_CUDA(cudaMemcpy(dp.items, cp.item_ptr.data(), cp.item_ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
@@ -618,14 +627,15 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
       a.err = h->d_err;
       a.spin_limit = h->spin_limit;
       a.withhold = h->take_withhold();  // the test hook applies to the CTA-wide kernel
-      if (dp.n_wide > 0) {
-        a.n_items = (int)dp.n_wide;
+      if (dp.split.wide > 0) {
+        a.n_items = (int)dp.split.wide;
         bw::stream_panels_kernel<S><<<h->grid, bw::threads_of<S>(), bw::SmemLayout<S>::kTotal, st>>>(a);
         BW_CUDA(cudaGetLastError());
       }
-      if (dp.n_wide < dp.n_items) {  // the small items, warp per item, on their own queue
-        a.item_ptr = dp.items + dp.n_wide;
-        a.n_items = (int)(dp.n_items - dp.n_wide);
+      if (dp.split.wide < dp.n_items) {  // the items of at most narrow_rows rows, on their own queue
+        a.item_ptr = dp.items + dp.split.wide;
+        a.n_items = (int)(dp.n_items - dp.split.wide);
+        a.n_coop = (int)(dp.split.coop - dp.split.wide);
         a.queue = dp.queue + 2;
         bw::narrow_items_kernel<S><<<2 * h->grid, 32 * bw::kNarrowWarps, 0, st>>>(a);
         BW_CUDA(cudaGetLastError());
@@ -784,6 +794,14 @@ int bw_set_tuning(bw_hmat *h, const char *key, int64_t value) {
       return BW_ERR_ARG;
     }
     t.narrow_rows = (int)value;
+    return BW_OK;
+  }
+  if (k == "narrow_coop") {
+    if (value < 0 || value > 1) {
+      h->err = "narrow_coop must be 0 or 1";
+      return BW_ERR_ARG;
+    }
+    t.narrow_coop = (int)value;
     return BW_OK;
   }
   if (k == "narrow_cols") {
@@ -1393,13 +1411,15 @@ int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, i
   return BW_OK;
 }
 
-int bw_plan_split(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_wide) {
-  if (!h || !n_wide || phase < 1 || phase > 2) return BW_ERR_ARG;
+int bw_plan_split(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_wide, int64_t *n_coop) {
+  if (!h || !n_wide || !n_coop || phase < 1 || phase > 2) return BW_ERR_ARG;
   const int p = prec_index(precision);
   if (p < 0 || !h->finalized || !(h->stored & (1 << p))) return BW_ERR_STATE;
   const int o = transposed ? 1 : 0;
   if (o == 1 && !h->has_t) return BW_ERR_UNSUPPORTED;
-  *n_wide = narrow_split(h->op[o].ph[phase - 1].cp[p], h->prob.tune);
+  const bw::NarrowSplit sp = narrow_split(h->op[o].ph[phase - 1].cp[p], h->prob.tune);
+  *n_wide = sp.wide;
+  *n_coop = sp.coop;
   return BW_OK;
 }
 

@@ -50,7 +50,9 @@ struct StreamArgs {
   const Chunk *chunks;        // item by item
   const int32_t *item_ptr;    // chunk ranges of the items, longest first (n_items + 1)
   int n_items;
-  int *queue;                 // [next item, CTAs done]: zero at launch, reset to zero by the last CTA
+  int n_coop;                 // warp-per-item kernel: units [0, n_coop) run CTA-cooperatively
+  int *queue;                 // [next item, CTAs done(, next CTA-cooperative unit)]: zero at launch, reset
+                              // to zero by the last CTA
   const void *gsrc;           // vector values: gathered x (phase 1) or G2 (phase 2), compute type
   void *t_out;                // phase-1 output (compute type; BF16: unscaled, G2 applies the block scales)
   double *y_out;              // phase-2 output
@@ -712,18 +714,22 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
 }
 
 // ----------------------------------------------------------------------------- narrow phases
-// Phases whose items all have at most kNarrowRows padded rows (the row panels
-// and B stacks of 2DS0-H matrices, 8 to 64 rows) run warp per item instead:
-// a warp takes an item from the queue, walks its chunks with ordinary 16-byte
-// loads straight from global memory (no staging), keeps every row of the
-// item in registers and writes the item's outputs itself.  The CTA-wide
-// kernel above spends a fixed ~1.3 us per chunk on such items (every consumer
-// warp takes part in every chunk's barrier round trip and in every item's
-// shared-memory reduction, measured with per-chunk clock stamps on the
-// 48 x 2DS0 batch); here nothing is shared between warps and 32 items are in
-// flight per SM.  The chunk descriptors, the data layout and the vector
-// sources are the ones the CTA-wide kernel reads, and an item's arithmetic
-// does not depend on the warp that takes it.
+// Items of at most kNarrowRows padded rows (the row panels and B stacks of
+// 2DS0-H matrices, 8 to 64 rows) run without staging: ordinary 16-byte loads
+// straight from global memory, every row of the item in registers.  The
+// CTA-wide kernel above spends a fixed ~1.3 us per chunk on such items (every
+// consumer warp takes part in every chunk's barrier round trip and in every
+// item's shared-memory reduction, measured with per-chunk clock stamps on the
+// 48 x 2DS0 batch).  Two modes, one launch:
+//   * CTA-cooperative (queue units [0, n_coop), the long ones: more than one
+//     chunk of columns): the CTA's 16 warps take the unit together, each a
+//     sixteenth of its columns, and add their rows in shared memory at the
+//     unit's end, in a fixed order;
+//   * warp per item (the rest): a warp takes a unit from the queue and writes
+//     its outputs itself; nothing is shared between warps.
+// The chunk descriptors, the data layout and the vector sources are the ones
+// the CTA-wide kernel reads, and an item's arithmetic does not depend on the
+// warp or CTA that takes it.
 constexpr int kNarrowRows = 64;
 constexpr int kNarrowWarps = 16;  // per CTA; two CTAs per SM
 
@@ -732,26 +738,35 @@ __device__ __forceinline__ float unpack_hilo(uint32_t w) {
   return __uint_as_float(w << 16) + __uint_as_float(w & 0xffff0000u);
 }
 
-// One chunk of a column-major FP64 / FP32 item.  Lanes hold R = 16 / es
-// adjacent rows of one column slot; lpc lanes cover the padded rows, 32 / lpc
-// column slots run side by side.
+// Lanes of a column-major FP64 / FP32 item: R = 16 / es adjacent rows of one
+// column slot each; lpc lanes cover the padded rows (a power of two), 32 /
+// lpc column slots side by side.
+__device__ __forceinline__ int narrow_lpc(int hpad, int R) {
+  int lpc = 1;
+  while (lpc * R < hpad) lpc <<= 1;
+  return lpc;
+}
+
+// One chunk of a column-major FP64 / FP32 item.  The lane's column slot is
+// c0 + lane / lpc, and it steps by cstep columns.
 template <typename S, int R>
 __device__ __forceinline__ void narrow_fma_chunk(const unsigned char *base, const typename Store<S>::G *g, int hpad,
-                                                 int ncols, int lpc, int lane, typename Store<S>::G (&acc)[R]) {
+                                                 int ncols, int lpc, int lane, int c0, int cstep,
+                                                 typename Store<S>::G (&acc)[R]) {
   using G = typename Store<S>::G;
   using V = typename std::conditional<sizeof(G) == 8, double2, float4>::type;
-  const int cpp = 32 / lpc, slot = lane / lpc, r0 = (lane % lpc) * R;
+  const int r0 = (lane % lpc) * R;
   if (r0 >= hpad) return;
   const G *d = reinterpret_cast<const G *>(base) + r0;
-  int c = slot;
+  int c = c0 + lane / lpc;
 #pragma unroll 1
-  for (; c + 3 * cpp < ncols; c += 4 * cpp) {
+  for (; c + 3 * cstep < ncols; c += 4 * cstep) {
     V v[4];
     G x[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      v[q] = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(c + q * cpp) * hpad));
-      x[q] = __ldg(g + c + q * cpp);
+      v[q] = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(c + q * cstep) * hpad));
+      x[q] = __ldg(g + c + q * cstep);
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -760,7 +775,7 @@ __device__ __forceinline__ void narrow_fma_chunk(const unsigned char *base, cons
       for (int k = 0; k < R; k++) acc[k] = fma(e[k], x[q], acc[k]);
     }
   }
-  for (; c < ncols; c += cpp) {
+  for (; c < ncols; c += cstep) {
     const V v = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(c) * hpad));
     const G x = __ldg(g + c);
     const G *e = reinterpret_cast<const G *>(&v);
@@ -769,31 +784,213 @@ __device__ __forceinline__ void narrow_fma_chunk(const unsigned char *base, cons
   }
 }
 
-// One chunk of an 8x8-tiled BF16 item: lane (c8, slot) takes column c8 of
-// every column group and the row groups slot and slot + 4; a 16-byte load is
-// 8 rows of one column (one tile column).
+// Lanes of an 8x8-tiled BF16 item with nrg = hpad / 8 row groups: lane
+// (c8, rl, cs) = (lane % 8, (lane / 8) % rgl, lane / (8 rgl)) takes column c8
+// of its column groups and the row groups rl (and rl + 4 when nrg > 4); rgl =
+// the row-group lanes (nrg rounded up to a power of two, at most 4), and
+// 4 / rgl column groups run side by side.  A 16-byte load is 8 rows of one
+// column (one tile column).
+__device__ __forceinline__ int narrow_rgl(int hpad) {
+  const int nrg = hpad >> 3;
+  return nrg <= 1 ? 1 : nrg <= 2 ? 2 : 4;
+}
+
+// One column group of a lane of an 8x8-tiled BF16 item: x and the lane's one
+// or two 16-byte tile columns (zero past the item's columns, whose tile
+// padding is not read).
+struct Bf16Step {
+  float x;
+  uint4 w[2];
+};
+
+__device__ __forceinline__ Bf16Step bf16_step_load(const uint16_t *lb, const uint32_t *g, int hpad, int ncols, int cg,
+                                                   int c8, bool one, bool two) {
+  Bf16Step s;
+  const int c = 8 * cg + c8;
+  const bool in = c < ncols;
+  s.x = in ? unpack_hilo(__ldg(g + c)) : 0.f;
+  s.w[0] = make_uint4(0, 0, 0, 0);
+  s.w[1] = make_uint4(0, 0, 0, 0);
+  const uint16_t *col = lb + static_cast<long long>(cg) * 8 * hpad;
+  if (in && one) s.w[0] = __ldg(reinterpret_cast<const uint4 *>(col));
+  if (in && two) s.w[1] = __ldg(reinterpret_cast<const uint4 *>(col + 256));
+  return s;
+}
+
+__device__ __forceinline__ void bf16_step_fma(const Bf16Step &s, float (&acc)[2][8]) {
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const uint32_t ww[4] = {s.w[j].x, s.w[j].y, s.w[j].z, s.w[j].w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      acc[j][2 * k] = fmaf(__uint_as_float(ww[k] << 16), s.x, acc[j][2 * k]);
+      acc[j][2 * k + 1] = fmaf(__uint_as_float(ww[k] & 0xffff0000u), s.x, acc[j][2 * k + 1]);
+    }
+  }
+}
+
+// One chunk of an 8x8-tiled BF16 item.  The lane's column group is
+// g0 + cs, and it steps by gstep column groups.
 __device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
-                                                  int lane, float (&acc)[2][8]) {
-  const int c8 = lane & 7, slot = lane >> 3, nrg = hpad >> 3;
+                                                  int lane, int g0, int gstep, float (&acc)[2][8]) {
+  const int nrg = hpad >> 3, rgl = narrow_rgl(hpad);
+  const int c8 = lane & 7, rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
   const int ncg = (ncols + 7) >> 3;
-#pragma unroll 2
-  for (int cg = 0; cg < ncg; cg++) {
-    const int c = 8 * cg + c8;
-    if (c >= ncols) continue;
-    const float x = unpack_hilo(__ldg(g + c));
-    const uint16_t *col = base + static_cast<long long>(cg) * 8 * hpad + c8 * 8;
+  const bool one = rl < nrg;      // no row group 3 when nrg = 3
+  const bool two = rl + 4 < nrg;  // a second row group (nrg > 4)
+  const uint16_t *lb = base + c8 * 8 + rl * 64;
+  int cg = g0 + cs;
+#pragma unroll 1
+  for (; cg + gstep < ncg; cg += 2 * gstep) {
+    const Bf16Step s0 = bf16_step_load(lb, g, hpad, ncols, cg, c8, one, two);
+    const Bf16Step s1 = bf16_step_load(lb, g, hpad, ncols, cg + gstep, c8, one, two);
+    bf16_step_fma(s0, acc);
+    bf16_step_fma(s1, acc);
+  }
+  if (cg < ncg) bf16_step_fma(bf16_step_load(lb, g, hpad, ncols, cg, c8, one, two), acc);
+}
+
+// Sum of a lane's BF16 row partials over the column lanes; lane (c8, rl, cs =
+// 0) then holds rows (rl + 4 j) * 8 + c8 in v[j].
+__device__ __forceinline__ void narrow_bf16_rows(float (&acc)[2][8], int hpad, int lane, float (&v)[2]) {
+  const int rgl = narrow_rgl(hpad), c8 = lane & 7;
 #pragma unroll
-    for (int j = 0; j < 2; j++) {
-      const int rg = slot + 4 * j;
-      if (rg < nrg) {
-        const uint4 w = __ldg(reinterpret_cast<const uint4 *>(col + rg * 64));
-        const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
+  for (int j = 0; j < 2; j++)
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          acc[j][2 * k] = fmaf(__uint_as_float(ww[k] << 16), x, acc[j][2 * k]);
-          acc[j][2 * k + 1] = fmaf(__uint_as_float(ww[k] & 0xffff0000u), x, acc[j][2 * k + 1]);
+    for (int k = 0; k < 8; k++) {
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
+      for (int o = 8 * rgl; o < 32; o <<= 1) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
+    }
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    v[j] = acc[j][0];
+#pragma unroll
+    for (int k = 1; k < 8; k++)
+      if (c8 == k) v[j] = acc[j][k];
+  }
+}
+
+template <typename G>
+__device__ __forceinline__ void narrow_store(const StreamArgs &a, int out_off, int r, G v) {
+  if (a.phase == 1) {
+    static_cast<G *>(a.t_out)[out_off + r] = v;
+  } else {
+    const int row = out_off + r;
+    a.y_out[a.perm_out ? static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof) : row] =
+        static_cast<double>(v);
+  }
+}
+
+struct NarrowChunk {
+  long long data_off;
+  int ncols, hpad, rows, out_off, g_off;
+  uint32_t flags;
+};
+
+__device__ __forceinline__ NarrowChunk narrow_desc(const Chunk *chunks, int i) {
+  const uint4 *dp = reinterpret_cast<const uint4 *>(chunks + i);
+  const uint4 w0 = __ldg(dp), w1 = __ldg(dp + 1);
+  NarrowChunk c;
+  c.data_off = static_cast<long long>((static_cast<unsigned long long>(w0.y) << 32) | w0.x);
+  c.ncols = static_cast<int>(w0.z);
+  c.hpad = static_cast<int>(w0.w);
+  c.rows = static_cast<int>(w1.x);
+  c.out_off = static_cast<int>(w1.y);
+  c.flags = w1.z;
+  c.g_off = static_cast<int>(w1.w);
+  return c;
+}
+
+// Walks the chunks [cb, ce) of one queue unit.  Warp-per-item mode: wid = 0,
+// nw = 1, red = null.  CTA-cooperative mode: the CTA's nw warps walk the same
+// chunks, warp wid takes every nw-th column slot (column group for BF16), and
+// at each item's last chunk the warps' rows meet in red (nw x kNarrowRows)
+// and are summed in warp order; every thread of the CTA must call it.
+template <typename S>
+__device__ __forceinline__ void narrow_unit(const StreamArgs &a, int cb, int ce, int lane, int wid, int nw,
+                                            typename Store<S>::G *red) {
+  using G = typename Store<S>::G;
+  constexpr int es = Store<S>::kEsize;
+  constexpr bool kTensor = Store<S>::kRows == 0;
+  constexpr int R = kTensor ? 1 : 16 / es;
+  const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
+  G acc[R];
+  float tacc[2][8];
+  for (int i = cb; i < ce; i++) {
+    NarrowChunk d = narrow_desc(a.chunks, i);
+    const bool bad = d.hpad <= 0 || d.hpad > kNarrowRows || (d.hpad & 7) || d.ncols < 0 || d.ncols > kMaxCols ||
+                     d.rows < 0 || d.rows > d.hpad;
+    if (bad) {  // uniform over the CTA: every warp reads the same descriptor
+      if (threadIdx.x == 0 || (red == nullptr && lane == 0)) set_error(a.err, kErrBadChunk);
+      d.ncols = 0;
+      d.hpad = 8;
+      d.rows = 0;
+    }
+    if (d.flags & kFirst) {
+#pragma unroll
+      for (int k = 0; k < R; k++) acc[k] = 0;
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) tacc[j][k] = 0.f;
+    }
+    if constexpr (kTensor) {
+      const int gpw = 4 / narrow_rgl(d.hpad);  // column groups per warp step
+      narrow_bf16_chunk(reinterpret_cast<const uint16_t *>(gdata) + d.data_off,
+                        static_cast<const uint32_t *>(a.gsrc) + d.g_off, d.hpad, d.ncols, lane, wid * gpw, nw * gpw,
+                        tacc);
+    } else {
+      const int lpc = narrow_lpc(d.hpad, R), cpp = 32 / lpc;
+      narrow_fma_chunk<S, R>(gdata + d.data_off * es, static_cast<const G *>(a.gsrc) + d.g_off, d.hpad, d.ncols,
+                             lpc, lane, wid * cpp, nw * cpp, acc);
+    }
+    if (!(d.flags & kLast)) continue;
+    // the item's rows: sums over the warp's column lanes, then (CTA mode)
+    // over the warps in shared memory
+    if constexpr (kTensor) {
+      float v[2];
+      narrow_bf16_rows(tacc, d.hpad, lane, v);
+      const int rgl = narrow_rgl(d.hpad), rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
+      if (cs == 0) {
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+          const int r = (rl + 4 * j) * 8 + (lane & 7);
+          if (r < d.hpad && (j == 0 || rl + 4 < (d.hpad >> 3))) {
+            if (red)
+              red[wid * kNarrowRows + r] = v[j];
+            else if (r < d.rows)
+              narrow_store<G>(a, d.out_off, r, v[j]);
+          }
         }
       }
+    } else {
+      const int lpc = narrow_lpc(d.hpad, R);
+      for (int o = lpc; o < 32; o <<= 1)
+#pragma unroll
+        for (int k = 0; k < R; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+      if (lane < lpc) {
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+          const int r = lane * R + k;
+          if (r < d.hpad) {
+            if (red)
+              red[wid * kNarrowRows + r] = acc[k];
+            else if (r < d.rows)
+              narrow_store<G>(a, d.out_off, r, acc[k]);
+          }
+        }
+      }
+    }
+    if (red) {
+      __syncthreads();
+      const int r = threadIdx.x;
+      if (r < d.rows) {
+        G sum = red[r];
+        for (int w = 1; w < nw; w++) sum += red[w * kNarrowRows + r];
+        narrow_store<G>(a, d.out_off, r, sum);
+      }
+      __syncthreads();
     }
   }
 }
@@ -801,106 +998,34 @@ __device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const ui
 template <typename S>
 __global__ void __launch_bounds__(32 * kNarrowWarps, 2) narrow_items_kernel(StreamArgs a) {
   using G = typename Store<S>::G;
-  constexpr int es = Store<S>::kEsize;
-  constexpr bool kTensor = Store<S>::kRows == 0;
-  constexpr int R = kTensor ? 1 : 16 / es;
-  const int lane = threadIdx.x & 31;
-  const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
+  __shared__ G red[kNarrowWarps * kNarrowRows];
+  __shared__ int unit;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // queue units [0, n_coop): the whole CTA per unit (queue[2] counts them)
+  for (;;) {
+    if (threadIdx.x == 0) unit = atomicAdd(&a.queue[2], 1);
+    __syncthreads();
+    const int u = unit;
+    __syncthreads();
+    if (u >= a.n_coop) break;
+    narrow_unit<S>(a, __ldg(a.item_ptr + u), __ldg(a.item_ptr + u + 1), lane, wid, kNarrowWarps, red);
+  }
+  // the rest: warp per unit (queue[0] counts them)
   for (;;) {
     int it = 0;
-    if (lane == 0) it = atomicAdd(&a.queue[0], 1);
+    if (lane == 0) it = a.n_coop + atomicAdd(&a.queue[0], 1);
     it = __shfl_sync(0xffffffffu, it, 0);
     if (it >= a.n_items) break;
-    const int cb = __ldg(a.item_ptr + it), ce = __ldg(a.item_ptr + it + 1);
-    G acc[R];
-    float tacc[2][8];
-    for (int i = cb; i < ce; i++) {
-      const uint4 *dp = reinterpret_cast<const uint4 *>(a.chunks + i);
-      const uint4 w0 = __ldg(dp), w1 = __ldg(dp + 1);
-      const long long data_off = static_cast<long long>((static_cast<unsigned long long>(w0.y) << 32) | w0.x);
-      const int ncols = static_cast<int>(w0.z), hpad = static_cast<int>(w0.w);
-      const int rows = static_cast<int>(w1.x), out_off = static_cast<int>(w1.y);
-      const uint32_t flags = w1.z;
-      const int g_off = static_cast<int>(w1.w);
-      if (hpad <= 0 || hpad > kNarrowRows || ncols < 0 || ncols > kMaxCols) {
-        if (lane == 0) set_error(a.err, kErrBadChunk);
-        continue;
-      }
-      if (flags & kFirst) {
-#pragma unroll
-        for (int k = 0; k < R; k++) acc[k] = 0;
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-#pragma unroll
-          for (int k = 0; k < 8; k++) tacc[j][k] = 0.f;
-      }
-      if constexpr (kTensor) {
-        narrow_bf16_chunk(reinterpret_cast<const uint16_t *>(gdata) + data_off,
-                          static_cast<const uint32_t *>(a.gsrc) + g_off, hpad, ncols, lane, tacc);
-      } else {
-        int lpc = 1;
-        while (lpc * R < hpad) lpc <<= 1;
-        narrow_fma_chunk<S, R>(gdata + data_off * es, static_cast<const G *>(a.gsrc) + g_off, hpad, ncols, lpc,
-                               lane, acc);
-      }
-      if (!(flags & kLast)) continue;
-      // the item's outputs: sums over the column slots, then one store per row
-      if constexpr (kTensor) {
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-#pragma unroll
-          for (int k = 0; k < 8; k++)
-#pragma unroll
-            for (int o = 1; o < 8; o <<= 1) tacc[j][k] += __shfl_xor_sync(0xffffffffu, tacc[j][k], o);
-        const int c8 = lane & 7, slot = lane >> 3;
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-          float v = tacc[j][0];
-#pragma unroll
-          for (int k = 1; k < 8; k++)
-            if (c8 == k) v = tacc[j][k];
-          const int r = (slot + 4 * j) * 8 + c8;
-          if (r < rows) {
-            if (a.phase == 1) {
-              static_cast<G *>(a.t_out)[out_off + r] = v;
-            } else {
-              const int row = out_off + r;
-              a.y_out[a.perm_out ? static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof) : row] =
-                  static_cast<double>(v);
-            }
-          }
-        }
-      } else {
-        int lpc = 1;
-        while (lpc * R < hpad) lpc <<= 1;
-        for (int o = lpc; o < 32; o <<= 1)
-#pragma unroll
-          for (int k = 0; k < R; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-        if (lane < lpc) {
-#pragma unroll
-          for (int k = 0; k < R; k++) {
-            const int r = lane * R + k;
-            if (r < rows) {
-              if (a.phase == 1) {
-                static_cast<G *>(a.t_out)[out_off + r] = acc[k];
-              } else {
-                const int row = out_off + r;
-                a.y_out[a.perm_out ? static_cast<long long>(a.dof) * a.perm_out[row / a.dof] + (row % a.dof) : row] =
-                    static_cast<double>(acc[k]);
-              }
-            }
-          }
-        }
-      }
-    }
+    narrow_unit<S>(a, __ldg(a.item_ptr + it), __ldg(a.item_ptr + it + 1), lane, 0, 1, nullptr);
   }
-  // This CTA takes no more items; the last CTA returns the queue to zero.
+  // This CTA takes no more units; the last CTA returns the queue to zero.
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     if (atomicAdd(&a.queue[1], 1) == static_cast<int>(gridDim.x) - 1) {
       a.queue[0] = 0;
       a.queue[1] = 0;
+      a.queue[2] = 0;
       __threadfence();
     }
   }

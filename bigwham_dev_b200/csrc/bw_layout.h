@@ -156,8 +156,15 @@ struct Tuning {
   int chunk_bytes = kStageBytes;                        // block data per chunk (<= kStageBytes)
   int mm_items_per_cta = kItemsPerCta;                  // matmat phase 1
   int unit_bytes = kUnitBytes;                          // streaming queue: minimum cost of a unit
-  int narrow_rows = 64;   // small items: at most this many padded rows (0: no warp-per-item launches) ...
-  int narrow_cols = 512;  // ... and this many columns; they run warp per item
+  int narrow_rows = 64;   // items of at most this many padded rows skip the staging (0: never) ...
+  int narrow_cols = 512;  // ... warp per item up to this many columns, CTA-cooperatively above
+  int narrow_coop = 1;    // 0: items above narrow_cols columns stay in the CTA-wide kernel
+};
+
+// Queue units [0, wide) of a phase run in the CTA-wide kernel; of the rest,
+// [wide, coop) CTA-cooperatively and [coop, end) warp per item.
+struct NarrowSplit {
+  int64_t wide = 0, coop = 0;
 };
 
 struct Problem {

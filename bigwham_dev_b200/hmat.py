@@ -117,7 +117,8 @@ class HmatGpu:
 
     def set_tuning(self, **kw) -> "HmatGpu":
         """Plan parameters (bw_set_tuning), before finalize: items_per_cta_phase1,
-        items_per_cta_phase2, chunk_bytes, mm_items_per_cta, unit_bytes, narrow_rows, narrow_cols."""
+        items_per_cta_phase2, chunk_bytes, mm_items_per_cta, unit_bytes, narrow_rows, narrow_cols,
+        narrow_coop."""
         for k, v in kw.items():
             A.check(self._lib.bw_set_tuning(self._h, k.encode(), int(v)), self._h)
         return self
@@ -380,9 +381,11 @@ class HmatGpu:
         A.check(self._lib.bw_plan_export(self._h, f, phase, int(transposed), C.byref(nc), chunks.ctypes.data,
                                          C.byref(ne), data.ctypes.data if with_data else None, C.byref(nt),
                                          items.ctypes.data), self._h)
-        n_wide = C.c_int64()
-        A.check(self._lib.bw_plan_split(self._h, f, phase, int(transposed), C.byref(n_wide)), self._h)
-        return {"chunks": chunks, "item_ptr": items, "data": data, "n_wide": int(n_wide.value)}
+        n_wide, n_coop = C.c_int64(), C.c_int64()
+        A.check(self._lib.bw_plan_split(self._h, f, phase, int(transposed), C.byref(n_wide), C.byref(n_coop)),
+                self._h)
+        return {"chunks": chunks, "item_ptr": items, "data": data, "n_wide": int(n_wide.value),
+                "n_coop": int(n_coop.value)}
 
     def set_timing(self, enable: bool = True) -> None:
         """Record CUDA events around each launch of every following matvec."""

@@ -113,12 +113,14 @@ int bw_test_withhold_chunk(bw_hmat *h, int index);
  *   "unit_bytes": the streaming queue hands out runs of consecutive items
  *       until a run's cost reaches this many bytes (0: one item at a time),
  *       0..2^30, default 0;
- *   "narrow_rows", "narrow_cols": the small items of a phase (at most
- *       narrow_rows padded rows, 0..64, default 64, and narrow_cols columns,
- *       default 512), those after the last larger item in the queue's
- *       cost order, run warp per item (no staging, no cross-warp reduction)
- *       in a second launch; narrow_rows 0 keeps every item in the CTA-wide
- *       kernel.
+ *   "narrow_rows", "narrow_cols", "narrow_coop": the items of a phase
+ *       after its last item of more than narrow_rows padded rows (0..64,
+ *       default 64) in the queue's cost order skip the staging: they run in a
+ *       second launch with direct loads, a CTA per item up to the last item
+ *       of more than narrow_cols columns (default 512), warp per item after
+ *       it.  narrow_coop 0 (default 1) keeps the items above narrow_cols
+ *       columns in the CTA-wide kernel; narrow_rows 0 keeps every item
+ *       there.
  * Results do not depend on them (each item is reduced in a fixed order).
  * BW_ERR_ARG for an unknown key or a value out of range. */
 int bw_set_tuning(bw_hmat *h, const char *key, int64_t value);
@@ -269,8 +271,9 @@ int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, i
 
 /* How one phase's items divide between the two streaming kernels: items
  * [0, n_wide) of bw_plan_export's item order run in the CTA-wide kernel, the
- * rest warp per item (see the "narrow_rows" tuning key). */
-int bw_plan_split(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_wide);
+ * rest in the unstaged kernel, [n_wide, n_coop) a CTA per item and the rest
+ * warp per item (the "narrow_*" tuning keys). */
+int bw_plan_split(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_wide, int64_t *n_coop);
 
 /* Per-launch timing for benchmarks.  With timing enabled every bw_matvec
  * records CUDA events on its stream around its four launches (x gather,
