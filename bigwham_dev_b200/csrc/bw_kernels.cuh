@@ -757,19 +757,20 @@ __device__ __forceinline__ void narrow_fma_chunk(const unsigned char *base, cons
   using V = typename std::conditional<sizeof(G) == 8, double2, float4>::type;
   const int r0 = (lane % lpc) * R;
   if (r0 >= hpad) return;
+  constexpr int kAhead = sizeof(G) == 8 ? 4 : 8;  // 16-byte loads in flight per lane
   const G *d = reinterpret_cast<const G *>(base) + r0;
   int c = c0 + lane / lpc;
 #pragma unroll 1
-  for (; c + 3 * cstep < ncols; c += 4 * cstep) {
-    V v[4];
-    G x[4];
+  for (; c + (kAhead - 1) * cstep < ncols; c += kAhead * cstep) {
+    V v[kAhead];
+    G x[kAhead];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < kAhead; q++) {
       v[q] = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(c + q * cstep) * hpad));
       x[q] = __ldg(g + c + q * cstep);
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < kAhead; q++) {
       const G *e = reinterpret_cast<const G *>(&v[q]);
 #pragma unroll
       for (int k = 0; k < R; k++) acc[k] = fma(e[k], x[q], acc[k]);
@@ -817,9 +818,10 @@ __device__ __forceinline__ Bf16Step bf16_step_load(const uint16_t *lb, const uin
   return s;
 }
 
+template <bool kTwo>
 __device__ __forceinline__ void bf16_step_fma(const Bf16Step &s, float (&acc)[2][8]) {
 #pragma unroll
-  for (int j = 0; j < 2; j++) {
+  for (int j = 0; j < (kTwo ? 2 : 1); j++) {
     const uint32_t ww[4] = {s.w[j].x, s.w[j].y, s.w[j].z, s.w[j].w};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -830,24 +832,38 @@ __device__ __forceinline__ void bf16_step_fma(const Bf16Step &s, float (&acc)[2]
 }
 
 // One chunk of an 8x8-tiled BF16 item.  The lane's column group is
-// g0 + cs, and it steps by gstep column groups.
-__device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
-                                                  int lane, int g0, int gstep, float (&acc)[2][8]) {
+// g0 + cs, and it steps by gstep column groups.  Items of at most 4 row
+// groups load one tile column per lane and column group, so four column
+// groups are loaded ahead; items of 5 to 8 row groups load two, so two.
+template <bool kTwo>
+__device__ __forceinline__ void narrow_bf16_chunk_t(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
+                                                    int lane, int g0, int gstep, float (&acc)[2][8]) {
+  constexpr int kAhead = kTwo ? 2 : 4;
   const int nrg = hpad >> 3, rgl = narrow_rgl(hpad);
   const int c8 = lane & 7, rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
   const int ncg = (ncols + 7) >> 3;
-  const bool one = rl < nrg;      // no row group 3 when nrg = 3
-  const bool two = rl + 4 < nrg;  // a second row group (nrg > 4)
+  const bool one = rl < nrg;               // no row group 3 when nrg = 3
+  const bool two = kTwo && rl + 4 < nrg;  // a second row group
   const uint16_t *lb = base + c8 * 8 + rl * 64;
   int cg = g0 + cs;
 #pragma unroll 1
-  for (; cg + gstep < ncg; cg += 2 * gstep) {
-    const Bf16Step s0 = bf16_step_load(lb, g, hpad, ncols, cg, c8, one, two);
-    const Bf16Step s1 = bf16_step_load(lb, g, hpad, ncols, cg + gstep, c8, one, two);
-    bf16_step_fma(s0, acc);
-    bf16_step_fma(s1, acc);
+  for (; cg + (kAhead - 1) * gstep < ncg; cg += kAhead * gstep) {
+    Bf16Step st[kAhead];
+#pragma unroll
+    for (int q = 0; q < kAhead; q++) st[q] = bf16_step_load(lb, g, hpad, ncols, cg + q * gstep, c8, one, two);
+#pragma unroll
+    for (int q = 0; q < kAhead; q++) bf16_step_fma<kTwo>(st[q], acc);
   }
-  if (cg < ncg) bf16_step_fma(bf16_step_load(lb, g, hpad, ncols, cg, c8, one, two), acc);
+#pragma unroll 1
+  for (; cg < ncg; cg += gstep) bf16_step_fma<kTwo>(bf16_step_load(lb, g, hpad, ncols, cg, c8, one, two), acc);
+}
+
+__device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
+                                                  int lane, int g0, int gstep, float (&acc)[2][8]) {
+  if (hpad > 32)
+    narrow_bf16_chunk_t<true>(base, g, hpad, ncols, lane, g0, gstep, acc);
+  else
+    narrow_bf16_chunk_t<false>(base, g, hpad, ncols, lane, g0, gstep, acc);
 }
 
 // Sum of a lane's BF16 row partials over the column lanes; lane (c8, rl, cs =
