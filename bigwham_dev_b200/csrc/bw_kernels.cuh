@@ -722,14 +722,17 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
 // item's shared-memory reduction, measured with per-chunk clock stamps on the
 // 48 x 2DS0 batch).  Two modes, one launch:
 //   * CTA-cooperative (queue units [0, n_coop), the long ones: more than one
-//     chunk of columns): the CTA's 16 warps take the unit together, each a
-//     sixteenth of its columns, and add their rows in shared memory at the
-//     unit's end, in a fixed order;
-//   * warp per item (the rest): a warp takes a unit from the queue and writes
+//     chunk of columns): the CTA's 16 warps take the unit's chunks round
+//     robin, and the warps' rows of each item are added in shared memory, in
+//     warp order;
+//   * warp per unit (the rest): a warp takes a unit from the queue and writes
 //     its outputs itself; nothing is shared between warps.
-// The chunk descriptors, the data layout and the vector sources are the ones
-// the CTA-wide kernel reads, and an item's arithmetic does not depend on the
-// warp or CTA that takes it.
+// A warp walks a chunk in rounds: each lane issues all of a round's loads
+// (the ones past the chunk's columns predicated off) before it uses any, so
+// short chunks keep as many bytes in flight as long ones.  The chunk
+// descriptors, the data layout and the vector sources are the ones the
+// CTA-wide kernel reads, and an item's arithmetic does not depend on the warp
+// or CTA that takes it.
 constexpr int kNarrowRows = 64;
 constexpr int kNarrowWarps = 16;  // per CTA; two CTAs per SM
 
@@ -747,27 +750,31 @@ __device__ __forceinline__ int narrow_lpc(int hpad, int R) {
   return lpc;
 }
 
-// One chunk of a column-major FP64 / FP32 item.  The lane's column slot is
-// c0 + lane / lpc, and it steps by cstep columns.
+// One chunk of a column-major FP64 / FP32 item: lane (slot, r0) takes columns
+// slot, slot + cpp, ... in rounds of kAhead.
 template <typename S, int R>
 __device__ __forceinline__ void narrow_fma_chunk(const unsigned char *base, const typename Store<S>::G *g, int hpad,
-                                                 int ncols, int lpc, int lane, int c0, int cstep,
-                                                 typename Store<S>::G (&acc)[R]) {
+                                                 int ncols, int lpc, int lane, typename Store<S>::G (&acc)[R]) {
   using G = typename Store<S>::G;
   using V = typename std::conditional<sizeof(G) == 8, double2, float4>::type;
-  const int r0 = (lane % lpc) * R;
+  constexpr int kAhead = sizeof(G) == 8 ? 4 : 6;  // 16-byte loads in flight per lane
+  const int r0 = (lane % lpc) * R, cpp = 32 / lpc;
   if (r0 >= hpad) return;
-  constexpr int kAhead = sizeof(G) == 8 ? 4 : 8;  // 16-byte loads in flight per lane
   const G *d = reinterpret_cast<const G *>(base) + r0;
-  int c = c0 + lane / lpc;
 #pragma unroll 1
-  for (; c + (kAhead - 1) * cstep < ncols; c += kAhead * cstep) {
+  for (int c = lane / lpc; c < ncols; c += kAhead * cpp) {
     V v[kAhead];
     G x[kAhead];
 #pragma unroll
     for (int q = 0; q < kAhead; q++) {
-      v[q] = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(c + q * cstep) * hpad));
-      x[q] = __ldg(g + c + q * cstep);
+      const int cq = c + q * cpp;
+      if (cq < ncols) {
+        v[q] = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(cq) * hpad));
+        x[q] = __ldg(g + cq);
+      } else {
+        v[q] = V{};
+        x[q] = 0;
+      }
     }
 #pragma unroll
     for (int q = 0; q < kAhead; q++) {
@@ -775,13 +782,6 @@ __device__ __forceinline__ void narrow_fma_chunk(const unsigned char *base, cons
 #pragma unroll
       for (int k = 0; k < R; k++) acc[k] = fma(e[k], x[q], acc[k]);
     }
-  }
-  for (; c < ncols; c += cstep) {
-    const V v = __ldg(reinterpret_cast<const V *>(d + static_cast<long long>(c) * hpad));
-    const G x = __ldg(g + c);
-    const G *e = reinterpret_cast<const G *>(&v);
-#pragma unroll
-    for (int k = 0; k < R; k++) acc[k] = fma(e[k], x, acc[k]);
   }
 }
 
@@ -796,74 +796,45 @@ __device__ __forceinline__ int narrow_rgl(int hpad) {
   return nrg <= 1 ? 1 : nrg <= 2 ? 2 : 4;
 }
 
-// One column group of a lane of an 8x8-tiled BF16 item: x and the lane's one
-// or two 16-byte tile columns (zero past the item's columns, whose tile
-// padding is not read).
-struct Bf16Step {
-  float x;
-  uint4 w[2];
-};
-
-__device__ __forceinline__ Bf16Step bf16_step_load(const uint16_t *lb, const uint32_t *g, int hpad, int ncols, int cg,
-                                                   int c8, bool one, bool two) {
-  Bf16Step s;
-  const int c = 8 * cg + c8;
-  const bool in = c < ncols;
-  s.x = in ? unpack_hilo(__ldg(g + c)) : 0.f;
-  s.w[0] = make_uint4(0, 0, 0, 0);
-  s.w[1] = make_uint4(0, 0, 0, 0);
-  const uint16_t *col = lb + static_cast<long long>(cg) * 8 * hpad;
-  if (in && one) s.w[0] = __ldg(reinterpret_cast<const uint4 *>(col));
-  if (in && two) s.w[1] = __ldg(reinterpret_cast<const uint4 *>(col + 256));
-  return s;
-}
-
-template <bool kTwo>
-__device__ __forceinline__ void bf16_step_fma(const Bf16Step &s, float (&acc)[2][8]) {
-#pragma unroll
-  for (int j = 0; j < (kTwo ? 2 : 1); j++) {
-    const uint32_t ww[4] = {s.w[j].x, s.w[j].y, s.w[j].z, s.w[j].w};
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      acc[j][2 * k] = fmaf(__uint_as_float(ww[k] << 16), s.x, acc[j][2 * k]);
-      acc[j][2 * k + 1] = fmaf(__uint_as_float(ww[k] & 0xffff0000u), s.x, acc[j][2 * k + 1]);
-    }
-  }
-}
-
-// One chunk of an 8x8-tiled BF16 item.  The lane's column group is
-// g0 + cs, and it steps by gstep column groups.  Items of at most 4 row
-// groups load one tile column per lane and column group, so four column
-// groups are loaded ahead; items of 5 to 8 row groups load two, so two.
+// One chunk of an 8x8-tiled BF16 item: lane (c8, rl, cs) takes column groups
+// cs, cs + gpw, ... in rounds of kAhead.  Items of at most 4 row groups load
+// one tile column per lane and column group (four column groups a round),
+// items of 5 to 8 row groups two (two a round).
 template <bool kTwo>
 __device__ __forceinline__ void narrow_bf16_chunk_t(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
-                                                    int lane, int g0, int gstep, float (&acc)[2][8]) {
+                                                    int lane, float (&acc)[2][8]) {
   constexpr int kAhead = kTwo ? 2 : 4;
-  const int nrg = hpad >> 3, rgl = narrow_rgl(hpad);
+  const int nrg = hpad >> 3, rgl = narrow_rgl(hpad), gpw = 4 / rgl;
   const int c8 = lane & 7, rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
   const int ncg = (ncols + 7) >> 3;
   const bool one = rl < nrg;               // no row group 3 when nrg = 3
   const bool two = kTwo && rl + 4 < nrg;  // a second row group
   const uint16_t *lb = base + c8 * 8 + rl * 64;
-  int cg = g0 + cs;
 #pragma unroll 1
-  for (; cg + (kAhead - 1) * gstep < ncg; cg += kAhead * gstep) {
-    Bf16Step st[kAhead];
+  for (int cg = cs; cg < ncg; cg += kAhead * gpw) {
+    float x[kAhead];
+    uint4 w[kAhead][kTwo ? 2 : 1];
 #pragma unroll
-    for (int q = 0; q < kAhead; q++) st[q] = bf16_step_load(lb, g, hpad, ncols, cg + q * gstep, c8, one, two);
+    for (int q = 0; q < kAhead; q++) {
+      const int cq = cg + q * gpw, c = 8 * cq + c8;
+      const bool in = cq < ncg && c < ncols;  // the tile's padding columns are not read
+      const uint16_t *col = lb + static_cast<long long>(cq) * 8 * hpad;
+      x[q] = in ? unpack_hilo(__ldg(g + c)) : 0.f;
+      w[q][0] = in && one ? __ldg(reinterpret_cast<const uint4 *>(col)) : make_uint4(0, 0, 0, 0);
+      if constexpr (kTwo) w[q][1] = in && two ? __ldg(reinterpret_cast<const uint4 *>(col + 256)) : make_uint4(0, 0, 0, 0);
+    }
 #pragma unroll
-    for (int q = 0; q < kAhead; q++) bf16_step_fma<kTwo>(st[q], acc);
+    for (int q = 0; q < kAhead; q++)
+#pragma unroll
+      for (int j = 0; j < (kTwo ? 2 : 1); j++) {
+        const uint32_t ww[4] = {w[q][j].x, w[q][j].y, w[q][j].z, w[q][j].w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          acc[j][2 * k] = fmaf(__uint_as_float(ww[k] << 16), x[q], acc[j][2 * k]);
+          acc[j][2 * k + 1] = fmaf(__uint_as_float(ww[k] & 0xffff0000u), x[q], acc[j][2 * k + 1]);
+        }
+      }
   }
-#pragma unroll 1
-  for (; cg < ncg; cg += gstep) bf16_step_fma<kTwo>(bf16_step_load(lb, g, hpad, ncols, cg, c8, one, two), acc);
-}
-
-__device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
-                                                  int lane, int g0, int gstep, float (&acc)[2][8]) {
-  if (hpad > 32)
-    narrow_bf16_chunk_t<true>(base, g, hpad, ncols, lane, g0, gstep, acc);
-  else
-    narrow_bf16_chunk_t<false>(base, g, hpad, ncols, lane, g0, gstep, acc);
 }
 
 // Sum of a lane's BF16 row partials over the column lanes; lane (c8, rl, cs =
@@ -904,8 +875,10 @@ struct NarrowChunk {
   uint32_t flags;
 };
 
-__device__ __forceinline__ NarrowChunk narrow_desc(const Chunk *chunks, int i) {
-  const uint4 *dp = reinterpret_cast<const uint4 *>(chunks + i);
+// Descriptor of chunk i; a malformed one (rows, columns or padded rows out of
+// the kernel's range) sets the error word and reads as an empty chunk.
+__device__ __forceinline__ NarrowChunk narrow_desc(const StreamArgs &a, int i, bool report) {
+  const uint4 *dp = reinterpret_cast<const uint4 *>(a.chunks + i);
   const uint4 w0 = __ldg(dp), w1 = __ldg(dp + 1);
   NarrowChunk c;
   c.data_off = static_cast<long long>((static_cast<unsigned long long>(w0.y) << 32) | w0.x);
@@ -915,99 +888,118 @@ __device__ __forceinline__ NarrowChunk narrow_desc(const Chunk *chunks, int i) {
   c.out_off = static_cast<int>(w1.y);
   c.flags = w1.z;
   c.g_off = static_cast<int>(w1.w);
+  if (c.hpad <= 0 || c.hpad > kNarrowRows || (c.hpad & 7) || c.ncols < 0 || c.ncols > kMaxCols || c.rows < 0 ||
+      c.rows > c.hpad) {
+    if (report) set_error(a.err, kErrBadChunk);
+    c.ncols = 0;
+    c.hpad = 8;
+    c.rows = 0;
+  }
   return c;
 }
 
-// Walks the chunks [cb, ce) of one queue unit.  Warp-per-item mode: wid = 0,
-// nw = 1, red = null.  CTA-cooperative mode: the CTA's nw warps walk the same
-// chunks, warp wid takes every nw-th column slot (column group for BF16), and
-// at each item's last chunk the warps' rows meet in red (nw x kNarrowRows)
-// and are summed in warp order; every thread of the CTA must call it.
+// Per-lane partial rows of an item: R rows (FP64 / FP32) or 2 x 8 (BF16).
 template <typename S>
-__device__ __forceinline__ void narrow_unit(const StreamArgs &a, int cb, int ce, int lane, int wid, int nw,
-                                            typename Store<S>::G *red) {
-  using G = typename Store<S>::G;
-  constexpr int es = Store<S>::kEsize;
-  constexpr bool kTensor = Store<S>::kRows == 0;
-  constexpr int R = kTensor ? 1 : 16 / es;
-  const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
-  G acc[R];
+struct NarrowAcc {
+  static constexpr bool kTensor = Store<S>::kRows == 0;
+  static constexpr int R = kTensor ? 1 : 16 / Store<S>::kEsize;
+  typename Store<S>::G acc[R];
   float tacc[2][8];
-  for (int i = cb; i < ce; i++) {
-    NarrowChunk d = narrow_desc(a.chunks, i);
-    const bool bad = d.hpad <= 0 || d.hpad > kNarrowRows || (d.hpad & 7) || d.ncols < 0 || d.ncols > kMaxCols ||
-                     d.rows < 0 || d.rows > d.hpad;
-    if (bad) {  // uniform over the CTA: every warp reads the same descriptor
-      if (threadIdx.x == 0 || (red == nullptr && lane == 0)) set_error(a.err, kErrBadChunk);
-      d.ncols = 0;
-      d.hpad = 8;
-      d.rows = 0;
-    }
-    if (d.flags & kFirst) {
+  __device__ __forceinline__ void zero() {
 #pragma unroll
-      for (int k = 0; k < R; k++) acc[k] = 0;
+    for (int k = 0; k < R; k++) acc[k] = 0;
 #pragma unroll
-      for (int j = 0; j < 2; j++)
+    for (int j = 0; j < 2; j++)
 #pragma unroll
-        for (int k = 0; k < 8; k++) tacc[j][k] = 0.f;
-    }
+      for (int k = 0; k < 8; k++) tacc[j][k] = 0.f;
+  }
+  __device__ __forceinline__ void add_chunk(const StreamArgs &a, const NarrowChunk &d, int lane) {
+    using G = typename Store<S>::G;
+    const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
     if constexpr (kTensor) {
-      const int gpw = 4 / narrow_rgl(d.hpad);  // column groups per warp step
-      narrow_bf16_chunk(reinterpret_cast<const uint16_t *>(gdata) + d.data_off,
-                        static_cast<const uint32_t *>(a.gsrc) + d.g_off, d.hpad, d.ncols, lane, wid * gpw, nw * gpw,
-                        tacc);
+      const uint16_t *base = reinterpret_cast<const uint16_t *>(gdata) + d.data_off;
+      const uint32_t *g = static_cast<const uint32_t *>(a.gsrc) + d.g_off;
+      if (d.hpad > 32)
+        narrow_bf16_chunk_t<true>(base, g, d.hpad, d.ncols, lane, tacc);
+      else
+        narrow_bf16_chunk_t<false>(base, g, d.hpad, d.ncols, lane, tacc);
     } else {
-      const int lpc = narrow_lpc(d.hpad, R), cpp = 32 / lpc;
-      narrow_fma_chunk<S, R>(gdata + d.data_off * es, static_cast<const G *>(a.gsrc) + d.g_off, d.hpad, d.ncols,
-                             lpc, lane, wid * cpp, nw * cpp, acc);
+      narrow_fma_chunk<S, R>(gdata + d.data_off * Store<S>::kEsize, static_cast<const G *>(a.gsrc) + d.g_off, d.hpad,
+                             d.ncols, narrow_lpc(d.hpad, R), lane, acc);
     }
-    if (!(d.flags & kLast)) continue;
-    // the item's rows: sums over the warp's column lanes, then (CTA mode)
-    // over the warps in shared memory
+  }
+  // The item's rows summed over the warp's lanes; f(r, value) for every row
+  // r < hpad, called by one lane per row.
+  template <typename F>
+  __device__ __forceinline__ void rows(int hpad, int lane, F &&f) {
     if constexpr (kTensor) {
       float v[2];
-      narrow_bf16_rows(tacc, d.hpad, lane, v);
-      const int rgl = narrow_rgl(d.hpad), rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
+      narrow_bf16_rows(tacc, hpad, lane, v);
+      const int rgl = narrow_rgl(hpad), rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
       if (cs == 0) {
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-          const int r = (rl + 4 * j) * 8 + (lane & 7);
-          if (r < d.hpad && (j == 0 || rl + 4 < (d.hpad >> 3))) {
-            if (red)
-              red[wid * kNarrowRows + r] = v[j];
-            else if (r < d.rows)
-              narrow_store<G>(a, d.out_off, r, v[j]);
-          }
-        }
+        const int nrg = hpad >> 3;
+        if (rl < nrg) f(rl * 8 + (lane & 7), v[0]);
+        if (rl + 4 < nrg) f((rl + 4) * 8 + (lane & 7), v[1]);
       }
     } else {
-      const int lpc = narrow_lpc(d.hpad, R);
+      const int lpc = narrow_lpc(hpad, R);
       for (int o = lpc; o < 32; o <<= 1)
 #pragma unroll
         for (int k = 0; k < R; k++) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
       if (lane < lpc) {
 #pragma unroll
-        for (int k = 0; k < R; k++) {
-          const int r = lane * R + k;
-          if (r < d.hpad) {
-            if (red)
-              red[wid * kNarrowRows + r] = acc[k];
-            else if (r < d.rows)
-              narrow_store<G>(a, d.out_off, r, acc[k]);
-          }
-        }
+        for (int k = 0; k < R; k++)
+          if (lane * R + k < hpad) f(lane * R + k, acc[k]);
       }
     }
-    if (red) {
-      __syncthreads();
-      const int r = threadIdx.x;
-      if (r < d.rows) {
-        G sum = red[r];
-        for (int w = 1; w < nw; w++) sum += red[w * kNarrowRows + r];
-        narrow_store<G>(a, d.out_off, r, sum);
-      }
-      __syncthreads();
+  }
+};
+
+// Warp per unit: the warp walks the unit's chunks in order and writes each
+// item's rows at its last chunk.
+template <typename S>
+__device__ __forceinline__ void narrow_unit_warp(const StreamArgs &a, int cb, int ce, int lane) {
+  using G = typename Store<S>::G;
+  NarrowAcc<S> ac;
+  for (int i = cb; i < ce; i++) {
+    const NarrowChunk d = narrow_desc(a, i, lane == 0);
+    if (d.flags & kFirst) ac.zero();
+    ac.add_chunk(a, d, lane);
+    if (d.flags & kLast)
+      ac.rows(d.hpad, lane, [&](int r, G v) {
+        if (r < d.rows) narrow_store<G>(a, d.out_off, r, v);
+      });
+  }
+}
+
+// CTA per unit: item by item, warp w takes the item's chunks w, w + 16, ...,
+// then the warps' rows meet in red (kNarrowWarps x kNarrowRows) and are summed
+// in warp order.  Every thread of the CTA calls it.
+template <typename S>
+__device__ __forceinline__ void narrow_unit_cta(const StreamArgs &a, int cb, int ce, int lane, int wid,
+                                                typename Store<S>::G *red) {
+  using G = typename Store<S>::G;
+  int i0 = cb;
+  while (i0 < ce) {
+    int i1 = i0;  // the item's last chunk
+    while (i1 + 1 < ce && !(__ldg(&a.chunks[i1].flags) & kLast)) i1++;
+    const NarrowChunk last = narrow_desc(a, i1, false);
+    NarrowAcc<S> ac;
+    ac.zero();
+    for (int i = i0 + wid; i <= i1; i += kNarrowWarps) {
+      const NarrowChunk d = narrow_desc(a, i, lane == 0);
+      if (d.hpad == last.hpad) ac.add_chunk(a, d, lane);
     }
+    ac.rows(last.hpad, lane, [&](int r, G v) { red[wid * kNarrowRows + r] = v; });
+    __syncthreads();
+    const int r = threadIdx.x;
+    if (r < last.rows) {
+      G sum = red[r];
+      for (int w = 1; w < kNarrowWarps; w++) sum += red[w * kNarrowRows + r];
+      narrow_store<G>(a, last.out_off, r, sum);
+    }
+    __syncthreads();
+    i0 = i1 + 1;
   }
 }
 
@@ -1024,7 +1016,7 @@ __global__ void __launch_bounds__(32 * kNarrowWarps, 2) narrow_items_kernel(Stre
     const int u = unit;
     __syncthreads();
     if (u >= a.n_coop) break;
-    narrow_unit<S>(a, __ldg(a.item_ptr + u), __ldg(a.item_ptr + u + 1), lane, wid, kNarrowWarps, red);
+    narrow_unit_cta<S>(a, __ldg(a.item_ptr + u), __ldg(a.item_ptr + u + 1), lane, wid, red);
   }
   // the rest: warp per unit (queue[0] counts them)
   for (;;) {
@@ -1032,7 +1024,7 @@ __global__ void __launch_bounds__(32 * kNarrowWarps, 2) narrow_items_kernel(Stre
     if (lane == 0) it = a.n_coop + atomicAdd(&a.queue[0], 1);
     it = __shfl_sync(0xffffffffu, it, 0);
     if (it >= a.n_items) break;
-    narrow_unit<S>(a, __ldg(a.item_ptr + it), __ldg(a.item_ptr + it + 1), lane, 0, 1, nullptr);
+    narrow_unit_warp<S>(a, __ldg(a.item_ptr + it), __ldg(a.item_ptr + it + 1), lane);
   }
   // This CTA takes no more units; the last CTA returns the queue to zero.
   __syncthreads();

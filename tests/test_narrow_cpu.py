@@ -2,7 +2,8 @@
 in numpy over an exported host plan: the same descriptor words, the same
 element indices (column slots of 16-byte row runs for FP64 / FP32, (column,
 row-group, column-group) lanes over 8x8 tiles for BF16), the same reductions
-over a warp's column lanes and, for CTA-cooperative units, over the 16 warps.
+over a warp's column lanes and, for CTA-cooperative units (an item's chunks
+dealt round robin to 16 warps), over the warps.
 
 Each phase's queue units divide at bw_plan_split: units before n_wide run in
 the CTA-wide kernel (restated by planreplay.run_phase), [n_wide, n_coop) a
@@ -23,8 +24,8 @@ NARROW_ROWS, NARROW_COLS = 64, 512
 TOL = {"fp64": 1e-13, "fp32": 2e-6, "bf16": 1e-2}
 
 
-def _lanes_fp(hpad, ncols, R, wid, nw):
-    """(lane, first row, columns) of one warp over a column-major chunk."""
+def _lanes_fp(hpad, ncols, R):
+    """(lane, first row, columns) of a warp over a column-major chunk."""
     lpc = 1
     while lpc * R < hpad:
         lpc *= 2
@@ -32,49 +33,62 @@ def _lanes_fp(hpad, ncols, R, wid, nw):
     for lane in range(32):
         r0 = (lane % lpc) * R
         if r0 < hpad:
-            yield lane, r0, range(wid * cpp + lane // lpc, ncols, nw * cpp)
+            yield lane, r0, range(lane // lpc, ncols, cpp)
 
 
-def _lanes_bf16(hpad, ncols, wid, nw):
-    """(lane, column, row groups) of one warp over an 8x8-tiled chunk."""
+def _lanes_bf16(hpad, ncols):
+    """(lane, column group, column, row groups) of a warp over an 8x8-tiled
+    chunk."""
     nrg = hpad // 8
     rgl = 1 if nrg <= 1 else 2 if nrg <= 2 else 4
     gpw = 4 // rgl
     ncg = (ncols + 7) // 8
     for lane in range(32):
         c8, rl, cs = lane & 7, (lane >> 3) % rgl, (lane >> 3) // rgl
-        rgs = [g for g in (rl, rl + 4) if g < nrg and (g == rl or rl + 4 < nrg)]
-        for cg in range(wid * gpw + cs, ncg, nw * gpw):
+        rgs = [g for g in (rl, rl + 4) if g < nrg and (g == rl or nrg > 4)]
+        for cg in range(cs, ncg, gpw):
             c = 8 * cg + c8
             if c < ncols:
                 yield lane, cg, c, rgs
 
 
-def narrow_unit(plan, gsrc, out, precision, cb, ce, nw):
-    """One queue unit: nw = 1 warp per unit, nw = 16 the CTA-cooperative mode."""
-    data, chunks = plan["data"], plan["chunks"]
-    R = {"fp64": 2, "fp32": 4, "bf16": 1}[precision]
-    acc = None
-    for i in range(cb, ce):
-        d = decode(chunks[i])
-        hpad, ncols, off, g = d["hpad"], d["ncols"], d["data_off"], d["g_off"]
-        assert 0 < hpad <= NARROW_ROWS and hpad % 8 == 0
-        if d["flags"] & 1:
-            acc = np.zeros((nw, 32, hpad))  # per warp, per lane, per item row
-        for w in range(nw):
-            if precision == "bf16":
-                for lane, cg, c, rgs in _lanes_bf16(hpad, ncols, w, nw):
-                    for rg in rgs:
-                        e = off + cg * 8 * hpad + rg * 64 + (c & 7) * 8
-                        acc[w, lane, rg * 8:rg * 8 + 8] += data[e:e + 8] * gsrc[g + c]
-            else:
-                for lane, r0, cols in _lanes_fp(hpad, ncols, R, w, nw):
-                    for c in cols:
-                        e = off + c * hpad + r0
-                        acc[w, lane, r0:r0 + R] += data[e:e + R] * gsrc[g + c]
+def _warp_chunk(plan, gsrc, precision, d, acc):
+    """One warp's pass over one chunk: acc[lane, row] += the lane's products."""
+    data = plan["data"]
+    hpad, ncols, off, g = d["hpad"], d["ncols"], d["data_off"], d["g_off"]
+    assert 0 < hpad <= NARROW_ROWS and hpad % 8 == 0
+    if precision == "bf16":
+        for lane, cg, c, rgs in _lanes_bf16(hpad, ncols):
+            for rg in rgs:
+                e = off + cg * 8 * hpad + rg * 64 + (c & 7) * 8
+                acc[lane, rg * 8:rg * 8 + 8] += data[e:e + 8] * gsrc[g + c]
+    else:
+        R = {"fp64": 2, "fp32": 4}[precision]
+        for lane, r0, cols in _lanes_fp(hpad, ncols, R):
+            for c in cols:
+                e = off + c * hpad + r0
+                acc[lane, r0:r0 + R] += data[e:e + R] * gsrc[g + c]
+
+
+def narrow_unit(plan, gsrc, out, precision, cb, ce, cta):
+    """One queue unit, warp per unit (cta False) or CTA per unit: warp w of 16
+    takes the item's chunks w, w + 16, ..., the warps' rows summed at the end."""
+    ds = [decode(plan["chunks"][i]) for i in range(cb, ce)]
+    items, start = [], 0
+    for k, d in enumerate(ds):
         if d["flags"] & 2:
-            rows = acc.sum(axis=1).sum(axis=0)[:d["rows"]]  # lanes by shuffles, then warps in order
-            out[d["out_off"]:d["out_off"] + d["rows"]] = rows
+            items.append(ds[start:k + 1])
+            start = k + 1
+    assert start == len(ds)
+    for item in items:
+        assert item[0]["flags"] & 1
+        last = item[-1]
+        nw = 16 if cta else 1
+        acc = np.zeros((nw, 32, last["hpad"]))  # per warp, per lane, per item row
+        for k, d in enumerate(item):
+            _warp_chunk(plan, gsrc, precision, d, acc[k % nw])
+        rows = acc.sum(axis=1).sum(axis=0)[:last["rows"]]  # lanes by shuffles, then warps in order
+        out[last["out_off"]:last["out_off"] + last["rows"]] = rows
     return out
 
 
@@ -98,7 +112,7 @@ def split_phase(plan, gsrc, out, precision, rows=NARROW_ROWS):
     run_phase(wide, gsrc, out, precision == "bf16")
     units = plan["item_ptr"]
     for u in range(n_wide, len(units) - 1):
-        narrow_unit(plan, gsrc, out, precision, units[u], units[u + 1], 16 if u < n_coop else 1)
+        narrow_unit(plan, gsrc, out, precision, units[u], units[u + 1], u < n_coop)
     return n_wide, n_coop, len(units) - 1
 
 
