@@ -393,11 +393,14 @@ def run_batch_only(a):
         hb.sync()
         hb.set_timing(True)
         ms = _events_ms(lambda: hb.matvec(x, p, out=y), a.steps)
-        launch_ms, nrec = hb.timing_read()
+        l6, nrec = hb.timing_read_launches()
         hb.set_timing(False)
         b1, b2 = hb.phase_bytes(p)
-        pe = [v / max(1, nrec) for v in launch_ms]
+        l6 = [v / max(1, nrec) for v in l6]
+        pe = [l6[0], l6[1] + l6[2], l6[3], l6[4] + l6[5]]
         out[p] = {"ms_per_matvec": ms, "launch_ms": pe, "phase_bytes": [b1, b2],
+                  "launch_ms_detail": dict(zip(["x_gather", "p1_cta_wide", "p1_unstaged", "g2_gather",
+                                                "p2_cta_wide", "p2_unstaged"], l6)),
                   "phase_gbs": [b1 / (pe[1] * 1e-3) / 1e9, b2 / (pe[3] * 1e-3) / 1e9],
                   "algorithmic_bytes": hb.algorithmic_bytes(p)}
         hb.sync()

@@ -52,6 +52,7 @@ _SIGS = {
     "bw_plan_split": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "bw_set_timing": (C.c_int, [_P, C.c_int]),
     "bw_timing_read": (C.c_int, [_P, _P, _P]),
+    "bw_timing_read_launches": (C.c_int, [_P, _P, _P]),
     "bw_phase_bytes": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
     "bw_plan_tscale": (C.c_int, [_P, C.c_int, _P, _P]),
     "bw_mm_plan_export": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),

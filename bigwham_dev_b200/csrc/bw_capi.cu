@@ -56,7 +56,9 @@ int prec_index(int flags) {
 }
 
 // launches of one matvec: x gather, phase 1, G2 gather, phase 2
-constexpr int kTimedLaunches = 4;
+// Timed spans of one matvec: x gather, phase 1 CTA-wide, phase 1 unstaged,
+// G2 gather, phase 2 CTA-wide, phase 2 unstaged.
+constexpr int kTimedLaunches = 6;
 constexpr size_t kEv = kTimedLaunches + 1;
 
 struct DevPhase {
@@ -458,12 +460,13 @@ void pack_phase_device(bw_hmat *h, int o, int prec, int phase, void *dst) {
 }
 
 // How a phase's queue units (in decreasing cost order) divide between the
-// streaming kernels.  wide: one past the last unit with an item of more than
-// narrow_rows padded rows (those need the CTA-wide kernel's staging); coop:
-// one past the last unit with an item of more than narrow_cols columns (the
-// few long items of a phase, thousands of columns in a 2DS0-H phase 1, which
-// the warp-per-item kernel's CTAs take whole).  narrow_coop 0 sends the long
-// items to the CTA-wide kernel instead; narrow_rows 0 sends everything there.
+// streaming kernels.  By default the CTA-wide kernel takes the units up to
+// the last one with an item of more than narrow_rows padded rows or more than
+// narrow_cols columns (the few long items of a phase, thousands of columns in
+// a 2DS0-H phase 1, stream best through its staging ring), and the unstaged
+// kernel the rest, warp per unit.  narrow_coop 1: the CTA-wide kernel only
+// up to the last tall unit, the unstaged kernel's CTAs take the long ones
+// after it whole (units [wide, coop)).  narrow_rows 0: everything CTA-wide.
 bw::NarrowSplit narrow_split(const bw::ChunkPlan &cp, const bw::Tuning &tune) {
   const int64_t n_units = std::max<int64_t>(0, (int64_t)cp.item_ptr.size() - 1);
   bw::NarrowSplit sp{n_units, n_units};
@@ -574,9 +577,10 @@ void compute_diagonal(bw_hmat *h) {
   }
 }
 
-// The four launches of one matvec: x gather (+ permutation), phase 1 (t),
-// G2 gather, phase 2 (y), with the given scratch vectors; `ev` (optional)
-// receives kTimedLaunches + 1 events around them.
+// The launches of one matvec: x gather (+ permutation), phase 1 (t), G2
+// gather, phase 2 (y), each phase in the CTA-wide and / or the unstaged
+// kernel, with the given scratch vectors; `ev` (optional) receives
+// kTimedLaunches + 1 events around them.
 template <typename S>
 void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y, bool permuted, cudaStream_t st,
                         void *xp_buf, void *t_buf, void *g2_buf, cudaEvent_t *ev) {
@@ -608,7 +612,7 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
             dp.gsegs, (int)dp.n_gsegs, xp, t, g2_buf);
         BW_CUDA(cudaGetLastError());
       }
-      if (ev) BW_CUDA(cudaEventRecord(ev[3], st));
+      if (ev) BW_CUDA(cudaEventRecord(ev[4], st));
     }
     if (dp.n_chunks > 0) {
       bw::StreamArgs a{};
@@ -632,6 +636,7 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
         bw::stream_panels_kernel<S><<<h->grid, bw::threads_of<S>(), bw::SmemLayout<S>::kTotal, st>>>(a);
         BW_CUDA(cudaGetLastError());
       }
+      if (ev) BW_CUDA(cudaEventRecord(ev[phase == 0 ? 2 : 5], st));
       if (dp.split.wide < dp.n_items) {  // the items of at most narrow_rows rows, on their own queue
         a.item_ptr = dp.items + dp.split.wide;
         a.n_items = (int)(dp.n_items - dp.split.wide);
@@ -641,7 +646,10 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
         BW_CUDA(cudaGetLastError());
       }
     }
-    if (ev) BW_CUDA(cudaEventRecord(ev[phase == 0 ? 2 : 4], st));
+    if (ev) {
+      if (dp.n_chunks == 0) BW_CUDA(cudaEventRecord(ev[phase == 0 ? 2 : 5], st));
+      BW_CUDA(cudaEventRecord(ev[phase == 0 ? 3 : 6], st));
+    }
   }
 }
 
@@ -1430,7 +1438,7 @@ int bw_set_timing(bw_hmat *h, int enable) {
   return BW_OK;
 }
 
-int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs) {
+int bw_timing_read_launches(bw_hmat *h, double *ms, int64_t *n_matvecs) {
   if (!h || !ms) return BW_ERR_ARG;
   return guarded(h, [&] {
     for (int k = 0; k < kTimedLaunches; k++) ms[k] = 0.0;
@@ -1448,6 +1456,18 @@ int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs) {
     h->ev_used = 0;
     return BW_OK;
   });
+}
+
+int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs) {
+  if (!h || !ms) return BW_ERR_ARG;
+  double d[kTimedLaunches];
+  const int st = bw_timing_read_launches(h, d, n_matvecs);
+  if (st != BW_OK) return st;
+  ms[0] = d[0];
+  ms[1] = d[1] + d[2];
+  ms[2] = d[3];
+  ms[3] = d[4] + d[5];
+  return BW_OK;
 }
 
 int bw_phase_bytes(const bw_hmat *h, int precision, int transposed, int64_t *phase1, int64_t *phase2) {

@@ -158,7 +158,7 @@ struct Tuning {
   int unit_bytes = kUnitBytes;                          // streaming queue: minimum cost of a unit
   int narrow_rows = 64;   // items of at most this many padded rows skip the staging (0: never) ...
   int narrow_cols = 512;  // ... warp per item up to this many columns, CTA-cooperatively above
-  int narrow_coop = 1;    // 0: items above narrow_cols columns stay in the CTA-wide kernel
+  int narrow_coop = 0;    // 1: items above narrow_cols columns run a CTA each in the unstaged kernel
 };
 
 // Queue units [0, wide) of a phase run in the CTA-wide kernel; of the rest,

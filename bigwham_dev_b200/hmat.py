@@ -391,6 +391,15 @@ class HmatGpu:
         """Record CUDA events around each launch of every following matvec."""
         A.check(self._lib.bw_set_timing(self._h, int(enable)), self._h)
 
+    def timing_read_launches(self):
+        """Summed durations (ms) of the (x gather, phase 1 CTA-wide, phase 1
+        unstaged, G2 gather, phase 2 CTA-wide, phase 2 unstaged) launches
+        recorded since the last read, and the number of matvecs."""
+        ms = (C.c_double * 6)()
+        n = C.c_int64()
+        A.check(self._lib.bw_timing_read_launches(self._h, ms, C.byref(n)), self._h)
+        return list(ms), int(n.value)
+
     def timing_read(self):
         """Summed durations (ms) of the (x gather, phase 1, G2 gather, phase 2)
         launches recorded since the last read, and the number of matvecs."""

@@ -116,11 +116,11 @@ int bw_test_withhold_chunk(bw_hmat *h, int index);
  *   "narrow_rows", "narrow_cols", "narrow_coop": the items of a phase
  *       after its last item of more than narrow_rows padded rows (0..64,
  *       default 64) in the queue's cost order skip the staging: they run in a
- *       second launch with direct loads, a CTA per item up to the last item
- *       of more than narrow_cols columns (default 512), warp per item after
- *       it.  narrow_coop 0 (default 1) keeps the items above narrow_cols
- *       columns in the CTA-wide kernel; narrow_rows 0 keeps every item
- *       there.
+ *       second launch with direct loads, warp per item, from the last item
+ *       of more than narrow_cols columns (default 512) on; narrow_coop 1
+ *       (default 0) runs the items before it there as well, a CTA per item,
+ *       instead of in the CTA-wide kernel.  narrow_rows 0 keeps every item
+ *       in the CTA-wide kernel.
  * Results do not depend on them (each item is reduced in a fixed order).
  * BW_ERR_ARG for an unknown key or a value out of range. */
 int bw_set_tuning(bw_hmat *h, const char *key, int64_t value);
@@ -276,12 +276,17 @@ int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, i
 int bw_plan_split(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_wide, int64_t *n_coop);
 
 /* Per-launch timing for benchmarks.  With timing enabled every bw_matvec
- * records CUDA events on its stream around its four launches (x gather,
- * phase 1, G2 gather, phase 2).  bw_timing_read waits for the last recorded
- * event, writes the summed durations in milliseconds of the four launch kinds
- * into ms[0..3] and the number of recorded matvecs, and clears the record. */
+ * records CUDA events on its stream around its launches (x gather, phase 1,
+ * G2 gather, phase 2; a phase is one launch of the CTA-wide kernel, of the
+ * unstaged kernel, or of both).  bw_timing_read waits for the last recorded
+ * event, writes the summed durations in milliseconds of the four steps into
+ * ms[0..3] and the number of recorded matvecs, and clears the record. */
 int bw_set_timing(bw_hmat *h, int enable);
 int bw_timing_read(bw_hmat *h, double *ms, int64_t *n_matvecs);
+/* The same record launch by launch, ms[0..5]: x gather, phase 1 CTA-wide,
+ * phase 1 unstaged, G2 gather, phase 2 CTA-wide, phase 2 unstaged (0 for a
+ * kernel a phase does not use).  Clears the record like bw_timing_read. */
+int bw_timing_read_launches(bw_hmat *h, double *ms, int64_t *n_matvecs);
 
 /* Algorithmic bytes of each streaming launch of one matvec: phase 1 reads the
  * low-rank B factors (+ x, + t written), phase 2 reads the full blocks and the

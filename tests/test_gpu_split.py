@@ -2,15 +2,16 @@
 (-m gpu).
 
 A phase's queue units, in decreasing cost order, run in stream_panels_kernel
-up to the last one with an item of more than narrow_rows padded rows, then in
-narrow_items_kernel: a CTA per unit up to the last unit with an item of more
-than 512 columns, warp per unit after it.  Checked against the oracle
-(oracle_matvec / oracle_rmatvec, the reference's Hmat::matvec,
-src/hmat/hmatrix/hmat.cc:496-558) on synthetic partitions whose phases use
-all three modes (narrow_rows 16) or the two unstaged ones (default), every
-precision within its rounding bound, and against the same blocks with
-narrow_rows 0 (every item in the CTA-wide kernel): the plans differ only in
-summation order.  The 48-member 2DS0-H batch the same way.
+up to the last one with an item of more than narrow_rows padded rows or 512
+columns, and warp per unit in narrow_items_kernel after it; with narrow_coop
+1 the long units after the last tall one run a CTA per unit in
+narrow_items_kernel instead.  Checked against the oracle (oracle_matvec /
+oracle_rmatvec, the reference's Hmat::matvec,
+src/hmat/hmatrix/hmat.cc:496-558) on synthetic partitions under four
+tunings that between them use every mode, every precision within its
+rounding bound, and against the same blocks with narrow_rows 0 (every item in
+the CTA-wide kernel): the plans differ only in summation order.  The 48-member
+2DS0-H batch the same way.
 """
 import numpy as np
 import pytest
@@ -26,7 +27,7 @@ TOL = {"fp64": 1e-13, "fp32": 2e-6, "bf16": 1e-2}
 ORDER = {"fp64": 1e-14, "fp32": 1e-6, "bf16": 1e-3}  # split vs all-wide: summation order only
 
 
-TUNINGS = [{}, {"narrow_rows": 16}, {"narrow_coop": 0}]
+TUNINGS = [{}, {"narrow_rows": 16}, {"narrow_coop": 1}, {"narrow_rows": 16, "narrow_coop": 1}]
 
 
 def _handles(arr, precs):

@@ -8,10 +8,11 @@ dealt round robin to 16 warps), over the warps.
 Each phase's queue units divide at bw_plan_split: units before n_wide run in
 the CTA-wide kernel (restated by planreplay.run_phase), [n_wide, n_coop) a
 CTA per unit and the rest warp per unit.  The split is checked against its
-rule (n_wide: one past the last unit with an item of more than 64 padded
-rows; n_coop: one past the last with an item of more than 512 columns), and
-the replay of both launches against the oracle on the golden cases and on
-synthetic partitions, H and H^T, every precision within its rounding bound.
+rule (by default n_wide = n_coop = one past the last unit with an item of
+more than 64 padded rows or 512 columns; with narrow_coop 1, n_wide stops at
+the last tall unit and n_coop at the last long one), and the replay of both
+launches against the oracle on the golden cases and on synthetic partitions,
+H and H^T, every precision within its rounding bound.
 """
 import numpy as np
 import pytest
@@ -92,7 +93,7 @@ def narrow_unit(plan, gsrc, out, precision, cb, ce, cta):
     return out
 
 
-def split_rule(plan, rows=NARROW_ROWS):
+def split_rule(plan, rows=NARROW_ROWS, coop=0):
     chunks, units = plan["chunks"], plan["item_ptr"]
     last_tall = last_long = -1
     for u in range(len(units) - 1):
@@ -102,12 +103,14 @@ def split_rule(plan, rows=NARROW_ROWS):
             cols = (0 if d["flags"] & 1 else cols) + d["ncols"]
             last_tall = u if d["hpad"] > rows else last_tall
             last_long = u if cols > NARROW_COLS else last_long
-    return last_tall + 1, max(last_tall + 1, last_long + 1)
+    if coop:
+        return last_tall + 1, max(last_tall + 1, last_long + 1)
+    return max(last_tall, last_long) + 1, max(last_tall, last_long) + 1
 
 
-def split_phase(plan, gsrc, out, precision, rows=NARROW_ROWS):
+def split_phase(plan, gsrc, out, precision, rows=NARROW_ROWS, coop=0):
     n_wide, n_coop = plan["n_wide"], plan["n_coop"]
-    assert (n_wide, n_coop) == split_rule(plan, rows)
+    assert (n_wide, n_coop) == split_rule(plan, rows, coop)
     wide = dict(plan, item_ptr=plan["item_ptr"][:n_wide + 1])
     run_phase(wide, gsrc, out, precision == "bf16")
     units = plan["item_ptr"]
@@ -116,14 +119,14 @@ def split_phase(plan, gsrc, out, precision, rows=NARROW_ROWS):
     return n_wide, n_coop, len(units) - 1
 
 
-def narrow_replay(h, x_perm, precision, transposed=False, rows=NARROW_ROWS):
+def narrow_replay(h, x_perm, precision, transposed=False, rows=NARROW_ROWS, coop=0):
     p1 = h.plan_export(precision, 1, transposed)
     p2 = h.plan_export(precision, 2, transposed)
     t = np.zeros(max(1, h.info()["sum_rank"]))
-    s1 = split_phase(p1, x_perm, t, precision, rows)
+    s1 = split_phase(p1, x_perm, t, precision, rows, coop)
     g2 = build_g2(gather_runs(h, precision, transposed), x_perm, t)
     y = np.full(h.n_cols if transposed else h.n_rows, np.nan)
-    s2 = split_phase(p2, g2, y, precision, rows)
+    s2 = split_phase(p2, g2, y, precision, rows, coop)
     return y, (s1, s2)
 
 
@@ -148,8 +151,8 @@ def test_split_restatement_on_the_golden_cases(golden, precision):
 
 def test_split_phases_are_mixed_on_larger_partitions():
     """With narrow_rows 16 the row panels of 24 rows go to the CTA-wide
-    kernel, and items of more than 512 columns run CTA-cooperatively: all
-    three modes run, so the replays below cover them."""
+    kernel, and with narrow_coop 1 items of more than 512 columns run
+    CTA-cooperatively: all three modes run, so the replays below cover them."""
     from synth import synthetic_hmat
 
     modes = set()
@@ -157,7 +160,7 @@ def test_split_phases_are_mixed_on_larger_partitions():
         arr = synthetic_hmat(npr, npc, dof, seed=npr + npc + leaf, leaf=leaf, rank0_share=0.2)
         h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
                               arr.perm1, device=-1, plan_only=True, precisions=("fp32",), transpose=True,
-                              tuning={"narrow_rows": 16})
+                              tuning={"narrow_rows": 16, "narrow_coop": 1})
         for ph in (1, 2):
             for t in (False, True):
                 p = h.plan_export("fp32", ph, t, with_data=False)
@@ -173,17 +176,17 @@ MIXED = [(300, 300, 2, 20), (600, 600, 2, 32)]
 @pytest.mark.parametrize("npr,npc,dof,leaf", [(40, 25, 2, 4), (96, 96, 2, 16), (17, 60, 3, 8), (200, 130, 1, 32),
                                               (90, 70, 3, 32)] + MIXED)
 @pytest.mark.parametrize("precision", ["fp64", "fp32", "bf16"])
-@pytest.mark.parametrize("rows", [64, 16])
-def test_split_restatement_on_synthetic_partitions(npr, npc, dof, leaf, precision, rows):
+@pytest.mark.parametrize("rows,coop", [(64, 0), (64, 1), (16, 1)])
+def test_split_restatement_on_synthetic_partitions(npr, npc, dof, leaf, precision, rows, coop):
     from synth import synthetic_hmat
 
     arr = synthetic_hmat(npr, npc, dof, seed=npr + npc + leaf, leaf=leaf, rank0_share=0.2)
     h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
                           arr.perm1, device=-1, plan_only=True, precisions=(precision,), transpose=True,
-                          tuning={"narrow_rows": rows})
+                          tuning={"narrow_rows": rows, "narrow_coop": coop})
     x = np.random.default_rng(3).uniform(-1, 1, arr.n_cols)
-    y, _ = narrow_replay(h, x, precision, rows=rows)
+    y, _ = narrow_replay(h, x, precision, rows=rows, coop=coop)
     assert _rel(y, oracle_matvec_perm(arr, x, 1)) < TOL[precision]
     g = np.random.default_rng(4).uniform(-1, 1, arr.n_rows)
-    yt, _ = narrow_replay(h, g, precision, transposed=True, rows=rows)
+    yt, _ = narrow_replay(h, g, precision, transposed=True, rows=rows, coop=coop)
     assert _rel(yt, oracle_rmatvec_perm(arr, g, 1)) < TOL[precision]
