@@ -797,23 +797,23 @@ __device__ __forceinline__ int narrow_rgl(int hpad) {
 }
 
 // One chunk of an 8x8-tiled BF16 item: lane (c8, rl, cs) takes column groups
-// cs, cs + gpw, ... in rounds of eight 16-byte loads.  Items of at most 4 row
-// groups (J = 1) load one tile column per lane and column group, items of 5
-// to 8 row groups (J = 2) two.
-template <int J>
-__device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
-                                                  int lane, float (&acc)[J][8]) {
-  constexpr int kAhead = 8 / J;
+// cs, cs + gpw, ... in rounds of kAhead.  Items of at most 4 row groups load
+// one tile column per lane and column group (four column groups a round),
+// items of 5 to 8 row groups two (two a round).
+template <bool kTwo>
+__device__ __forceinline__ void narrow_bf16_chunk_t(const uint16_t *base, const uint32_t *g, int hpad, int ncols,
+                                                    int lane, float (&acc)[2][8]) {
+  constexpr int kAhead = kTwo ? 2 : 4;
   const int nrg = hpad >> 3, rgl = narrow_rgl(hpad), gpw = 4 / rgl;
   const int c8 = lane & 7, rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
   const int ncg = (ncols + 7) >> 3;
-  const bool one = rl < nrg;              // no row group 3 when nrg = 3
-  const bool two = J == 2 && rl + 4 < nrg;  // a second row group
+  const bool one = rl < nrg;               // no row group 3 when nrg = 3
+  const bool two = kTwo && rl + 4 < nrg;  // a second row group
   const uint16_t *lb = base + c8 * 8 + rl * 64;
 #pragma unroll 1
   for (int cg = cs; cg < ncg; cg += kAhead * gpw) {
     float x[kAhead];
-    uint4 w[kAhead][J];
+    uint4 w[kAhead][kTwo ? 2 : 1];
 #pragma unroll
     for (int q = 0; q < kAhead; q++) {
       const int cq = cg + q * gpw, c = 8 * cq + c8;
@@ -821,12 +821,12 @@ __device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const ui
       const uint16_t *col = lb + static_cast<long long>(cq) * 8 * hpad;
       x[q] = in ? unpack_hilo(__ldg(g + c)) : 0.f;
       w[q][0] = in && one ? __ldg(reinterpret_cast<const uint4 *>(col)) : make_uint4(0, 0, 0, 0);
-      if constexpr (J == 2) w[q][1] = in && two ? __ldg(reinterpret_cast<const uint4 *>(col + 256)) : make_uint4(0, 0, 0, 0);
+      if constexpr (kTwo) w[q][1] = in && two ? __ldg(reinterpret_cast<const uint4 *>(col + 256)) : make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
     for (int q = 0; q < kAhead; q++)
 #pragma unroll
-      for (int j = 0; j < J; j++) {
+      for (int j = 0; j < (kTwo ? 2 : 1); j++) {
         const uint32_t ww[4] = {w[q][j].x, w[q][j].y, w[q][j].z, w[q][j].w};
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -834,6 +834,27 @@ __device__ __forceinline__ void narrow_bf16_chunk(const uint16_t *base, const ui
           acc[j][2 * k + 1] = fmaf(__uint_as_float(ww[k] & 0xffff0000u), x[q], acc[j][2 * k + 1]);
         }
       }
+  }
+}
+
+// Sum of a lane's BF16 row partials over the column lanes; lane (c8, rl, cs =
+// 0) then holds rows (rl + 4 j) * 8 + c8 in v[j].
+__device__ __forceinline__ void narrow_bf16_rows(float (&acc)[2][8], int hpad, int lane, float (&v)[2]) {
+  const int rgl = narrow_rgl(hpad), c8 = lane & 7;
+#pragma unroll
+  for (int j = 0; j < 2; j++)
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
+      for (int o = 8 * rgl; o < 32; o <<= 1) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
+    }
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    v[j] = acc[j][0];
+#pragma unroll
+    for (int k = 1; k < 8; k++)
+      if (c8 == k) v[j] = acc[j][k];
   }
 }
 
@@ -877,53 +898,48 @@ __device__ __forceinline__ NarrowChunk narrow_desc(const StreamArgs &a, int i, b
   return c;
 }
 
-// Per-lane partial rows of one item: R rows (FP64 / FP32) or J x 8 (BF16,
-// J = 2 for items of more than 32 padded rows).
-template <typename S, int J>
+// Per-lane partial rows of an item: R rows (FP64 / FP32) or 2 x 8 (BF16).
+template <typename S>
 struct NarrowAcc {
   static constexpr bool kTensor = Store<S>::kRows == 0;
   static constexpr int R = kTensor ? 1 : 16 / Store<S>::kEsize;
-  using G = typename Store<S>::G;
-  G acc[R];
-  float tacc[J][8];
+  typename Store<S>::G acc[R];
+  float tacc[2][8];
   __device__ __forceinline__ void zero() {
 #pragma unroll
     for (int k = 0; k < R; k++) acc[k] = 0;
 #pragma unroll
-    for (int j = 0; j < J; j++)
+    for (int j = 0; j < 2; j++)
 #pragma unroll
       for (int k = 0; k < 8; k++) tacc[j][k] = 0.f;
   }
   __device__ __forceinline__ void add_chunk(const StreamArgs &a, const NarrowChunk &d, int lane) {
+    using G = typename Store<S>::G;
     const unsigned char *gdata = static_cast<const unsigned char *>(a.data);
-    if constexpr (kTensor)
-      narrow_bf16_chunk<J>(reinterpret_cast<const uint16_t *>(gdata) + d.data_off,
-                           static_cast<const uint32_t *>(a.gsrc) + d.g_off, d.hpad, d.ncols, lane, tacc);
-    else
+    if constexpr (kTensor) {
+      const uint16_t *base = reinterpret_cast<const uint16_t *>(gdata) + d.data_off;
+      const uint32_t *g = static_cast<const uint32_t *>(a.gsrc) + d.g_off;
+      if (d.hpad > 32)
+        narrow_bf16_chunk_t<true>(base, g, d.hpad, d.ncols, lane, tacc);
+      else
+        narrow_bf16_chunk_t<false>(base, g, d.hpad, d.ncols, lane, tacc);
+    } else {
       narrow_fma_chunk<S, R>(gdata + d.data_off * Store<S>::kEsize, static_cast<const G *>(a.gsrc) + d.g_off, d.hpad,
                              d.ncols, narrow_lpc(d.hpad, R), lane, acc);
+    }
   }
   // The item's rows summed over the warp's lanes; f(r, value) for every row
-  // r < hpad, called by one lane per row.  BF16: the shuffles add the column
-  // lanes (c8, then cs); lane (c8, rl, cs = 0) holds rows (rl + 4 j) * 8 + c8.
+  // r < hpad, called by one lane per row.
   template <typename F>
   __device__ __forceinline__ void rows(int hpad, int lane, F &&f) {
     if constexpr (kTensor) {
-      const int rgl = narrow_rgl(hpad), c8 = lane & 7, rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
-      const int nrg = hpad >> 3;
-#pragma unroll
-      for (int j = 0; j < J; j++) {
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-#pragma unroll
-          for (int o = 1; o < 8; o <<= 1) tacc[j][k] += __shfl_xor_sync(0xffffffffu, tacc[j][k], o);
-          for (int o = 8 * rgl; o < 32; o <<= 1) tacc[j][k] += __shfl_xor_sync(0xffffffffu, tacc[j][k], o);
-        }
-        float v = tacc[j][0];
-#pragma unroll
-        for (int k = 1; k < 8; k++)
-          if (c8 == k) v = tacc[j][k];
-        if (cs == 0 && rl + 4 * j < nrg) f((rl + 4 * j) * 8 + c8, v);
+      float v[2];
+      narrow_bf16_rows(tacc, hpad, lane, v);
+      const int rgl = narrow_rgl(hpad), rl = (lane >> 3) & (rgl - 1), cs = (lane >> 3) / rgl;
+      if (cs == 0) {
+        const int nrg = hpad >> 3;
+        if (rl < nrg) f(rl * 8 + (lane & 7), v[0]);
+        if (rl + 4 < nrg) f((rl + 4) * 8 + (lane & 7), v[1]);
       }
     } else {
       const int lpc = narrow_lpc(hpad, R);
@@ -939,55 +955,26 @@ struct NarrowAcc {
   }
 };
 
-// One item of a warp-per-unit unit, from chunk i (descriptor d) to its last
-// chunk.  Returns the index after the item's last chunk.
-template <typename S, int J>
-__device__ __forceinline__ int narrow_item_warp(const StreamArgs &a, int i, int ce, NarrowChunk d, int lane) {
+// Warp per unit: the warp walks the unit's chunks in order and writes each
+// item's rows at its last chunk.
+template <typename S>
+__device__ __forceinline__ void narrow_unit_warp(const StreamArgs &a, int cb, int ce, int lane) {
   using G = typename Store<S>::G;
-  NarrowAcc<S, J> ac;
-  ac.zero();
-  for (;;) {
+  NarrowAcc<S> ac;
+  for (int i = cb; i < ce; i++) {
+    const NarrowChunk d = narrow_desc(a, i, lane == 0);
+    if (d.flags & kFirst) ac.zero();
     ac.add_chunk(a, d, lane);
-    if ((d.flags & kLast) || i + 1 == ce) {
+    if (d.flags & kLast)
       ac.rows(d.hpad, lane, [&](int r, G v) {
         if (r < d.rows) narrow_store<G>(a, d.out_off, r, v);
       });
-      return i + 1;
-    }
-    d = narrow_desc(a, ++i, lane == 0);
-  }
-}
-
-// Warp per unit: the warp walks the unit's chunks [cb, ce) in order and
-// writes each item's rows at its last chunk.
-template <typename S>
-__device__ __forceinline__ void narrow_unit_warp(const StreamArgs &a, int cb, int ce, int lane) {
-  int i = cb;
-  while (i < ce) {
-    const NarrowChunk d = narrow_desc(a, i, lane == 0);
-    if (Store<S>::kRows == 0 && d.hpad > 32)
-      i = narrow_item_warp<S, 2>(a, i, ce, d, lane);
-    else
-      i = narrow_item_warp<S, 1>(a, i, ce, d, lane);
   }
 }
 
 // CTA per unit: item by item, warp w takes the item's chunks w, w + 16, ...,
 // then the warps' rows meet in red (kNarrowWarps x kNarrowRows) and are summed
 // in warp order.  Every thread of the CTA calls it.
-template <typename S, int J>
-__device__ __forceinline__ void narrow_item_cta(const StreamArgs &a, int i0, int i1, const NarrowChunk &last,
-                                                int lane, int wid, typename Store<S>::G *red) {
-  using G = typename Store<S>::G;
-  NarrowAcc<S, J> ac;
-  ac.zero();
-  for (int i = i0 + wid; i <= i1; i += kNarrowWarps) {
-    const NarrowChunk d = narrow_desc(a, i, lane == 0);
-    if (d.hpad == last.hpad) ac.add_chunk(a, d, lane);
-  }
-  ac.rows(last.hpad, lane, [&](int r, G v) { red[wid * kNarrowRows + r] = v; });
-}
-
 template <typename S>
 __device__ __forceinline__ void narrow_unit_cta(const StreamArgs &a, int cb, int ce, int lane, int wid,
                                                 typename Store<S>::G *red) {
@@ -997,10 +984,13 @@ __device__ __forceinline__ void narrow_unit_cta(const StreamArgs &a, int cb, int
     int i1 = i0;  // the item's last chunk
     while (i1 + 1 < ce && !(__ldg(&a.chunks[i1].flags) & kLast)) i1++;
     const NarrowChunk last = narrow_desc(a, i1, false);
-    if (Store<S>::kRows == 0 && last.hpad > 32)
-      narrow_item_cta<S, 2>(a, i0, i1, last, lane, wid, red);
-    else
-      narrow_item_cta<S, 1>(a, i0, i1, last, lane, wid, red);
+    NarrowAcc<S> ac;
+    ac.zero();
+    for (int i = i0 + wid; i <= i1; i += kNarrowWarps) {
+      const NarrowChunk d = narrow_desc(a, i, lane == 0);
+      if (d.hpad == last.hpad) ac.add_chunk(a, d, lane);
+    }
+    ac.rows(last.hpad, lane, [&](int r, G v) { red[wid * kNarrowRows + r] = v; });
     __syncthreads();
     const int r = threadIdx.x;
     if (r < last.rows) {
@@ -1028,10 +1018,7 @@ __global__ void __launch_bounds__(32 * kNarrowWarps, 2) narrow_items_kernel(Stre
     if (u >= a.n_coop) break;
     narrow_unit_cta<S>(a, __ldg(a.item_ptr + u), __ldg(a.item_ptr + u + 1), lane, wid, red);
   }
-  // The rest: warp per unit (queue[0] counts them).  A unit is claimed only
-  // when the warp is free: the units are few per warp (1.5 to 3 on the
-  // 48 x 2DS0 batch), and claiming one ahead measured 1.8x slower there
-  // (warps holding two large units while others idle).
+  // the rest: warp per unit (queue[0] counts them)
   for (;;) {
     int it = 0;
     if (lane == 0) it = a.n_coop + atomicAdd(&a.queue[0], 1);
