@@ -1048,47 +1048,62 @@ __device__ __forceinline__ uint32_t pack_hilo(float v) {
 }
 
 // G2[dst + c] = scale * src[src_off + c] for every run (src: gathered x or t):
-// the phase-2 vector values laid out chunk by chunk.  Runs are short (tens of
-// values), so each warp takes kG2Runs of them at once: lanes 0..kG2Runs-1
-// fetch the run descriptors together, and every lane keeps one load per run
-// in flight per step, instead of one dependent chain per run.
-// kPacked: store pack_hilo(value) words (BF16 path) instead of G values.
-constexpr int kG2Runs = 4;
+// the phase-2 vector values laid out chunk by chunk.  Runs are short (10 to
+// 60 values on 2DS0-H matrices), so a warp takes kG2Runs = 32 of them at
+// once and deals their values to its lanes densely: lane k loads run k's
+// descriptor, a warp scan gives each run its first position in the warp's
+// value list, and each value finds its run by a 5-step binary search over
+// the lanes' starts (shuffles), so every lane has a value in every step but
+// the last.  kPacked: store pack_hilo(value) words (BF16 path) instead of G
+// values.
+constexpr int kG2Runs = 32;
+constexpr int kG2Unroll = 4;  // values in flight per lane
 
 template <typename G, bool kPacked>
 __global__ void gather_g2_kernel(const GatherSeg *__restrict__ runs, int n_runs, const G *__restrict__ xp,
                                  const G *__restrict__ t, void *__restrict__ g2) {
   const int lane = threadIdx.x & 31;
   const int r0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kG2Runs;
-  if (r0 >= n_runs) return;
-  GatherSeg mine{};
-  if (lane < kG2Runs && r0 + lane < n_runs) mine = runs[r0 + lane];  // cols = 0 past the end
-  int dst[kG2Runs], off[kG2Runs], cols[kG2Runs], from_t[kG2Runs];
-  float sc[kG2Runs];
-  int most = 0;
+  if (r0 >= n_runs) return;  // warp-uniform
+  GatherSeg mine{};          // cols = 0 past the end
+  if (r0 + lane < n_runs) mine = runs[r0 + lane];
+  const int cols = static_cast<int>(mine.cols_src & 0x7fffffffu);
+  int incl = cols;  // inclusive scan of the run lengths over the lanes
 #pragma unroll
-  for (int q = 0; q < kG2Runs; q++) {
-    dst[q] = __shfl_sync(0xffffffffu, mine.dst, q);
-    off[q] = __shfl_sync(0xffffffffu, mine.src_off, q);
-    const uint32_t cs = __shfl_sync(0xffffffffu, mine.cols_src, q);
-    cols[q] = static_cast<int>(cs & 0x7fffffffu);
-    from_t[q] = static_cast<int>(cs >> 31);
-    sc[q] = __shfl_sync(0xffffffffu, mine.scale, q);
-    most = max(most, cols[q]);
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
   }
-  for (int c = lane; c < most; c += 32) {
-    G v[kG2Runs];
+  const int start = incl - cols;
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  for (int base = 0; base < total; base += 32 * kG2Unroll) {
+    G v[kG2Unroll];
+    int dst[kG2Unroll];
+    float sc[kG2Unroll];
 #pragma unroll
-    for (int q = 0; q < kG2Runs; q++)
-      if (c < cols[q]) v[q] = (from_t[q] ? t : xp)[off[q] + c];
+    for (int u = 0; u < kG2Unroll; u++) {
+      const int e = base + 32 * u + lane;
+      // the last run starting at or before e (empty runs share the start of
+      // the next one, so the last such run holds e when e < total)
+      int r = 0;
 #pragma unroll
-    for (int q = 0; q < kG2Runs; q++) {
-      if (c < cols[q]) {
-        const G w = static_cast<G>(sc[q]) * v[q];
+      for (int step = 16; step > 0; step >>= 1)
+        if (__shfl_sync(0xffffffffu, start, r + step) <= e) r += step;
+      const int k = e - __shfl_sync(0xffffffffu, start, r);
+      const int off = __shfl_sync(0xffffffffu, mine.src_off, r);
+      const uint32_t cs = __shfl_sync(0xffffffffu, mine.cols_src, r);
+      dst[u] = __shfl_sync(0xffffffffu, mine.dst, r) + k;
+      sc[u] = __shfl_sync(0xffffffffu, mine.scale, r);
+      v[u] = e < total ? ((cs >> 31) ? t : xp)[off + k] : G(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kG2Unroll; u++) {
+      if (base + 32 * u + lane < total) {
+        const G w = static_cast<G>(sc[u]) * v[u];
         if constexpr (kPacked)
-          static_cast<uint32_t *>(g2)[dst[q] + c] = pack_hilo(static_cast<float>(w));
+          static_cast<uint32_t *>(g2)[dst[u]] = pack_hilo(static_cast<float>(w));
         else
-          static_cast<G *>(g2)[dst[q] + c] = w;
+          static_cast<G *>(g2)[dst[u]] = w;
       }
     }
   }
