@@ -50,6 +50,7 @@ _SIGS = {
     "bw_set_device_limit": (C.c_int, [_P, _I64]),
     "bw_plan_export": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
     "bw_plan_split": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P, _P]),
+    "bw_matvec_launches": (C.c_int, [_P, C.c_int, C.c_int, _P]),
     "bw_set_timing": (C.c_int, [_P, C.c_int]),
     "bw_timing_read": (C.c_int, [_P, _P, _P]),
     "bw_timing_read_launches": (C.c_int, [_P, _P, _P]),

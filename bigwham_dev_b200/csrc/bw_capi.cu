@@ -1431,6 +1431,25 @@ int bw_plan_split(const bw_hmat *h, int precision, int phase, int transposed, in
   return BW_OK;
 }
 
+int bw_matvec_launches(const bw_hmat *h, int precision, int transposed, int64_t *n) {
+  if (!h || !n) return BW_ERR_ARG;
+  const int p = prec_index(precision);
+  if (p < 0 || !h->finalized || !(h->stored & (1 << p))) return BW_ERR_STATE;
+  const int o = transposed ? 1 : 0;
+  if (o == 1 && !h->has_t) return BW_ERR_UNSUPPORTED;
+  int64_t k = h->op[o].n_in > 0 ? 1 : 0;  // x gather
+  for (int ph = 0; ph < 2; ph++) {
+    const bw::ChunkPlan &cp = h->op[o].ph[ph].cp[p];
+    const int64_t units = std::max<int64_t>(0, (int64_t)cp.item_ptr.size() - 1);
+    if (ph == 1 && !cp.gsegs.empty()) k++;  // G2 gather
+    if (cp.chunks.empty()) continue;
+    const bw::NarrowSplit sp = narrow_split(cp, h->prob.tune);
+    k += (sp.wide > 0 ? 1 : 0) + (sp.wide < units ? 1 : 0);
+  }
+  *n = k;
+  return BW_OK;
+}
+
 int bw_set_timing(bw_hmat *h, int enable) {
   if (!h) return BW_ERR_ARG;
   h->timing = enable != 0;

@@ -387,6 +387,12 @@ class HmatGpu:
         return {"chunks": chunks, "item_ptr": items, "data": data, "n_wide": int(n_wide.value),
                 "n_coop": int(n_coop.value)}
 
+    def launches(self, precision="fp64", transposed=False) -> int:
+        """Kernel launches of one matvec (bw_matvec_launches)."""
+        n = C.c_int64()
+        A.check(self._lib.bw_matvec_launches(self._h, _prec_flag(precision), int(transposed), C.byref(n)), self._h)
+        return int(n.value)
+
     def set_timing(self, enable: bool = True) -> None:
         """Record CUDA events around each launch of every following matvec."""
         A.check(self._lib.bw_set_timing(self._h, int(enable)), self._h)

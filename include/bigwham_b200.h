@@ -275,6 +275,10 @@ int bw_plan_export(const bw_hmat *h, int precision, int phase, int transposed, i
  * warp per item (the "narrow_*" tuning keys). */
 int bw_plan_split(const bw_hmat *h, int precision, int phase, int transposed, int64_t *n_wide, int64_t *n_coop);
 
+/* Kernel launches of one bw_matvec in this precision and direction: the x
+ * gather, the G2 gather and one or two per phase (CTA-wide, unstaged). */
+int bw_matvec_launches(const bw_hmat *h, int precision, int transposed, int64_t *n);
+
 /* Per-launch timing for benchmarks.  With timing enabled every bw_matvec
  * records CUDA events on its stream around its launches (x gather, phase 1,
  * G2 gather, phase 2; a phase is one launch of the CTA-wide kernel, of the

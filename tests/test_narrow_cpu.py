@@ -190,3 +190,20 @@ def test_split_restatement_on_synthetic_partitions(npr, npc, dof, leaf, precisio
     g = np.random.default_rng(4).uniform(-1, 1, arr.n_rows)
     yt, _ = narrow_replay(h, g, precision, transposed=True, rows=rows, coop=coop)
     assert _rel(yt, oracle_rmatvec_perm(arr, g, 1)) < TOL[precision]
+
+
+def test_launch_count_follows_the_split():
+    """bw_matvec_launches: the x gather, the G2 gather and one launch per
+    kernel a phase uses."""
+    from synth import synthetic_hmat
+
+    arr = synthetic_hmat(600, 600, 2, seed=1264, leaf=32, rank0_share=0.2)
+    for tune in ({}, {"narrow_rows": 0}, {"narrow_rows": 16, "narrow_coop": 1}):
+        h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
+                              arr.perm1, device=-1, plan_only=True, precisions=("fp32",), tuning=tune)
+        want = 2  # x gather, G2 gather
+        for ph in (1, 2):
+            p = h.plan_export("fp32", ph, with_data=False)
+            n = len(p["item_ptr"]) - 1
+            want += (p["n_wide"] > 0) + (p["n_wide"] < n)
+        assert h.launches("fp32") == want, tune
