@@ -278,44 +278,6 @@ template <typename S> struct SmemLayout {
   static_assert(kTotal <= 232448, "shared memory above the 227 KB per-CTA limit");
 };
 
-// Where a chunk lands in a stage: its block data [lo, lo + data_bytes) copied
-// to the stage's start, its vector window [glo, glo + win_bytes) right after
-// it, both 16-byte rounded.  ok: a well-formed chunk whose data and window fit
-// the stage's data and window areas together (the layout sizes chunks by
-// stage_cols so that they always do).  Producer and consumers compute it from
-// the same descriptor fields.
-struct StageFit {
-  unsigned long long lo, glo;
-  uint32_t data_bytes, win_bytes;
-  bool ok;
-};
-
-template <typename S>
-__device__ __forceinline__ StageFit stage_fit(const unsigned char *gdata, const unsigned char *gvec, long long data_off,
-                                              int ncols, int hpad, int g_off) {
-  using G = typename Store<S>::G;
-  using L = SmemLayout<S>;
-  constexpr int es = Store<S>::kEsize;
-  constexpr bool kTensor = Store<S>::kRows == 0;
-  StageFit f{};
-  if (ncols <= 0 || ncols > kMaxChunkCols || hpad <= 0 || hpad > kHMax) return f;
-  const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
-                                          : static_cast<unsigned long long>(ncols);
-  const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
-                                 static_cast<unsigned long long>(data_off) * es;
-  f.lo = src & ~15ull;
-  const unsigned long long hi = (src + cols * hpad * es + 15ull) & ~15ull;
-  const unsigned long long gsa = reinterpret_cast<unsigned long long>(gvec) +
-                                 static_cast<unsigned long long>(g_off) * sizeof(G);
-  f.glo = gsa & ~15ull;
-  const unsigned long long ghi = (gsa + static_cast<unsigned long long>(ncols) * sizeof(G) + 15ull) & ~15ull;
-  if ((hi - f.lo) + (ghi - f.glo) > static_cast<unsigned long long>(L::kDataBytes + L::kGBytes)) return f;
-  f.data_bytes = static_cast<uint32_t>(hi - f.lo);
-  f.win_bytes = static_cast<uint32_t>(ghi - f.glo);
-  f.ok = true;
-  return f;
-}
-
 struct DescRegs {
   uint32_t w[kChunkWords];
 };
@@ -462,10 +424,16 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
 #pragma unroll
             for (int q = 0; q < kChunkWords / 4; q++)
               dd[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-            const StageFit f = stage_fit<S>(gdata, gvec, data_off, ncols, hpad, g_off);
-            if (f.ok) {
-              const unsigned long long lo = f.lo, hi = f.lo + f.data_bytes;
-              const unsigned long long glo = f.glo, ghi = f.glo + f.win_bytes;
+            const unsigned long long cols = kTensor ? (static_cast<unsigned long long>(ncols) + 7ull) & ~7ull
+                                                    : static_cast<unsigned long long>(ncols);
+            const unsigned long long bytes = cols * hpad * es;
+            if (ncols > 0 && ncols <= kMaxCols && bytes <= static_cast<unsigned long long>(kStageBytes)) {
+              const unsigned long long src = reinterpret_cast<unsigned long long>(gdata) +
+                                             static_cast<unsigned long long>(data_off) * es;
+              const unsigned long long lo = src & ~15ull, hi = (src + bytes + 15ull) & ~15ull;
+              const unsigned long long gs = reinterpret_cast<unsigned long long>(gvec) +
+                                            static_cast<unsigned long long>(g_off) * sizeof(G);
+              const unsigned long long glo = gs & ~15ull, ghi = (gs + ncols * sizeof(G) + 15ull) & ~15ull;
               mbar_arrive_expect_tx(&full[s], static_cast<uint32_t>((hi - lo) + (ghi - glo)));
               // evict-first helps the BF16 launches (measured A/B at 196,608 DoF:
               // -2 to -4%) and slows the FP32 / FP64 row panels (+1 to +3%)
@@ -474,7 +442,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
                               stream_policy);
               else
                 bulk_g2s(st, reinterpret_cast<const void *>(lo), static_cast<uint32_t>(hi - lo), &full[s]);
-              bulk_g2s(st + (hi - lo), reinterpret_cast<const void *>(glo), static_cast<uint32_t>(ghi - glo),
+              bulk_g2s(st + L::kDataBytes, reinterpret_cast<const void *>(glo), static_cast<uint32_t>(ghi - glo),
                        &full[s]);
             } else {
               if (ncols > 0) set_error(a.err, kErrBadChunk);
@@ -561,17 +529,13 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
     const unsigned char *st = stage0 + s * L::kStageSize;
     const Chunk &d = *reinterpret_cast<const Chunk *>(st + L::kDataBytes + L::kGBytes);
     if (d.flags & kEnd) return;  // the producer has no more items for this CTA
-    // the vector window follows the staged block data and starts at the
-    // 16-byte boundary below gsrc + g_off; a chunk the producer refused to
-    // stage (stage_fit) is skipped here too
-    const StageFit fit = stage_fit<S>(static_cast<const unsigned char *>(a.data),
-                                      static_cast<const unsigned char *>(a.gsrc), d.data_off, d.ncols, d.hpad, d.g_off);
+    // the vector window starts at the 16-byte boundary below gsrc + g_off
     const G *gs = reinterpret_cast<const G *>(
-        st + fit.data_bytes +
+        st + L::kDataBytes +
         ((reinterpret_cast<unsigned long long>(a.gsrc) + static_cast<unsigned long long>(d.g_off) * sizeof(G)) &
          15ull));
     const uint32_t flags = d.flags;
-    const int ncols = fit.ok ? d.ncols : 0;
+    const int ncols = d.ncols;
     const int hpad = d.hpad;
     const int rows = d.rows, out_off = d.out_off;
     if (flags & kFirst) {
@@ -597,7 +561,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
 #pragma unroll
         for (int r = 0; r < R; r++) acc[r] = 0;
       }
-      if (active && ncols > 0) {
+      if (active && ncols > 0 && ncols <= kMaxCols) {
         const int c0 = (cq * ncols) / Q, c1 = ((cq + 1) * ncols) / Q;
         const int soff = static_cast<int>((static_cast<unsigned long long>(d.data_off) * es) & 15ull);
         chunk_dot<S, R>(st + soff, gs, hv, rv, c0, c1, acc);
@@ -616,7 +580,7 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
 #pragma unroll
           for (int q = 0; q < 4; q++) tacc[j][q] = 0.f;
       }
-      if (wact && ncols > 0) {
+      if (wact && ncols > 0 && ncols <= kMaxCols) {
         const int grp = lane >> 2, tq = lane & 3;
         const int nks = (ncols + 15) >> 4;
         // ldmatrix.x4.trans: lane l addresses row (l & 7) of 8x8 matrix l >> 3;
@@ -924,7 +888,7 @@ __device__ __forceinline__ NarrowChunk narrow_desc(const StreamArgs &a, int i, b
   c.out_off = static_cast<int>(w1.y);
   c.flags = w1.z;
   c.g_off = static_cast<int>(w1.w);
-  if (c.hpad <= 0 || c.hpad > kNarrowRows || (c.hpad & 7) || c.ncols < 0 || c.ncols > kMaxChunkCols || c.rows < 0 ||
+  if (c.hpad <= 0 || c.hpad > kNarrowRows || (c.hpad & 7) || c.ncols < 0 || c.ncols > kMaxCols || c.rows < 0 ||
       c.rows > c.hpad) {
     if (report) set_error(a.err, kErrBadChunk);
     c.ncols = 0;

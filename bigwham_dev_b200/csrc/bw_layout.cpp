@@ -20,13 +20,6 @@ namespace bw {
 
 int esize_of(int prec) { return prec == 0 ? 8 : (prec == 1 ? 4 : 2); }
 
-int64_t stage_cols(int prec, int64_t hpad) {
-  const int64_t gsz = prec == 0 ? 8 : 4;
-  int64_t c = (kStageBytes + int64_t(kMaxCols) * gsz) / (std::max<int64_t>(1, hpad) * esize_of(prec) + gsz);
-  if (prec == 2) c = c / 8 * 8;
-  return std::max<int64_t>(prec == 2 ? 8 : 1, std::min<int64_t>(c, kMaxChunkCols));
-}
-
 // Round-to-nearest-even FP32 -> BF16 on the bit pattern (NaN kept quiet).
 uint16_t to_bf16(float f) {
   uint32_t u;
@@ -389,11 +382,10 @@ void chunk_item(const OperatorPlan &op, const Item &it, int prec, int phase, int
   const int es = esize_of(prec);
   const bool tiled = prec == 2;
   int64_t cap;
-  const int64_t room = stage_cols(prec, it.hpad);
   if (tiled)
-    cap = std::max<int64_t>(8, std::min<int64_t>(room, (chunk_bytes / (8 * int64_t(it.hpad) * es)) * 8));
+    cap = std::max<int64_t>(8, std::min<int64_t>(kMaxCols, (chunk_bytes / (8 * int64_t(it.hpad) * es)) * 8));
   else
-    cap = std::max<int64_t>(1, std::min<int64_t>(room, chunk_bytes / (int64_t(it.hpad) * es)));
+    cap = std::max<int64_t>(1, std::min<int64_t>(kMaxCols, chunk_bytes / (int64_t(it.hpad) * es)));
   std::vector<int64_t> seg_start(it.segs.size() + 1, 0);
   for (size_t s = 0; s < it.segs.size(); s++) seg_start[s + 1] = seg_start[s] + it.segs[s].ncols;
   int64_t c0 = 0;

@@ -31,8 +31,7 @@
 namespace bw {
 
 constexpr int kStageBytes = 32768;   // bytes of block data per pipeline stage
-constexpr int kMaxCols = 512;        // vector values of a stage's window area
-constexpr int kMaxChunkCols = 2048;  // bound of any chunk's columns (descriptor check)
+constexpr int kMaxCols = 512;        // columns per chunk (size of a stage's gather buffer)
 constexpr int kHMax = 512;           // max padded rows of one item
 constexpr int kRowAlign = 8;         // padded rows are a multiple of this
 constexpr int kItemAlign = 64;       // item start alignment, in elements
@@ -214,14 +213,6 @@ inline int64_t item_elems(int prec, int64_t hpad, int64_t ncols) {
 }
 
 int esize_of(int prec);
-
-// Columns of one chunk of an item with hpad padded rows in precision prec: a
-// stage holds the chunk's block data and its vector window (8-byte values for
-// FP64, 4-byte for FP32 and for BF16's packed words) back to back in its
-// kStageBytes + kMaxCols-value area, so short items take more than kMaxCols
-// columns (960 for 16-row BF16 stacks, whose data alone fills half a stage at
-// 512).  Multiple of 8 for BF16's 8-column tiles.
-int64_t stage_cols(int prec, int64_t hpad);
 uint16_t to_bf16(float f);
 float from_bf16(uint16_t b);
 

@@ -56,11 +56,7 @@ def test_plan_structure(golden):
                 d = decode(w)
                 assert d["hpad"] % 8 == 0 and d["rows"] <= d["hpad"] <= 512
                 cols = (d["ncols"] + 7) // 8 * 8 if prec == "bf16" else d["ncols"]
-                # block data within a stage, and data + vector window within
-                # the stage's data and window areas (stage_cols)
-                gsz = 8 if prec == "fp64" else 4
-                assert cols * d["hpad"] * es <= 32768 and d["ncols"] <= 2048
-                assert cols * d["hpad"] * es + d["ncols"] * gsz <= 32768 + 512 * gsz
+                assert cols * d["hpad"] * es <= 32768 and d["ncols"] <= 512
                 assert (d["data_off"] * es) % 16 == 0  # every chunk starts 16-byte aligned
                 if phase == 2:
                     assert d["g_off"] % 4 == 0  # 16-byte aligned slice of the gather array
@@ -243,28 +239,3 @@ def test_tuning_rejects_bad_values():
     with pytest.raises(BigWhamError) as e:
         h.set_tuning(chunk_bytes=8192)
     assert e.value.status == A.BW_ERR_STATE
-
-
-def test_short_items_take_wide_chunks():
-    """Items of few rows get more than 512 columns per chunk where block data
-    and vector window fit a stage together: 16-row BF16 stacks 960, 8-row
-    ones 1,736, 8-row FP32 ones 960; FP64 and taller items stay within a
-    32 KB stage of data."""
-    from synth import synthetic_hmat
-
-    arr = synthetic_hmat(600, 600, 2, seed=1264, leaf=32, rank0_share=0.2)
-    seen = {}
-    for prec, es in (("fp64", 8), ("fp32", 4), ("bf16", 2)):
-        h = HmatGpu.from_flat(arr.dof, arr.n_rows, arr.n_cols, arr.fr, arr.lr, arr.fr_data, arr.lr_data, arr.perm0,
-                              arr.perm1, device=-1, plan_only=True, precisions=(prec,))
-        for phase in (1, 2):
-            for w in h.plan_export(prec, phase, with_data=False)["chunks"]:
-                d = decode(w)
-                gsz = 8 if prec == "fp64" else 4
-                room = (32768 + 512 * gsz) // (d["hpad"] * es + gsz)
-                room = room // 8 * 8 if prec == "bf16" else room
-                cap = min(room, 32768 // (d["hpad"] * es) // (8 if prec == "bf16" else 1) * (8 if prec == "bf16" else 1))
-                assert d["ncols"] <= cap
-                key = (prec, d["hpad"])
-                seen[key] = max(seen.get(key, 0), d["ncols"])
-    assert seen.get(("bf16", 16), 0) > 512 or seen.get(("bf16", 8), 0) > 512
