@@ -411,6 +411,51 @@ def run_batch_only(a):
     return 0
 
 
+def time_penny(a, dev):
+    """C3: a pressurised penny-shaped crack, 3DT0-H (radius 1, hexagonal
+    lattice of spacing h clipped to the disk, jitter U(+-0.1h) seed 2,
+    Delaunay; E = 1, nu = 0.2, leaf 64, eta 3, eps 1e-4), built by the
+    reference's host code; one matvec per step in FP64, FP32 and BF16, with
+    the reduced precisions' distance from the FP64 GPU matvec."""
+    import torch
+
+    from bigwham_dev_b200 import HmatGpu
+    from bigwham_dev_b200.bigwham4py import BigWhamIOGpu
+    from bigwham_dev_b200.meshes import penny_crack_3d
+
+    t0 = time.time()
+    coor, conn = penny_crack_3d(a.c3_h, seed=2)
+    io = BigWhamIOGpu(coor, conn, "3DT0-H", [1.0, 0.2], os.cpu_count() or 1, useCuda=False)
+    io.build_hierarchical_matrix(64, 3.0, 1e-4)
+    ex = io.export_blocks()
+    io.close()
+    build_s = time.time() - t0
+    precs = ("fp64", "fp32", "bf16")
+    h = HmatGpu.from_flat(ex["dof"], ex["n_rows"], ex["n_cols"], ex["fr"], ex["lr"], ex["fr_data"], ex["lr_data"],
+                          ex["perm0"], ex["perm1"], device=dev.index or 0, precisions=precs)
+    del ex
+    x = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, h.n_cols)).to(dev)
+    out = {"workload": f"3DT0-H penny-shaped crack, h = {a.c3_h} ({len(conn):,} triangles, {h.n_rows:,} DoF), "
+                       "E=1 nu=0.2, leaf 64, eta 3, ACA eps 1e-4, x~U(-1,1) seed 1",
+           "host_build_s": round(build_s, 1)}
+    ys = {}
+    steps = max(3, min(a.steps, 50))
+    for p in precs:
+        y = torch.empty(h.n_rows, dtype=torch.float64, device=dev)
+        for _ in range(a.warmup):
+            h.matvec(x, p, out=y)
+        ms = _events_ms(lambda: h.matvec(x, p, out=y), steps)
+        ys[p] = y
+        ab = h.algorithmic_bytes(p)
+        out[p] = {"ms_per_matvec": ms, "matvec_per_s": 1e3 / ms, "algorithmic_bytes": ab,
+                  "gbs": ab / (ms * 1e-3) / 1e9, "launches": h.launches(p)}
+    for p in ("fp32", "bf16"):
+        out[p]["rel_err_vs_fp64_gpu"] = float(torch.linalg.vector_norm(ys[p] - ys["fp64"]) /
+                                              torch.linalg.vector_norm(ys["fp64"]))
+    h.close()
+    return out
+
+
 def time_batch(a, dev):
     """48 independent 2DS0-H straight cracks on [-1,1], segment counts
     log-uniform in [256, 16,384] (seed 3), leaf 32, eta 3, eps 1e-5, built by
@@ -608,7 +653,7 @@ def run_ours(a):
     world, rank, local = dist_setup(a.gpus)
     torch.cuda.set_device(local)
     if world > 1:  # the matmat and batch lines run on one GPU only
-        a.matmat, a.no_batch = False, True
+        a.matmat, a.no_batch, a.c3_h = False, True, 0.0
     io, h, setup = build_hmatrix(a, world, rank, local)
     dev = torch.device("cuda", local)
     n_in, n_out = h.n_cols, h.n_rows
@@ -689,6 +734,8 @@ def run_ours(a):
         extra["matmat_64rhs"], mm_cols = time_matmat(a, h, dev, peak, res["bf16"]["ms_per_step"])
     if world == 1 and not a.no_batch:
         extra["batched_2ds0_48"] = time_batch(a, dev)
+    if world == 1 and a.c3_h > 0:
+        extra["penny_3dt0"] = time_penny(a, dev)
     if world == 1 and not a.no_devbuild:
         extra["device_build_3dr0"] = device_build(a, h, x_host, setup.get("host_build_s"))
     if rank != 0:
@@ -753,6 +800,9 @@ def main(argv=None):
     ap.add_argument("--no-matmat", dest="matmat", action="store_false",
                     help="skip the 64-right-hand-side tensor-core matmat line (N = 1 only)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 48 x 2DS0 batched line (N = 1 only)")
+    ap.add_argument("--c3-h", type=float, default=0.0128,
+                    help="mesh spacing of the 3DT0-H penny line (0.0128: 132,690 DoF; 0.0064: 531,111 DoF; "
+                         "0 skips it; N = 1 only)")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="plan parameter (bw_set_tuning) for every handle of the run, e.g. narrow_rows=0; repeatable")
     ap.add_argument("--no-devbuild", action="store_true",
