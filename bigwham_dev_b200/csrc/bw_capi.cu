@@ -642,8 +642,19 @@ void launch_matvec_impl(bw_hmat *h, int o, int prec, const double *x, double *y,
         a.n_items = (int)(dp.n_items - dp.split.wide);
         a.n_coop = (int)(dp.split.coop - dp.split.wide);
         a.queue = dp.queue + 2;
-        bw::narrow_items_kernel<S><<<2 * h->grid, 32 * bw::kNarrowWarps, 0, st>>>(a);
-        BW_CUDA(cudaGetLastError());
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2 * h->grid);
+        cfg.blockDim = dim3(32 * bw::kNarrowWarps);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        // After the phase's CTA-wide launch (and no timing event between
+        // them) it may start on the SMs that launch leaves free or frees.
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = (dp.split.wide > 0 && !ev) ? 1 : 0;
+        BW_CUDA(cudaLaunchKernelEx(&cfg, bw::narrow_items_kernel<S>, a));
       }
     }
     if (ev) {

@@ -114,6 +114,16 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32
       "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
       : "memory");
 }
+// Programmatic dependent launch: a kernel launched right after this one with
+// the programmatic-serialization attribute may start once every CTA of this
+// one has issued launch_dependents (or exited); wait blocks until the grids
+// this one depends on have completed and their writes are visible.  Both are
+// no-ops without such a launch.
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -379,6 +389,10 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
     fence_barrier_init();
   }
   __syncthreads();
+  // Every CTA is resident and holds its shared memory: a phase's unstaged
+  // launch (independent items, its own queue) may start filling the SMs this
+  // launch leaves free, and the SMs it frees as its CTAs run out of items.
+  pdl_launch_dependents();
 
   if (warp == 0) {
     // ------------------------------------------------------------------ producer
@@ -1037,6 +1051,10 @@ __global__ void __launch_bounds__(32 * kNarrowWarps, 2) narrow_items_kernel(Stre
       __threadfence();
     }
   }
+  // Launched programmatically after the phase's CTA-wide launch (whose
+  // outputs it neither reads nor writes), this launch completes only after
+  // that one has: the next launch on the stream sees both phases' outputs.
+  pdl_wait();
 }
 
 // BF16 path: a vector value v is handed to the tensor cores as two BF16
