@@ -735,12 +735,14 @@ __global__ void __launch_bounds__(threads_of<S>(), 1) stream_panels_kernel(Strea
 // consumer warp takes part in every chunk's barrier round trip and in every
 // item's shared-memory reduction, measured with per-chunk clock stamps on the
 // 48 x 2DS0 batch).  Two modes, one launch:
-//   * CTA-cooperative (queue units [0, n_coop), the long ones: more than one
-//     chunk of columns): the CTA's 16 warps take the unit's chunks round
-//     robin, and the warps' rows of each item are added in shared memory, in
-//     warp order;
+//   * CTA-cooperative (queue units [0, n_coop), long units of few rows; only
+//     with the narrow_coop tuning, by default those stay in the CTA-wide
+//     kernel): the CTA's 16 warps take the unit's chunks round robin, and the
+//     warps' rows of each item are added in shared memory, in warp order;
 //   * warp per unit (the rest): a warp takes a unit from the queue and writes
 //     its outputs itself; nothing is shared between warps.
+// After a CTA-wide launch of the same phase it runs as that launch's
+// programmatic dependent (pdl_launch_dependents / pdl_wait).
 // A warp walks a chunk in rounds: each lane issues all of a round's loads
 // (the ones past the chunk's columns predicated off) before it uses any, so
 // short chunks keep as many bytes in flight as long ones.  The chunk
