@@ -24,7 +24,6 @@ LR block A then B), ``perm0`` and ``perm1``.
 """
 from __future__ import annotations
 
-import ctypes as C
 import os
 
 import numpy as np

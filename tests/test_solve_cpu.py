@@ -1,6 +1,5 @@
 """GMRES / iterative refinement logic on CPU tensors (no graph capture)."""
 import numpy as np
-import pytest
 import torch
 
 from bigwham_dev_b200.solve import Gmres, refine
