@@ -1069,15 +1069,20 @@ __device__ __forceinline__ uint32_t pack_hilo(float v) {
 
 // G2[dst + c] = scale * src[src_off + c] for every run (src: gathered x or t):
 // the phase-2 vector values laid out chunk by chunk.  Runs are short (10 to
-// 60 values on 2DS0-H matrices), so a warp takes kG2Runs = 32 of them at
-// once and deals their values to its lanes densely: lane k loads run k's
-// descriptor, a warp scan gives each run its first position in the warp's
-// value list, and each value finds its run by a 5-step binary search over
-// the lanes' starts (shuffles), so every lane has a value in every step but
-// the last.  kPacked: store pack_hilo(value) words (BF16 path) instead of G
-// values.
+// 60 values), so a warp takes kG2Runs = 32 of them at once and deals their
+// values to its lanes densely: lane k loads run k's descriptor and a warp
+// scan gives each run its first position in the warp's value list.  A round
+// covers 32 consecutive positions [w0, w0 + 32): the run holding w0 is the
+// last one starting at or before it (one ballot), every later run starting
+// inside the window sets its bit in a 32-bit mask (one OR reduction), and the
+// value at w0 + j belongs to the run holding w0 plus the number of bits at or
+// below j.  This needs the runs to be non-empty, which the layout guarantees
+// (build_chunks makes no empty run); a value whose run does not hold it is
+// skipped, so malformed runs cannot index outside their source or G2.
+// kPacked: store pack_hilo(value) words (BF16 path) instead of G values, and
+// apply the runs' block scales (1 on the other paths).
 constexpr int kG2Runs = 32;
-constexpr int kG2Unroll = 4;  // values in flight per lane
+constexpr int kG2Unroll = 4;  // rounds in flight per lane
 
 template <typename G, bool kPacked>
 __global__ void gather_g2_kernel(const GatherSeg *__restrict__ runs, int n_runs, const G *__restrict__ xp,
@@ -1096,34 +1101,37 @@ __global__ void gather_g2_kernel(const GatherSeg *__restrict__ runs, int n_runs,
   }
   const int start = incl - cols;
   const int total = __shfl_sync(0xffffffffu, incl, 31);
+  const unsigned below = (2u << lane) - 1u;  // bits 0..lane
   for (int base = 0; base < total; base += 32 * kG2Unroll) {
     G v[kG2Unroll];
     int dst[kG2Unroll];
     float sc[kG2Unroll];
+    bool ok[kG2Unroll];
 #pragma unroll
     for (int u = 0; u < kG2Unroll; u++) {
-      const int e = base + 32 * u + lane;
-      // the last run starting at or before e (empty runs share the start of
-      // the next one, so the last such run holds e when e < total)
-      int r = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1)
-        if (__shfl_sync(0xffffffffu, start, r + step) <= e) r += step;
-      const int k = e - __shfl_sync(0xffffffffu, start, r);
-      const int off = __shfl_sync(0xffffffffu, mine.src_off, r);
-      const uint32_t cs = __shfl_sync(0xffffffffu, mine.cols_src, r);
-      dst[u] = __shfl_sync(0xffffffffu, mine.dst, r) + k;
-      sc[u] = __shfl_sync(0xffffffffu, mine.scale, r);
-      v[u] = e < total ? ((cs >> 31) ? t : xp)[off + k] : G(0);
+      const int w0 = base + 32 * u, e = w0 + lane;
+      const unsigned holds = __ballot_sync(0xffffffffu, cols > 0 && start <= w0);
+      const int off = start - w0;
+      const unsigned starts = __reduce_or_sync(0xffffffffu, (cols > 0 && off > 0 && off < 32) ? (1u << off) : 0u);
+      const int r = (holds ? 31 - __clz(holds) : 0) + __popc(starts & below);
+      const int rs = __shfl_sync(0xffffffffu, start, r);
+      const int rc = __shfl_sync(0xffffffffu, cols, r);
+      const int ro = __shfl_sync(0xffffffffu, mine.src_off, r);
+      const uint32_t rf = __shfl_sync(0xffffffffu, mine.cols_src, r);
+      const int rd = __shfl_sync(0xffffffffu, mine.dst, r);
+      sc[u] = kPacked ? __shfl_sync(0xffffffffu, mine.scale, r) : 1.0f;
+      const int k = e - rs;
+      ok[u] = e < total && k >= 0 && k < rc;
+      dst[u] = rd + k;
+      v[u] = ok[u] ? ((rf >> 31) ? t : xp)[ro + k] : G(0);
     }
 #pragma unroll
     for (int u = 0; u < kG2Unroll; u++) {
-      if (base + 32 * u + lane < total) {
-        const G w = static_cast<G>(sc[u]) * v[u];
+      if (ok[u]) {
         if constexpr (kPacked)
-          static_cast<uint32_t *>(g2)[dst[u]] = pack_hilo(static_cast<float>(w));
+          static_cast<uint32_t *>(g2)[dst[u]] = pack_hilo(sc[u] * static_cast<float>(v[u]));
         else
-          static_cast<G *>(g2)[dst[u]] = w;
+          static_cast<G *>(g2)[dst[u]] = v[u];
       }
     }
   }
