@@ -14,7 +14,7 @@ M^-1 = blockdiag(D_1^-1, ..., D_K^-1), D_k the diagonal full-rank blocks.
   full rank, and in the clustered ordering these blocks tile the diagonal.
 * The inverses come from an FP64 LU on the host, once.
 * They are the members of one batched handle (bw_create_batch, one member per
-  block).  Applying M^-1 is one batched product: the four launches of a
+  block).  Applying M^-1 is one batched product: the launches of a
   matvec, over sum_k m_k^2 entries.  For 3DR0-H 256 x 256 (196,608 DoF) that
   is 151 MB in FP64, 1.3% of the H-matrix.
 * It is stream-ordered and allocation-free after the first call, so
