@@ -207,3 +207,26 @@ def test_launch_count_follows_the_split():
             n = len(p["item_ptr"]) - 1
             want += (p["n_wide"] > 0) + (p["n_wide"] < n)
         assert h.launches("fp32") == want, tune
+
+
+def test_batch_split_of_the_48_crack_workload():
+    """The 48 x 2DS0-H batch (segments log-uniform in [256, 16,384], seed 3):
+    phase 1 splits (long 16-row stacks CTA-wide, the small stacks unstaged),
+    phase 2 runs unstaged entirely (row panels of at most 64 rows and 512
+    columns); five launches per matvec."""
+    from oracle import RefHmat, ref_available
+    from bigwham_dev_b200.meshes import straight_crack_2d
+
+    if not ref_available():
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(3)
+    sizes = np.round(np.exp(rng.uniform(np.log(256), np.log(16384), 48))).astype(int)
+    ms = [RefHmat("2DS0-H", *straight_crack_2d(int(n)), [1.0, 0.25], 32, 3.0, 1e-5, n_threads=8).arrays()
+          for n in sizes]
+    h = HmatGpu.batch(ms, device=-1, precisions=("bf16",), plan_only=True)
+    p1 = h.plan_export("bf16", 1, with_data=False)
+    p2 = h.plan_export("bf16", 2, with_data=False)
+    n1 = len(p1["item_ptr"]) - 1
+    assert 0 < p1["n_wide"] < n1 and p1["n_coop"] == p1["n_wide"]
+    assert p2["n_wide"] == 0
+    assert h.launches("bf16") == 5
