@@ -13,9 +13,9 @@ Workload: the 3DR0-H square crack of bench.py.
   `--steps` matvecs with CUDA events after `--warmup` untimed ones.  x is
   U(-1,1), seed 1.
 
-Parameters (the items_per_cta ones leave results bit for bit unchanged;
-chunk_bytes moves the chunk boundaries and with them the order of the
-additions inside an item, so results agree to rounding):
+Parameters (they move item and chunk boundaries, and with them the order of
+the additions that make an output row, so results agree to rounding; for
+fixed parameters they are repeatable bit for bit):
 * items_per_cta_phase1 / items_per_cta_phase2: granularity of the work queue
   (items per CTA share; more items balance better but cost more item ends);
 * chunk_bytes: block data per pipeline chunk (fewer bytes mean more chunks

@@ -121,10 +121,10 @@ int bw_test_withhold_chunk(bw_hmat *h, int index);
  *       (default 0) runs the items before it there as well, a CTA per item,
  *       instead of in the CTA-wide kernel.  narrow_rows 0 keeps every item
  *       in the CTA-wide kernel.
- * chunk_bytes and the narrow_* keys change the order of the additions inside
- * an item (results agree to rounding); for fixed settings results are
- * repeatable bit for bit and do not depend on the schedule (each item is
- * reduced in a fixed order).
+ * They move item and chunk boundaries or the kernel an item runs in, and
+ * with them the order of the additions that make an output row (results
+ * agree to rounding); for fixed settings results are repeatable bit for bit
+ * and do not depend on the schedule (each item is reduced in a fixed order).
  * BW_ERR_ARG for an unknown key or a value out of range. */
 int bw_set_tuning(bw_hmat *h, const char *key, int64_t value);
 
