@@ -230,10 +230,13 @@ def test_tuning_changes_the_plan_not_the_result(golden):
 
 def test_tuning_rejects_bad_values():
     h = _simple()
-    for k, v in (("chunk_bytes", 1000), ("chunk_bytes", 65536), ("items_per_cta_phase1", 0), ("nope", 1)):
+    for k, v in (("chunk_bytes", 1000), ("chunk_bytes", 65536), ("items_per_cta_phase1", 0), ("nope", 1),
+                 ("narrow_rows", -1), ("narrow_rows", 65), ("narrow_cols", 0), ("narrow_coop", 2),
+                 ("unit_bytes", -1)):
         with pytest.raises(BigWhamError) as e:
             h.set_tuning(**{k: v})
         assert e.value.status == A.BW_ERR_ARG
+    h.set_tuning(narrow_rows=0, narrow_cols=1, narrow_coop=1, unit_bytes=0)  # in range
     h.add_full(0, 0, np.ones((8, 8)))
     h.finalize(plan_only=True)
     with pytest.raises(BigWhamError) as e:
